@@ -1,0 +1,365 @@
+#!/usr/bin/env python
+"""Throughput of the voxelG hierarchical-DDA traversal on B200.
+
+Workload (one step = one frame): the 2048x256x2048 seeded world (32x4x32
+chunks), 1920x1080 primary rays with the uniform-brick/tile LUTs, the 1/8-res
+beam pre-pass and the 400/520-voxel LOD on, plus one shadow ray per primary
+hit toward normalize(0.3, 0.8, 0.5) jittered in a 0.5-degree cone.
+Every record is bit-exact against the CPU oracle (tests/test_gpu_parity.py).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+value      Mrays/s over all ranks (primary + shadow rays), world and rays
+           resident in HBM, per-step device time from CUDA events on the
+           launching stream, L2 flushed (256 MiB write) before every step
+           outside the events, max over ranks.
+e2e        the same metric through vx_render_primary_host: camera in, every
+           record copied to pinned host memory inside the timed region.
+roofline   the primary kernel: algorithmic bytes per launch (method loads as
+           counted by the oracle's rules + record writes) / mean event time,
+           against the measured HBM copy bandwidth.
+cpu_baseline  the oracle (C restatement of the reference traversal) on all
+           host threads over a bounded row sample of the same frame.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Mrays/s bit-exact vs CPU DDA (plain vs learned-proposal); ray-query p50/p99 ms"
+UNIT = "Mrays/s"
+CONFIG_NAME = "c2"
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-sample-seconds", type=float, default=10.0)
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ helpers
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, local_index: int):
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+        ids = [v.strip() for v in vis.split(",") if v.strip()]
+        gpu_index = ids[local_index] if local_index < len(ids) else str(local_index)
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader",
+                 "-lms", "200", "-i", str(gpu_index)], stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self) -> dict:
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        rows = [r.split(",") for r in Path(self.f.name).read_text().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            if len(r) < 10:
+                continue
+            m = re.match(r"\s*(\d+)", r[2])
+            if m:
+                sm.append(int(m.group(1)))
+            m = re.match(r"\s*(\d+)", r[3])
+            if m:
+                smax.append(int(m.group(1)))
+            for name, v in zip(names, r[6:10]):
+                if "Active" in v and "Not" not in v:
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": d["hbm_gbs"], "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+def profiled_traffic() -> float | None:
+    """dram bytes per launch of the primary kernel from the committed ncu
+    summary (profiles/primary_c2_1080p.md), if present."""
+    p = ROOT / "profiles" / "primary_c2_1080p.md"
+    if not p.exists():
+        return None
+    m = re.search(r"traffic_bytes_per_launch:\s*([0-9.eE+]+)", p.read_text())
+    return float(m.group(1)) if m else None
+
+
+def dist_setup(n_gpus: int):
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    return rank, world, local
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x: float, world: int, device) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def frame_setup(vg, cfg, device: int):
+    dw = vg.DeviceWorld(*cfg.bricks, device=device)
+    dw.generate(cfg.terrain)
+    cam = vg.default_camera(dw, cfg.width, cfg.height)
+    params = vg.default_params(cfg.flags, frame=7.0)
+    return dw, cam, params
+
+
+# -------------------------------------------------------------- cpu sample
+def cpu_sample(ow, cam, params, seconds: float, threads: int, offset0: int = 0):
+    """Time the oracle on rows offset, offset+s, ... of the frame, growing
+    the sample until it takes about `seconds` of wall time."""
+    from oracle import pyoracle as po
+    beam, _ = po.beam_pass(ow, cam)
+    H = int(cam.res_y)
+    stride = 64
+    total_rays, total_s, rows = 0, 0.0, 0
+    offset = offset0
+    while True:
+        rec, sh, secs, _ = po.render_row_set(ow, cam, params, beam, stride, offset % stride,
+                                             threads)
+        total_rays += len(rec) + int(sh["traced"].sum())
+        total_s += secs
+        rows += len(rec) // int(cam.res_x)
+        offset += 1
+        if total_s >= seconds or rows >= H:
+            break
+    return total_rays / total_s / 1e6, rows, total_s
+
+
+def run_reference(args, cfg):
+    """The reference's CPU traversal (the oracle restatement: the Rust
+    reference cannot be built here) on all host threads."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import math
+
+    from oracle import pyoracle as po
+    threads = os.cpu_count() or 1
+    ow = po.World(*cfg.bricks)
+    ow.generate(cfg.terrain, threads=threads)
+    # camera + params built on the oracle side: nothing of libvoxrt runs here
+    cx, cz = cfg.bricks[0] * 2, cfg.bricks[2] * 2
+    cam = po.camera_from_pose((cx, 140.0, cz), 0.0, math.radians(-15.0), math.radians(70.0),
+                              cfg.width, cfg.height)
+    params = po.default_params(cfg.flags, frame=7.0)
+    beam, _ = po.beam_pass(ow, cam)
+    stride = 16
+    per_step = []
+    rays_step = []
+    for s in range(args.warmup + args.steps):
+        rec, sh, secs, _ = po.render_row_set(ow, cam, params, beam, stride, s % stride, threads)
+        if s >= args.warmup:
+            per_step.append(secs)
+            rays_step.append(len(rec) + int(sh["traced"].sum()))
+    value = sum(rays_step) / sum(per_step) / 1e6
+    out = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 3), "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(1e3 * statistics.mean(per_step), 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"{CONFIG_NAME}: 2048x256x2048 world, 1920x1080 primary + shadow "
+                               "rays, beam/LUT/LOD on", "sample": f"every {stride}th row per step"},
+        "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": threads,
+                         "kind": "port",
+                         "sample": f"rows offset+{stride}k of the 1920x1080 frame per step "
+                                   f"(~{int(sum(rays_step) / len(rays_step))} rays), "
+                                   "oracle restatement of raycast/raymarch traversal"},
+        "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+# ----------------------------------------------------------------- ours
+def run_ours(args, cfg):
+    import numpy as np
+    import torch
+
+    import voxelg_b200 as vg
+    from voxelg_b200 import _lib as L
+
+    rank, world, local = dist_setup(args.gpus)
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    dw, cam, params = frame_setup(vg, cfg, local)
+    W, H = cfg.width, cfg.height
+    n = W * H
+    rec = torch.empty(n * 24, dtype=torch.uint8, device=device)
+    sh = torch.empty(n * 8, dtype=torch.uint8, device=device)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=device)
+    stream = torch.cuda.current_stream(device).cuda_stream
+
+    # algorithmic bytes of one frame (counting pass, untimed)
+    stats = vg.render_stats(dw, cam, params)
+    vg.render_primary(dw, cam, params, rec, sh, stream=stream)
+    torch.cuda.synchronize(device)
+    shadows = vg.shadows(sh)
+    n_shadow = int(shadows["traced"].sum())
+    rays_per_step = n + n_shadow
+    record_bytes = n * (24 + 8)
+
+    for _ in range(max(args.warmup, 3)):
+        vg.render_primary_timed(dw, cam, params, rec, sh, stream=stream)
+
+    sampler = ClockSampler(local) if rank == 0 or world > 1 else None
+    barrier(world)
+    torch.cuda.synchronize(device)
+    beam_ms, prim_ms = [], []
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        flush.zero_()
+        b, p = vg.render_primary_timed(dw, cam, params, rec, sh, stream=stream)
+        beam_ms.append(b)
+        prim_ms.append(p)
+    torch.cuda.synchronize(device)
+    barrier(world)
+    wall = time.perf_counter() - t0
+    clocks = sampler.stop() if sampler else None
+    dev_ms = sum(beam_ms) + sum(prim_ms)
+    dev_ms_max = max_over_ranks(dev_ms, world, device)
+    value = world * rays_per_step * args.steps / (dev_ms_max / 1e3) / 1e6
+
+    # end to end through the host-buffer entry point
+    rec_h = torch.empty(n * 24, dtype=torch.uint8).pin_memory()
+    sh_h = torch.empty(n * 8, dtype=torch.uint8).pin_memory()
+    rec_np = rec_h.numpy().view(L.RECORD_DTYPE)
+    sh_np = sh_h.numpy().view(L.SHADOW_DTYPE)
+    for _ in range(3):
+        vg.render_primary_host(dw, cam, params, rec_np, sh_np)
+    e2e_steps = max(10, min(args.steps, 100))
+    barrier(world)
+    torch.cuda.synchronize(device)
+    t1 = time.perf_counter()
+    for _ in range(e2e_steps):
+        vg.render_primary_host(dw, cam, params, rec_np, sh_np)
+    torch.cuda.synchronize(device)
+    barrier(world)
+    e2e_s = max_over_ranks(time.perf_counter() - t1, world, device)
+    e2e_value = world * rays_per_step * e2e_steps / e2e_s / 1e6
+    assert np.array_equal(rec_h.numpy(), rec.cpu().numpy()), "host path differs from device path"
+
+    peaks = measured_peaks()
+    prim_mean = statistics.mean(prim_ms)
+    alg_bytes = stats["primary"][0] + record_bytes
+    achieved = alg_bytes / (prim_mean / 1e3) / 1e9
+    traffic = profiled_traffic()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import pyoracle as po
+        arrays = dw.download()
+        ow = po.World(*cfg.bricks, arrays=arrays)
+        threads = os.cpu_count() or 1
+        cval, rows, secs = cpu_sample(ow, cam, params, args.cpu_sample_seconds, threads)
+        cpu = {"value": round(cval, 3), "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"{rows} of {H} rows (every 64th row, rotating) of the same frame, "
+                         f"{secs:.1f} s wall; oracle restatement of the reference traversal"}
+        del ow, arrays
+
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(dev_ms_max / args.steps, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {
+                "workload": f"{CONFIG_NAME}: 2048x256x2048 world (32x4x32 chunks, seed "
+                            f"{cfg.terrain.seed:#x}), 1920x1080 primary rays, beam/LUT/LOD on, "
+                            "one shadow ray per hit",
+                "rays_per_step": rays_per_step, "primary_rays": n, "shadow_rays": n_shadow,
+                "primary_mrays_s": round(world * n * args.steps / (dev_ms_max / 1e3) / 1e6, 3),
+                "beam_ms": round(statistics.mean(beam_ms), 4),
+                "primary_ms": round(prim_mean, 4),
+                "wall_s_timed_loop": round(wall, 3),
+                "l2": "flushed before every step (256 MiB write, outside the step events)",
+                "parallelism": f"replicas: {world} x full frame (weak scaling)",
+            },
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": peaks["hbm_gbs"],
+                         "unit": "GB/s", "frac": round(achieved / peaks["hbm_gbs"], 4),
+                         "traffic": traffic, "kernel": "k_primary (trace + shadow)",
+                         "algorithmic_bytes_per_launch": alg_bytes,
+                         "peak_source": peaks["source"]},
+            "e2e": {"value": round(e2e_value, 3), "unit": UNIT,
+                    "h2d_bytes_per_step": 80 + 76,
+                    "d2h_bytes_per_step": record_bytes},
+            "gpu_launches": 2 * args.steps,
+            "clocks": clocks,
+        }
+        if cpu:
+            out["cpu_baseline"] = cpu
+        print(json.dumps(out), flush=True)
+    dw.close()
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse_args()
+    import voxelg_b200.configs as configs
+    cfg = configs.CONFIGS[CONFIG_NAME]
+    if args.impl == "reference":
+        run_reference(args, cfg)
+    else:
+        run_ours(args, cfg)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,247 @@
+/*
+ * voxrt.h -- C ABI of the B200-native voxel ray-traversal engine for voxelG.
+ *
+ * A drop-in for voxelG's traversal boundary: the CPU picking call
+ * `raycast()` (src/raycast.rs:21) and the GPU hierarchical DDA that
+ * shaders/raymarch.wgsl + shaders/beam.wgsl run over the world pyramid that
+ * src/voxel.rs maintains.  All kernels are hand-written CUDA for sm_100a; the
+ * library has no CPU fallback -- every traversal entry point fails with
+ * VX_ERR_CUDA when no usable GPU is present.
+ *
+ * Conventions
+ *   - Every entry point returns an int status (VX_OK = 0, negative = error)
+ *     except where stated; vx_last_error() returns a thread-local message.
+ *     No exceptions cross the ABI, nothing aborts.
+ *   - Ownership: the caller owns every pointer it passes; the library owns
+ *     the device copy of a world.  No pointer is retained after a call.
+ *   - "_dev" pointers are device memory on the world's device; other pointers
+ *     are host memory.  Calls taking a `stream` (a cudaStream_t, NULL = the
+ *     legacy default stream) are asynchronous and stream-ordered; the others
+ *     are synchronous.
+ *   - Host layouts are exactly voxelG's: Brick is repr(C) 72 bytes
+ *     (src/voxel.rs:296-301), masks are u64 per cell with child bit
+ *     x + z*4 + y*16 (src/voxel.rs:282-294), uniform LUTs one byte per cell.
+ */
+#ifndef VOXRT_H
+#define VOXRT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VX_OK 0
+#define VX_ERR_INVALID (-1)   /* bad argument, size or dims                  */
+#define VX_ERR_CUDA (-2)      /* CUDA runtime error (incl. no device)        */
+#define VX_ERR_OOM (-3)       /* device memory exhausted / over budget       */
+#define VX_ERR_DEVICE (-4)    /* a kernel reported an error status word      */
+#define VX_ERR_BUSY (-5)      /* admission refused (serving loop)            */
+
+#define VX_ABI_VERSION 1
+
+/* ---- plain data -------------------------------------------------------- */
+
+/* src/voxel.rs:296-301 -- occupancy bit i = voxel x + z*4 + y*16. */
+typedef struct {
+    uint64_t occupancy;
+    uint8_t materials[64];
+} VxBrick;
+
+/* World dims in bricks (src/world_dims.rs:12-14 made runtime values).
+ * bricks_x and bricks_z must be multiples of 64 (whole 256-voxel L4 cells,
+ * so toroidal folding keeps every level aligned); bricks_y a multiple of 16. */
+typedef struct {
+    int32_t bricks_x, bricks_y, bricks_z;
+    int32_t device; /* CUDA device ordinal */
+} VxWorldDesc;
+
+/* Camera uniform subset the traversal reads (shaders/common.wgsl:7-42). */
+typedef struct {
+    float origin[3];
+    float forward[3];
+    float right[3];
+    float up[3];
+    float tan_half_fov;
+    float res_x, res_y;
+    float jitter_x, jitter_y;      /* sub-pixel jitter in pixels            */
+    int32_t world_origin[3];       /* loaded-window corner, world voxels    */
+} VxCamera;
+
+/* Method switches.  The reference method is L4|LUT|LOD|BEAM. */
+#define VX_F_L4 (1u << 0)      /* L4 + chunk-in-L4 skip (!PROFILE_NO_L4)   */
+#define VX_F_LUT (1u << 1)     /* uniform tile/brick early-out             */
+#define VX_F_LOD (1u << 2)     /* tile LOD (t>520) + brick LOD (t>400)     */
+#define VX_F_BEAM (1u << 3)    /* 1/8-res beam pre-pass fast-forward       */
+#define VX_F_SHADOW (1u << 4)  /* one any-hit shadow ray per primary hit   */
+
+typedef struct {
+    float max_dist;          /* MAX_RAY_DIST 700    raymarch.wgsl:4501 */
+    float lod_brick_t;       /* LOD_BRICK_T 400     raymarch.wgsl:4489 */
+    float tile_lod_t;        /* TILE_LOD_T 520      raymarch.wgsl:4494 */
+    float shadow_max_dist;   /* SHADOW_MAX_DIST 480 raymarch.wgsl:4517 */
+    float beam_margin;       /* 16                  raymarch.wgsl:608  */
+    int32_t max_iters;       /* 1024                raymarch.wgsl:4625 */
+    int32_t any_max_iters;   /* 768                 raymarch.wgsl:4359 */
+    uint32_t flags;          /* VX_F_*                                 */
+    float sun[3];            /* unit sun direction                     */
+    float sun_tangent[3];    /* raymarch.wgsl:3984-3988                */
+    float sun_bitangent[3];
+    float cone_tan;          /* tan(cone half-angle)                   */
+    float frame;             /* interleaved-gradient-noise frame term  */
+} VxTraceParams;
+
+/* One ray's record (24 bytes).  face = 2*axis + (entering along +axis), i.e.
+ * 0:+x 1:-x 2:+y 3:-y 4:+z 5:-z outward normal; 0xFF on a miss.  t is the hit
+ * distance from the ray origin (camera for primary rays); steps the number
+ * of traversal-loop iterations begun, including the last. */
+typedef struct {
+    int32_t voxel[3];
+    uint8_t face;
+    uint8_t mat;
+    uint8_t flags;    /* bit0 hit, bit1 uniform/LOD early-out */
+    uint8_t pad;
+    float t;
+    uint32_t steps;
+} VxHitRecord;
+
+typedef struct {
+    uint32_t steps;
+    uint8_t occluded;
+    uint8_t traced;
+    uint16_t pad;
+} VxShadowRecord;
+
+/* src/raycast.rs:13-17 */
+typedef struct {
+    int32_t voxel[3];
+    int32_t normal[3];
+} VxPickHit;
+
+/* Generic ray for vx_trace: kind 0 first hit (trace), 1 any hit (trace_any,
+ * record.flags bit0 = occluded), 2 first non-transparent hit
+ * (trace_no_water).  tmax replaces MAX_RAY_DIST / max_dist / t_cap. */
+typedef struct {
+    float org[3];
+    float dir[3];
+    float tmax;
+    uint32_t kind;
+} VxRay;
+
+/* Seeded synthetic terrain: h = floor(base + amp*fbm_2d(x/wl, z/wl, oct)),
+ * grass top, dirt_depth dirt, stone below, water (material 12) up to
+ * water_level, caves where value_noise_3d(p/cave_wl) > cave_threshold
+ * (noise primitives of src/voxel.rs:1163-1232, :1999-2021). */
+typedef struct {
+    uint64_t seed;
+    float base_height;
+    float amplitude;
+    float inv_wavelength;
+    uint32_t octaves;
+    int32_t water_level;
+    float cave_inv_wavelength;
+    float cave_threshold;
+    int32_t dirt_depth;
+} VxTerrainParams;
+
+typedef struct VxWorld VxWorld;          /* device-resident world pyramid */
+typedef struct VxHostWorld VxHostWorld;  /* host mirror of src/voxel.rs World */
+
+/* ---- library ----------------------------------------------------------- */
+int vx_abi_version(void);
+const char *vx_last_error(void);
+/* Fill *p with the reference constants, flags L4|LUT|LOD|BEAM|SHADOW, sun =
+ * normalize(0.3, 0.8, 0.5) with its tangent frame, a 0.5-degree cone. */
+int vx_default_params(VxTraceParams *p);
+/* Camera basis from a pose: src/camera.rs:25-42 (forward/right/up) and
+ * :140-166 (CameraUniform::from_camera). */
+int vx_camera_from_pose(const float pos[3], float yaw, float pitch, float fov_y,
+                        uint32_t width, uint32_t height, const int32_t world_origin[3],
+                        VxCamera *out);
+
+/* ---- device world (replaces Renderer::upload_world, renderer.rs:1248) -- */
+int vx_world_create(const VxWorldDesc *desc, VxWorld **out);
+int vx_world_destroy(VxWorld *w);
+/* Full upload from voxelG's host arrays (renderer.rs:1248-1344 all_dirty). */
+int vx_world_upload(VxWorld *w, const VxBrick *bricks, const uint64_t *tile_mask,
+                    const uint64_t *chunk_mask, const uint64_t *l4_mask,
+                    const uint8_t *brick_uniform, const uint8_t *tile_uniform);
+/* Copy the device pyramid back into voxelG's host layout (any pointer may
+ * be NULL to skip that array). */
+int vx_world_download(VxWorld *w, VxBrick *bricks, uint64_t *tile_mask, uint64_t *chunk_mask,
+                      uint64_t *l4_mask, uint8_t *brick_uniform, uint8_t *tile_uniform);
+/* Generate the seeded synthetic terrain on the device and build masks and
+ * uniform LUTs there (src/voxel.rs:946-1000 semantics). */
+int vx_world_generate(VxWorld *w, const VxTerrainParams *t);
+/* Incremental update from dirty bricks (renderer.rs:1345-1394): writes the
+ * given bricks and recomputes the touched tile/chunk/L4 masks and uniform
+ * LUT entries on the device (voxel.rs:879-946 semantics).  brick_idx and
+ * bricks are host arrays of n entries; duplicates allowed (last wins). */
+int vx_world_apply_dirty(VxWorld *w, const uint32_t *brick_idx, const VxBrick *bricks,
+                         size_t n, void *stream);
+/* Counts of each array: bricks, tiles, chunks, l4 cells. */
+int vx_world_counts(const VxWorld *w, uint64_t counts[4]);
+
+/* ---- traversal --------------------------------------------------------- */
+/* raycast(camera_world, dir, world, world_origin) (src/raycast.rs:21): returns
+ * 1 on a hit (fills *out), 0 on a miss, <0 on error.  Synchronous. */
+int vx_raycast(VxWorld *w, const float cam[3], const float dir[3], const int32_t origin[3],
+               VxPickHit *out);
+/* Batched raycast over device arrays: cams/dirs are n*3 floats, hit[i] = 1/0. */
+int vx_raycast_batch(VxWorld *w, const int32_t origin[3], const float *cams_dev,
+                     const float *dirs_dev, size_t n, VxPickHit *out_dev, int32_t *hit_dev,
+                     void *stream);
+/* Batched generic rays (trace / trace_any / trace_no_water) over device
+ * arrays; origin is the loaded-window corner. */
+int vx_trace(VxWorld *w, const int32_t origin[3], const VxRay *rays_dev, size_t n,
+             const VxTraceParams *p, VxHitRecord *out_dev, void *stream);
+/* One primary frame: beam pre-pass (VX_F_BEAM) + per-pixel trace
+ * (raymarch.wgsl:576-631) + one shadow ray per hit (VX_F_SHADOW).
+ * rec_dev: res_x*res_y records, row-major; shadow_dev may be NULL when
+ * VX_F_SHADOW is off.  The beam scratch is owned by the world. */
+int vx_render_primary(VxWorld *w, const VxCamera *cam, const VxTraceParams *p,
+                      VxHitRecord *rec_dev, VxShadowRecord *shadow_dev, void *stream);
+/* Same frame through host buffers: the records are copied to rec_host /
+ * shadow_host (pinned memory recommended) before the call returns. */
+int vx_render_primary_host(VxWorld *w, const VxCamera *cam, const VxTraceParams *p,
+                           VxHitRecord *rec_host, VxShadowRecord *shadow_host);
+/* The frame of vx_render_primary, run once more with algorithmic load
+ * counters on: bytes the method reads (8 per mask word / occupancy, 1 per
+ * LUT or material byte) and loop iterations, summed over all rays.
+ * stats = {beam bytes, beam iterations, primary+shadow bytes, primary+shadow
+ * iterations}. */
+int vx_render_primary_stats(VxWorld *w, const VxCamera *cam, const VxTraceParams *p,
+                            uint64_t stats[4]);
+/* vx_render_primary followed by a stream synchronize, with CUDA events
+ * recorded on `stream` around each kernel: ms[0] = beam pre-pass,
+ * ms[1] = primary (+shadow) kernel. */
+int vx_render_primary_timed(VxWorld *w, const VxCamera *cam, const VxTraceParams *p,
+                            VxHitRecord *rec_dev, VxShadowRecord *shadow_dev, void *stream,
+                            float ms[2]);
+
+/* ---- host world (mirror of src/voxel.rs World, for C/C++ callers) ------ */
+int vx_host_world_create(int32_t bricks_x, int32_t bricks_y, int32_t bricks_z,
+                         VxHostWorld **out);
+int vx_host_world_destroy(VxHostWorld *h);
+/* Borrow the array pointers (valid until destroy). */
+int vx_host_world_arrays(VxHostWorld *h, VxBrick **bricks, uint64_t **tile_mask,
+                         uint64_t **chunk_mask, uint64_t **l4_mask, uint8_t **brick_uniform,
+                         uint8_t **tile_uniform);
+/* World::set_voxel (voxel.rs:916-935) at slot coords. */
+int vx_host_world_set_voxel(VxHostWorld *h, uint32_t x, uint32_t y, uint32_t z, uint8_t mat);
+/* World::apply_edit (voxel.rs:450-474) at world coords for a window origin. */
+int vx_host_world_apply_edit(VxHostWorld *h, int32_t wx, int32_t wy, int32_t wz, uint8_t mat,
+                             const int32_t origin[3]);
+/* rebuild_all_masks + rebuild_all_uniform (voxel.rs:946-1000); marks all dirty. */
+int vx_host_world_rebuild(VxHostWorld *h);
+/* Number of pending dirty bricks (sorted + deduped on read). */
+int64_t vx_host_world_dirty_count(VxHostWorld *h);
+/* Renderer::upload_world: full upload if all-dirty, else the dirty bricks
+ * only through vx_world_apply_dirty; clears the dirty state. */
+int vx_world_sync(VxWorld *w, VxHostWorld *h, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VOXRT_H */

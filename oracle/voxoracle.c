@@ -1,0 +1,1220 @@
+/*
+ * voxoracle.c -- CPU oracle (TEST INFRASTRUCTURE ONLY; see voxoracle.h).
+ *
+ * A line-by-line C restatement of the reference traversal.  Every function
+ * cites the reference file:line it follows.  Arithmetic is IEEE binary32 with
+ * FMA contraction disabled at compile time (-ffp-contract=off), in the
+ * reference's operation order, so that the CUDA kernels (built with
+ * --fmad=false) reproduce it bit for bit.
+ *
+ * Conventions shared with the CUDA library (the reference leaves these
+ * implementation-defined in WGSL):
+ *   - min(a,b) = (b < a) ? b : a ; max(a,b) = (a < b) ? b : a
+ *   - normalize(v) = v / sqrt((x*x + y*y) + z*z) with IEEE sqrt and divide
+ *   - f32 -> i32 conversion saturates (NaN -> 0), clamped to +-2^30 so the
+ *     integer cell arithmetic that follows cannot overflow; such voxels lie
+ *     far outside any window and end the ray exactly as a saturated i32 would.
+ *   - Sub-voxel shading (water surface, foliage cutouts) is out of scope: a
+ *     solid voxel resolves by the reference's far-distance rule at every
+ *     distance -- decoration materials never stop a ray, everything else is
+ *     an opaque cube (raymarch.wgsl:4541-4545 with t beyond WATER_FAR_T).
+ */
+#include "voxoracle.h"
+
+#include <math.h>
+#include <pthread.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+
+/* ------------------------------------------------------------------ */
+/* scalar helpers                                                      */
+/* ------------------------------------------------------------------ */
+static inline float vmin(float a, float b) { return (b < a) ? b : a; }
+static inline float vmax(float a, float b) { return (a < b) ? b : a; }
+static inline float clampf(float x, float lo, float hi) { return vmin(vmax(x, lo), hi); }
+
+static inline int32_t f2i(float x) {
+    if (x != x) return 0;
+    if (x >= 1073741824.0f) return 1073741824;
+    if (x <= -1073741824.0f) return -1073741824;
+    return (int32_t)x;
+}
+
+/* common.wgsl:49-52 */
+static inline int32_t pos_mod(int32_t a, int32_t b) {
+    if (a >= 0) return a % b;
+    return (b - 1) - ((-1 - a) % b);
+}
+
+/* common.wgsl:55-58 ; raycast.rs:139-141 */
+static inline float safe_inv(float x) {
+    if (fabsf(x) < 1e-8f) return 1e30f;
+    return 1.0f / x;
+}
+
+/* WGSL sign() converted to i32 ; raycast.rs:135-137 */
+static inline int32_t sgn(float x) { return x > 0.0f ? 1 : (x < 0.0f ? -1 : 0); }
+
+static inline float fractf(float x) { return x - floorf(x); }
+
+/* Materials: src/voxel.rs:100-157, raymarch.wgsl:875-920 */
+enum { MAT_GRASS = 2, MAT_DIRT = 3, MAT_STONE = 4, MAT_WATER = 12, MAT_GLASS = 18,
+       MAT_LEAF_FRINGE = 33, MAT_TURF = 35 };
+static inline int is_water(uint32_t m) { return m >= 5u && m <= 12u; }
+static inline int is_transparent(uint32_t m) { return is_water(m) || m == MAT_GLASS; }
+static inline int is_foliage(uint32_t m) {
+    return m == 14u || m == 25u || m == 26u || m == 27u || m == 30u || m == 31u ||
+           m == 33u || m == 34u || m == 35u || m == 36u || m == 37u;
+}
+static inline int is_decoration(uint32_t m) {
+    return m == 30u || m == 31u || m == 33u || m == 34u || m == 35u || m == 36u || m == 37u;
+}
+static inline int is_uniform_optimisable(uint32_t m) {
+    return !is_foliage(m) && !is_transparent(m);
+}
+/* resolves_as_opaque_cube (raymarch.wgsl:4541-4545) evaluated beyond both
+ * sub-voxel radii: only decoration is non-opaque. */
+static inline int resolves_cube(uint32_t m) { return !is_decoration(m); }
+/* shadow_voxel_occludes (raymarch.wgsl:4314-4343), far-distance branch. */
+static inline int shadow_occludes(uint32_t m) {
+    if (m == MAT_LEAF_FRINGE || m == MAT_TURF) return 0;
+    if (is_decoration(m)) return 0;
+    return 1;
+}
+
+/* ------------------------------------------------------------------ */
+/* world dims + index functions (world_dims.rs:9-37, voxel.rs:190-294) */
+/* ------------------------------------------------------------------ */
+typedef struct {
+    int32_t bx, by, bz, vx, vy, vz, tx, ty, tz, cx, cy, cz, lx, ly, lz;
+} Dims;
+
+static Dims dims_of(const OrWorld *w) {
+    Dims d;
+    d.bx = w->bx; d.by = w->by; d.bz = w->bz;
+    d.vx = d.bx * 4; d.vy = d.by * 4; d.vz = d.bz * 4;
+    d.tx = d.bx / 4; d.ty = d.by / 4; d.tz = d.bz / 4;
+    d.cx = (d.tx + 3) / 4; d.cy = (d.ty + 3) / 4; d.cz = (d.tz + 3) / 4;
+    d.lx = (d.cx + 3) / 4; d.ly = (d.cy + 3) / 4; d.lz = (d.cz + 3) / 4;
+    return d;
+}
+static inline int64_t brick_idx(const Dims *d, int32_t x, int32_t y, int32_t z) {
+    return (int64_t)x + (int64_t)y * d->bx + (int64_t)z * d->bx * d->by;
+}
+static inline int64_t tile_idx(const Dims *d, int32_t x, int32_t y, int32_t z) {
+    return (int64_t)x + (int64_t)y * d->tx + (int64_t)z * d->tx * d->ty;
+}
+static inline int64_t chunk_idx(const Dims *d, int32_t x, int32_t y, int32_t z) {
+    return (int64_t)x + (int64_t)y * d->cx + (int64_t)z * d->cx * d->cy;
+}
+static inline int64_t l4_idx(const Dims *d, int32_t x, int32_t y, int32_t z) {
+    return (int64_t)x + (int64_t)y * d->lx + (int64_t)z * d->lx * d->ly;
+}
+static inline int child_bit(int32_t lx, int32_t ly, int32_t lz) { return lx + lz * 4 + ly * 16; }
+
+/* voxel.rs:233-247 */
+uint8_t or_brick_uniform_of(const OrBrick *b) {
+    if (b->occupancy != ~0ull) return 0;
+    uint8_t m0 = b->materials[0];
+    if (m0 == 0) return 0;
+    for (int i = 1; i < 64; ++i)
+        if (b->materials[i] != m0) return 0;
+    return m0;
+}
+
+/* voxel.rs:253-272 */
+static uint8_t tile_uniform_of(const Dims *d, const uint8_t *bu, int64_t ti) {
+    int32_t tx = (int32_t)(ti % d->tx);
+    int32_t ty = (int32_t)((ti / d->tx) % d->ty);
+    int32_t tz = (int32_t)(ti / ((int64_t)d->tx * d->ty));
+    int32_t bx0 = tx * 4, by0 = ty * 4, bz0 = tz * 4;
+    uint8_t m0 = bu[brick_idx(d, bx0, by0, bz0)];
+    if (m0 == 0) return 0;
+    for (int dz = 0; dz < 4; ++dz)
+        for (int dy = 0; dy < 4; ++dy)
+            for (int dx = 0; dx < 4; ++dx)
+                if (bu[brick_idx(d, bx0 + dx, by0 + dy, bz0 + dz)] != m0) return 0;
+    return m0;
+}
+
+/* voxel.rs:946-957 */
+void or_rebuild_all_uniform(const OrWorld *w) {
+    Dims d = dims_of(w);
+    int64_t nb = (int64_t)d.bx * d.by * d.bz;
+    int64_t nt = (int64_t)d.tx * d.ty * d.tz;
+    for (int64_t i = 0; i < nb; ++i) w->brick_uniform[i] = or_brick_uniform_of(&w->bricks[i]);
+    for (int64_t i = 0; i < nt; ++i) w->tile_uniform[i] = tile_uniform_of(&d, w->brick_uniform, i);
+}
+
+/* voxel.rs:958-1000 */
+void or_rebuild_all_masks(const OrWorld *w) {
+    Dims d = dims_of(w);
+    memset(w->tile_mask, 0, sizeof(uint64_t) * (size_t)d.tx * d.ty * d.tz);
+    memset(w->chunk_mask, 0, sizeof(uint64_t) * (size_t)d.cx * d.cy * d.cz);
+    memset(w->l4_mask, 0, sizeof(uint64_t) * (size_t)d.lx * d.ly * d.lz);
+    for (int32_t bz = 0; bz < d.bz; ++bz)
+        for (int32_t by = 0; by < d.by; ++by)
+            for (int32_t bx = 0; bx < d.bx; ++bx)
+                if (w->bricks[brick_idx(&d, bx, by, bz)].occupancy != 0)
+                    w->tile_mask[tile_idx(&d, bx / 4, by / 4, bz / 4)] |=
+                        1ull << child_bit(bx & 3, by & 3, bz & 3);
+    for (int32_t tz = 0; tz < d.tz; ++tz)
+        for (int32_t ty = 0; ty < d.ty; ++ty)
+            for (int32_t tx = 0; tx < d.tx; ++tx)
+                if (w->tile_mask[tile_idx(&d, tx, ty, tz)] != 0)
+                    w->chunk_mask[chunk_idx(&d, tx / 4, ty / 4, tz / 4)] |=
+                        1ull << child_bit(tx & 3, ty & 3, tz & 3);
+    for (int32_t cz = 0; cz < d.cz; ++cz)
+        for (int32_t cy = 0; cy < d.cy; ++cy)
+            for (int32_t cx = 0; cx < d.cx; ++cx)
+                if (w->chunk_mask[chunk_idx(&d, cx, cy, cz)] != 0)
+                    w->l4_mask[l4_idx(&d, cx / 4, cy / 4, cz / 4)] |=
+                        1ull << child_bit(cx & 3, cy & 3, cz & 3);
+}
+
+/* refresh_masks_for_brick, voxel.rs:879-914 */
+static void refresh_masks_for_brick(const OrWorld *w, const Dims *d, int32_t bx, int32_t by,
+                                    int32_t bz) {
+    int64_t bi = brick_idx(d, bx, by, bz);
+    int solid = w->bricks[bi].occupancy != 0;
+    int32_t tx = bx / 4, ty = by / 4, tz = bz / 4;
+    int64_t ti = tile_idx(d, tx, ty, tz);
+    int bit = child_bit(bx & 3, by & 3, bz & 3);
+    uint64_t prev = w->tile_mask[ti];
+    if (solid) w->tile_mask[ti] |= 1ull << bit;
+    else w->tile_mask[ti] &= ~(1ull << bit);
+    uint64_t now = w->tile_mask[ti];
+    if ((prev == 0) != (now == 0)) {
+        int32_t cx = tx / 4, cy = ty / 4, cz = tz / 4;
+        int64_t ci = chunk_idx(d, cx, cy, cz);
+        int cbit = child_bit(tx & 3, ty & 3, tz & 3);
+        uint64_t cprev = w->chunk_mask[ci];
+        if (now == 0) w->chunk_mask[ci] &= ~(1ull << cbit);
+        else w->chunk_mask[ci] |= 1ull << cbit;
+        uint64_t cnow = w->chunk_mask[ci];
+        if ((cprev == 0) != (cnow == 0)) {
+            int64_t li = l4_idx(d, cx / 4, cy / 4, cz / 4);
+            int lbit = child_bit(cx & 3, cy & 3, cz & 3);
+            if (cnow == 0) w->l4_mask[li] &= ~(1ull << lbit);
+            else w->l4_mask[li] |= 1ull << lbit;
+        }
+    }
+}
+
+/* set_voxel, voxel.rs:916-935 (+ Brick::set :309-319) */
+int64_t or_set_voxel(const OrWorld *w, uint32_t x, uint32_t y, uint32_t z, uint8_t mat) {
+    Dims d = dims_of(w);
+    if (x >= (uint32_t)d.vx || y >= (uint32_t)d.vy || z >= (uint32_t)d.vz) return -1;
+    int32_t bx = x / 4, by = y / 4, bz = z / 4;
+    int vi = child_bit(x % 4, y % 4, z % 4);
+    int64_t bi = brick_idx(&d, bx, by, bz);
+    OrBrick *b = &w->bricks[bi];
+    int was_empty = b->occupancy == 0;
+    if (mat == 0) {
+        b->occupancy &= ~(1ull << vi);
+        b->materials[vi] = 0;
+    } else {
+        b->occupancy |= 1ull << vi;
+        b->materials[vi] = mat;
+    }
+    int is_empty = b->occupancy == 0;
+    if (was_empty != is_empty) refresh_masks_for_brick(w, &d, bx, by, bz);
+    w->brick_uniform[bi] = or_brick_uniform_of(b);
+    int64_t ti = tile_idx(&d, bx / 4, by / 4, bz / 4);
+    w->tile_uniform[ti] = tile_uniform_of(&d, w->brick_uniform, ti);
+    return bi;
+}
+
+/* ------------------------------------------------------------------ */
+/* noise (voxel.rs:1163-1232, :1999-2021)                             */
+/* ------------------------------------------------------------------ */
+void or_seed_offset_xz(uint64_t seed, float out[2]) {
+    float hi = (float)(int32_t)(uint32_t)(seed >> 32);
+    float lo = (float)(int32_t)(uint32_t)(seed & 0xFFFFFFFFull);
+    out[0] = hi * 0.01734f;
+    out[1] = lo * 0.02153f;
+}
+
+static inline float hash2(int32_t x, int32_t z) {
+    uint32_t h = (uint32_t)x * 0x9E3779B1u + (uint32_t)z * 0x85EBCA77u;
+    h = h * 0xC2B2AE3Du;
+    h = h ^ (h >> 16);
+    h = h * 0x85EBCA6Bu;
+    return (((float)(h & 0xFFFFFFu)) / 16777215.0f) * 2.0f - 1.0f;
+}
+
+static inline float hash3(int32_t x, int32_t y, int32_t z) {
+    uint32_t h = (uint32_t)x * 0x9E3779B1u + (uint32_t)y * 0x85EBCA77u + (uint32_t)z * 0xC2B2AE3Du;
+    h = h * 0xD2B74407u;
+    h = h ^ (h >> 16);
+    h = h * 0x85EBCA6Bu;
+    return (((float)(h & 0xFFFFFFu)) / 16777215.0f) * 2.0f - 1.0f;
+}
+
+static inline float smooth(float t) { return t * t * (3.0f - 2.0f * t); }
+
+static float value_noise_2d(float x, float z) {
+    int32_t xi = f2i(floorf(x));
+    int32_t zi = f2i(floorf(z));
+    float xf = smooth(x - (float)xi);
+    float zf = smooth(z - (float)zi);
+    float v00 = hash2(xi, zi);
+    float v10 = hash2(xi + 1, zi);
+    float v01 = hash2(xi, zi + 1);
+    float v11 = hash2(xi + 1, zi + 1);
+    float a = v00 * (1.0f - xf) + v10 * xf;
+    float b = v01 * (1.0f - xf) + v11 * xf;
+    return a * (1.0f - zf) + b * zf;
+}
+
+float or_fbm_2d(float x, float z, uint32_t octaves) {
+    float total = 0.0f, amp = 1.0f, freq = 1.0f, max_amp = 0.0f;
+    for (uint32_t i = 0; i < octaves; ++i) {
+        total += value_noise_2d(x * freq, z * freq) * amp;
+        max_amp += amp;
+        amp *= 0.5f;
+        freq *= 2.0f;
+    }
+    return total / max_amp;
+}
+
+float or_value_noise_3d(float x, float y, float z) {
+    int32_t xi = f2i(floorf(x)), yi = f2i(floorf(y)), zi = f2i(floorf(z));
+    float xf = smooth(x - (float)xi);
+    float yf = smooth(y - (float)yi);
+    float zf = smooth(z - (float)zi);
+    float v000 = hash3(xi, yi, zi);
+    float v100 = hash3(xi + 1, yi, zi);
+    float v010 = hash3(xi, yi + 1, zi);
+    float v110 = hash3(xi + 1, yi + 1, zi);
+    float v001 = hash3(xi, yi, zi + 1);
+    float v101 = hash3(xi + 1, yi, zi + 1);
+    float v011 = hash3(xi, yi + 1, zi + 1);
+    float v111 = hash3(xi + 1, yi + 1, zi + 1);
+    float a = v000 * (1.0f - xf) + v100 * xf;
+    float b = v010 * (1.0f - xf) + v110 * xf;
+    float c = v001 * (1.0f - xf) + v101 * xf;
+    float d = v011 * (1.0f - xf) + v111 * xf;
+    float ab = a * (1.0f - yf) + b * yf;
+    float cd = c * (1.0f - yf) + d * yf;
+    return ab * (1.0f - zf) + cd * zf;
+}
+
+/* ------------------------------------------------------------------ */
+/* synthetic terrain (the benchmark worlds).  Noise primitives and the   */
+/* seed offset are the reference's; the column recipe is the workload's: */
+/* h = floor(base + amp * fbm(x/128, z/128, 5)), grass top, dirt below,  */
+/* stone beneath, water up to the level, caves where 3D noise > thr      */
+/* (carved only strictly inside the column, the guard of voxel.rs:1128). */
+/* ------------------------------------------------------------------ */
+typedef struct {
+    const OrWorld *w;
+    const OrTerrain *t;
+    int32_t z0, z1;
+} GenJob;
+
+static void gen_columns(const OrWorld *w, const OrTerrain *t, int32_t z0, int32_t z1) {
+    Dims d = dims_of(w);
+    float off[2];
+    or_seed_offset_xz(t->seed, off);
+    for (int32_t z = z0; z < z1; ++z) {
+        for (int32_t x = 0; x < d.vx; ++x) {
+            float fx = (float)x + off[0];
+            float fz = (float)z + off[1];
+            float n = or_fbm_2d(fx * t->inv_wavelength, fz * t->inv_wavelength, t->octaves);
+            int32_t h = f2i(floorf(t->base_height + t->amplitude * n));
+            if (h < 1) h = 1;
+            if (h > d.vy - 1) h = d.vy - 1;
+            for (int32_t y = 0; y <= h; ++y) {
+                if (y > 4 && y + 3 < h) {
+                    float c = or_value_noise_3d(fx * t->cave_inv_wavelength,
+                                                (float)y * t->cave_inv_wavelength,
+                                                fz * t->cave_inv_wavelength);
+                    if (c > t->cave_threshold) continue;
+                }
+                uint8_t m = (y == h) ? MAT_GRASS : ((y + t->dirt_depth >= h) ? MAT_DIRT : MAT_STONE);
+                OrBrick *b = &w->bricks[brick_idx(&d, x / 4, y / 4, z / 4)];
+                int vi = child_bit(x & 3, y & 3, z & 3);
+                b->occupancy |= 1ull << vi;
+                b->materials[vi] = m;
+            }
+            for (int32_t y = h + 1; y <= t->water_level && y < d.vy; ++y) {
+                OrBrick *b = &w->bricks[brick_idx(&d, x / 4, y / 4, z / 4)];
+                int vi = child_bit(x & 3, y & 3, z & 3);
+                b->occupancy |= 1ull << vi;
+                b->materials[vi] = MAT_WATER;
+            }
+        }
+    }
+}
+
+static void *gen_thread(void *arg) {
+    GenJob *j = (GenJob *)arg;
+    gen_columns(j->w, j->t, j->z0, j->z1);
+    return NULL;
+}
+
+void or_generate_terrain(const OrWorld *w, const OrTerrain *t, int nthreads) {
+    Dims d = dims_of(w);
+    memset(w->bricks, 0, sizeof(OrBrick) * (size_t)d.bx * d.by * d.bz);
+    if (nthreads < 1) nthreads = 1;
+    if (nthreads > 256) nthreads = 256;
+    /* split along z at brick boundaries so threads never share a brick */
+    int32_t nb = d.bz;
+    pthread_t th[256];
+    GenJob jobs[256];
+    int used = 0;
+    for (int i = 0; i < nthreads; ++i) {
+        int32_t b0 = (int32_t)((int64_t)nb * i / nthreads);
+        int32_t b1 = (int32_t)((int64_t)nb * (i + 1) / nthreads);
+        if (b1 <= b0) continue;
+        jobs[used].w = w; jobs[used].t = t; jobs[used].z0 = b0 * 4; jobs[used].z1 = b1 * 4;
+        used++;
+    }
+    for (int i = 1; i < used; ++i) pthread_create(&th[i], NULL, gen_thread, &jobs[i]);
+    if (used > 0) gen_thread(&jobs[0]);
+    for (int i = 1; i < used; ++i) pthread_join(th[i], NULL);
+}
+
+/* ------------------------------------------------------------------ */
+/* ray generation                                                      */
+/* ------------------------------------------------------------------ */
+static inline void normalize3(const float v[3], float out[3]) {
+    float len = sqrtf((v[0] * v[0] + v[1] * v[1]) + v[2] * v[2]);
+    out[0] = v[0] / len;
+    out[1] = v[1] / len;
+    out[2] = v[2] / len;
+}
+
+/* ray_dir_uv, raymarch.wgsl:430-438 (beam.wgsl:38-45 is the same formula) */
+void or_ray_dir_uv(const OrCamera *c, float u, float v, float out[3]) {
+    float ndc_x = u * 2.0f - 1.0f;
+    float ndc_y = 1.0f - v * 2.0f;
+    float aspect = c->res_x / c->res_y;
+    float a = ndc_x * c->tan_half_fov * aspect;
+    float b = ndc_y * c->tan_half_fov;
+    float r[3];
+    for (int k = 0; k < 3; ++k) r[k] = (c->forward[k] + c->right[k] * a) + c->up[k] * b;
+    normalize3(r, out);
+}
+
+/* ign, raymarch.wgsl:394-396 */
+float or_ign(float x, float y, float frame) {
+    float a = x + frame * 5.588238f;
+    float b = y + frame * 4.182857f;
+    return fractf(52.9829189f * fractf(0.06711056f * a + 0.00583715f * b));
+}
+
+/* sin/cos by the Maclaurin series, nested in x^2 (terms through x^17 /
+ * x^18; truncation < 2e-10 on [0, 2.4]).  Written out so the CPU and the
+ * GPU evaluate the identical operation sequence. */
+void or_sincos(float x, float *s, float *c) {
+    float x2 = x * x;
+    float ps = 1.0f - x2 * 0.0036764706f;      /* 1/272 */
+    ps = 1.0f - x2 * 0.0047619049f * ps;       /* 1/210 */
+    ps = 1.0f - x2 * 0.0064102565f * ps;       /* 1/156 */
+    ps = 1.0f - x2 * 0.0090909088f * ps;       /* 1/110 */
+    ps = 1.0f - x2 * 0.013888889f * ps;        /* 1/72  */
+    ps = 1.0f - x2 * 0.023809524f * ps;        /* 1/42  */
+    ps = 1.0f - x2 * 0.050000001f * ps;        /* 1/20  */
+    ps = 1.0f - x2 * 0.16666667f * ps;         /* 1/6   */
+    *s = x * ps;
+    float pc = 1.0f - x2 * 0.0032679739f;      /* 1/306 */
+    pc = 1.0f - x2 * 0.0041666669f * pc;       /* 1/240 */
+    pc = 1.0f - x2 * 0.0054945056f * pc;       /* 1/182 */
+    pc = 1.0f - x2 * 0.0075757578f * pc;       /* 1/132 */
+    pc = 1.0f - x2 * 0.011111111f * pc;        /* 1/90  */
+    pc = 1.0f - x2 * 0.017857144f * pc;        /* 1/56  */
+    pc = 1.0f - x2 * 0.033333335f * pc;        /* 1/30  */
+    pc = 1.0f - x2 * 0.083333336f * pc;        /* 1/12  */
+    pc = 1.0f - x2 * 0.5f * pc;                /* 1/2   */
+    *c = pc;
+}
+
+/* ------------------------------------------------------------------ */
+/* O2 hierarchical DDA                                                 */
+/* ------------------------------------------------------------------ */
+typedef struct {
+    float org[3], inv[3], tdel[3], tmin3[3], tmax[3];
+    float t_enter;
+    int32_t step[3], voxel[3], slot[3];
+} Dda;
+
+/* dda_init, raymarch.wgsl:3369-3411 */
+static int dda_init(const Dims *d, const int32_t ro[3], const float origin[3],
+                    const float dir[3], Dda *s) {
+    float dims[3] = {(float)d->vx, (float)d->vy, (float)d->vz};
+    float tmax3[3];
+    for (int k = 0; k < 3; ++k) {
+        s->org[k] = origin[k] - (float)ro[k];
+        s->inv[k] = safe_inv(dir[k]);
+        float t0 = (0.0f - s->org[k]) * s->inv[k];
+        float t1 = (dims[k] - s->org[k]) * s->inv[k];
+        s->tmin3[k] = vmin(t0, t1);
+        tmax3[k] = vmax(t0, t1);
+    }
+    s->t_enter = vmax(vmax(s->tmin3[0], s->tmin3[1]), vmax(s->tmin3[2], 0.0f));
+    float t_exit = vmin(vmin(tmax3[0], tmax3[1]), tmax3[2]);
+    if (s->t_enter >= t_exit || t_exit < 0.0f) return 0;
+    for (int k = 0; k < 3; ++k) {
+        float p = s->org[k] + dir[k] * (s->t_enter + 1e-3f);
+        p = clampf(p, 0.01f, dims[k] - 0.01f);
+        s->step[k] = sgn(dir[k]);
+        s->tdel[k] = fabsf(s->inv[k]);
+        int32_t vl0 = f2i(floorf(p));
+        s->voxel[k] = vl0 + ro[k];
+        if (s->step[k] > 0) s->tmax[k] = ((float)(vl0 + 1) - s->org[k]) * s->inv[k];
+        else s->tmax[k] = ((float)vl0 - s->org[k]) * s->inv[k];
+    }
+    s->slot[0] = pos_mod(s->voxel[0], d->vx);
+    s->slot[1] = s->voxel[1];
+    s->slot[2] = pos_mod(s->voxel[2], d->vz);
+    return 1;
+}
+
+/* dda_step, raymarch.wgsl:3416-3448 */
+static inline void dda_step(const Dims *d, Dda *s, float *t_cur, int32_t *last_axis) {
+    int ax;
+    if (s->tmax[0] < s->tmax[1] && s->tmax[0] < s->tmax[2]) ax = 0;
+    else if (s->tmax[1] < s->tmax[2]) ax = 1;
+    else ax = 2;
+    *t_cur = s->tmax[ax];
+    s->voxel[ax] += s->step[ax];
+    s->slot[ax] += s->step[ax];
+    if (ax == 0) {
+        if (s->slot[0] >= d->vx) s->slot[0] -= d->vx;
+        else if (s->slot[0] < 0) s->slot[0] += d->vx;
+    } else if (ax == 2) {
+        if (s->slot[2] >= d->vz) s->slot[2] -= d->vz;
+        else if (s->slot[2] < 0) s->slot[2] += d->vz;
+    }
+    s->tmax[ax] = s->tmax[ax] + s->tdel[ax];
+    *last_axis = ax;
+}
+
+/* skip_to_cell, raymarch.wgsl:4807-4864 */
+static void skip_to_cell(const Dims *d, int32_t cell, Dda *s, const int32_t ro[3],
+                         const float dir[3], int32_t *last_axis) {
+    int32_t co[3];
+    float tf[3];
+    for (int k = 0; k < 3; ++k) {
+        co[k] = s->voxel[k] - pos_mod(s->voxel[k], cell);
+        int32_t b = (s->step[k] > 0 ? co[k] + cell : co[k]) - ro[k];
+        tf[k] = ((float)b - s->org[k]) * s->inv[k];
+    }
+    const float eps = 1e-6f;
+    float t_min = 1e30f;
+    int ax = 0;
+    if (s->step[0] != 0 && tf[0] > eps && tf[0] < t_min) { t_min = tf[0]; ax = 0; }
+    if (s->step[1] != 0 && tf[1] > eps && tf[1] < t_min) { t_min = tf[1]; ax = 1; }
+    if (s->step[2] != 0 && tf[2] > eps && tf[2] < t_min) { t_min = tf[2]; ax = 2; }
+    int32_t nv[3];
+    for (int k = 0; k < 3; ++k) {
+        float p = s->org[k] + dir[k] * (t_min + 1e-3f);
+        nv[k] = f2i(floorf(p)) + ro[k];
+    }
+    nv[ax] = s->step[ax] > 0 ? co[ax] + cell : co[ax] - 1;
+    for (int k = 0; k < 3; ++k) {
+        s->voxel[k] = nv[k];
+        int32_t vl = nv[k] - ro[k];
+        if (s->step[k] > 0) s->tmax[k] = ((float)(vl + 1) - s->org[k]) * s->inv[k];
+        else s->tmax[k] = ((float)vl - s->org[k]) * s->inv[k];
+    }
+    *last_axis = ax;
+    s->slot[0] = pos_mod(nv[0], d->vx);
+    s->slot[1] = nv[1];
+    s->slot[2] = pos_mod(nv[2], d->vz);
+}
+
+/* last_axis_after_entry, raymarch.wgsl:4800-4805 */
+static inline int entry_axis(int32_t la, const float tmin3[3]) {
+    if (la >= 0) return la;
+    if (tmin3[0] >= tmin3[1] && tmin3[0] >= tmin3[2]) return 0;
+    if (tmin3[1] >= tmin3[2]) return 1;
+    return 2;
+}
+
+/* entry_normal_and_t (raymarch.wgsl:3321-3342) -> record fields */
+static void fill_hit(const Dda *s, int32_t last_axis, uint32_t m, int early, OrRecord *out) {
+    int ax = entry_axis(last_axis, s->tmin3);
+    float t;
+    if (last_axis >= 0) t = s->tmax[last_axis] - s->tdel[last_axis];
+    else t = s->t_enter;
+    out->voxel[0] = s->voxel[0];
+    out->voxel[1] = s->voxel[1];
+    out->voxel[2] = s->voxel[2];
+    out->face = (uint8_t)(2 * ax + (s->step[ax] > 0 ? 1 : 0));
+    out->mat = (uint8_t)m;
+    out->flags = (uint8_t)(1u | (early ? 2u : 0u));
+    out->t = t;
+}
+
+static void miss_record(OrRecord *out) {
+    memset(out, 0, sizeof(*out));
+    out->face = 0xFF;
+}
+
+/* brick_topmost_material, raymarch.wgsl:253-295 */
+static uint32_t brick_topmost_material(const OrBrick *b, uint64_t *bytes) {
+    uint32_t occ_lo = (uint32_t)b->occupancy, occ_hi = (uint32_t)(b->occupancy >> 32);
+    uint32_t layers[4] = {(occ_hi >> 16) & 0xFFFFu, occ_hi & 0xFFFFu, (occ_lo >> 16) & 0xFFFFu,
+                          occ_lo & 0xFFFFu};
+    int base[4] = {48, 32, 16, 0};
+    for (int i = 0; i < 4; ++i) {
+        if (layers[i] != 0u) {
+            int bit = __builtin_ctz(layers[i]);
+            uint32_t m = b->materials[base[i] + bit];
+            *bytes += 1;
+            if (m != MAT_TURF) return m;
+        }
+    }
+    return (occ_lo | occ_hi) != 0u ? (uint32_t)MAT_TURF : 0u;
+}
+
+/* tile_representative_material, raymarch.wgsl:4782-4798 */
+static uint32_t tile_representative_material(const OrWorld *w, const Dims *d, int64_t ti,
+                                             const int32_t tp[3], uint64_t *bytes) {
+    uint64_t tm = w->tile_mask[ti];
+    *bytes += 8;
+    int lin = -1;
+    uint32_t lo = (uint32_t)tm, hi = (uint32_t)(tm >> 32);
+    if (lo != 0u) lin = __builtin_ctz(lo);
+    else if (hi != 0u) lin = 32 + __builtin_ctz(hi);
+    if (lin < 0) return 0u;
+    int lx = lin & 3, lz = (lin >> 2) & 3, ly = (lin >> 4) & 3;
+    int64_t bi = brick_idx(d, tp[0] * 4 + lx, tp[1] * 4 + ly, tp[2] * 4 + lz);
+    *bytes += 8;
+    return brick_topmost_material(&w->bricks[bi], bytes);
+}
+
+static inline int in_window(const Dims *d, const int32_t v[3], const int32_t ro[3]) {
+    int32_t rx = v[0] - ro[0], ry = v[1] - ro[1], rz = v[2] - ro[2];
+    return !(rx < 0 || rx >= d->vx || ry < 0 || ry >= d->vy || rz < 0 || rz >= d->vz);
+}
+
+#define SKIP(cell)                                                          \
+    do {                                                                    \
+        skip_to_cell(&d, (cell), &s, ro, dir, &last_axis);                  \
+        t_cur = s.tmax[last_axis] - s.tdel[last_axis];                      \
+    } while (0)
+
+/* trace, raymarch.wgsl:4600-4777 (cube resolution, see file header) */
+void or_trace(const OrWorld *w, const int32_t ro[3], const float origin[3],
+              const float dir[3], float max_dist, const OrParams *p, OrRecord *out,
+              OrStats *st) {
+    Dims d = dims_of(w);
+    uint64_t bytes = 0, iters = 0;
+    miss_record(out);
+    Dda s;
+    if (!dda_init(&d, ro, origin, dir, &s)) goto done;
+    int32_t last_axis = -1;
+    float t_cur = s.t_enter;
+    const uint32_t fl = p->flags;
+    int32_t it;
+    for (it = 0; it < p->max_iters; ++it) {
+        iters++;
+        if (t_cur > max_dist) break;
+        if (!in_window(&d, s.voxel, ro)) break;
+        int32_t bp[3] = {s.slot[0] >> 2, s.slot[1] >> 2, s.slot[2] >> 2};
+        int32_t tp[3] = {s.slot[0] >> 4, s.slot[1] >> 4, s.slot[2] >> 4};
+        int32_t cp[3] = {s.slot[0] >> 6, s.slot[1] >> 6, s.slot[2] >> 6};
+        if (fl & OR_F_L4) {
+            int64_t li = l4_idx(&d, s.slot[0] >> 8, s.slot[1] >> 8, s.slot[2] >> 8);
+            uint64_t lw = w->l4_mask[li];
+            bytes += 8;
+            if (lw == 0) { SKIP(256); continue; }
+            if (!((lw >> child_bit(cp[0] & 3, cp[1] & 3, cp[2] & 3)) & 1ull)) { SKIP(64); continue; }
+        }
+        int64_t ci = chunk_idx(&d, cp[0], cp[1], cp[2]);
+        uint64_t cw = w->chunk_mask[ci];
+        bytes += 8;
+        if (!((cw >> child_bit(tp[0] & 3, tp[1] & 3, tp[2] & 3)) & 1ull)) { SKIP(16); continue; }
+        int64_t ti = tile_idx(&d, tp[0], tp[1], tp[2]);
+        if ((fl & OR_F_LOD) && t_cur > p->tile_lod_t) {
+            uint32_t lm = tile_representative_material(w, &d, ti, tp, &bytes);
+            if (lm != 0u && is_uniform_optimisable(lm)) {
+                fill_hit(&s, last_axis, lm, 1, out);
+                goto hit;
+            }
+        }
+        if (fl & OR_F_LUT) {
+            uint32_t tum = w->tile_uniform[ti];
+            bytes += 1;
+            if (tum != 0u && is_uniform_optimisable(tum)) {
+                fill_hit(&s, last_axis, tum, 1, out);
+                goto hit;
+            }
+        }
+        uint64_t tw = w->tile_mask[ti];
+        bytes += 8;
+        if (!((tw >> child_bit(bp[0] & 3, bp[1] & 3, bp[2] & 3)) & 1ull)) { SKIP(4); continue; }
+        int64_t bi = brick_idx(&d, bp[0], bp[1], bp[2]);
+        if (fl & OR_F_LUT) {
+            uint32_t bum = w->brick_uniform[bi];
+            bytes += 1;
+            if (bum != 0u && is_uniform_optimisable(bum)) {
+                fill_hit(&s, last_axis, bum, 1, out);
+                goto hit;
+            }
+        }
+        const OrBrick *b = &w->bricks[bi];
+        if ((fl & OR_F_LOD) && t_cur > p->lod_brick_t) {
+            bytes += 8;
+            if (b->occupancy == 0) { SKIP(4); continue; }
+            uint32_t m = brick_topmost_material(b, &bytes);
+            if (!is_foliage(m)) {
+                fill_hit(&s, last_axis, m, 1, out);
+                goto hit;
+            }
+        }
+        int vi = child_bit(s.slot[0] - bp[0] * 4, s.slot[1] - bp[1] * 4, s.slot[2] - bp[2] * 4);
+        bytes += 8;
+        if ((b->occupancy >> vi) & 1ull) {
+            uint32_t m = b->materials[vi];
+            bytes += 1;
+            if (resolves_cube(m)) {
+                fill_hit(&s, last_axis, m, 0, out);
+                goto hit;
+            }
+        }
+        dda_step(&d, &s, &t_cur, &last_axis);
+    }
+hit:
+done:
+    out->steps = (uint32_t)iters; /* iterations begun, including the last */
+    if (st) { st->bytes += bytes; st->iters += iters; }
+}
+
+/* trace_any, raymarch.wgsl:4345-4409 (far-distance occluder rule) */
+int or_trace_any(const OrWorld *w, const int32_t ro[3], const float origin[3],
+                 const float dir[3], float max_dist, const OrParams *p,
+                 uint32_t *steps_out, OrStats *st) {
+    Dims d = dims_of(w);
+    uint64_t bytes = 0, iters = 0;
+    int occluded = 0;
+    uint32_t steps = 0;
+    Dda s;
+    if (!dda_init(&d, ro, origin, dir, &s)) goto done;
+    int32_t last_axis = -1;
+    float t_cur = s.t_enter;
+    int32_t it;
+    for (it = 0; it < p->any_max_iters; ++it) {
+        iters++;
+        if (t_cur > max_dist) break;
+        if (!in_window(&d, s.voxel, ro)) break;
+        int32_t bp[3] = {s.slot[0] >> 2, s.slot[1] >> 2, s.slot[2] >> 2};
+        int32_t tp[3] = {s.slot[0] >> 4, s.slot[1] >> 4, s.slot[2] >> 4};
+        int32_t cp[3] = {s.slot[0] >> 6, s.slot[1] >> 6, s.slot[2] >> 6};
+        int64_t li = l4_idx(&d, s.slot[0] >> 8, s.slot[1] >> 8, s.slot[2] >> 8);
+        uint64_t lw = w->l4_mask[li];
+        bytes += 8;
+        if (lw == 0) { SKIP(256); continue; }
+        if (!((lw >> child_bit(cp[0] & 3, cp[1] & 3, cp[2] & 3)) & 1ull)) { SKIP(64); continue; }
+        uint64_t cw = w->chunk_mask[chunk_idx(&d, cp[0], cp[1], cp[2])];
+        bytes += 8;
+        if (!((cw >> child_bit(tp[0] & 3, tp[1] & 3, tp[2] & 3)) & 1ull)) { SKIP(16); continue; }
+        uint64_t tw = w->tile_mask[tile_idx(&d, tp[0], tp[1], tp[2])];
+        bytes += 8;
+        if (!((tw >> child_bit(bp[0] & 3, bp[1] & 3, bp[2] & 3)) & 1ull)) { SKIP(4); continue; }
+        const OrBrick *b = &w->bricks[brick_idx(&d, bp[0], bp[1], bp[2])];
+        int vi = child_bit(s.slot[0] - bp[0] * 4, s.slot[1] - bp[1] * 4, s.slot[2] - bp[2] * 4);
+        bytes += 8;
+        if ((b->occupancy >> vi) & 1ull) {
+            uint32_t m = b->materials[vi];
+            bytes += 1;
+            if (shadow_occludes(m)) { occluded = 1; break; }
+        }
+        dda_step(&d, &s, &t_cur, &last_axis);
+    }
+    steps = (uint32_t)iters;
+done:
+    if (steps_out) *steps_out = steps;
+    if (st) { st->bytes += bytes; st->iters += iters; }
+    return occluded;
+}
+
+/* trace_no_water, raymarch.wgsl:3450-3532 */
+void or_trace_no_water(const OrWorld *w, const int32_t ro[3], const float origin[3],
+                       const float dir[3], float t_cap, const OrParams *p, OrRecord *out,
+                       OrStats *st) {
+    Dims d = dims_of(w);
+    uint64_t bytes = 0, iters = 0;
+    miss_record(out);
+    Dda s;
+    if (!dda_init(&d, ro, origin, dir, &s)) goto done;
+    int32_t last_axis = -1;
+    float t_cur = s.t_enter;
+    int32_t it;
+    for (it = 0; it < p->max_iters; ++it) {
+        iters++;
+        if (t_cur > t_cap) break;
+        if (!in_window(&d, s.voxel, ro)) break;
+        int32_t bp[3] = {s.slot[0] >> 2, s.slot[1] >> 2, s.slot[2] >> 2};
+        int32_t tp[3] = {s.slot[0] >> 4, s.slot[1] >> 4, s.slot[2] >> 4};
+        int32_t cp[3] = {s.slot[0] >> 6, s.slot[1] >> 6, s.slot[2] >> 6};
+        int64_t li = l4_idx(&d, s.slot[0] >> 8, s.slot[1] >> 8, s.slot[2] >> 8);
+        uint64_t lw = w->l4_mask[li];
+        bytes += 8;
+        if (lw == 0) { skip_to_cell(&d, 256, &s, ro, dir, &last_axis); continue; }
+        if (!((lw >> child_bit(cp[0] & 3, cp[1] & 3, cp[2] & 3)) & 1ull)) {
+            skip_to_cell(&d, 64, &s, ro, dir, &last_axis);
+            continue;
+        }
+        uint64_t cw = w->chunk_mask[chunk_idx(&d, cp[0], cp[1], cp[2])];
+        bytes += 8;
+        if (!((cw >> child_bit(tp[0] & 3, tp[1] & 3, tp[2] & 3)) & 1ull)) {
+            skip_to_cell(&d, 16, &s, ro, dir, &last_axis);
+            continue;
+        }
+        uint64_t tw = w->tile_mask[tile_idx(&d, tp[0], tp[1], tp[2])];
+        bytes += 8;
+        if (!((tw >> child_bit(bp[0] & 3, bp[1] & 3, bp[2] & 3)) & 1ull)) {
+            skip_to_cell(&d, 4, &s, ro, dir, &last_axis);
+            continue;
+        }
+        const OrBrick *b = &w->bricks[brick_idx(&d, bp[0], bp[1], bp[2])];
+        int vi = child_bit(s.slot[0] - bp[0] * 4, s.slot[1] - bp[1] * 4, s.slot[2] - bp[2] * 4);
+        bytes += 8;
+        if ((b->occupancy >> vi) & 1ull) {
+            uint32_t m = b->materials[vi];
+            bytes += 1;
+            if (!is_transparent(m)) {
+                fill_hit(&s, last_axis, m, 0, out);
+                goto done;
+            }
+        }
+        dda_step(&d, &s, &t_cur, &last_axis);
+    }
+done:
+    out->steps = (uint32_t)iters;
+    if (st) { st->bytes += bytes; st->iters += iters; }
+}
+#undef SKIP
+
+/* trace_first_tile, beam.wgsl:51-113 (world, non-rebased coordinates) */
+float or_beam_first_tile(const OrWorld *w, const OrCamera *c, const float dir[3], OrStats *st) {
+    Dims d = dims_of(w);
+    uint64_t bytes = 0, iters = 0;
+    float result = 1e9f;
+    float win_min[3], win_max[3], inv[3], tmin3[3], tmax3[3];
+    float dims[3] = {(float)d.vx, (float)d.vy, (float)d.vz};
+    for (int k = 0; k < 3; ++k) {
+        win_min[k] = (float)c->world_origin[k];
+        win_max[k] = win_min[k] + dims[k];
+        inv[k] = safe_inv(dir[k]);
+        float t0 = (win_min[k] - c->origin[k]) * inv[k];
+        float t1 = (win_max[k] - c->origin[k]) * inv[k];
+        tmin3[k] = vmin(t0, t1);
+        tmax3[k] = vmax(t0, t1);
+    }
+    float t_enter = vmax(vmax(tmin3[0], tmin3[1]), vmax(tmin3[2], 0.0f));
+    float t_exit = vmin(vmin(tmax3[0], tmax3[1]), tmax3[2]);
+    if (t_enter >= t_exit || t_exit < 0.0f) goto done;
+    int32_t tile[3], step[3], origin_tile[3];
+    float tdel[3], tmax[3];
+    for (int k = 0; k < 3; ++k) {
+        float p = c->origin[k] + dir[k] * (t_enter + 0.05f);
+        p = clampf(p, win_min[k] + 0.01f, win_max[k] - 0.01f);
+        tile[k] = f2i(floorf(p / 16.0f));
+        step[k] = sgn(dir[k]);
+        tdel[k] = fabsf(inv[k]) * 16.0f;
+        if (step[k] > 0) tmax[k] = ((float)((tile[k] + 1) * 16) - c->origin[k]) * inv[k];
+        else tmax[k] = ((float)(tile[k] * 16) - c->origin[k]) * inv[k];
+        origin_tile[k] = c->world_origin[k] / 16;
+    }
+    float t_cur = t_enter;
+    for (int s = 0; s < 80; ++s) {
+        iters++;
+        int32_t rx = tile[0] - origin_tile[0], ry = tile[1] - origin_tile[1],
+                rz = tile[2] - origin_tile[2];
+        if (rx < 0 || rx >= d.tx || ry < 0 || ry >= d.ty || rz < 0 || rz >= d.tz) goto done;
+        int32_t st_[3] = {pos_mod(tile[0], d.tx), tile[1], pos_mod(tile[2], d.tz)};
+        int64_t ci = chunk_idx(&d, st_[0] / 4, st_[1] / 4, st_[2] / 4);
+        int lin = (st_[0] & 3) + (st_[2] & 3) * 4 + (st_[1] & 3) * 16;
+        bytes += 8;
+        if ((w->chunk_mask[ci] >> lin) & 1ull) { result = t_cur; goto done; }
+        if (tmax[0] < tmax[1] && tmax[0] < tmax[2]) {
+            tile[0] += step[0]; t_cur = tmax[0]; tmax[0] = tmax[0] + tdel[0];
+        } else if (tmax[1] < tmax[2]) {
+            tile[1] += step[1]; t_cur = tmax[1]; tmax[1] = tmax[1] + tdel[1];
+        } else {
+            tile[2] += step[2]; t_cur = tmax[2]; tmax[2] = tmax[2] + tdel[2];
+        }
+    }
+done:
+    if (st) { st->bytes += bytes; st->iters += iters; }
+    return result;
+}
+
+/* cs_beam, beam.wgsl:30-49 */
+void or_beam_pass(const OrWorld *w, const OrCamera *c, float *beam_out, OrStats *st) {
+    uint32_t bw = ((uint32_t)c->res_x + 7u) / 8u;
+    uint32_t bh = ((uint32_t)c->res_y + 7u) / 8u;
+    for (uint32_t gy = 0; gy < bh; ++gy)
+        for (uint32_t gx = 0; gx < bw; ++gx) {
+            float u = ((float)gx * 8.0f + 4.0f) / c->res_x;
+            float v = ((float)gy * 8.0f + 4.0f) / c->res_y;
+            float dir[3];
+            or_ray_dir_uv(c, u, v, dir);
+            beam_out[gy * bw + gx] = or_beam_first_tile(w, c, dir, st);
+        }
+}
+
+/* Shadow ray of raymarch.wgsl:3953-3994 with the workload's cone:
+ * theta = ign * golden angle, radius = tan(cone) * sqrt(ign). */
+void or_shadow_ray(const OrCamera *c, const OrParams *p, uint32_t px, uint32_t py,
+                   const float dir[3], const OrRecord *hit, float o_out[3], float d_out[3]) {
+    int ax = hit->face >> 1;
+    float nval = (hit->face & 1) ? -1.0f : 1.0f;
+    for (int k = 0; k < 3; ++k) {
+        float ph = c->origin[k] + dir[k] * hit->t;
+        float n = (k == ax) ? nval : 0.0f;
+        o_out[k] = ph + n * 0.001f;
+    }
+    float jit = or_ign((float)px, (float)py, p->frame);
+    float theta = jit * 2.39996323f;
+    float radius = p->cone_tan * sqrtf(jit);
+    float sn, cs;
+    or_sincos(theta, &sn, &cs);
+    float v[3];
+    for (int k = 0; k < 3; ++k) {
+        float off = (p->sun_tangent[k] * cs + p->sun_bitangent[k] * sn) * radius;
+        v[k] = p->sun[k] + off;
+    }
+    normalize3(v, d_out);
+}
+
+/* cs_main traversal part, raymarch.wgsl:576-631 (all tiles dirty, camera
+ * above water) + one shadow ray per hit. */
+void or_render_rows(const OrWorld *w, const OrCamera *c, const OrParams *p,
+                    const float *beam, uint32_t y0, uint32_t y1, OrRecord *rec,
+                    OrShadow *sh, OrStats *st) {
+    uint32_t W = (uint32_t)c->res_x;
+    uint32_t bw = (W + 7u) / 8u;
+    for (uint32_t gy = y0; gy < y1; ++gy) {
+        for (uint32_t gx = 0; gx < W; ++gx) {
+            size_t i = (size_t)gy * W + gx;
+            float u = (((float)gx + 0.5f) + c->jitter_x) / c->res_x;
+            float v = (((float)gy + 0.5f) + c->jitter_y) / c->res_y;
+            float dir[3];
+            or_ray_dir_uv(c, u, v, dir);
+            float skip = 0.0f;
+            float org[3] = {c->origin[0], c->origin[1], c->origin[2]};
+            if (p->flags & OR_F_BEAM) {
+                float bt = beam[(gy / 8u) * bw + gx / 8u];
+                skip = vmax(0.0f, bt - p->beam_margin);
+                for (int k = 0; k < 3; ++k) org[k] = c->origin[k] + dir[k] * skip;
+            }
+            or_trace(w, c->world_origin, org, dir, p->max_dist, p, &rec[i], st);
+            if ((p->flags & OR_F_BEAM) && (rec[i].flags & 1u)) rec[i].t = rec[i].t + skip;
+            if (sh) {
+                memset(&sh[i], 0, sizeof(OrShadow));
+                if ((p->flags & OR_F_SHADOW) && (rec[i].flags & 1u)) {
+                    float so[3], sd[3];
+                    or_shadow_ray(c, p, gx, gy, dir, &rec[i], so, sd);
+                    uint32_t ssteps = 0;
+                    sh[i].occluded = (uint8_t)or_trace_any(w, c->world_origin, so, sd,
+                                                           p->shadow_max_dist, p, &ssteps, st);
+                    sh[i].steps = ssteps;
+                    sh[i].traced = 1;
+                }
+            }
+        }
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* threading                                                           */
+/* ------------------------------------------------------------------ */
+static double now_s(void) {
+    struct timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
+}
+
+typedef struct {
+    const OrWorld *w;
+    const OrCamera *c;
+    const OrParams *p;
+    const float *beam;
+    uint32_t y0, y1;
+    OrRecord *rec;
+    OrShadow *sh;
+    OrStats st;
+} RowJob;
+
+static void *row_thread(void *arg) {
+    RowJob *j = (RowJob *)arg;
+    or_render_rows(j->w, j->c, j->p, j->beam, j->y0, j->y1, j->rec, j->sh, &j->st);
+    return NULL;
+}
+
+double or_render_frame(const OrWorld *w, const OrCamera *c, const OrParams *p, OrRecord *rec,
+                       OrShadow *sh, float *beam, int nthreads, OrStats *st) {
+    double t0 = now_s();
+    if (nthreads < 1) nthreads = 1;
+    if (nthreads > 256) nthreads = 256;
+    if (p->flags & OR_F_BEAM) or_beam_pass(w, c, beam, st);
+    uint32_t H = (uint32_t)c->res_y;
+    pthread_t th[256];
+    RowJob jobs[256];
+    int used = 0;
+    for (int i = 0; i < nthreads; ++i) {
+        uint32_t a = (uint32_t)((uint64_t)H * i / nthreads);
+        uint32_t b = (uint32_t)((uint64_t)H * (i + 1) / nthreads);
+        if (b <= a) continue;
+        RowJob *j = &jobs[used++];
+        j->w = w; j->c = c; j->p = p; j->beam = beam; j->y0 = a; j->y1 = b;
+        j->rec = rec; j->sh = sh;
+        j->st.bytes = 0; j->st.iters = 0;
+    }
+    for (int i = 1; i < used; ++i) pthread_create(&th[i], NULL, row_thread, &jobs[i]);
+    if (used > 0) row_thread(&jobs[0]);
+    for (int i = 1; i < used; ++i) pthread_join(th[i], NULL);
+    if (st)
+        for (int i = 0; i < used; ++i) { st->bytes += jobs[i].st.bytes; st->iters += jobs[i].st.iters; }
+    return now_s() - t0;
+}
+
+typedef struct {
+    const OrWorld *w;
+    const OrCamera *c;
+    const OrParams *p;
+    const float *beam;
+    uint32_t stride, offset, first, last; /* rows first..last-1 of the set */
+    OrRecord *rec;
+    OrShadow *sh;
+    OrStats st;
+} RowSetJob;
+
+static void *rowset_thread(void *arg) {
+    RowSetJob *j = (RowSetJob *)arg;
+    for (uint32_t k = j->first; k < j->last; ++k) {
+        uint32_t y = j->offset + k * j->stride;
+        or_render_rows(j->w, j->c, j->p, j->beam, y, y + 1, j->rec, j->sh, &j->st);
+    }
+    return NULL;
+}
+
+/* Rows offset, offset+stride, ... of a frame (the beam buffer is given) on
+ * nthreads threads; records land at their full-frame indices.  Returns wall
+ * seconds.  Used for bounded CPU samples of a frame. */
+double or_render_row_set(const OrWorld *w, const OrCamera *c, const OrParams *p,
+                         const float *beam, uint32_t stride, uint32_t offset, OrRecord *rec,
+                         OrShadow *sh, int nthreads, OrStats *st) {
+    double t0 = now_s();
+    if (nthreads < 1) nthreads = 1;
+    if (nthreads > 256) nthreads = 256;
+    if (stride < 1) stride = 1;
+    uint32_t H = (uint32_t)c->res_y;
+    uint32_t nrows = offset < H ? (H - offset + stride - 1) / stride : 0;
+    pthread_t th[256];
+    RowSetJob jobs[256];
+    int used = 0;
+    for (int i = 0; i < nthreads; ++i) {
+        uint32_t a = (uint32_t)((uint64_t)nrows * i / nthreads);
+        uint32_t b = (uint32_t)((uint64_t)nrows * (i + 1) / nthreads);
+        if (b <= a) continue;
+        RowSetJob *j = &jobs[used++];
+        j->w = w; j->c = c; j->p = p; j->beam = beam; j->stride = stride; j->offset = offset;
+        j->first = a; j->last = b; j->rec = rec; j->sh = sh;
+        j->st.bytes = 0; j->st.iters = 0;
+    }
+    for (int i = 1; i < used; ++i) pthread_create(&th[i], NULL, rowset_thread, &jobs[i]);
+    if (used > 0) rowset_thread(&jobs[0]);
+    for (int i = 1; i < used; ++i) pthread_join(th[i], NULL);
+    if (st)
+        for (int i = 0; i < used; ++i) { st->bytes += jobs[i].st.bytes; st->iters += jobs[i].st.iters; }
+    return now_s() - t0;
+}
+
+typedef struct {
+    const OrWorld *w;
+    const int32_t *ro;
+    const OrRay *rays;
+    size_t a, b;
+    const OrParams *p;
+    OrRecord *out;
+    OrStats st;
+} BatchJob;
+
+static void *batch_thread(void *arg) {
+    BatchJob *j = (BatchJob *)arg;
+    for (size_t i = j->a; i < j->b; ++i) {
+        const OrRay *r = &j->rays[i];
+        if (r->kind == 1u) {
+            uint32_t steps = 0;
+            int occ = or_trace_any(j->w, j->ro, r->org, r->dir, r->tmax, j->p, &steps, &j->st);
+            miss_record(&j->out[i]);
+            j->out[i].flags = (uint8_t)(occ ? 1u : 0u);
+            j->out[i].steps = steps;
+        } else if (r->kind == 2u) {
+            or_trace_no_water(j->w, j->ro, r->org, r->dir, r->tmax, j->p, &j->out[i], &j->st);
+        } else {
+            or_trace(j->w, j->ro, r->org, r->dir, r->tmax, j->p, &j->out[i], &j->st);
+        }
+    }
+    return NULL;
+}
+
+double or_trace_batch(const OrWorld *w, const int32_t ro[3], const OrRay *rays, size_t n,
+                      const OrParams *p, OrRecord *out, int nthreads, OrStats *st) {
+    double t0 = now_s();
+    if (nthreads < 1) nthreads = 1;
+    if (nthreads > 256) nthreads = 256;
+    pthread_t th[256];
+    BatchJob jobs[256];
+    int used = 0;
+    for (int i = 0; i < nthreads; ++i) {
+        size_t a = n * (size_t)i / (size_t)nthreads, b = n * (size_t)(i + 1) / (size_t)nthreads;
+        if (b <= a) continue;
+        BatchJob *j = &jobs[used++];
+        j->w = w; j->ro = ro; j->rays = rays; j->a = a; j->b = b; j->p = p; j->out = out;
+        j->st.bytes = 0; j->st.iters = 0;
+    }
+    for (int i = 1; i < used; ++i) pthread_create(&th[i], NULL, batch_thread, &jobs[i]);
+    if (used > 0) batch_thread(&jobs[0]);
+    for (int i = 1; i < used; ++i) pthread_join(th[i], NULL);
+    if (st)
+        for (int i = 0; i < used; ++i) { st->bytes += jobs[i].st.bytes; st->iters += jobs[i].st.iters; }
+    return now_s() - t0;
+}
+
+/* ------------------------------------------------------------------ */
+/* O1: flat CPU DDA, src/raycast.rs:21-133                             */
+/* ------------------------------------------------------------------ */
+static int o1_in_window(const Dims *d, const int32_t v[3], const int32_t o[3]) {
+    int32_t rx = v[0] - o[0], ry = v[1] - o[1], rz = v[2] - o[2];
+    return rx >= 0 && ry >= 0 && rz >= 0 && (uint32_t)rx < (uint32_t)d->vx &&
+           (uint32_t)ry < (uint32_t)d->vy && (uint32_t)rz < (uint32_t)d->vz;
+}
+
+static int o1_in_solid(const OrWorld *w, const Dims *d, const int32_t v[3], const int32_t o[3]) {
+    if (!o1_in_window(d, v, o)) return 0;
+    int32_t sx = pos_mod(v[0], d->vx);  /* rem_euclid */
+    int32_t sy = v[1];
+    int32_t sz = pos_mod(v[2], d->vz);
+    const OrBrick *b = &w->bricks[brick_idx(d, sx / 4, sy / 4, sz / 4)];
+    if (b->occupancy == 0) return 0;
+    int vi = child_bit(sx % 4, sy % 4, sz % 4);
+    if (!((b->occupancy >> vi) & 1ull)) return 0;
+    return b->materials[vi] != MAT_LEAF_FRINGE;
+}
+
+int or_raycast(const OrWorld *w, const float cam[3], const float dir_in[3],
+               const int32_t origin[3], OrPickHit *out, uint32_t *steps_out) {
+    Dims d = dims_of(w);
+    if (steps_out) *steps_out = 0;
+    /* glam 0.29.3 Vec3::normalize_or_zero: self * (1 / sqrt(dot(self, self))) */
+    float len = sqrtf((dir_in[0] * dir_in[0] + dir_in[1] * dir_in[1]) + dir_in[2] * dir_in[2]);
+    float rcp = 1.0f / len;
+    if (!(isfinite(rcp) && rcp > 0.0f)) return 0;
+    float dir[3] = {dir_in[0] * rcp, dir_in[1] * rcp, dir_in[2] * rcp};
+    if (dir[0] == 0.0f && dir[1] == 0.0f && dir[2] == 0.0f) return 0;
+    float dims[3] = {(float)d.vx, (float)d.vy, (float)d.vz};
+    float wmin[3], wmax[3], inv[3], tmin[3], tmax[3];
+    for (int k = 0; k < 3; ++k) {
+        wmin[k] = (float)origin[k];
+        wmax[k] = wmin[k] + dims[k];
+        inv[k] = safe_inv(dir[k]);
+        float t0 = (wmin[k] - cam[k]) * inv[k];
+        float t1 = (wmax[k] - cam[k]) * inv[k];
+        tmin[k] = vmin(t0, t1);
+        tmax[k] = vmax(t0, t1);
+    }
+    /* max_element / min_element: x.max(y.max(z)) */
+    float t_enter = vmax(vmax(tmin[0], vmax(tmin[1], tmin[2])), 0.0f);
+    float t_exit = vmin(tmax[0], vmin(tmax[1], tmax[2]));
+    if (t_enter >= t_exit || t_exit < 0.0f) return 0;
+    int32_t voxel[3], step[3];
+    float tdel[3], tm[3];
+    for (int k = 0; k < 3; ++k) {
+        float p = cam[k] + dir[k] * (t_enter + 1e-3f);
+        p = vmin(vmax(p, wmin[k] + 1e-3f), wmax[k] - 1e-3f); /* glam clamp */
+        voxel[k] = f2i(floorf(p));
+        step[k] = sgn(dir[k]);
+        tdel[k] = fabsf(inv[k]);
+    }
+    for (int k = 0; k < 3; ++k) {
+        float nxt = step[k] > 0 ? (float)(voxel[k] + 1) : (float)voxel[k];
+        tm[k] = (nxt - cam[k]) * inv[k];
+    }
+    int32_t last_axis = -1;
+    int32_t steps_left = 4096;
+#define ARGMIN_STEP(axv)                                                        \
+    do {                                                                        \
+        int32_t a_ = -1;                                                        \
+        float m_ = INFINITY;                                                    \
+        for (int k = 0; k < 3; ++k)                                             \
+            if (step[k] != 0 && tm[k] < m_) { a_ = k; m_ = tm[k]; }             \
+        if (a_ >= 0) { voxel[a_] += step[a_]; tm[a_] += tdel[a_]; }             \
+        (axv) = a_;                                                             \
+    } while (0)
+    while (steps_left > 0 && o1_in_solid(w, &d, voxel, origin)) {
+        int32_t ax;
+        ARGMIN_STEP(ax);
+        if (ax < 0) goto miss;
+        last_axis = ax;
+        steps_left--;
+        if (!o1_in_window(&d, voxel, origin)) goto miss;
+    }
+    while (steps_left > 0) {
+        if (!o1_in_window(&d, voxel, origin)) goto miss;
+        if (o1_in_solid(w, &d, voxel, origin)) {
+            out->voxel[0] = voxel[0]; out->voxel[1] = voxel[1]; out->voxel[2] = voxel[2];
+            out->normal[0] = out->normal[1] = out->normal[2] = 0;
+            if (last_axis >= 0) out->normal[last_axis] = -step[last_axis];
+            if (steps_out) *steps_out = (uint32_t)(4096 - steps_left);
+            return 1;
+        }
+        int32_t ax;
+        ARGMIN_STEP(ax);
+        if (ax < 0) goto miss;
+        last_axis = ax;
+        steps_left--;
+    }
+#undef ARGMIN_STEP
+miss:
+    if (steps_out) *steps_out = (uint32_t)(4096 - steps_left);
+    return 0;
+}
+
+typedef struct {
+    const OrWorld *w;
+    const int32_t *origin;
+    const float *cams, *dirs;
+    size_t a, b;
+    OrPickHit *out;
+    int32_t *hit;
+} PickJob;
+
+static void *pick_thread(void *arg) {
+    PickJob *j = (PickJob *)arg;
+    for (size_t i = j->a; i < j->b; ++i) {
+        memset(&j->out[i], 0, sizeof(OrPickHit));
+        j->hit[i] = or_raycast(j->w, &j->cams[3 * i], &j->dirs[3 * i], j->origin, &j->out[i], NULL);
+    }
+    return NULL;
+}
+
+double or_raycast_batch(const OrWorld *w, const int32_t origin[3], const float *cams,
+                        const float *dirs, size_t n, OrPickHit *out, int32_t *hit, int nthreads) {
+    double t0 = now_s();
+    if (nthreads < 1) nthreads = 1;
+    if (nthreads > 256) nthreads = 256;
+    pthread_t th[256];
+    PickJob jobs[256];
+    int used = 0;
+    for (int i = 0; i < nthreads; ++i) {
+        size_t a = n * (size_t)i / (size_t)nthreads, b = n * (size_t)(i + 1) / (size_t)nthreads;
+        if (b <= a) continue;
+        PickJob *j = &jobs[used++];
+        j->w = w; j->origin = origin; j->cams = cams; j->dirs = dirs; j->a = a; j->b = b;
+        j->out = out; j->hit = hit;
+    }
+    for (int i = 1; i < used; ++i) pthread_create(&th[i], NULL, pick_thread, &jobs[i]);
+    if (used > 0) pick_thread(&jobs[0]);
+    for (int i = 1; i < used; ++i) pthread_join(th[i], NULL);
+    return now_s() - t0;
+}

@@ -1,0 +1,371 @@
+"""GPU parity: every CUDA entry point against the CPU oracle, bit-exact
+(hit voxel, face, material, flags, t and step count; integer and float
+fields compared as raw bytes), through the C ABI of libvoxrt."""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import pyoracle as po
+
+pytestmark = pytest.mark.gpu
+
+f32 = np.float32
+METHOD = po.OR_F_L4 | po.OR_F_LUT | po.OR_F_LOD | po.OR_F_BEAM
+
+
+@pytest.fixture(scope="module")
+def vg():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.fail("CUDA GPU required for -m gpu tests")
+    import voxelg_b200
+    return voxelg_b200
+
+
+@pytest.fixture(scope="module")
+def dev_c1(vg):
+    cfg = vg.CONFIGS["c1"]
+    w = vg.DeviceWorld(*cfg.bricks)
+    w.generate(cfg.terrain)
+    yield w
+    w.close()
+
+
+def upload_oracle(vg, ow):
+    w = vg.DeviceWorld(*ow.dims)
+    w.upload(ow.a)
+    return w
+
+
+def assert_same_records(got, want, what=""):
+    got = np.ascontiguousarray(got).view(po.RECORD)
+    want = np.ascontiguousarray(want).view(po.RECORD)
+    assert got.shape == want.shape
+    bad = np.flatnonzero((got.view(np.uint8).reshape(-1, 24) !=
+                          want.view(np.uint8).reshape(-1, 24)).any(axis=1))
+    assert bad.size == 0, f"{what}: {bad.size} records differ, first {bad[:5]}: " \
+                          f"got {got[bad[:3]]} want {want[bad[:3]]}"
+
+
+def frame_pair(vg, dw, ow, cam, flags):
+    p = vg.default_params(flags)
+    rec, sh = vg.render_primary(dw, cam, p)
+    import torch
+    torch.cuda.synchronize()
+    want = po.render_frame(ow, cam, p)
+    return vg.records(rec), (vg.shadows(sh) if sh is not None else None), want
+
+
+def test_device_worldgen_matches_oracle(vg, dev_c1, c1_oracle_world):
+    got = dev_c1.download()
+    for k in po.World.NAMES:
+        assert np.array_equal(got[k].view(np.uint8), c1_oracle_world.a[k].view(np.uint8)), k
+
+
+def test_upload_download_roundtrip(vg):
+    from scenes import stone_blocks
+    ow = stone_blocks()
+    w = upload_oracle(vg, ow)
+    got = w.download()
+    for k in po.World.NAMES:
+        assert np.array_equal(got[k].view(np.uint8), ow.a[k].view(np.uint8)), k
+    w.close()
+
+
+@pytest.mark.parametrize("flags", [po.OR_F_L4, 0, METHOD, METHOD | po.OR_F_SHADOW,
+                                   po.OR_F_L4 | po.OR_F_LUT | po.OR_F_SHADOW])
+def test_c1_frame_bit_exact(vg, dev_c1, c1_oracle_world, flags):
+    cfg = vg.CONFIGS["c1"]
+    cam = vg.default_camera(dev_c1, cfg.width, cfg.height)
+    rec, sh, (wrec, wsh, _, _, _) = frame_pair(vg, dev_c1, c1_oracle_world, cam, flags)
+    assert_same_records(rec, wrec, f"c1 flags={flags}")
+    assert (rec["flags"] & 1).mean() > 0.3
+    if flags & po.OR_F_SHADOW:
+        assert np.array_equal(sh.view(np.uint8), wsh.view(np.uint8))
+        assert sh["traced"].sum() == (rec["flags"] & 1).sum()
+
+
+def test_frame_stats_match_oracle(vg, dev_c1, c1_oracle_world):
+    cfg = vg.CONFIGS["c1"]
+    cam = vg.default_camera(dev_c1, 320, 180)
+    for flags in (po.OR_F_L4, METHOD | po.OR_F_SHADOW):
+        p = vg.default_params(flags)
+        s = vg.render_stats(dev_c1, cam, p)
+        st = po.render_frame(c1_oracle_world, cam, p)[4]
+        b = s["beam"][0] + s["primary"][0]
+        i = s["beam"][1] + s["primary"][1]
+        assert (b, i) == (st.bytes, st.iters), flags
+        if flags & po.OR_F_BEAM:
+            bst = po.beam_pass(c1_oracle_world, cam)[1]
+            assert s["beam"] == (bst.bytes, bst.iters)
+
+
+@pytest.mark.parametrize("res", [(1, 1), (17, 13), (64, 36), (333, 7)])
+def test_odd_resolutions_and_jitter(vg, dev_c1, c1_oracle_world, res):
+    cam = vg.default_camera(dev_c1, *res)
+    cam.jitter_x, cam.jitter_y = 0.37, -0.21
+    rec, sh, (wrec, wsh, _, _, _) = frame_pair(vg, dev_c1, c1_oracle_world, cam,
+                                               METHOD | po.OR_F_SHADOW)
+    assert_same_records(rec, wrec, f"res {res}")
+    assert np.array_equal(sh.view(np.uint8), wsh.view(np.uint8))
+
+
+@pytest.mark.parametrize("pose", [
+    ((256.0, 300.0, 256.0), 0.0, -1.5, "above the window looking down"),
+    ((-40.0, 120.0, -30.0), 0.8, -0.2, "outside the window"),
+    ((256.0, 70.0, 256.0), 1.3, 0.1, "inside terrain"),
+    ((600.0, 140.0, 100.0), -2.0, -0.3, "outside, facing in"),
+])
+def test_camera_poses(vg, dev_c1, c1_oracle_world, pose):
+    pos, yaw, pitch, _ = pose
+    cam = vg.camera_from_pose(pos, yaw, pitch, math.radians(70), 96, 64)
+    for flags in (po.OR_F_L4, METHOD | po.OR_F_SHADOW):
+        rec, sh, (wrec, wsh, _, _, _) = frame_pair(vg, dev_c1, c1_oracle_world, cam, flags)
+        assert_same_records(rec, wrec, str(pose))
+
+
+def test_shifted_window_origin(vg):
+    """Toroidal storage: a window origin away from 0 folds world voxels into
+    slots (raymarch.wgsl:17-23)."""
+    from scenes import floor_pillars
+    ow, wo, _ = floor_pillars((3, 5))
+    dw = upload_oracle(vg, ow)
+    cam = vg.camera_from_pose((wo[0] + 6.0, 96.0, wo[2] + 6.0), 0.78, -0.5, math.radians(70),
+                              128, 72, world_origin=wo)
+    for flags in (po.OR_F_L4, METHOD | po.OR_F_SHADOW):
+        rec, sh, (wrec, wsh, _, _, _) = frame_pair(vg, dw, ow, cam, flags)
+        assert_same_records(rec, wrec, "shifted origin")
+        assert (rec["flags"] & 1).any()
+    dw.close()
+
+
+def random_rays(rng, n, vox, kinds=(0, 1, 2)):
+    rays = np.zeros(n, po.RAY)
+    lo = np.array([-40, -20, -40], np.float32)
+    hi = np.array(vox, np.float32) + np.array([40, 60, 40], np.float32)
+    rays["org"] = rng.uniform(lo, hi, size=(n, 3)).astype(np.float32)
+    d = rng.normal(size=(n, 3)).astype(np.float32)
+    # a share of axis-aligned and zero-component directions
+    m = rng.random(n) < 0.1
+    d[m, rng.integers(0, 3, m.sum())] = 0.0
+    m2 = rng.random(n) < 0.05
+    d[m2] = np.array([0.0, -1.0, 0.0], np.float32)
+    d /= np.sqrt((d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1]) + d[:, 2] * d[:, 2])[:, None]
+    rays["dir"] = d
+    rays["tmax"] = rng.choice(np.array([8.0, 64.0, 256.0, 480.0, 700.0], np.float32), n)
+    rays["kind"] = rng.choice(np.array(kinds, np.uint32), n)
+    return rays
+
+
+def test_trace_kinds_bit_exact(vg, dev_c1, c1_oracle_world):
+    from scenes import stone_blocks
+    rng = np.random.default_rng(3)
+    for ow, dw in ((c1_oracle_world, dev_c1), (stone_blocks(), None)):
+        dw_ = dw or upload_oracle(vg, ow)
+        rays = random_rays(rng, 20000, ow.voxels)
+        for flags in (po.OR_F_L4, METHOD):
+            p = vg.default_params(flags)
+            got = vg.records(vg.trace(dw_, rays, p))
+            want = po.trace_batch(ow, rays, p)[0]
+            assert_same_records(got, want, f"kinds flags={flags}")
+        if dw is None:
+            dw_.close()
+
+
+def test_raycast_matches_o1(vg, dev_c1, c1_oracle_world):
+    rng = np.random.default_rng(5)
+    n = 20000
+    vox = c1_oracle_world.voxels
+    cams = rng.uniform([-20, 40, -20], [vox[0] + 20, 200, vox[2] + 20], size=(n, 3)).astype(np.float32)
+    dirs = rng.normal(size=(n, 3)).astype(np.float32)
+    dirs[::17] = 0.0                      # zero direction -> None
+    dirs[1::23] *= np.float32(1e-20)      # denormal-ish length
+    got, hit = vg.raycast_batch(dev_c1, cams, dirs)
+    want, whit, _ = po.raycast_batch(c1_oracle_world, cams, dirs)
+    assert np.array_equal(hit, whit)
+    assert np.array_equal(got.view(np.uint8), want.view(np.uint8))
+    assert 0.2 < hit.mean() < 0.95
+    # the single-call drop-in
+    for i in range(0, 60, 3):
+        h = vg.raycast(cams[i], dirs[i], dev_c1)
+        assert (h is not None) == bool(whit[i])
+        if h is not None:
+            assert h.voxel == tuple(want[i]["voxel"]) and h.normal == tuple(want[i]["normal"])
+
+
+def test_raycast_bench_case(vg, dev_c1, c1_oracle_world):
+    """benches/trace.rs:24-40: origin (256, 90, 256), dir normalize(sin a,
+    -0.5, cos a), a += 0.013."""
+    n = 4096
+    a = (np.arange(1, n + 1, dtype=np.float32) * np.float32(0.013)).astype(np.float32)
+    dirs = np.stack([np.sin(a), np.full(n, -0.5, np.float32), np.cos(a)], 1).astype(np.float32)
+    cams = np.tile(np.array([256.0, 90.0, 256.0], np.float32), (n, 1))
+    got, hit = vg.raycast_batch(dev_c1, cams, dirs)
+    want, whit, _ = po.raycast_batch(c1_oracle_world, cams, dirs)
+    assert np.array_equal(hit, whit) and np.array_equal(got.view(np.uint8), want.view(np.uint8))
+
+
+def test_reference_patterns_on_gpu(vg):
+    """accel.rs:529-942 patterns through the GPU entry points."""
+    from scenes import (face_normal, flat_floor, floor_pillars, lattice_touch, normalize,
+                        ray_box_entry, shadow_scene)
+    # flat floor
+    ow = flat_floor(16, 16, 48)
+    dw = upload_oracle(vg, ow)
+    d = normalize((0.03, -1.0, 0.017))
+    rays = np.zeros(36, po.RAY)
+    for i in range(36):
+        rays[i]["org"] = (22.0 + (i % 6) * 6.0, 120.0, 22.0 + (i // 6) * 6.0)
+        rays[i]["dir"] = d
+        rays[i]["tmax"] = 700.0
+    rec = vg.records(vg.trace(dw, rays, vg.default_params(METHOD)))
+    assert (rec["voxel"][:, 1] == 60).all() and (rec["flags"] & 1).all()
+    hy = rays["org"][:, 1] + rec["t"] * d[1]
+    assert np.abs(hy - 61.0).max() < 0.05
+    dw.close()
+    # floor + pillars, shifted origin: GPU trace vs GPU raycast on clean hits
+    ow, wo, fan = floor_pillars((3, 5))
+    dw = upload_oracle(vg, ow)
+    rays = np.zeros(len(fan), po.RAY)
+    for i, (e, dd) in enumerate(fan):
+        rays[i]["org"], rays[i]["dir"], rays[i]["tmax"] = e, dd, 700.0
+    rec = vg.records(vg.trace(dw, rays, vg.default_params(METHOD), origin=wo))
+    picks, hits = vg.raycast_batch(dw, rays["org"], rays["dir"], origin=wo)
+    clean = 0
+    for i, (e, dd) in enumerate(fan):
+        if hits[i] and (rec[i]["flags"] & 1) and tuple(rec[i]["voxel"]) == tuple(picks[i]["voxel"]):
+            if lattice_touch(e + f32(ray_box_entry(e, dd, picks[i]["voxel"])) * dd) < 2:
+                clean += 1
+                assert face_normal(rec[i]["face"]) == tuple(picks[i]["normal"])
+    assert clean > len(fan) / 3
+    dw.close()
+    # shadow occlusion
+    ow, sun, samples = shadow_scene()
+    dw = upload_oracle(vg, ow)
+    rays = np.zeros(len(samples), po.RAY)
+    rays["org"] = np.array([s[0] for s in samples])
+    rays["dir"] = sun
+    rays["tmax"] = 480.0
+    rays["kind"] = 1
+    occ = vg.records(vg.trace(dw, rays, vg.default_params(METHOD)))["flags"] & 1
+    _, cpu = vg.raycast_batch(dw, rays["org"], np.tile(sun, (len(samples), 1)))
+    dec = np.array([u or o for _, u, o in samples])
+    assert np.array_equal(occ[dec] == 1, cpu[dec] == 1)
+    under = np.array([u for _, u, _ in samples])
+    assert occ[under].sum() > 20 and (occ[~under & dec] == 0).sum() > 20
+    dw.close()
+    # empty world
+    dw = vg.DeviceWorld(128, 64, 128)
+    cam = vg.camera_from_pose((256.0, 200.0, 256.0), 0.0, -0.7, 1.2, 64, 64)
+    rec, sh = vg.render_primary(dw, cam, vg.default_params())
+    r = vg.records(rec)
+    assert not (r["flags"] & 1).any() and (r["face"] == 0xFF).all()
+    dw.close()
+
+
+def test_apply_dirty_matches_oracle(vg, c1_oracle_world):
+    """Incremental device update from dirty bricks (renderer.rs:1345-1394)
+    leaves the same pyramid as the host's set_voxel maintenance, and frames
+    traced after it match the oracle."""
+    src = c1_oracle_world
+    hw = vg.HostWorld(*src.dims)
+    for k in po.World.NAMES:
+        hw.arrays[k][...] = src.a[k].view(hw.arrays[k].dtype)
+    hw.rebuild()
+    dw = vg.DeviceWorld(*src.dims)
+    dw.sync(hw)                 # all-dirty: full upload
+    assert hw.dirty_count() == 0
+    ow = po.World(*src.dims, arrays={k: v.copy() for k, v in src.a.items()})
+    rng = np.random.default_rng(9)
+    vx, vy, vz = ow.voxels
+    cam = vg.default_camera(dw, 160, 90)
+    for rnd in range(3):
+        for _ in range(5000):
+            x, y, z = int(rng.integers(vx)), int(rng.integers(vy)), int(rng.integers(vz))
+            m = int(rng.choice([0, 0, 2, 4, 12]))
+            hw.set_voxel(x, y, z, m)
+            ow.set_voxel(x, y, z, m)
+        # empty a column stack so tiles, chunks and an L4 bit flip
+        for x in range(rnd * 64, rnd * 64 + 64):
+            for z in range(0, 64):
+                for y in range(0, 256, 1):
+                    hw.set_voxel(x, y, z, 0)
+                    ow.set_voxel(x, y, z, 0)
+        assert hw.dirty_count() > 0
+        dw.sync(hw)
+        got = dw.download()
+        for k in po.World.NAMES:
+            assert np.array_equal(got[k].view(np.uint8), ow.a[k].view(np.uint8)), (rnd, k)
+        rec, sh, (wrec, wsh, _, _, _) = frame_pair(vg, dw, ow, cam, METHOD | po.OR_F_SHADOW)
+        assert_same_records(rec, wrec, f"after edits round {rnd}")
+    dw.close()
+    hw.close()
+
+
+def test_apply_dirty_duplicates_last_wins(vg):
+    dw = vg.DeviceWorld(64, 16, 64)
+    idx = np.array([5, 9, 5], np.uint32)
+    b = np.zeros(3, po.BRICK)
+    b[0]["occupancy"] = 1
+    b[0]["materials"][0] = 4
+    b[1]["occupancy"] = np.uint64(0xFFFFFFFFFFFFFFFF)
+    b[1]["materials"][:] = 3
+    b[2]["occupancy"] = 2
+    b[2]["materials"][1] = 2
+    dw.apply_dirty(idx, b)
+    got = dw.download()
+    assert got["bricks"][5]["occupancy"] == 2 and got["bricks"][5]["materials"][1] == 2
+    assert got["brick_uniform"][9] == 3 and got["brick_uniform"][5] == 0
+    assert got["tile_mask"][1] != 0 and got["tile_mask"][2] != 0
+    assert got["chunk_mask"][0] != 0 and got["l4_mask"][0] != 0
+    dw.close()
+
+
+def test_render_host_equals_device(vg, dev_c1):
+    cam = vg.default_camera(dev_c1, 320, 180)
+    p = vg.default_params()
+    rec, sh = vg.render_primary(dev_c1, cam, p)
+    hrec, hsh = vg.render_primary_host(dev_c1, cam, p)
+    assert np.array_equal(vg.records(rec).view(np.uint8), hrec.view(np.uint8))
+    assert np.array_equal(vg.shadows(sh).view(np.uint8), hsh.view(np.uint8))
+
+
+def test_c2_full_frame_bit_exact(vg):
+    """The full benchmark workload: 2048x256x2048 world, 1920x1080 primary
+    rays with beam/LUT/LOD, one shadow ray per hit."""
+    import torch
+    cfg = vg.CONFIGS["c2"]
+    dw = vg.DeviceWorld(*cfg.bricks)
+    dw.generate(cfg.terrain)
+    ow = po.World(*cfg.bricks)
+    ow.generate(cfg.terrain)
+    got = dw.download()
+    for k in po.World.NAMES:
+        assert np.array_equal(got[k].view(np.uint8), ow.a[k].view(np.uint8)), k
+    del got
+    cam = vg.default_camera(dw, cfg.width, cfg.height)
+    p = vg.default_params(cfg.flags)
+    rec, sh = vg.render_primary(dw, cam, p)
+    torch.cuda.synchronize()
+    wrec, wsh, _, _, _ = po.render_frame(ow, cam, p)
+    assert_same_records(vg.records(rec), wrec, "c2")
+    assert np.array_equal(vg.shadows(sh).view(np.uint8), wsh.view(np.uint8))
+    r = vg.records(rec)
+    assert (r["flags"] & 2).any(), "LOD / uniform early-outs never fired"
+    dw.close()
+
+
+def test_invalid_calls_fail_loudly(vg, dev_c1):
+    from voxelg_b200 import _lib as L
+    import ctypes as C
+    lib = L.load()
+    cam = vg.default_camera(dev_c1, 16, 16)
+    cam.res_x = 0.0
+    p = vg.default_params()
+    rc = lib.vx_render_primary(dev_c1.handle, C.byref(cam), C.byref(p), C.c_void_p(8),
+                               C.c_void_p(0), C.c_void_p(0))
+    assert rc == L.VX_ERR_INVALID
+    idx = np.array([10 ** 9], np.uint32)
+    with pytest.raises(L.VxError):
+        dev_c1.apply_dirty(idx, np.zeros(1, po.BRICK))

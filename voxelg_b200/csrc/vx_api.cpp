@@ -1,0 +1,589 @@
+// vx_api.cpp -- the C ABI of libvoxrt (include/voxrt.h): device world
+// lifetime, uploads, the traversal entry points and error reporting.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+#include <unordered_map>
+#include <vector>
+
+#include "vx_internal.h"
+
+namespace vx {
+namespace {
+thread_local std::string g_last_error;
+}
+void set_error(const std::string &msg) { g_last_error = msg; }
+}  // namespace vx
+
+struct VxWorld {
+    int device = 0;
+    vx::DevWorld dw{};
+    cudaStream_t stream = nullptr;   // library stream for synchronous calls
+    std::mutex mu;                   // guards the scratch buffers below
+    float *beam = nullptr;
+    size_t beam_cap = 0;
+    uint32_t *d_idx = nullptr;
+    size_t idx_cap = 0;
+    VxBrick *d_bricks = nullptr;
+    size_t bricks_cap = 0;
+    unsigned long long *d_stats = nullptr;
+    VxHitRecord *rec = nullptr;
+    size_t rec_cap = 0;
+    VxShadowRecord *sh = nullptr;
+    size_t sh_cap = 0;
+    float *pick_in = nullptr;        // 6 floats
+    VxPickHit *pick_out = nullptr;
+    int32_t *pick_hit = nullptr;
+    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+};
+
+namespace {
+
+#define VX_CK(call)                                                                   \
+    do {                                                                              \
+        cudaError_t e_ = (call);                                                      \
+        if (e_ != cudaSuccess) {                                                      \
+            vx::set_error(std::string(__func__) + ": " #call " failed: " +           \
+                          cudaGetErrorString(e_));                                    \
+            return e_ == cudaErrorMemoryAllocation ? VX_ERR_OOM : VX_ERR_CUDA;        \
+        }                                                                             \
+    } while (0)
+
+inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+
+int use_device(VxWorld *w) {
+    VX_CK(cudaSetDevice(w->device));
+    return VX_OK;
+}
+
+template <typename T>
+int ensure(T **p, size_t *cap, size_t n) {
+    if (*cap >= n && *p) return VX_OK;
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+    *cap = 0;
+    VX_CK(cudaMalloc(reinterpret_cast<void **>(p), std::max<size_t>(n, 1) * sizeof(T)));
+    *cap = n;
+    return VX_OK;
+}
+
+void free_world(VxWorld *w) {
+    cudaFree(w->dw.occ);
+    cudaFree(w->dw.mat);
+    cudaFree(w->dw.tile_mask);
+    cudaFree(w->dw.chunk_mask);
+    cudaFree(w->dw.l4_mask);
+    cudaFree(w->dw.brick_uniform);
+    cudaFree(w->dw.tile_uniform);
+    cudaFree(w->beam);
+    cudaFree(w->d_idx);
+    cudaFree(w->d_bricks);
+    cudaFree(w->d_stats);
+    cudaFree(w->rec);
+    cudaFree(w->sh);
+    cudaFree(w->pick_in);
+    cudaFree(w->pick_out);
+    cudaFree(w->pick_hit);
+    for (auto &e : w->ev)
+        if (e) cudaEventDestroy(e);
+    if (w->stream) cudaStreamDestroy(w->stream);
+}
+
+int check_frame(const VxCamera *cam) {
+    if (!cam || !(cam->res_x >= 1.0f) || !(cam->res_y >= 1.0f) || cam->res_x > 32768.0f ||
+        cam->res_y > 32768.0f || cam->res_x != std::floor(cam->res_x) ||
+        cam->res_y != std::floor(cam->res_y)) {
+        vx::set_error("camera resolution must be an integer in [1, 32768]");
+        return VX_ERR_INVALID;
+    }
+    return VX_OK;
+}
+
+vx::FrameArgs make_frame(VxWorld *w, const VxCamera *cam, const VxTraceParams *p) {
+    vx::FrameArgs fa{};
+    fa.ta.w = w->dw;
+    fa.ta.p = *p;
+    fa.ta.ro[0] = cam->world_origin[0];
+    fa.ta.ro[1] = cam->world_origin[1];
+    fa.ta.ro[2] = cam->world_origin[2];
+    fa.cam = *cam;
+    fa.W = (uint32_t)cam->res_x;
+    fa.H = (uint32_t)cam->res_y;
+    fa.bw = (fa.W + 7u) / 8u;
+    fa.bh = (fa.H + 7u) / 8u;
+    return fa;
+}
+
+// beam + primary on one stream; caller holds w->mu
+int run_frame(VxWorld *w, vx::FrameArgs &fa, cudaStream_t s) {
+    if (fa.ta.p.flags & VX_F_BEAM) {
+        int rc = ensure(&w->beam, &w->beam_cap, (size_t)fa.bw * fa.bh);
+        if (rc != VX_OK) return rc;
+        fa.beam = w->beam;
+        VX_CK(vx::launch_beam(fa, w->beam, s));
+    }
+    VX_CK(vx::launch_primary(fa, s));
+    return VX_OK;
+}
+
+int check_params(const VxTraceParams *p) {
+    if (!p || p->max_iters < 0 || p->any_max_iters < 0 || p->max_iters > (1 << 20) ||
+        p->any_max_iters > (1 << 20)) {
+        vx::set_error("invalid VxTraceParams (null or iteration caps outside [0, 2^20])");
+        return VX_ERR_INVALID;
+    }
+    return VX_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int vx_abi_version(void) { return VX_ABI_VERSION; }
+
+const char *vx_last_error(void) { return vx::g_last_error.c_str(); }
+
+int vx_default_params(VxTraceParams *p) {
+    if (!p) return VX_ERR_INVALID;
+    std::memset(p, 0, sizeof(*p));
+    p->max_dist = 700.0f;
+    p->lod_brick_t = 400.0f;
+    p->tile_lod_t = 520.0f;
+    p->shadow_max_dist = 480.0f;
+    p->beam_margin = 16.0f;
+    p->max_iters = 1024;
+    p->any_max_iters = 768;
+    p->flags = VX_F_L4 | VX_F_LUT | VX_F_LOD | VX_F_BEAM | VX_F_SHADOW;
+    // sun = normalize(0.3, 0.8, 0.5); tangent frame as raymarch.wgsl:3984-3988
+    const float s0 = 0.3f, s1 = 0.8f, s2 = 0.5f;
+    const float sl = std::sqrt((s0 * s0 + s1 * s1) + s2 * s2);
+    p->sun[0] = s0 / sl;
+    p->sun[1] = s1 / sl;
+    p->sun[2] = s2 / sl;
+    // cross(s, (0,1,0)) = (-s.z, 0, s.x)
+    float t0 = -p->sun[2], t1 = 0.0f, t2 = p->sun[0];
+    const float tl = std::sqrt((t0 * t0 + t1 * t1) + t2 * t2);
+    if (tl < 0.01f) {
+        t0 = 1.0f; t1 = 0.0f; t2 = 0.0f;
+    } else {
+        t0 = t0 / tl; t1 = t1 / tl; t2 = t2 / tl;
+    }
+    p->sun_tangent[0] = t0;
+    p->sun_tangent[1] = t1;
+    p->sun_tangent[2] = t2;
+    p->sun_bitangent[0] = p->sun[1] * t2 - p->sun[2] * t1;
+    p->sun_bitangent[1] = p->sun[2] * t0 - p->sun[0] * t2;
+    p->sun_bitangent[2] = p->sun[0] * t1 - p->sun[1] * t0;
+    p->cone_tan = 0.0087268678f;  // tan(0.5 degrees)
+    p->frame = 0.0f;
+    return VX_OK;
+}
+
+int vx_camera_from_pose(const float pos[3], float yaw, float pitch, float fov_y, uint32_t width,
+                        uint32_t height, const int32_t world_origin[3], VxCamera *out) {
+    if (!pos || !out || width == 0 || height == 0) return VX_ERR_INVALID;
+    std::memset(out, 0, sizeof(*out));
+    // camera.rs:25-42 with glam's normalize = v * (1 / length)
+    auto norm = [](float v[3]) {
+        const float r = 1.0f / std::sqrt((v[0] * v[0] + v[1] * v[1]) + v[2] * v[2]);
+        v[0] = v[0] * r; v[1] = v[1] * r; v[2] = v[2] * r;
+    };
+    float f[3] = {std::sin(yaw) * std::cos(pitch), std::sin(pitch), std::cos(yaw) * std::cos(pitch)};
+    norm(f);
+    float r[3] = {f[2], 0.0f, -f[0]};
+    norm(r);
+    float u[3] = {f[1] * r[2] - r[1] * f[2], f[2] * r[0] - r[2] * f[0], f[0] * r[1] - r[0] * f[1]};
+    norm(u);
+    for (int k = 0; k < 3; ++k) {
+        out->origin[k] = pos[k];
+        out->forward[k] = f[k];
+        out->right[k] = r[k];
+        out->up[k] = u[k];
+        out->world_origin[k] = world_origin ? world_origin[k] : 0;
+    }
+    out->tan_half_fov = std::tan(fov_y * 0.5f);
+    out->res_x = (float)width;
+    out->res_y = (float)height;
+    return VX_OK;
+}
+
+int vx_world_create(const VxWorldDesc *desc, VxWorld **out) {
+    if (!desc || !out) {
+        vx::set_error("vx_world_create: null argument");
+        return VX_ERR_INVALID;
+    }
+    const int32_t bx = desc->bricks_x, by = desc->bricks_y, bz = desc->bricks_z;
+    if (bx <= 0 || by <= 0 || bz <= 0 || bx % 64 || bz % 64 || by % 16 || bx > 65536 ||
+        bz > 65536 || by > 65536) {
+        vx::set_error("vx_world_create: bricks_x/z must be multiples of 64, bricks_y a "
+                      "multiple of 16");
+        return VX_ERR_INVALID;
+    }
+    VxWorld *w = new (std::nothrow) VxWorld();
+    if (!w) return VX_ERR_OOM;
+    w->device = desc->device;
+    w->dw.d = vx::make_dims(bx, by, bz);
+    const vx::Dims &d = w->dw.d;
+    auto fail = [&](int rc) {
+        free_world(w);
+        delete w;
+        return rc;
+    };
+    int rc = use_device(w);
+    if (rc != VX_OK) return fail(rc);
+#define VX_CKW(call)                                                                    \
+    do {                                                                                \
+        cudaError_t e_ = (call);                                                        \
+        if (e_ != cudaSuccess) {                                                        \
+            vx::set_error(std::string("vx_world_create: ") + cudaGetErrorString(e_));   \
+            return fail(e_ == cudaErrorMemoryAllocation ? VX_ERR_OOM : VX_ERR_CUDA);    \
+        }                                                                               \
+    } while (0)
+    VX_CKW(cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking));
+    VX_CKW(cudaMalloc(&w->dw.occ, d.n_bricks * sizeof(uint64_t)));
+    VX_CKW(cudaMalloc(&w->dw.mat, d.n_bricks * 64));
+    VX_CKW(cudaMalloc(&w->dw.tile_mask, d.n_tiles * sizeof(uint64_t)));
+    VX_CKW(cudaMalloc(&w->dw.chunk_mask, d.n_chunks * sizeof(uint64_t)));
+    VX_CKW(cudaMalloc(&w->dw.l4_mask, d.n_l4 * sizeof(uint64_t)));
+    VX_CKW(cudaMalloc(&w->dw.brick_uniform, d.n_bricks));
+    VX_CKW(cudaMalloc(&w->dw.tile_uniform, d.n_tiles));
+    VX_CKW(cudaMalloc(&w->d_stats, 4 * sizeof(unsigned long long)));
+    VX_CKW(cudaMalloc(&w->pick_in, 8 * sizeof(float)));
+    VX_CKW(cudaMalloc(&w->pick_out, sizeof(VxPickHit)));
+    VX_CKW(cudaMalloc(&w->pick_hit, sizeof(int32_t)));
+    VX_CKW(cudaMemsetAsync(w->dw.occ, 0, d.n_bricks * sizeof(uint64_t), w->stream));
+    VX_CKW(cudaMemsetAsync(w->dw.mat, 0, d.n_bricks * 64, w->stream));
+    VX_CKW(cudaMemsetAsync(w->dw.tile_mask, 0, d.n_tiles * sizeof(uint64_t), w->stream));
+    VX_CKW(cudaMemsetAsync(w->dw.chunk_mask, 0, d.n_chunks * sizeof(uint64_t), w->stream));
+    VX_CKW(cudaMemsetAsync(w->dw.l4_mask, 0, d.n_l4 * sizeof(uint64_t), w->stream));
+    VX_CKW(cudaMemsetAsync(w->dw.brick_uniform, 0, d.n_bricks, w->stream));
+    VX_CKW(cudaMemsetAsync(w->dw.tile_uniform, 0, d.n_tiles, w->stream));
+    VX_CKW(cudaStreamSynchronize(w->stream));
+#undef VX_CKW
+    *out = w;
+    return VX_OK;
+}
+
+int vx_world_destroy(VxWorld *w) {
+    if (!w) return VX_OK;
+    cudaSetDevice(w->device);
+    if (w->stream) cudaStreamSynchronize(w->stream);
+    free_world(w);
+    delete w;
+    return VX_OK;
+}
+
+int vx_world_counts(const VxWorld *w, uint64_t counts[4]) {
+    if (!w || !counts) return VX_ERR_INVALID;
+    counts[0] = (uint64_t)w->dw.d.n_bricks;
+    counts[1] = (uint64_t)w->dw.d.n_tiles;
+    counts[2] = (uint64_t)w->dw.d.n_chunks;
+    counts[3] = (uint64_t)w->dw.d.n_l4;
+    return VX_OK;
+}
+
+int vx_world_upload(VxWorld *w, const VxBrick *bricks, const uint64_t *tile_mask,
+                    const uint64_t *chunk_mask, const uint64_t *l4_mask,
+                    const uint8_t *brick_uniform, const uint8_t *tile_uniform) {
+    if (!w || !bricks || !tile_mask || !chunk_mask || !l4_mask || !brick_uniform || !tile_uniform) {
+        vx::set_error("vx_world_upload: null argument");
+        return VX_ERR_INVALID;
+    }
+    int rc = use_device(w);
+    if (rc != VX_OK) return rc;
+    std::lock_guard<std::mutex> lk(w->mu);
+    const vx::Dims &d = w->dw.d;
+    const size_t chunk = (size_t)1 << 20;  // bricks per staging round (72 MiB)
+    rc = ensure(&w->d_bricks, &w->bricks_cap, std::min<size_t>(chunk, (size_t)d.n_bricks));
+    if (rc != VX_OK) return rc;
+    for (int64_t first = 0; first < d.n_bricks; first += (int64_t)chunk) {
+        const int64_t cnt = std::min<int64_t>((int64_t)chunk, d.n_bricks - first);
+        VX_CK(cudaMemcpyAsync(w->d_bricks, bricks + first, (size_t)cnt * sizeof(VxBrick),
+                              cudaMemcpyHostToDevice, w->stream));
+        VX_CK(vx::launch_bricks_from_aos(w->dw, w->d_bricks, first, cnt, w->stream));
+    }
+    VX_CK(cudaMemcpyAsync(w->dw.tile_mask, tile_mask, d.n_tiles * 8, cudaMemcpyHostToDevice, w->stream));
+    VX_CK(cudaMemcpyAsync(w->dw.chunk_mask, chunk_mask, d.n_chunks * 8, cudaMemcpyHostToDevice, w->stream));
+    VX_CK(cudaMemcpyAsync(w->dw.l4_mask, l4_mask, d.n_l4 * 8, cudaMemcpyHostToDevice, w->stream));
+    VX_CK(cudaMemcpyAsync(w->dw.brick_uniform, brick_uniform, d.n_bricks, cudaMemcpyHostToDevice, w->stream));
+    VX_CK(cudaMemcpyAsync(w->dw.tile_uniform, tile_uniform, d.n_tiles, cudaMemcpyHostToDevice, w->stream));
+    VX_CK(cudaStreamSynchronize(w->stream));
+    return VX_OK;
+}
+
+int vx_world_download(VxWorld *w, VxBrick *bricks, uint64_t *tile_mask, uint64_t *chunk_mask,
+                      uint64_t *l4_mask, uint8_t *brick_uniform, uint8_t *tile_uniform) {
+    if (!w) return VX_ERR_INVALID;
+    int rc = use_device(w);
+    if (rc != VX_OK) return rc;
+    std::lock_guard<std::mutex> lk(w->mu);
+    const vx::Dims &d = w->dw.d;
+    if (bricks) {
+        const size_t chunk = (size_t)1 << 20;
+        rc = ensure(&w->d_bricks, &w->bricks_cap, std::min<size_t>(chunk, (size_t)d.n_bricks));
+        if (rc != VX_OK) return rc;
+        const size_t step = std::min(chunk, w->bricks_cap);
+        for (int64_t first = 0; first < d.n_bricks; first += (int64_t)step) {
+            const int64_t cnt = std::min<int64_t>((int64_t)step, d.n_bricks - first);
+            VX_CK(vx::launch_bricks_to_aos(w->dw, w->d_bricks, first, cnt, w->stream));
+            VX_CK(cudaMemcpyAsync(bricks + first, w->d_bricks, (size_t)cnt * sizeof(VxBrick),
+                                  cudaMemcpyDeviceToHost, w->stream));
+            VX_CK(cudaStreamSynchronize(w->stream));
+        }
+    }
+    if (tile_mask) VX_CK(cudaMemcpyAsync(tile_mask, w->dw.tile_mask, d.n_tiles * 8, cudaMemcpyDeviceToHost, w->stream));
+    if (chunk_mask) VX_CK(cudaMemcpyAsync(chunk_mask, w->dw.chunk_mask, d.n_chunks * 8, cudaMemcpyDeviceToHost, w->stream));
+    if (l4_mask) VX_CK(cudaMemcpyAsync(l4_mask, w->dw.l4_mask, d.n_l4 * 8, cudaMemcpyDeviceToHost, w->stream));
+    if (brick_uniform) VX_CK(cudaMemcpyAsync(brick_uniform, w->dw.brick_uniform, d.n_bricks, cudaMemcpyDeviceToHost, w->stream));
+    if (tile_uniform) VX_CK(cudaMemcpyAsync(tile_uniform, w->dw.tile_uniform, d.n_tiles, cudaMemcpyDeviceToHost, w->stream));
+    VX_CK(cudaStreamSynchronize(w->stream));
+    return VX_OK;
+}
+
+int vx_world_generate(VxWorld *w, const VxTerrainParams *t) {
+    if (!w || !t || t->octaves > 32) {
+        vx::set_error("vx_world_generate: null argument or octaves > 32");
+        return VX_ERR_INVALID;
+    }
+    int rc = use_device(w);
+    if (rc != VX_OK) return rc;
+    std::lock_guard<std::mutex> lk(w->mu);
+    const vx::Dims &d = w->dw.d;
+    int16_t *heights = nullptr;
+    VX_CK(cudaMallocAsync(&heights, (size_t)d.vx * d.vz * sizeof(int16_t), w->stream));
+    cudaError_t e = vx::launch_generate(w->dw, *t, heights, w->stream);
+    cudaFreeAsync(heights, w->stream);
+    VX_CK(e);
+    VX_CK(cudaStreamSynchronize(w->stream));
+    return VX_OK;
+}
+
+int vx_world_apply_dirty(VxWorld *w, const uint32_t *brick_idx, const VxBrick *bricks, size_t n,
+                         void *stream) {
+    if (!w || (n > 0 && (!brick_idx || !bricks))) {
+        vx::set_error("vx_world_apply_dirty: null argument");
+        return VX_ERR_INVALID;
+    }
+    if (n == 0) return VX_OK;
+    const vx::Dims &d = w->dw.d;
+    // last occurrence of an index wins (the order the caller edited in)
+    std::vector<uint32_t> idx;
+    std::vector<VxBrick> pay;
+    idx.reserve(n);
+    pay.reserve(n);
+    {
+        std::unordered_map<uint32_t, size_t> last;
+        last.reserve(n * 2);
+        for (size_t i = 0; i < n; ++i) {
+            if ((int64_t)brick_idx[i] >= d.n_bricks) {
+                vx::set_error("vx_world_apply_dirty: brick index out of range");
+                return VX_ERR_INVALID;
+            }
+            last[brick_idx[i]] = i;
+        }
+        for (size_t i = 0; i < n; ++i)
+            if (last[brick_idx[i]] == i) {
+                idx.push_back(brick_idx[i]);
+                pay.push_back(bricks[i]);
+            }
+    }
+    int rc = use_device(w);
+    if (rc != VX_OK) return rc;
+    std::lock_guard<std::mutex> lk(w->mu);
+    cudaStream_t s = stream ? as_stream(stream) : w->stream;
+    if (w->idx_cap < idx.size() || w->bricks_cap < idx.size()) VX_CK(cudaStreamSynchronize(s));
+    rc = ensure(&w->d_idx, &w->idx_cap, idx.size());
+    if (rc == VX_OK) rc = ensure(&w->d_bricks, &w->bricks_cap, idx.size());
+    if (rc != VX_OK) return rc;
+    VX_CK(cudaMemcpyAsync(w->d_idx, idx.data(), idx.size() * sizeof(uint32_t),
+                          cudaMemcpyHostToDevice, s));
+    VX_CK(cudaMemcpyAsync(w->d_bricks, pay.data(), pay.size() * sizeof(VxBrick),
+                          cudaMemcpyHostToDevice, s));
+    VX_CK(vx::launch_apply_dirty(w->dw, w->d_idx, w->d_bricks, idx.size(), s));
+    // the staging vectors die with this call: finish the copies first
+    VX_CK(cudaStreamSynchronize(s));
+    return VX_OK;
+}
+
+int vx_raycast(VxWorld *w, const float cam[3], const float dir[3], const int32_t origin[3],
+               VxPickHit *out) {
+    if (!w || !cam || !dir || !origin || !out) {
+        vx::set_error("vx_raycast: null argument");
+        return VX_ERR_INVALID;
+    }
+    int rc = use_device(w);
+    if (rc != VX_OK) return rc;
+    std::lock_guard<std::mutex> lk(w->mu);
+    float in[6] = {cam[0], cam[1], cam[2], dir[0], dir[1], dir[2]};
+    VX_CK(cudaMemcpyAsync(w->pick_in, in, sizeof(in), cudaMemcpyHostToDevice, w->stream));
+    VX_CK(vx::launch_raycast(w->dw, origin, w->pick_in, w->pick_in + 3, 1, w->pick_out,
+                             w->pick_hit, w->stream));
+    int32_t hit = 0;
+    VX_CK(cudaMemcpyAsync(out, w->pick_out, sizeof(VxPickHit), cudaMemcpyDeviceToHost, w->stream));
+    VX_CK(cudaMemcpyAsync(&hit, w->pick_hit, sizeof(int32_t), cudaMemcpyDeviceToHost, w->stream));
+    VX_CK(cudaStreamSynchronize(w->stream));
+    return hit ? 1 : 0;
+}
+
+int vx_raycast_batch(VxWorld *w, const int32_t origin[3], const float *cams_dev,
+                     const float *dirs_dev, size_t n, VxPickHit *out_dev, int32_t *hit_dev,
+                     void *stream) {
+    if (!w || !origin || (n > 0 && (!cams_dev || !dirs_dev || !out_dev || !hit_dev))) {
+        vx::set_error("vx_raycast_batch: null argument");
+        return VX_ERR_INVALID;
+    }
+    int rc = use_device(w);
+    if (rc != VX_OK) return rc;
+    VX_CK(vx::launch_raycast(w->dw, origin, cams_dev, dirs_dev, n, out_dev, hit_dev,
+                             as_stream(stream)));
+    return VX_OK;
+}
+
+int vx_trace(VxWorld *w, const int32_t origin[3], const VxRay *rays_dev, size_t n,
+             const VxTraceParams *p, VxHitRecord *out_dev, void *stream) {
+    if (!w || !origin || (n > 0 && (!rays_dev || !out_dev))) {
+        vx::set_error("vx_trace: null argument");
+        return VX_ERR_INVALID;
+    }
+    int rc = check_params(p);
+    if (rc != VX_OK) return rc;
+    if ((reinterpret_cast<uintptr_t>(rays_dev) & 15u) || (reinterpret_cast<uintptr_t>(out_dev) & 7u)) {
+        vx::set_error("vx_trace: rays must be 16-byte and records 8-byte aligned");
+        return VX_ERR_INVALID;
+    }
+    rc = use_device(w);
+    if (rc != VX_OK) return rc;
+    vx::TraceArgs ta{};
+    ta.w = w->dw;
+    ta.p = *p;
+    ta.ro[0] = origin[0]; ta.ro[1] = origin[1]; ta.ro[2] = origin[2];
+    VX_CK(vx::launch_trace_rays(ta, rays_dev, n, out_dev, as_stream(stream)));
+    return VX_OK;
+}
+
+int vx_render_primary(VxWorld *w, const VxCamera *cam, const VxTraceParams *p,
+                      VxHitRecord *rec_dev, VxShadowRecord *shadow_dev, void *stream) {
+    if (!w || !rec_dev) {
+        vx::set_error("vx_render_primary: null argument");
+        return VX_ERR_INVALID;
+    }
+    int rc = check_frame(cam);
+    if (rc == VX_OK) rc = check_params(p);
+    if (rc != VX_OK) return rc;
+    if (reinterpret_cast<uintptr_t>(rec_dev) & 7u) {
+        vx::set_error("vx_render_primary: records must be 8-byte aligned");
+        return VX_ERR_INVALID;
+    }
+    rc = use_device(w);
+    if (rc != VX_OK) return rc;
+    std::lock_guard<std::mutex> lk(w->mu);
+    vx::FrameArgs fa = make_frame(w, cam, p);
+    fa.rec = rec_dev;
+    fa.shadow = shadow_dev;
+    return run_frame(w, fa, as_stream(stream));
+}
+
+int vx_render_primary_host(VxWorld *w, const VxCamera *cam, const VxTraceParams *p,
+                           VxHitRecord *rec_host, VxShadowRecord *shadow_host) {
+    if (!w || !rec_host) {
+        vx::set_error("vx_render_primary_host: null argument");
+        return VX_ERR_INVALID;
+    }
+    int rc = check_frame(cam);
+    if (rc == VX_OK) rc = check_params(p);
+    if (rc != VX_OK) return rc;
+    rc = use_device(w);
+    if (rc != VX_OK) return rc;
+    std::lock_guard<std::mutex> lk(w->mu);
+    vx::FrameArgs fa = make_frame(w, cam, p);
+    const size_t n = (size_t)fa.W * fa.H;
+    rc = ensure(&w->rec, &w->rec_cap, n);
+    if (rc == VX_OK) rc = ensure(&w->sh, &w->sh_cap, n);
+    if (rc != VX_OK) return rc;
+    fa.rec = w->rec;
+    fa.shadow = shadow_host ? w->sh : nullptr;
+    rc = run_frame(w, fa, w->stream);
+    if (rc != VX_OK) return rc;
+    VX_CK(cudaMemcpyAsync(rec_host, w->rec, n * sizeof(VxHitRecord), cudaMemcpyDeviceToHost, w->stream));
+    if (shadow_host)
+        VX_CK(cudaMemcpyAsync(shadow_host, w->sh, n * sizeof(VxShadowRecord), cudaMemcpyDeviceToHost, w->stream));
+    VX_CK(cudaStreamSynchronize(w->stream));
+    return VX_OK;
+}
+
+int vx_render_primary_stats(VxWorld *w, const VxCamera *cam, const VxTraceParams *p,
+                            uint64_t stats[4]) {
+    if (!w || !stats) {
+        vx::set_error("vx_render_primary_stats: null argument");
+        return VX_ERR_INVALID;
+    }
+    int rc = check_frame(cam);
+    if (rc == VX_OK) rc = check_params(p);
+    if (rc != VX_OK) return rc;
+    rc = use_device(w);
+    if (rc != VX_OK) return rc;
+    std::lock_guard<std::mutex> lk(w->mu);
+    vx::FrameArgs fa = make_frame(w, cam, p);
+    const size_t n = (size_t)fa.W * fa.H;
+    rc = ensure(&w->rec, &w->rec_cap, n);
+    if (rc == VX_OK) rc = ensure(&w->sh, &w->sh_cap, n);
+    if (rc == VX_OK) rc = ensure(&w->beam, &w->beam_cap, (size_t)fa.bw * fa.bh);
+    if (rc != VX_OK) return rc;
+    fa.rec = w->rec;
+    fa.shadow = w->sh;
+    fa.beam = w->beam;
+    unsigned long long h[4] = {0, 0, 0, 0};
+    VX_CK(cudaMemsetAsync(w->d_stats, 0, 4 * sizeof(unsigned long long), w->stream));
+    if (fa.ta.p.flags & VX_F_BEAM) {
+        fa.stats = w->d_stats;
+        VX_CK(vx::launch_beam(fa, w->beam, w->stream));
+    }
+    fa.stats = w->d_stats + 2;
+    VX_CK(vx::launch_primary(fa, w->stream));
+    VX_CK(cudaMemcpyAsync(h, w->d_stats, sizeof(h), cudaMemcpyDeviceToHost, w->stream));
+    VX_CK(cudaStreamSynchronize(w->stream));
+    for (int k = 0; k < 4; ++k) stats[k] = h[k];
+    return VX_OK;
+}
+
+int vx_render_primary_timed(VxWorld *w, const VxCamera *cam, const VxTraceParams *p,
+                            VxHitRecord *rec_dev, VxShadowRecord *shadow_dev, void *stream,
+                            float ms[2]) {
+    if (!w || !rec_dev || !ms) {
+        vx::set_error("vx_render_primary_timed: null argument");
+        return VX_ERR_INVALID;
+    }
+    int rc = check_frame(cam);
+    if (rc == VX_OK) rc = check_params(p);
+    if (rc != VX_OK) return rc;
+    rc = use_device(w);
+    if (rc != VX_OK) return rc;
+    std::lock_guard<std::mutex> lk(w->mu);
+    if (!w->ev[0])
+        for (int k = 0; k < 3; ++k) VX_CK(cudaEventCreate(&w->ev[k]));
+    cudaStream_t s = as_stream(stream);
+    vx::FrameArgs fa = make_frame(w, cam, p);
+    fa.rec = rec_dev;
+    fa.shadow = shadow_dev;
+    VX_CK(cudaEventRecord(w->ev[0], s));
+    if (fa.ta.p.flags & VX_F_BEAM) {
+        rc = ensure(&w->beam, &w->beam_cap, (size_t)fa.bw * fa.bh);
+        if (rc != VX_OK) return rc;
+        fa.beam = w->beam;
+        VX_CK(vx::launch_beam(fa, w->beam, s));
+    }
+    VX_CK(cudaEventRecord(w->ev[1], s));
+    VX_CK(vx::launch_primary(fa, s));
+    VX_CK(cudaEventRecord(w->ev[2], s));
+    VX_CK(cudaEventSynchronize(w->ev[2]));
+    VX_CK(cudaEventElapsedTime(&ms[0], w->ev[0], w->ev[1]));
+    VX_CK(cudaEventElapsedTime(&ms[1], w->ev[1], w->ev[2]));
+    return VX_OK;
+}
+
+}  // extern "C"

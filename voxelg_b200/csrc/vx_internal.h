@@ -1,0 +1,92 @@
+// vx_internal.h -- definitions shared by the CUDA kernels and the C++ host
+// side of libvoxrt.  Not part of the public ABI (include/voxrt.h is).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "voxrt.h"
+
+namespace vx {
+
+// World dimensions; the derived counts follow src/world_dims.rs:12-37.
+struct Dims {
+    int32_t bx, by, bz;  // bricks
+    int32_t vx, vy, vz;  // voxels
+    int32_t tx, ty, tz;  // tiles (16^3 voxels)
+    int32_t cx, cy, cz;  // chunks (64^3)
+    int32_t lx, ly, lz;  // L4 cells (256^3)
+    int64_t n_bricks, n_tiles, n_chunks, n_l4;
+};
+
+inline Dims make_dims(int32_t bx, int32_t by, int32_t bz) {
+    Dims d;
+    d.bx = bx; d.by = by; d.bz = bz;
+    d.vx = bx * 4; d.vy = by * 4; d.vz = bz * 4;
+    d.tx = bx / 4; d.ty = by / 4; d.tz = bz / 4;
+    d.cx = (d.tx + 3) / 4; d.cy = (d.ty + 3) / 4; d.cz = (d.tz + 3) / 4;
+    d.lx = (d.cx + 3) / 4; d.ly = (d.cy + 3) / 4; d.lz = (d.cz + 3) / 4;
+    d.n_bricks = (int64_t)bx * by * bz;
+    d.n_tiles = (int64_t)d.tx * d.ty * d.tz;
+    d.n_chunks = (int64_t)d.cx * d.cy * d.cz;
+    d.n_l4 = (int64_t)d.lx * d.ly * d.lz;
+    return d;
+}
+
+// Device-resident pyramid.  Bricks are split structure-of-arrays: the 8-byte
+// occupancy words (read on every voxel-level iteration) are packed densely,
+// the 64 material bytes of a brick sit in their own 64-byte-aligned row and
+// are only touched on a solid voxel.
+struct DevWorld {
+    Dims d;
+    uint64_t *occ;            // n_bricks
+    uint8_t *mat;             // n_bricks * 64
+    uint64_t *tile_mask;      // n_tiles
+    uint64_t *chunk_mask;     // n_chunks
+    uint64_t *l4_mask;        // n_l4
+    uint8_t *brick_uniform;   // n_bricks
+    uint8_t *tile_uniform;    // n_tiles
+};
+
+// Per-frame constants of the traversal kernels (passed by value).
+struct TraceArgs {
+    DevWorld w;
+    VxTraceParams p;
+    int32_t ro[3];            // loaded-window corner (camera.world_origin)
+};
+
+struct FrameArgs {
+    TraceArgs ta;
+    VxCamera cam;
+    const float *beam;        // beam depth (bw*bh) or nullptr
+    uint32_t W, H, bw, bh;
+    VxHitRecord *rec;
+    VxShadowRecord *shadow;
+    unsigned long long *stats;  // [bytes, iters] or nullptr
+};
+
+// ---- kernel launchers (vx_trace.cu / vx_world.cu) ----
+cudaError_t launch_beam(const FrameArgs &fa, float *beam_out, cudaStream_t s);
+cudaError_t launch_primary(const FrameArgs &fa, cudaStream_t s);
+cudaError_t launch_trace_rays(const TraceArgs &ta, const VxRay *rays, size_t n, VxHitRecord *out,
+                              cudaStream_t s);
+cudaError_t launch_raycast(const DevWorld &w, const int32_t origin[3], const float *cams,
+                           const float *dirs, size_t n, VxPickHit *out, int32_t *hit,
+                           cudaStream_t s);
+
+cudaError_t launch_bricks_from_aos(const DevWorld &w, const VxBrick *aos, int64_t first,
+                                   int64_t count, cudaStream_t s);
+cudaError_t launch_bricks_to_aos(const DevWorld &w, VxBrick *aos, int64_t first, int64_t count,
+                                 cudaStream_t s);
+cudaError_t launch_generate(const DevWorld &w, const VxTerrainParams &t, int16_t *heights,
+                            cudaStream_t s);
+cudaError_t launch_rebuild_pyramid(const DevWorld &w, cudaStream_t s);
+cudaError_t launch_apply_dirty(const DevWorld &w, const uint32_t *idx, const VxBrick *bricks,
+                               size_t n, cudaStream_t s);
+
+// thread-local error text
+void set_error(const std::string &msg);
+
+}  // namespace vx
