@@ -50,6 +50,9 @@ def parse_args():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-seconds", type=float, default=10.0)
+    ap.add_argument("--profile", action="store_true",
+                    help="frames only (one counting pass, warm-up, K timed frames): the "
+                         "command profiled with ncu")
     return ap.parse_args()
 
 
@@ -257,6 +260,16 @@ def run_ours(args, cfg):
 
     for _ in range(max(args.warmup, 3)):
         vg.render_primary_timed(dw, cam, params, rec, sh, stream=stream)
+
+    if args.profile:
+        ms = []
+        for _ in range(args.steps):
+            flush.zero_()
+            ms.append(sum(vg.render_primary_timed(dw, cam, params, rec, sh, stream=stream)))
+        print(json.dumps({"profile_frames": args.steps, "ms_per_frame": statistics.mean(ms),
+                          "rays_per_frame": rays_per_step}), flush=True)
+        dw.close()
+        return
 
     sampler = ClockSampler(local) if rank == 0 or world > 1 else None
     barrier(world)
