@@ -220,6 +220,39 @@ int vx_render_primary_timed(VxWorld *w, const VxCamera *cam, const VxTraceParams
                             VxHitRecord *rec_dev, VxShadowRecord *shadow_dev, void *stream,
                             float ms[2]);
 
+/* ---- frames for callers that cannot allocate ------------------------------
+ * No counterpart in the reference: an addition for hosts that reserve all
+ * device memory up front and forbid (or cannot afford) cudaMalloc once
+ * running -- a plugin handed pre-allocated buffers, a frame loop where the
+ * device synchronization of cudaMalloc/cudaFree is a hitch.
+ *
+ * The caller owns the world in device memory, laid out as this library keeps
+ * it: occupancy = one u64 per brick (brick index bx + by*BX + bz*BX*BY),
+ * materials = 64 bytes per brick in the same order (voxel x + z*4 + y*16),
+ * masks / LUTs exactly as the host arrays of vx_world_upload. */
+typedef struct {
+    int32_t bricks_x, bricks_y, bricks_z;  /* same rules as VxWorldDesc */
+    const uint64_t *occupancy;             /* n_bricks                  */
+    const uint8_t *materials;              /* n_bricks * 64             */
+    const uint64_t *tile_mask;
+    const uint64_t *chunk_mask;
+    const uint64_t *l4_mask;
+    const uint8_t *brick_uniform;
+    const uint8_t *tile_uniform;
+} VxWorldView;
+
+/* vx_render_primary over a caller-owned world, allocating nothing: the beam
+ * scratch is a static device array of 480x270 cells built into the library
+ * (each GPU that loads it holds 512 KiB until exit), so frames whose beam
+ * grid exceeds 129600 cells (beyond 3840x2160) are rejected with
+ * VX_ERR_INVALID.  Runs on the calling thread's current device.  The first
+ * call on a device looks up the array's address there (make it before any
+ * stream capture).  All calls share the array: calls that overlap on the GPU
+ * race.  Asynchronous on `stream`. */
+int vx_render_primary_noalloc(const VxWorldView *world, const VxCamera *cam,
+                              const VxTraceParams *p, VxHitRecord *rec_dev,
+                              VxShadowRecord *shadow_dev, void *stream);
+
 /* ---- host world (mirror of src/voxel.rs World, for C/C++ callers) ------ */
 int vx_host_world_create(int32_t bricks_x, int32_t bricks_y, int32_t bricks_z,
                          VxHostWorld **out);

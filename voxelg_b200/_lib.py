@@ -59,6 +59,13 @@ class VxPickHit(C.Structure):
     _fields_ = [("voxel", C.c_int32 * 3), ("normal", C.c_int32 * 3)]
 
 
+class VxWorldView(C.Structure):
+    _fields_ = [("bricks_x", C.c_int32), ("bricks_y", C.c_int32), ("bricks_z", C.c_int32),
+                ("occupancy", C.c_void_p), ("materials", C.c_void_p), ("tile_mask", C.c_void_p),
+                ("chunk_mask", C.c_void_p), ("l4_mask", C.c_void_p),
+                ("brick_uniform", C.c_void_p), ("tile_uniform", C.c_void_p)]
+
+
 class VxTerrainParams(C.Structure):
     _fields_ = [("seed", C.c_uint64), ("base_height", C.c_float), ("amplitude", C.c_float),
                 ("inv_wavelength", C.c_float), ("octaves", C.c_uint32),
@@ -102,6 +109,8 @@ SIGNATURES = [
                                           _P(C.c_uint64)]),
     ("vx_render_primary_timed", C.c_int, [_vp, _P(VxCamera), _P(VxTraceParams), _vp, _vp, _vp,
                                           _P(C.c_float)]),
+    ("vx_render_primary_noalloc", C.c_int, [_P(VxWorldView), _P(VxCamera), _P(VxTraceParams),
+                                            _vp, _vp, _vp]),
     ("vx_host_world_create", C.c_int, [C.c_int32, C.c_int32, C.c_int32, _P(_vp)]),
     ("vx_host_world_destroy", C.c_int, [_vp]),
     ("vx_host_world_arrays", C.c_int, [_vp, _P(_vp), _P(_vp), _P(_vp), _P(_vp), _P(_vp), _P(_vp)]),
