@@ -183,6 +183,16 @@ int vx_world_apply_dirty(VxWorld *w, const uint32_t *brick_idx, const VxBrick *b
 /* Counts of each array: bricks, tiles, chunks, l4 cells. */
 int vx_world_counts(const VxWorld *w, uint64_t counts[4]);
 
+/* Launch shape of the frame kernels.  persistent = 0: one CTA per 16x8
+ * pixels (default); 1: one wave of CTAs whose warps pull 8x4 pixel tiles from
+ * a counter.  Results are identical either way. */
+typedef struct {
+    int32_t persistent;
+    int32_t reserved[7];
+} VxTuning;
+int vx_world_set_tuning(VxWorld *w, const VxTuning *t);
+int vx_world_get_tuning(const VxWorld *w, VxTuning *t);
+
 /* ---- traversal --------------------------------------------------------- */
 /* raycast(camera_world, dir, world, world_origin) (src/raycast.rs:21): returns
  * 1 on a hit (fills *out), 0 on a miss, <0 on error.  Synchronous. */

@@ -86,6 +86,30 @@ def test_c1_frame_bit_exact(vg, dev_c1, c1_oracle_world, flags):
         assert sh["traced"].sum() == (rec["flags"] & 1).sum()
 
 
+@pytest.mark.parametrize("res", [(640, 360), (333, 7), (17, 13)])
+def test_refill_schedule_bit_exact(vg, dev_c1, c1_oracle_world, res):
+    """The persistent per-lane refill kernel gives the oracle's records."""
+    cam = vg.default_camera(dev_c1, *res)
+    dev_c1.set_persistent(True)
+    try:
+        for flags in (po.OR_F_L4, METHOD | po.OR_F_SHADOW, po.OR_F_L4 | po.OR_F_SHADOW):
+            rec, sh, (wrec, wsh, _, _, _) = frame_pair(vg, dev_c1, c1_oracle_world, cam, flags)
+            assert_same_records(rec, wrec, f"refill {res} flags={flags}")
+            if sh is not None:
+                assert np.array_equal(sh.view(np.uint8), wsh.view(np.uint8))
+        # repeated launches: the self-resetting work counters start from zero
+        p = vg.default_params()
+        a = vg.render_primary(dev_c1, cam, p)
+        b = vg.render_primary(dev_c1, cam, p)
+        import torch
+        torch.cuda.synchronize()
+        assert torch.equal(a[0], b[0]) and torch.equal(a[1], b[1])
+        s = vg.render_stats(dev_c1, cam, p)
+    finally:
+        dev_c1.set_persistent(False)
+    assert s == vg.render_stats(dev_c1, cam, p)
+
+
 def test_frame_stats_match_oracle(vg, dev_c1, c1_oracle_world):
     cfg = vg.CONFIGS["c1"]
     cam = vg.default_camera(dev_c1, 320, 180)
@@ -353,6 +377,10 @@ def test_c2_full_frame_bit_exact(vg):
     assert np.array_equal(vg.shadows(sh).view(np.uint8), wsh.view(np.uint8))
     r = vg.records(rec)
     assert (r["flags"] & 2).any(), "LOD / uniform early-outs never fired"
+    dw.set_persistent(True)
+    rec2, sh2 = vg.render_primary(dw, cam, p)
+    torch.cuda.synchronize()
+    assert torch.equal(rec, rec2) and torch.equal(sh, sh2), "refill schedule differs"
     dw.close()
 
 

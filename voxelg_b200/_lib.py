@@ -66,6 +66,10 @@ class VxWorldView(C.Structure):
                 ("brick_uniform", C.c_void_p), ("tile_uniform", C.c_void_p)]
 
 
+class VxTuning(C.Structure):
+    _fields_ = [("persistent", C.c_int32), ("reserved", C.c_int32 * 7)]
+
+
 class VxTerrainParams(C.Structure):
     _fields_ = [("seed", C.c_uint64), ("base_height", C.c_float), ("amplitude", C.c_float),
                 ("inv_wavelength", C.c_float), ("octaves", C.c_uint32),
@@ -100,6 +104,8 @@ SIGNATURES = [
     ("vx_world_generate", C.c_int, [_vp, _P(VxTerrainParams)]),
     ("vx_world_apply_dirty", C.c_int, [_vp, _vp, _vp, C.c_size_t, _vp]),
     ("vx_world_counts", C.c_int, [_vp, _P(C.c_uint64)]),
+    ("vx_world_set_tuning", C.c_int, [_vp, _P(VxTuning)]),
+    ("vx_world_get_tuning", C.c_int, [_vp, _P(VxTuning)]),
     ("vx_raycast", C.c_int, [_vp, _P(C.c_float), _P(C.c_float), _P(C.c_int32), _P(VxPickHit)]),
     ("vx_raycast_batch", C.c_int, [_vp, _P(C.c_int32), _vp, _vp, C.c_size_t, _vp, _vp, _vp]),
     ("vx_trace", C.c_int, [_vp, _P(C.c_int32), _vp, C.c_size_t, _P(VxTraceParams), _vp, _vp]),

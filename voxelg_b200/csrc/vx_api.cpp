@@ -40,6 +40,8 @@ struct VxWorld {
     VxPickHit *pick_out = nullptr;
     int32_t *pick_hit = nullptr;
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+    uint32_t *d_work = nullptr;      // persistent-schedule counters (self-resetting)
+    VxTuning tuning{0, {0, 0, 0, 0, 0, 0, 0}};
 };
 
 namespace {
@@ -89,6 +91,7 @@ void free_world(VxWorld *w) {
     cudaFree(w->pick_in);
     cudaFree(w->pick_out);
     cudaFree(w->pick_hit);
+    cudaFree(w->d_work);
     for (auto &e : w->ev)
         if (e) cudaEventDestroy(e);
     if (w->stream) cudaStreamDestroy(w->stream);
@@ -116,6 +119,7 @@ vx::FrameArgs make_frame(VxWorld *w, const VxCamera *cam, const VxTraceParams *p
     fa.H = (uint32_t)cam->res_y;
     fa.bw = (fa.W + 7u) / 8u;
     fa.bh = (fa.H + 7u) / 8u;
+    fa.work = w->tuning.persistent ? w->d_work : nullptr;
     return fa;
 }
 
@@ -253,6 +257,8 @@ int vx_world_create(const VxWorldDesc *desc, VxWorld **out) {
     VX_CKW(cudaMalloc(&w->dw.brick_uniform, d.n_bricks));
     VX_CKW(cudaMalloc(&w->dw.tile_uniform, d.n_tiles));
     VX_CKW(cudaMalloc(&w->d_stats, 4 * sizeof(unsigned long long)));
+    VX_CKW(cudaMalloc(&w->d_work, 2 * sizeof(uint32_t)));
+    VX_CKW(cudaMemsetAsync(w->d_work, 0, 2 * sizeof(uint32_t), w->stream));
     VX_CKW(cudaMalloc(&w->pick_in, 8 * sizeof(float)));
     VX_CKW(cudaMalloc(&w->pick_out, sizeof(VxPickHit)));
     VX_CKW(cudaMalloc(&w->pick_hit, sizeof(int32_t)));
@@ -275,6 +281,22 @@ int vx_world_destroy(VxWorld *w) {
     if (w->stream) cudaStreamSynchronize(w->stream);
     free_world(w);
     delete w;
+    return VX_OK;
+}
+
+int vx_world_set_tuning(VxWorld *w, const VxTuning *t) {
+    if (!w || !t || (t->persistent != 0 && t->persistent != 1)) {
+        vx::set_error("vx_world_set_tuning: persistent must be 0 or 1");
+        return VX_ERR_INVALID;
+    }
+    std::lock_guard<std::mutex> lk(w->mu);
+    w->tuning = *t;
+    return VX_OK;
+}
+
+int vx_world_get_tuning(const VxWorld *w, VxTuning *t) {
+    if (!w || !t) return VX_ERR_INVALID;
+    *t = w->tuning;
     return VX_OK;
 }
 
@@ -475,7 +497,7 @@ int vx_render_primary(VxWorld *w, const VxCamera *cam, const VxTraceParams *p,
     int rc = check_frame(cam);
     if (rc == VX_OK) rc = check_params(p);
     if (rc != VX_OK) return rc;
-    if (reinterpret_cast<uintptr_t>(rec_dev) & 7u) {
+    if ((reinterpret_cast<uintptr_t>(rec_dev) & 7u) || (reinterpret_cast<uintptr_t>(shadow_dev) & 7u)) {
         vx::set_error("vx_render_primary: records must be 8-byte aligned");
         return VX_ERR_INVALID;
     }

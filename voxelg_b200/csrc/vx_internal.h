@@ -65,6 +65,7 @@ struct FrameArgs {
     VxHitRecord *rec;
     VxShadowRecord *shadow;
     unsigned long long *stats;  // [bytes, iters] or nullptr
+    uint32_t *work;             // persistent schedule: {next tile, warps done}, or nullptr
 };
 
 // ---- kernel launchers (vx_trace.cu / vx_world.cu) ----

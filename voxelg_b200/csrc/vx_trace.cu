@@ -38,16 +38,30 @@ __device__ __forceinline__ float vmax(float a, float b) { return (a < b) ? b : a
 __device__ __forceinline__ float clampf(float x, float lo, float hi) {
     return vmin(vmax(x, lo), hi);
 }
+// f32 -> i32 toward zero, saturating (NaN -> 0), clamped to +-2^30.  The PTX
+// conversion (cvt.rzi.s32.f32) already saturates and maps NaN to 0; the clamp
+// narrows the range so later integer cell arithmetic cannot overflow.
 __device__ __forceinline__ int32_t f2i(float x) {
-    if (x != x) return 0;
-    if (x >= 1073741824.0f) return 1073741824;
-    if (x <= -1073741824.0f) return -1073741824;
-    return (int32_t)x;
+    return min(max(__float2int_rz(x), -1073741824), 1073741824);
 }
 // common.wgsl:49-52
 __device__ __forceinline__ int32_t pos_mod(int32_t a, int32_t b) {
     if (a >= 0) return a % b;
     return (b - 1) - ((-1 - a) % b);
+}
+// v reduced into [0, n) where v is known congruent to the wanted slot; a
+// jump of a few cells needs at most two corrections, far jumps (only the
+// degenerate skip with no forward face) fall back to the division.
+__device__ __forceinline__ int32_t wrap_near(int32_t v, int32_t n) {
+    if (v < 0) {
+        v += n;
+        if (v < 0) v += n;
+    } else if (v >= n) {
+        v -= n;
+        if (v >= n) v -= n;
+    }
+    if ((uint32_t)v >= (uint32_t)n) v = pos_mod(v, n);
+    return v;
 }
 // common.wgsl:55-58
 __device__ __forceinline__ float safe_inv(float x) {
@@ -60,6 +74,20 @@ __device__ __forceinline__ bool bit64(uint64_t w, int b) { return (w >> b) & 1ul
 
 template <typename T>
 __device__ __forceinline__ T ldg(const T *p) { return __ldg(p); }
+
+#ifndef VX_MIN_BLOCKS
+#define VX_MIN_BLOCKS 0
+#endif
+// Idle lanes a warp of the refill kernel waits for before it hands out new
+// pixels (32 = refill only when the whole warp is idle).
+#ifndef VX_REFILL_MIN
+#define VX_REFILL_MIN 16
+#endif
+#if VX_MIN_BLOCKS > 0
+#define VX_FRAME_BOUNDS __launch_bounds__(128, VX_MIN_BLOCKS)
+#else
+#define VX_FRAME_BOUNDS __launch_bounds__(128)
+#endif
 
 // Materials (src/voxel.rs:100-157, raymarch.wgsl:875-920)
 __device__ __forceinline__ bool is_water(uint32_t m) { return m >= 5u && m <= 12u; }
@@ -177,9 +205,13 @@ __device__ __forceinline__ void skip_to_cell(const Dims &d, Ro ro, int32_t cell,
                                              int &la) {
     const int32_t hi = ~(cell - 1);
     const int32_t cox = s.vx & hi, coy = s.vy & hi, coz = s.vz & hi;
-    const float tfx = ((float)((s.stx > 0 ? cox + cell : cox) - ro.x) - s.ox) * s.ix;
-    const float tfy = ((float)((s.sty > 0 ? coy + cell : coy) - ro.y) - s.oy) * s.iy;
-    const float tfz = ((float)((s.stz > 0 ? coz + cell : coz) - ro.z) - s.oz) * s.iz;
+    // exit-face boundary per axis and the voxel just across it
+    const int32_t bx = s.stx > 0 ? cox + cell : cox, nbx = s.stx > 0 ? bx : cox - 1;
+    const int32_t by = s.sty > 0 ? coy + cell : coy, nby = s.sty > 0 ? by : coy - 1;
+    const int32_t bz = s.stz > 0 ? coz + cell : coz, nbz = s.stz > 0 ? bz : coz - 1;
+    const float tfx = ((float)(bx - ro.x) - s.ox) * s.ix;
+    const float tfy = ((float)(by - ro.y) - s.oy) * s.iy;
+    const float tfz = ((float)(bz - ro.z) - s.oz) * s.iz;
     const float eps = 1e-6f;
     float t_min = 1e30f;
     int ax = 0;
@@ -190,17 +222,18 @@ __device__ __forceinline__ void skip_to_cell(const Dims &d, Ro ro, int32_t cell,
     int32_t nx = f2i(floorf(s.ox + s.dx * tb)) + ro.x;
     int32_t ny = f2i(floorf(s.oy + s.dy * tb)) + ro.y;
     int32_t nz = f2i(floorf(s.oz + s.dz * tb)) + ro.z;
-    if (ax == 0) nx = s.stx > 0 ? cox + cell : cox - 1;
-    else if (ax == 1) ny = s.sty > 0 ? coy + cell : coy - 1;
-    else nz = s.stz > 0 ? coz + cell : coz - 1;
+    nx = ax == 0 ? nbx : nx;
+    ny = ax == 1 ? nby : ny;
+    nz = ax == 2 ? nbz : nz;
+    // slot of the new voxel: old slot + displacement, folded (== pos_mod(n, dims))
+    s.sx = wrap_near(s.sx + (nx - s.vx), d.vx);
+    s.sz = wrap_near(s.sz + (nz - s.vz), d.vz);
     s.vx = nx; s.vy = ny; s.vz = nz;
     const int32_t lx = nx - ro.x, ly = ny - ro.y, lz = nz - ro.z;
-    s.mx = s.stx > 0 ? ((float)(lx + 1) - s.ox) * s.ix : ((float)lx - s.ox) * s.ix;
-    s.my = s.sty > 0 ? ((float)(ly + 1) - s.oy) * s.iy : ((float)ly - s.oy) * s.iy;
-    s.mz = s.stz > 0 ? ((float)(lz + 1) - s.oz) * s.iz : ((float)lz - s.oz) * s.iz;
+    s.mx = ((float)(s.stx > 0 ? lx + 1 : lx) - s.ox) * s.ix;
+    s.my = ((float)(s.sty > 0 ? ly + 1 : ly) - s.oy) * s.iy;
+    s.mz = ((float)(s.stz > 0 ? lz + 1 : lz) - s.oz) * s.iz;
     la = ax;
-    s.sx = pos_mod(nx, d.vx);
-    s.sz = pos_mod(nz, d.vz);
 }
 
 // t of the face just crossed: t_max[la] - t_delta[la]
@@ -268,269 +301,241 @@ __device__ __forceinline__ uint32_t brick_topmost(const uint8_t *__restrict__ mr
     return (lo | hi) != 0u ? 35u : 0u;
 }
 
-// ------------------------------------------------------------------ trace
-// trace(), raymarch.wgsl:4600-4777, far-distance cube resolution.
-template <bool STATS>
+// 32-bit strides of every level (all cell indices of a world that fits in
+// device memory are below 2^32; only the material row offset is widened).
+struct Geo {
+    uint32_t bx, bxy, tx, txy, cx, cxy, lx, lxy;
+};
+__device__ __forceinline__ Geo geo_of(const Dims &d) {
+    Geo g;
+    g.bx = (uint32_t)d.bx;
+    g.bxy = (uint32_t)(d.bx * d.by);
+    g.tx = (uint32_t)d.tx;
+    g.txy = (uint32_t)(d.tx * d.ty);
+    g.cx = (uint32_t)d.cx;
+    g.cxy = (uint32_t)(d.cx * d.cy);
+    g.lx = (uint32_t)d.lx;
+    g.lxy = (uint32_t)(d.lx * d.ly);
+    return g;
+}
+__device__ __forceinline__ uint32_t l4_index(const Geo &g, uint32_t sx, uint32_t sy, uint32_t sz) {
+    return (sx >> 8) + (sy >> 8) * g.lx + (sz >> 8) * g.lxy;
+}
+__device__ __forceinline__ uint32_t chunk_index(const Geo &g, uint32_t sx, uint32_t sy, uint32_t sz) {
+    return (sx >> 6) + (sy >> 6) * g.cx + (sz >> 6) * g.cxy;
+}
+__device__ __forceinline__ uint32_t tile_index(const Geo &g, uint32_t sx, uint32_t sy, uint32_t sz) {
+    return (sx >> 4) + (sy >> 4) * g.tx + (sz >> 4) * g.txy;
+}
+__device__ __forceinline__ uint32_t brick_index(const Geo &g, uint32_t bx, uint32_t by, uint32_t bz) {
+    return bx + by * g.bx + bz * g.bxy;
+}
+// child bit x + z*4 + y*16 of the level whose cell size is 1 << sh
+__device__ __forceinline__ int child_of(uint32_t sx, uint32_t sy, uint32_t sz, int sh) {
+    return (int)(((sx >> sh) & 3u) + ((sz >> sh) & 3u) * 4u + ((sy >> sh) & 3u) * 16u);
+}
+
+// ------------------------------------------------------------------ walk
+// One traversal = dda_init + repeated cascade iterations.  The three kinds
+// share the level cascade and differ only where the reference differs:
+//   KIND_TRACE    trace()           raymarch.wgsl:4600-4777 (L4 optional,
+//                                   LUT + LOD per method flags, cube rule)
+//   KIND_ANY      trace_any()       raymarch.wgsl:4345-4409 (occluder rule)
+//   KIND_NO_WATER trace_no_water()  raymarch.wgsl:3450-3532 (first
+//                                   non-transparent voxel; t_cur not
+//                                   refreshed after a skip)
+enum : uint32_t { KIND_TRACE = 0, KIND_ANY = 1, KIND_NO_WATER = 2 };
+
+struct Walk {
+    Dda s;
+    float t_cur;
+    float tmax;       // MAX_RAY_DIST / max_dist / t_cap of this ray
+    int la;           // last_axis
+    uint32_t iters;   // loop iterations begun
+    uint32_t cap;     // iteration cap (1024 / 768 / 1024)
+    uint32_t kind;
+};
+
+enum : int { WALK_CONT = 0, WALK_END = 1, WALK_HIT = 2 };
+
+__device__ __forceinline__ bool walk_init(const Dims &d, Ro ro, uint32_t kind,
+                                          const VxTraceParams &p, float o0, float o1, float o2,
+                                          float d0, float d1, float d2, float tmax, Walk &k) {
+    k.kind = kind;
+    k.tmax = tmax;
+    k.la = -1;
+    k.iters = 0;
+    k.cap = (uint32_t)(kind == KIND_ANY ? p.any_max_iters : p.max_iters);
+    return dda_init(d, ro, o0, o1, o2, d0, d1, d2, k.s, &k.t_cur);
+}
+
+// One cascade iteration.  On WALK_HIT the record fields of h are set (for
+// KIND_ANY only "occluded" matters).  FL holds VX_F_L4|VX_F_LUT|VX_F_LOD as
+// compile-time bits; KNOWN >= 0 fixes the kind at compile time.
+template <uint32_t FL, bool STATS, int KNOWN>
+__device__ __forceinline__ int walk_step(const DevWorld &w, const Geo &g, const VxTraceParams &p,
+                                         Ro ro, Walk &k, Hit &h, uint64_t &bytes) {
+    const uint32_t kind = KNOWN >= 0 ? (uint32_t)KNOWN : k.kind;
+    const bool is_trace = kind == KIND_TRACE;
+    const bool use_l4 = !is_trace || (FL & VX_F_L4) != 0u;
+    const bool f_lut = is_trace && (FL & VX_F_LUT) != 0u;
+    const bool f_lod = is_trace && (FL & VX_F_LOD) != 0u;
+    const Dims &d = w.d;
+    Dda &s = k.s;
+    if (k.iters >= k.cap) return WALK_END;
+    ++k.iters;
+    if (k.t_cur > k.tmax) return WALK_END;
+    if (out_of_window(d, s, ro)) return WALK_END;
+    const uint32_t sx = (uint32_t)s.sx, sy = (uint32_t)s.vy, sz = (uint32_t)s.sz;
+    const uint32_t ti = tile_index(g, sx, sy, sz);
+    // batch 1: every coarse word addressed by the slot coordinate
+    uint64_t lw = ~0ull;
+    if (use_l4) lw = ldg(w.l4_mask + l4_index(g, sx, sy, sz));
+    const uint64_t cw = ldg(w.chunk_mask + chunk_index(g, sx, sy, sz));
+    const uint64_t tw = ldg(w.tile_mask + ti);
+    const uint32_t tum = f_lut ? (uint32_t)ldg(w.tile_uniform + ti) : 0u;
+    int32_t cell = 0;
+    if (use_l4) {
+        if (STATS) bytes += 8;
+        if (lw == 0ull) cell = 256;
+        else if (!bit64(lw, child_of(sx, sy, sz, 6))) cell = 64;
+    }
+    if (cell == 0) {
+        if (STATS) bytes += 8;
+        if (!bit64(cw, child_of(sx, sy, sz, 4))) cell = 16;
+    }
+    if (cell == 0) {
+        // tile-level LOD (raymarch.wgsl:4672-4689)
+        if (f_lod && k.t_cur > p.tile_lod_t) {
+            if (STATS) bytes += 8;
+            uint32_t lm = 0u;
+            if (tw != 0ull) {
+                const int lin = __ffsll((long long)tw) - 1;
+                const uint32_t rbi = brick_index(g, (sx >> 4) * 4u + (uint32_t)(lin & 3),
+                                                 (sy >> 4) * 4u + (uint32_t)((lin >> 4) & 3),
+                                                 (sz >> 4) * 4u + (uint32_t)((lin >> 2) & 3));
+                if (STATS) bytes += 8;
+                lm = brick_topmost<STATS>(w.mat + (size_t)rbi * 64u, ldg(w.occ + rbi), bytes);
+            }
+            if (lm != 0u && is_uniform_optimisable(lm)) {
+                set_hit(d, s, k.la, lm, true, h);
+                return WALK_HIT;
+            }
+        }
+        if (f_lut) {
+            if (STATS) bytes += 1;
+            if (tum != 0u && is_uniform_optimisable(tum)) {
+                set_hit(d, s, k.la, tum, true, h);
+                return WALK_HIT;
+            }
+        }
+        if (STATS) bytes += 8;
+        if (!bit64(tw, child_of(sx, sy, sz, 2))) {
+            cell = 4;
+        } else {
+            const uint32_t bi = brick_index(g, sx >> 2, sy >> 2, sz >> 2);
+            // batch 2: brick occupancy + brick LUT byte
+            const uint64_t occ = ldg(w.occ + bi);
+            const uint32_t bum = f_lut ? (uint32_t)ldg(w.brick_uniform + bi) : 0u;
+            if (f_lut) {
+                if (STATS) bytes += 1;
+                if (bum != 0u && is_uniform_optimisable(bum)) {
+                    set_hit(d, s, k.la, bum, true, h);
+                    return WALK_HIT;
+                }
+            }
+            const uint8_t *mrow = w.mat + (size_t)bi * 64u;
+            bool lod_done = false;
+            if (f_lod && k.t_cur > p.lod_brick_t) {
+                if (STATS) bytes += 8;
+                if (occ == 0ull) {
+                    cell = 4;
+                    lod_done = true;
+                } else {
+                    const uint32_t m = brick_topmost<STATS>(mrow, occ, bytes);
+                    if (!is_foliage(m)) {
+                        set_hit(d, s, k.la, m, true, h);
+                        return WALK_HIT;
+                    }
+                }
+            }
+            if (!lod_done) {
+                const int vi = child_of(sx, sy, sz, 0);
+                if (STATS) bytes += 8;
+                if (bit64(occ, vi)) {
+                    // batch 3: the material byte of a solid voxel
+                    const uint32_t m = ldg(mrow + vi);
+                    if (STATS) bytes += 1;
+                    const bool stop = kind == KIND_TRACE ? resolves_cube(m)
+                                      : (kind == KIND_ANY ? shadow_occludes(m) : !is_transparent(m));
+                    if (stop) {
+                        if (kind != KIND_ANY) set_hit(d, s, k.la, m, false, h);
+                        return WALK_HIT;
+                    }
+                }
+            }
+        }
+    }
+    if (cell != 0) {
+        skip_to_cell(d, ro, cell, s, k.la);
+        if (kind != KIND_NO_WATER) k.t_cur = crossed_t(s, k.la);
+    } else {
+        dda_step(d, s, k.t_cur, k.la);
+    }
+    return WALK_CONT;
+}
+
+// trace() over one ray
+template <uint32_t FL, bool STATS>
 __device__ __forceinline__ void trace_ray(const DevWorld &w, const VxTraceParams &p, Ro ro,
                                           float o0, float o1, float o2, float d0, float d1,
                                           float d2, float max_dist, Hit &h, uint64_t &bytes) {
-    const Dims &d = w.d;
+    const Geo g = geo_of(w.d);
     set_miss(h);
-    Dda s;
-    float t_cur;
-    uint32_t iters = 0;
-    if (!dda_init(d, ro, o0, o1, o2, d0, d1, d2, s, &t_cur)) {
+    Walk k;
+    if (!walk_init(w.d, ro, KIND_TRACE, p, o0, o1, o2, d0, d1, d2, max_dist, k)) {
         h.steps = 0;
         return;
     }
-    const bool f_l4 = (p.flags & VX_F_L4) != 0u;
-    const bool f_lut = (p.flags & VX_F_LUT) != 0u;
-    const bool f_lod = (p.flags & VX_F_LOD) != 0u;
-    int la = -1;
-    for (int it = 0; it < p.max_iters; ++it) {
-        ++iters;
-        if (t_cur > max_dist) break;
-        if (out_of_window(d, s, ro)) break;
-        const int32_t sx = s.sx, sy = s.vy, sz = s.sz;
-        const int64_t ci = (int64_t)(sx >> 6) + (int64_t)(sy >> 6) * d.cx +
-                           (int64_t)(sz >> 6) * d.cx * d.cy;
-        const int64_t ti = (int64_t)(sx >> 4) + (int64_t)(sy >> 4) * d.tx +
-                           (int64_t)(sz >> 4) * d.tx * d.ty;
-        // batch 1: every coarse word addressed by the slot coordinate
-        uint64_t lw = ~0ull;
-        if (f_l4) {
-            const int64_t li = (int64_t)(sx >> 8) + (int64_t)(sy >> 8) * d.lx +
-                               (int64_t)(sz >> 8) * d.lx * d.ly;
-            lw = ldg(w.l4_mask + li);
-        }
-        const uint64_t cw = ldg(w.chunk_mask + ci);
-        const uint64_t tw = ldg(w.tile_mask + ti);
-        const uint32_t tum = f_lut ? (uint32_t)ldg(w.tile_uniform + ti) : 0u;
-        int32_t cell = 0;
-        if (f_l4) {
-            if (STATS) bytes += 8;
-            if (lw == 0ull) cell = 256;
-            else if (!bit64(lw, child_bit((sx >> 6) & 3, (sy >> 6) & 3, (sz >> 6) & 3))) cell = 64;
-        }
-        if (cell == 0) {
-            if (STATS) bytes += 8;
-            if (!bit64(cw, child_bit((sx >> 4) & 3, (sy >> 4) & 3, (sz >> 4) & 3))) cell = 16;
-        }
-        if (cell == 0) {
-            // tile-level LOD (raymarch.wgsl:4672-4689)
-            if (f_lod && t_cur > p.tile_lod_t) {
-                if (STATS) bytes += 8;
-                uint32_t lm = 0u;
-                const uint32_t tlo = (uint32_t)tw, thi = (uint32_t)(tw >> 32);
-                int lin = -1;
-                if (tlo != 0u) lin = __ffs(tlo) - 1;
-                else if (thi != 0u) lin = 32 + __ffs(thi) - 1;
-                if (lin >= 0) {
-                    const int64_t rbi = (int64_t)((sx >> 4) * 4 + (lin & 3)) +
-                                        (int64_t)((sy >> 4) * 4 + ((lin >> 4) & 3)) * d.bx +
-                                        (int64_t)((sz >> 4) * 4 + ((lin >> 2) & 3)) * d.bx * d.by;
-                    if (STATS) bytes += 8;
-                    lm = brick_topmost<STATS>(w.mat + rbi * 64, ldg(w.occ + rbi), bytes);
-                }
-                if (lm != 0u && is_uniform_optimisable(lm)) {
-                    set_hit(d, s, la, lm, true, h);
-                    break;
-                }
-            }
-            if (f_lut) {
-                if (STATS) bytes += 1;
-                if (tum != 0u && is_uniform_optimisable(tum)) {
-                    set_hit(d, s, la, tum, true, h);
-                    break;
-                }
-            }
-            if (STATS) bytes += 8;
-            const int bx = sx >> 2, by = sy >> 2, bz = sz >> 2;
-            if (!bit64(tw, child_bit(bx & 3, by & 3, bz & 3))) {
-                cell = 4;
-            } else {
-                const int64_t bi = (int64_t)bx + (int64_t)by * d.bx + (int64_t)bz * d.bx * d.by;
-                // batch 2: brick occupancy + brick LUT byte
-                const uint64_t occ = ldg(w.occ + bi);
-                const uint32_t bum = f_lut ? (uint32_t)ldg(w.brick_uniform + bi) : 0u;
-                if (f_lut) {
-                    if (STATS) bytes += 1;
-                    if (bum != 0u && is_uniform_optimisable(bum)) {
-                        set_hit(d, s, la, bum, true, h);
-                        break;
-                    }
-                }
-                const uint8_t *mrow = w.mat + bi * 64;
-                bool lod_done = false;
-                if (f_lod && t_cur > p.lod_brick_t) {
-                    if (STATS) bytes += 8;
-                    if (occ == 0ull) {
-                        cell = 4;
-                        lod_done = true;
-                    } else {
-                        const uint32_t m = brick_topmost<STATS>(mrow, occ, bytes);
-                        if (!is_foliage(m)) {
-                            set_hit(d, s, la, m, true, h);
-                            break;
-                        }
-                    }
-                }
-                if (!lod_done) {
-                    const int vi = child_bit(sx - bx * 4, sy - by * 4, sz - bz * 4);
-                    if (STATS) bytes += 8;
-                    if (bit64(occ, vi)) {
-                        // batch 3: the material byte of a solid voxel
-                        const uint32_t m = ldg(mrow + vi);
-                        if (STATS) bytes += 1;
-                        if (resolves_cube(m)) {
-                            set_hit(d, s, la, m, false, h);
-                            break;
-                        }
-                    }
-                }
-            }
-        }
-        if (cell != 0) {
-            skip_to_cell(d, ro, cell, s, la);
-            t_cur = crossed_t(s, la);
-        } else {
-            dda_step(d, s, t_cur, la);
-        }
+    while (walk_step<FL, STATS, KIND_TRACE>(w, g, p, ro, k, h, bytes) == WALK_CONT) {
     }
-    h.steps = iters;
-    if (STATS) bytes += 0;
+    h.steps = k.iters;
 }
 
-// trace_any(), raymarch.wgsl:4345-4409 -- returns occluded.
+// trace_any() over one ray: returns occluded
 template <bool STATS>
 __device__ __forceinline__ bool trace_any_ray(const DevWorld &w, const VxTraceParams &p, Ro ro,
                                               float o0, float o1, float o2, float d0, float d1,
                                               float d2, float max_dist, uint32_t &steps,
                                               uint64_t &bytes) {
-    const Dims &d = w.d;
-    Dda s;
-    float t_cur;
-    uint32_t iters = 0;
+    const Geo g = geo_of(w.d);
+    Walk k;
+    Hit h;
     steps = 0;
-    if (!dda_init(d, ro, o0, o1, o2, d0, d1, d2, s, &t_cur)) return false;
-    int la = -1;
-    bool occluded = false;
-    for (int it = 0; it < p.any_max_iters; ++it) {
-        ++iters;
-        if (t_cur > max_dist) break;
-        if (out_of_window(d, s, ro)) break;
-        const int32_t sx = s.sx, sy = s.vy, sz = s.sz;
-        const int64_t li = (int64_t)(sx >> 8) + (int64_t)(sy >> 8) * d.lx +
-                           (int64_t)(sz >> 8) * d.lx * d.ly;
-        const int64_t ci = (int64_t)(sx >> 6) + (int64_t)(sy >> 6) * d.cx +
-                           (int64_t)(sz >> 6) * d.cx * d.cy;
-        const int64_t ti = (int64_t)(sx >> 4) + (int64_t)(sy >> 4) * d.tx +
-                           (int64_t)(sz >> 4) * d.tx * d.ty;
-        const uint64_t lw = ldg(w.l4_mask + li);
-        const uint64_t cw = ldg(w.chunk_mask + ci);
-        const uint64_t tw = ldg(w.tile_mask + ti);
-        int32_t cell = 0;
-        if (STATS) bytes += 8;
-        if (lw == 0ull) cell = 256;
-        else if (!bit64(lw, child_bit((sx >> 6) & 3, (sy >> 6) & 3, (sz >> 6) & 3))) cell = 64;
-        if (cell == 0) {
-            if (STATS) bytes += 8;
-            if (!bit64(cw, child_bit((sx >> 4) & 3, (sy >> 4) & 3, (sz >> 4) & 3))) cell = 16;
-        }
-        if (cell == 0) {
-            if (STATS) bytes += 8;
-            const int bx = sx >> 2, by = sy >> 2, bz = sz >> 2;
-            if (!bit64(tw, child_bit(bx & 3, by & 3, bz & 3))) {
-                cell = 4;
-            } else {
-                const int64_t bi = (int64_t)bx + (int64_t)by * d.bx + (int64_t)bz * d.bx * d.by;
-                const uint64_t occ = ldg(w.occ + bi);
-                const int vi = child_bit(sx - bx * 4, sy - by * 4, sz - bz * 4);
-                if (STATS) bytes += 8;
-                if (bit64(occ, vi)) {
-                    const uint32_t m = ldg(w.mat + bi * 64 + vi);
-                    if (STATS) bytes += 1;
-                    if (shadow_occludes(m)) {
-                        occluded = true;
-                        break;
-                    }
-                }
-            }
-        }
-        if (cell != 0) {
-            skip_to_cell(d, ro, cell, s, la);
-            t_cur = crossed_t(s, la);
-        } else {
-            dda_step(d, s, t_cur, la);
-        }
+    if (!walk_init(w.d, ro, KIND_ANY, p, o0, o1, o2, d0, d1, d2, max_dist, k)) return false;
+    int r;
+    while ((r = walk_step<0, STATS, KIND_ANY>(w, g, p, ro, k, h, bytes)) == WALK_CONT) {
     }
-    steps = iters;
-    return occluded;
+    steps = k.iters;
+    return r == WALK_HIT;
 }
 
-// trace_no_water(), raymarch.wgsl:3450-3532 (t_cur is not refreshed after
-// a skip there; reproduced).
+// trace_no_water() over one ray
 template <bool STATS>
 __device__ __forceinline__ void trace_no_water_ray(const DevWorld &w, const VxTraceParams &p,
                                                    Ro ro, float o0, float o1, float o2,
                                                    float d0, float d1, float d2, float t_cap,
                                                    Hit &h, uint64_t &bytes) {
-    const Dims &d = w.d;
+    const Geo g = geo_of(w.d);
     set_miss(h);
-    Dda s;
-    float t_cur;
-    uint32_t iters = 0;
-    if (!dda_init(d, ro, o0, o1, o2, d0, d1, d2, s, &t_cur)) {
+    Walk k;
+    if (!walk_init(w.d, ro, KIND_NO_WATER, p, o0, o1, o2, d0, d1, d2, t_cap, k)) {
         h.steps = 0;
         return;
     }
-    int la = -1;
-    for (int it = 0; it < p.max_iters; ++it) {
-        ++iters;
-        if (t_cur > t_cap) break;
-        if (out_of_window(d, s, ro)) break;
-        const int32_t sx = s.sx, sy = s.vy, sz = s.sz;
-        const int64_t li = (int64_t)(sx >> 8) + (int64_t)(sy >> 8) * d.lx +
-                           (int64_t)(sz >> 8) * d.lx * d.ly;
-        const int64_t ci = (int64_t)(sx >> 6) + (int64_t)(sy >> 6) * d.cx +
-                           (int64_t)(sz >> 6) * d.cx * d.cy;
-        const int64_t ti = (int64_t)(sx >> 4) + (int64_t)(sy >> 4) * d.tx +
-                           (int64_t)(sz >> 4) * d.tx * d.ty;
-        const uint64_t lw = ldg(w.l4_mask + li);
-        const uint64_t cw = ldg(w.chunk_mask + ci);
-        const uint64_t tw = ldg(w.tile_mask + ti);
-        int32_t cell = 0;
-        if (STATS) bytes += 8;
-        if (lw == 0ull) cell = 256;
-        else if (!bit64(lw, child_bit((sx >> 6) & 3, (sy >> 6) & 3, (sz >> 6) & 3))) cell = 64;
-        if (cell == 0) {
-            if (STATS) bytes += 8;
-            if (!bit64(cw, child_bit((sx >> 4) & 3, (sy >> 4) & 3, (sz >> 4) & 3))) cell = 16;
-        }
-        if (cell == 0) {
-            if (STATS) bytes += 8;
-            const int bx = sx >> 2, by = sy >> 2, bz = sz >> 2;
-            if (!bit64(tw, child_bit(bx & 3, by & 3, bz & 3))) {
-                cell = 4;
-            } else {
-                const int64_t bi = (int64_t)bx + (int64_t)by * d.bx + (int64_t)bz * d.bx * d.by;
-                const uint64_t occ = ldg(w.occ + bi);
-                const int vi = child_bit(sx - bx * 4, sy - by * 4, sz - bz * 4);
-                if (STATS) bytes += 8;
-                if (bit64(occ, vi)) {
-                    const uint32_t m = ldg(w.mat + bi * 64 + vi);
-                    if (STATS) bytes += 1;
-                    if (!is_transparent(m)) {
-                        set_hit(d, s, la, m, false, h);
-                        break;
-                    }
-                }
-            }
-        }
-        if (cell != 0) skip_to_cell(d, ro, cell, s, la);
-        else dda_step(d, s, t_cur, la);
+    while (walk_step<0, STATS, KIND_NO_WATER>(w, g, p, ro, k, h, bytes) == WALK_CONT) {
     }
-    h.steps = iters;
+    h.steps = k.iters;
 }
 
 // normalize with IEEE sqrt + divide
@@ -671,19 +676,15 @@ __global__ void __launch_bounds__(128) k_beam(FrameArgs fa, float *beam_out) {
 }
 
 // ------------------------------------------------------------- primary
-// One thread per pixel; a warp covers an 8x4 pixel tile, a 128-thread CTA a
-// 16x8 region, so the 32 rays of a warp share one beam cell and start
-// coherent.
-template <bool STATS>
-__global__ void __launch_bounds__(128) k_primary(FrameArgs fa) {
-    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    const uint32_t px = blockIdx.x * 16u + (warp & 1u) * 8u + (lane & 7u);
-    const uint32_t py = blockIdx.y * 8u + (warp >> 1) * 4u + (lane >> 3);
-    if (px >= fa.W || py >= fa.H) return;
+// Per-pixel work of cs_main's traversal part (raymarch.wgsl:576-631): ray
+// through the pixel centre, beam fast-forward, trace, t re-based to the
+// camera, then one shadow any-hit ray from the hit (raymarch.wgsl:3953-3994).
+template <uint32_t FL, bool STATS>
+__device__ __forceinline__ void primary_pixel(const FrameArgs &fa, uint32_t px, uint32_t py,
+                                              uint64_t &bytes, uint64_t &iters) {
     const VxCamera &c = fa.cam;
     const VxTraceParams &p = fa.ta.p;
     const Ro ro{fa.ta.ro[0], fa.ta.ro[1], fa.ta.ro[2]};
-    uint64_t bytes = 0;
     float dx, dy, dz;
     const float u = (((float)px + 0.5f) + c.jitter_x) / c.res_x;
     const float v = (((float)py + 0.5f) + c.jitter_y) / c.res_y;
@@ -699,16 +700,15 @@ __global__ void __launch_bounds__(128) k_primary(FrameArgs fa) {
         oz = c.origin[2] + dz * skip;
     }
     Hit h;
-    trace_ray<STATS>(fa.ta.w, p, ro, ox, oy, oz, dx, dy, dz, p.max_dist, h, bytes);
+    trace_ray<FL, STATS>(fa.ta.w, p, ro, ox, oy, oz, dx, dy, dz, p.max_dist, h, bytes);
     if (beam_on && (h.flags & 1u)) h.t = h.t + skip;
     const size_t idx = (size_t)py * fa.W + px;
     store_record(fa.rec + idx, h);
-    uint64_t iters = h.steps;
+    iters += h.steps;
     if (fa.shadow) {
-        VxShadowRecord sr;
-        sr.steps = 0; sr.occluded = 0; sr.traced = 0; sr.pad = 0;
+        uint32_t ssteps = 0, occ = 0, traced = 0;
         if ((p.flags & VX_F_SHADOW) && (h.flags & 1u)) {
-            // raymarch.wgsl:3953-3994: p_off = p_hit + n*0.001, cone jitter
+            // p_off = p_hit + n*0.001; golden-angle jitter in the sun cone
             const int ax = (int)(h.face >> 1);
             const float nv = (h.face & 1u) ? -1.0f : 1.0f;
             const float sox = (c.origin[0] + dx * h.t) + (ax == 0 ? nv : 0.0f) * 0.001f;
@@ -723,20 +723,157 @@ __global__ void __launch_bounds__(128) k_primary(FrameArgs fa) {
             float sdy = p.sun[1] + (p.sun_tangent[1] * cs + p.sun_bitangent[1] * sn) * radius;
             float sdz = p.sun[2] + (p.sun_tangent[2] * cs + p.sun_bitangent[2] * sn) * radius;
             normalize3(sdx, sdy, sdz);
-            uint32_t ssteps;
-            const bool occ = trace_any_ray<STATS>(fa.ta.w, p, ro, sox, soy, soz, sdx, sdy, sdz,
-                                                  p.shadow_max_dist, ssteps, bytes);
-            sr.steps = ssteps;
-            sr.occluded = occ ? 1 : 0;
-            sr.traced = 1;
+            occ = trace_any_ray<STATS>(fa.ta.w, p, ro, sox, soy, soz, sdx, sdy, sdz,
+                                       p.shadow_max_dist, ssteps, bytes) ? 1u : 0u;
+            traced = 1u;
             iters += ssteps;
         }
-        fa.shadow[idx] = sr;
+        reinterpret_cast<uint2 *>(fa.shadow)[idx] = make_uint2(ssteps, occ | (traced << 8));
     }
+}
+
+// Grid form: one thread per pixel; a warp covers an 8x4 pixel tile, a
+// 128-thread CTA a 16x8 region, so a warp's rays share one beam cell.
+template <uint32_t FL, bool STATS>
+__global__ void VX_FRAME_BOUNDS k_primary(FrameArgs fa) {
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint32_t px = blockIdx.x * 16u + (warp & 1u) * 8u + (lane & 7u);
+    const uint32_t py = blockIdx.y * 8u + (warp >> 1) * 4u + (lane >> 3);
+    if (px >= fa.W || py >= fa.H) return;
+    uint64_t bytes = 0, iters = 0;
+    primary_pixel<FL, STATS>(fa, px, py, bytes, iters);
     if (STATS) flush_stats(fa.stats, bytes, iters);
 }
 
+// Persistent form with per-lane refill: one wave of CTAs; every lane walks
+// one ray at a time and, the moment its ray ends, takes the next one -- its
+// own shadow ray after a primary hit, else the next pixel -- so no lane of a
+// warp idles while the others finish long rays.  Pixels are handed out in
+// 8x4 tiles (32 consecutive work items) so that lanes start coherent; a
+// warp-aggregated atomic on work[0] hands out items.  The last warp out
+// resets both counters (next item, warps done) for the next launch.
+template <uint32_t FL, bool STATS>
+__global__ void VX_FRAME_BOUNDS k_primary_refill(FrameArgs fa) {
+    constexpr uint32_t FULL = 0xFFFFFFFFu, IDLE = 0xFFFFFFFFu, DONE = 0xFFFFFFFEu;
+    const uint32_t lane = threadIdx.x & 31u;
+    const DevWorld &w = fa.ta.w;
+    const Geo g = geo_of(w.d);
+    const VxTraceParams &p = fa.ta.p;
+    const VxCamera &c = fa.cam;
+    const Ro ro{fa.ta.ro[0], fa.ta.ro[1], fa.ta.ro[2]};
+    const bool beam_on = (p.flags & VX_F_BEAM) != 0u;
+    const bool shadows_on = fa.shadow != nullptr && (p.flags & VX_F_SHADOW) != 0u;
+    const uint32_t tiles_x = (fa.W + 7u) / 8u;
+    const uint32_t total = tiles_x * ((fa.H + 3u) / 4u) * 32u;
+    uint64_t bytes = 0, iters_acc = 0;
+    Walk k;
+    Hit h;
+    uint32_t item = IDLE, px = 0, py = 0;
+    float skip = 0.0f;
+    for (;;) {
+        const bool need = item == IDLE;
+        const unsigned ask = __ballot_sync(FULL, need);
+        // refill in batches: a lane's set-up runs while the rest of the warp
+        // waits, so wait until enough lanes are idle (or no lane is walking)
+        const unsigned busy = __ballot_sync(FULL, item < DONE);
+        if (ask && ((uint32_t)__popc(ask) >= VX_REFILL_MIN || busy == 0u)) {
+            uint32_t base = 0;
+            if (lane == 0) base = atomicAdd(fa.work, (uint32_t)__popc(ask));
+            base = __shfl_sync(FULL, base, 0);
+            if (need) {
+                const uint32_t idx = base + (uint32_t)__popc(ask & ((1u << lane) - 1u));
+                if (idx >= total) {
+                    item = DONE;
+                } else {
+                    const uint32_t tile = idx >> 5, in = idx & 31u;
+                    px = (tile % tiles_x) * 8u + (in & 7u);
+                    py = (tile / tiles_x) * 4u + (in >> 3);
+                    if (px < fa.W && py < fa.H) {
+                        item = idx;
+                        float dx, dy, dz;
+                        const float u = (((float)px + 0.5f) + c.jitter_x) / c.res_x;
+                        const float v = (((float)py + 0.5f) + c.jitter_y) / c.res_y;
+                        ray_dir_uv(c, u, v, dx, dy, dz);
+                        float ox = c.origin[0], oy = c.origin[1], oz = c.origin[2];
+                        skip = 0.0f;
+                        if (beam_on) {
+                            const float bt = fa.beam[(size_t)(py >> 3) * fa.bw + (px >> 3)];
+                            skip = vmax(0.0f, bt - p.beam_margin);
+                            ox = c.origin[0] + dx * skip;
+                            oy = c.origin[1] + dy * skip;
+                            oz = c.origin[2] + dz * skip;
+                        }
+                        set_miss(h);
+                        if (!walk_init(w.d, ro, KIND_TRACE, p, ox, oy, oz, dx, dy, dz,
+                                       p.max_dist, k)) {
+                            // misses the window: empty record, no shadow ray
+                            h.steps = 0;
+                            const size_t pi = (size_t)py * fa.W + px;
+                            store_record(fa.rec + pi, h);
+                            if (fa.shadow) reinterpret_cast<uint2 *>(fa.shadow)[pi] = make_uint2(0u, 0u);
+                            item = IDLE;
+                        }
+                    }
+                    // else: a pad item beyond the frame edge; stays IDLE
+                }
+            }
+        }
+        if (__all_sync(FULL, item == DONE)) break;
+        if (item < DONE) {
+            const int r = walk_step<FL, STATS, -1>(w, g, p, ro, k, h, bytes);
+            if (r != WALK_CONT) {
+                const size_t pi = (size_t)py * fa.W + px;
+                iters_acc += k.iters;
+                if (k.kind == KIND_TRACE) {
+                    h.steps = k.iters;
+                    if (r == WALK_HIT && beam_on) h.t = h.t + skip;
+                    store_record(fa.rec + pi, h);
+                    item = IDLE;
+                    if (r == WALK_HIT && shadows_on) {
+                        // raymarch.wgsl:3953-3994: p_off = p_hit + n*0.001, cone jitter
+                        const int ax = (int)(h.face >> 1);
+                        const float nv = (h.face & 1u) ? -1.0f : 1.0f;
+                        const float sox = (c.origin[0] + k.s.dx * h.t) + (ax == 0 ? nv : 0.0f) * 0.001f;
+                        const float soy = (c.origin[1] + k.s.dy * h.t) + (ax == 1 ? nv : 0.0f) * 0.001f;
+                        const float soz = (c.origin[2] + k.s.dz * h.t) + (ax == 2 ? nv : 0.0f) * 0.001f;
+                        const float jit = ign((float)px, (float)py, p.frame);
+                        const float theta = jit * 2.39996323f;
+                        const float radius = p.cone_tan * sqrtf(jit);
+                        float sn, cs;
+                        sincos_series(theta, sn, cs);
+                        float sdx = p.sun[0] + (p.sun_tangent[0] * cs + p.sun_bitangent[0] * sn) * radius;
+                        float sdy = p.sun[1] + (p.sun_tangent[1] * cs + p.sun_bitangent[1] * sn) * radius;
+                        float sdz = p.sun[2] + (p.sun_tangent[2] * cs + p.sun_bitangent[2] * sn) * radius;
+                        normalize3(sdx, sdy, sdz);
+                        if (walk_init(w.d, ro, KIND_ANY, p, sox, soy, soz, sdx, sdy, sdz,
+                                      p.shadow_max_dist, k)) {
+                            item = 0u;  // keep walking: the shadow ray of this pixel
+                        } else {
+                            reinterpret_cast<uint2 *>(fa.shadow)[pi] = make_uint2(0u, 1u << 8);
+                        }
+                    } else if (fa.shadow) {
+                        reinterpret_cast<uint2 *>(fa.shadow)[pi] = make_uint2(0u, 0u);
+                    }
+                } else {
+                    reinterpret_cast<uint2 *>(fa.shadow)[pi] =
+                        make_uint2(k.iters, (r == WALK_HIT ? 1u : 0u) | (1u << 8));
+                    item = IDLE;
+                }
+            }
+        }
+    }
+    if (lane == 0) {
+        const uint32_t warps = gridDim.x * (blockDim.x >> 5);
+        if (atomicAdd(fa.work + 1, 1u) == warps - 1u) {
+            fa.work[0] = 0u;
+            fa.work[1] = 0u;
+        }
+    }
+    if (STATS) flush_stats(fa.stats, bytes, iters_acc);
+}
+
 // --------------------------------------------------------- generic rays
+template <uint32_t FL>
 __global__ void __launch_bounds__(128) k_trace_rays(TraceArgs ta, const VxRay *__restrict__ rays,
                                                     size_t n, VxHitRecord *out) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -757,7 +894,7 @@ __global__ void __launch_bounds__(128) k_trace_rays(TraceArgs ta, const VxRay *_
     } else if (kind == 2u) {
         trace_no_water_ray<false>(ta.w, ta.p, ro, a.x, a.y, a.z, a.w, b.x, b.y, b.z, h, bytes);
     } else {
-        trace_ray<false>(ta.w, ta.p, ro, a.x, a.y, a.z, a.w, b.x, b.y, b.z, h, bytes);
+        trace_ray<FL, false>(ta.w, ta.p, ro, a.x, a.y, a.z, a.w, b.x, b.y, b.z, h, bytes);
     }
     store_record(out + i, h);
 }
@@ -895,19 +1032,74 @@ cudaError_t launch_beam(const FrameArgs &fa, float *beam_out, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-cudaError_t launch_primary(const FrameArgs &fa, cudaStream_t s) {
-    dim3 block(128), grid((fa.W + 15) / 16, (fa.H + 7) / 8);
-    if (fa.stats) k_primary<true><<<grid, block, 0, s>>>(fa);
-    else k_primary<false><<<grid, block, 0, s>>>(fa);
-    return cudaGetLastError();
+// Method flags (L4 | LUT | LOD) -> the matching kernel instantiation.
+template <uint32_t FL, bool STATS>
+struct GridK {
+    static void *fn() { return reinterpret_cast<void *>(&k_primary<FL, STATS>); }
+};
+template <uint32_t FL, bool STATS>
+struct PersistK {
+    static void *fn() { return reinterpret_cast<void *>(&k_primary_refill<FL, STATS>); }
+};
+
+template <template <uint32_t, bool> class K, bool STATS>
+void *pick_kernel(uint32_t fl) {
+    switch (fl & 7u) {
+        case 0: return K<0, STATS>::fn();
+        case 1: return K<1, STATS>::fn();
+        case 2: return K<2, STATS>::fn();
+        case 3: return K<3, STATS>::fn();
+        case 4: return K<4, STATS>::fn();
+        case 5: return K<5, STATS>::fn();
+        case 6: return K<6, STATS>::fn();
+        default: return K<7, STATS>::fn();
+    }
 }
+
+cudaError_t launch_primary(const FrameArgs &fa, cudaStream_t s) {
+    const uint32_t fl = fa.ta.p.flags;
+    FrameArgs a = fa;
+    void *args[] = {&a};
+    if (fa.work) {
+        void *fn = fa.stats ? pick_kernel<PersistK, true>(fl) : pick_kernel<PersistK, false>(fl);
+        int dev = 0, sms = 0, per_sm = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 128, 0);
+        if (e != cudaSuccess) return e;
+        if (per_sm < 1) per_sm = 1;
+        return cudaLaunchKernel(fn, dim3((unsigned)(sms * per_sm)), dim3(128), args, 0, s);
+    }
+    void *fn = fa.stats ? pick_kernel<GridK, true>(fl) : pick_kernel<GridK, false>(fl);
+    return cudaLaunchKernel(fn, dim3((fa.W + 15) / 16, (fa.H + 7) / 8), dim3(128), args, 0, s);
+}
+
+template <uint32_t FL>
+struct TraceK {
+    static void *fn() { return reinterpret_cast<void *>(&k_trace_rays<FL>); }
+};
 
 cudaError_t launch_trace_rays(const TraceArgs &ta, const VxRay *rays, size_t n, VxHitRecord *out,
                               cudaStream_t s) {
     if (n == 0) return cudaSuccess;
     const unsigned blocks = (unsigned)((n + 127) / 128);
-    k_trace_rays<<<blocks, 128, 0, s>>>(ta, rays, n, out);
-    return cudaGetLastError();
+    void *fn;
+    switch (ta.p.flags & 7u) {
+        case 0: fn = TraceK<0>::fn(); break;
+        case 1: fn = TraceK<1>::fn(); break;
+        case 2: fn = TraceK<2>::fn(); break;
+        case 3: fn = TraceK<3>::fn(); break;
+        case 4: fn = TraceK<4>::fn(); break;
+        case 5: fn = TraceK<5>::fn(); break;
+        case 6: fn = TraceK<6>::fn(); break;
+        default: fn = TraceK<7>::fn(); break;
+    }
+    TraceArgs a = ta;
+    const VxRay *r = rays;
+    size_t nn = n;
+    VxHitRecord *o = out;
+    void *args[] = {&a, &r, &nn, &o};
+    return cudaLaunchKernel(fn, dim3(blocks), dim3(128), args, 0, s);
 }
 
 cudaError_t launch_raycast(const DevWorld &w, const int32_t origin[3], const float *cams,

@@ -96,6 +96,14 @@ class DeviceWorld:
         L.check(self._lib.vx_world_counts(self.handle, c))
         return tuple(int(x) for x in c)
 
+    def set_persistent(self, on: bool):
+        """Frame kernels as one persistent wave pulling pixel tiles, or one
+        CTA per 16x8 pixels (default); results are identical."""
+        t = L.VxTuning()
+        L.check(self._lib.vx_world_get_tuning(self.handle, C.byref(t)))
+        t.persistent = 1 if on else 0
+        L.check(self._lib.vx_world_set_tuning(self.handle, C.byref(t)))
+
     def upload(self, arrays: dict):
         a = {k: np.ascontiguousarray(arrays[k]) for k in ARRAY_NAMES}
         L.check(self._lib.vx_world_upload(self.handle, *[L.ptr(a[k]) for k in ARRAY_NAMES]))
