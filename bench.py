@@ -321,9 +321,12 @@ def run_ours(args, cfg):
         ow = po.World(*cfg.bricks, arrays=arrays)
         threads = os.cpu_count() or 1
         cval, rows, secs = cpu_sample(ow, cam, params, args.cpu_sample_seconds, threads)
+        what = ("the full frame" if rows >= H else
+                f"{rows} of {H} rows (every 64th row, rotating offsets)")
         cpu = {"value": round(cval, 3), "unit": UNIT, "cores": threads, "kind": "port",
-               "sample": f"{rows} of {H} rows (every 64th row, rotating) of the same frame, "
-                         f"{secs:.1f} s wall; oracle restatement of the reference traversal"}
+               "sample": f"{what} of the same frame incl. beam pre-pass and shadow rays, "
+                         f"{secs:.1f} s wall on {threads} threads; C restatement of the "
+                         "reference traversal (the Rust reference cannot be built here)"}
         del ow, arrays
 
     if rank == 0:

@@ -41,6 +41,8 @@ struct VxWorld {
     int32_t *pick_hit = nullptr;
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
     uint32_t *d_work = nullptr;      // persistent-schedule counters (self-resetting)
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t band_ev[8] = {};
     VxTuning tuning{0, {0, 0, 0, 0, 0, 0, 0}};
 };
 
@@ -57,6 +59,8 @@ namespace {
     } while (0)
 
 inline cudaStream_t as_stream(void *s) { return reinterpret_cast<cudaStream_t>(s); }
+
+constexpr uint32_t kBands = 8;  // row bands of the host-buffer frame path
 
 int use_device(VxWorld *w) {
     VX_CK(cudaSetDevice(w->device));
@@ -94,6 +98,9 @@ void free_world(VxWorld *w) {
     cudaFree(w->d_work);
     for (auto &e : w->ev)
         if (e) cudaEventDestroy(e);
+    for (auto &e : w->band_ev)
+        if (e) cudaEventDestroy(e);
+    if (w->copy_stream) cudaStreamDestroy(w->copy_stream);
     if (w->stream) cudaStreamDestroy(w->stream);
 }
 
@@ -119,6 +126,8 @@ vx::FrameArgs make_frame(VxWorld *w, const VxCamera *cam, const VxTraceParams *p
     fa.H = (uint32_t)cam->res_y;
     fa.bw = (fa.W + 7u) / 8u;
     fa.bh = (fa.H + 7u) / 8u;
+    fa.y0 = 0;
+    fa.y1 = fa.H;
     fa.work = w->tuning.persistent ? w->d_work : nullptr;
     return fa;
 }
@@ -529,11 +538,36 @@ int vx_render_primary_host(VxWorld *w, const VxCamera *cam, const VxTraceParams 
     if (rc != VX_OK) return rc;
     fa.rec = w->rec;
     fa.shadow = shadow_host ? w->sh : nullptr;
-    rc = run_frame(w, fa, w->stream);
-    if (rc != VX_OK) return rc;
-    VX_CK(cudaMemcpyAsync(rec_host, w->rec, n * sizeof(VxHitRecord), cudaMemcpyDeviceToHost, w->stream));
-    if (shadow_host)
-        VX_CK(cudaMemcpyAsync(shadow_host, w->sh, n * sizeof(VxShadowRecord), cudaMemcpyDeviceToHost, w->stream));
+    if (!w->copy_stream) {
+        VX_CK(cudaStreamCreateWithFlags(&w->copy_stream, cudaStreamNonBlocking));
+        for (auto &e : w->band_ev) VX_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    // Bands of rows: the copy of band b to the host overlaps the traversal of
+    // band b+1 (the grid form only; the persistent form renders in one go).
+    const uint32_t nb = fa.work ? 1u : kBands;
+    const uint32_t band = ((fa.H + nb - 1) / nb + 7u) & ~7u;
+    if (fa.ta.p.flags & VX_F_BEAM) {
+        rc = ensure(&w->beam, &w->beam_cap, (size_t)fa.bw * fa.bh);
+        if (rc != VX_OK) return rc;
+        fa.beam = w->beam;
+        VX_CK(vx::launch_beam(fa, w->beam, w->stream));
+    }
+    for (uint32_t b = 0; b < nb; ++b) {
+        fa.y0 = std::min(fa.H, b * band);
+        fa.y1 = std::min(fa.H, (b + 1) * band);
+        if (fa.work) fa.y0 = 0, fa.y1 = fa.H;
+        if (fa.y1 <= fa.y0) break;
+        VX_CK(vx::launch_primary(fa, w->stream));
+        VX_CK(cudaEventRecord(w->band_ev[b], w->stream));
+        VX_CK(cudaStreamWaitEvent(w->copy_stream, w->band_ev[b], 0));
+        const size_t r0 = (size_t)fa.y0 * fa.W, rn = (size_t)(fa.y1 - fa.y0) * fa.W;
+        VX_CK(cudaMemcpyAsync(rec_host + r0, w->rec + r0, rn * sizeof(VxHitRecord),
+                              cudaMemcpyDeviceToHost, w->copy_stream));
+        if (shadow_host)
+            VX_CK(cudaMemcpyAsync(shadow_host + r0, w->sh + r0, rn * sizeof(VxShadowRecord),
+                                  cudaMemcpyDeviceToHost, w->copy_stream));
+    }
+    VX_CK(cudaStreamSynchronize(w->copy_stream));
     VX_CK(cudaStreamSynchronize(w->stream));
     return VX_OK;
 }

@@ -62,6 +62,7 @@ struct FrameArgs {
     VxCamera cam;
     const float *beam;        // beam depth (bw*bh) or nullptr
     uint32_t W, H, bw, bh;
+    uint32_t y0, y1;            // rows [y0, y1) of this launch (grid form)
     VxHitRecord *rec;
     VxShadowRecord *shadow;
     unsigned long long *stats;  // [bytes, iters] or nullptr

@@ -96,6 +96,8 @@ extern "C" int vx_render_primary_noalloc(const VxWorldView *view, const VxCamera
     fa.H = (uint32_t)cam->res_y;
     fa.bw = (fa.W + 7u) / 8u;
     fa.bh = (fa.H + 7u) / 8u;
+    fa.y0 = 0;
+    fa.y1 = fa.H;
     if ((p->flags & VX_F_BEAM) && (size_t)fa.bw * fa.bh > kMaxBeamCells) {
         vx::set_error("vx_render_primary_noalloc: frame too large for the static beam scratch "
                       "(at most 129600 beam cells, e.g. 3840x2160); use vx_render_primary");

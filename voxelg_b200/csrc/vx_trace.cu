@@ -738,8 +738,8 @@ template <uint32_t FL, bool STATS>
 __global__ void VX_FRAME_BOUNDS k_primary(FrameArgs fa) {
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t px = blockIdx.x * 16u + (warp & 1u) * 8u + (lane & 7u);
-    const uint32_t py = blockIdx.y * 8u + (warp >> 1) * 4u + (lane >> 3);
-    if (px >= fa.W || py >= fa.H) return;
+    const uint32_t py = fa.y0 + blockIdx.y * 8u + (warp >> 1) * 4u + (lane >> 3);
+    if (px >= fa.W || py >= fa.y1) return;
     uint64_t bytes = 0, iters = 0;
     primary_pixel<FL, STATS>(fa, px, py, bytes, iters);
     if (STATS) flush_stats(fa.stats, bytes, iters);
@@ -1071,7 +1071,9 @@ cudaError_t launch_primary(const FrameArgs &fa, cudaStream_t s) {
         return cudaLaunchKernel(fn, dim3((unsigned)(sms * per_sm)), dim3(128), args, 0, s);
     }
     void *fn = fa.stats ? pick_kernel<GridK, true>(fl) : pick_kernel<GridK, false>(fl);
-    return cudaLaunchKernel(fn, dim3((fa.W + 15) / 16, (fa.H + 7) / 8), dim3(128), args, 0, s);
+    if (fa.y1 <= fa.y0) return cudaSuccess;
+    return cudaLaunchKernel(fn, dim3((fa.W + 15) / 16, (fa.y1 - fa.y0 + 7) / 8), dim3(128), args,
+                            0, s);
 }
 
 template <uint32_t FL>
