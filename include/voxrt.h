@@ -230,6 +230,26 @@ int vx_render_primary_timed(VxWorld *w, const VxCamera *cam, const VxTraceParams
                             VxHitRecord *rec_dev, VxShadowRecord *shadow_dev, void *stream,
                             float ms[2]);
 
+/* ---- temporal differential (src/temporal.rs, src/app.rs:643-767) ------- */
+/* Screen tiles are 8x8 pixels, tiles_w = ceil(W/8); bit ti of the u32 word
+ * ti/32 of a tile mask marks tile ti dirty (the tile_dirty buffer of
+ * shaders/raymarch.wgsl:580-587). */
+/* OR into tile_mask_dev the tiles covered by the world AABBs of the given
+ * slot bricks as seen by cam (temporal::project_brick_to_tiles,
+ * src/temporal.rs:16-111).  brick_idx is a host array; returns after the
+ * launch is enqueued and the indices are consumed. */
+int vx_project_dirty(VxWorld *w, const VxCamera *cam, const uint32_t *brick_idx, size_t n,
+                     uint32_t *tile_mask_dev, void *stream);
+/* OR in the rotating hash-scattered refresh set of src/app.rs:706-725 for a
+ * width x height frame: tiles with hash % spread == phase. */
+int vx_tile_refresh(uint32_t width, uint32_t height, uint32_t spread, uint32_t phase,
+                    uint32_t *tile_mask_dev, void *stream);
+/* vx_render_primary with cs_main's tile gate: pixels of tiles whose bit is
+ * clear are not traced and their records are left as they were. */
+int vx_render_primary_gated(VxWorld *w, const VxCamera *cam, const VxTraceParams *p,
+                            const uint32_t *tile_mask_dev, VxHitRecord *rec_dev,
+                            VxShadowRecord *shadow_dev, void *stream);
+
 /* ---- frames for callers that cannot allocate ------------------------------
  * No counterpart in the reference: an addition for hosts that reserve all
  * device memory up front and forbid (or cannot afford) cudaMalloc once

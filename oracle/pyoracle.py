@@ -101,6 +101,8 @@ def load():
                                          C.c_int, P(OrStats)]),
         "or_render_rows": (None, [P(OrWorld), P(OrCamera), P(OrParams), vp, C.c_uint32,
                                   C.c_uint32, vp, vp, P(OrStats)]),
+        "or_project_brick_to_tiles": (None, [P(OrWorld), P(OrCamera), C.c_uint32, vp]),
+        "or_refresh_tiles": (None, [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, vp]),
         "or_render_row_set": (C.c_double, [P(OrWorld), P(OrCamera), P(OrParams), vp, C.c_uint32,
                                            C.c_uint32, vp, vp, C.c_int, P(OrStats)]),
         "or_trace_batch": (C.c_double, [P(OrWorld), P(C.c_int32), vp, C.c_size_t, P(OrParams),
@@ -223,6 +225,22 @@ def render_row_set(world: World, cam, params, beam, stride, offset, threads=None
     rows = np.arange(offset, H, stride)
     idx = (rows[:, None] * W + np.arange(W)[None, :]).reshape(-1)
     return rec[idx], sh[idx], secs, st
+
+
+def project_dirty(world: World, cam, brick_idx, mask=None):
+    """temporal.rs:16-111 over a list of slot bricks -> u32 tile mask."""
+    cam = camera_from(cam)
+    W, H = int(cam.res_x), int(cam.res_y)
+    if mask is None:
+        mask = np.zeros((((W + 7) // 8) * ((H + 7) // 8) + 31) // 32, np.uint32)
+    for bi in brick_idx:
+        load().or_project_brick_to_tiles(C.byref(world.c), C.byref(cam), int(bi), mask.ctypes.data)
+    return mask
+
+
+def refresh_tiles(W, H, spread, phase, mask):
+    load().or_refresh_tiles((W + 7) // 8, (H + 7) // 8, spread, phase, mask.ctypes.data)
+    return mask
 
 
 def beam_pass(world: World, cam):

@@ -925,6 +925,85 @@ void or_render_rows(const OrWorld *w, const OrCamera *c, const OrParams *p,
 }
 
 /* ------------------------------------------------------------------ */
+/* temporal tile gating (src/temporal.rs:16-111, src/app.rs:643-725)   */
+/* ------------------------------------------------------------------ */
+
+/* project_brick_to_tiles: the world AABB of slot brick bi (window corner
+ * c->world_origin; slot -> world fold as the toroidal storage implies) is
+ * projected through the camera and the covered 8x8 screen tiles are set in
+ * mask (tiles_w = ceil(W/8), bit ti of word ti>>5). */
+void or_project_brick_to_tiles(const OrWorld *w, const OrCamera *c, uint32_t bi, uint32_t *mask) {
+    Dims d = dims_of(w);
+    int32_t bx = (int32_t)(bi % (uint32_t)d.bx);
+    int32_t by = (int32_t)((bi / (uint32_t)d.bx) % (uint32_t)d.by);
+    int32_t bz = (int32_t)(bi / ((uint32_t)d.bx * (uint32_t)d.by));
+    int32_t wx = c->world_origin[0] + pos_mod(bx * 4 - c->world_origin[0], d.vx);
+    int32_t wy = by * 4;
+    int32_t wz = c->world_origin[2] + pos_mod(bz * 4 - c->world_origin[2], d.vz);
+    float base[3] = {(float)wx, (float)wy, (float)wz};
+    uint32_t W = (uint32_t)c->res_x, H = (uint32_t)c->res_y;
+    uint32_t tiles_w = (W + 7u) / 8u, tiles_h = (H + 7u) / 8u;
+    float tan_half = c->tan_half_fov;
+    float aspect = (float)W / (float)H;
+    float wf = (float)W, hf = (float)H;
+    int32_t min_x = INT32_MAX, min_y = INT32_MAX, max_x = INT32_MIN, max_y = INT32_MIN;
+    int any_visible = 0, any_behind = 0;
+    for (int ci = 0; ci < 8; ++ci) {
+        float corner[3] = {base[0] + (float)(ci & 1) * 4.0f, base[1] + (float)((ci >> 1) & 1) * 4.0f,
+                           base[2] + (float)((ci >> 2) & 1) * 4.0f};
+        float dv[3] = {corner[0] - c->origin[0], corner[1] - c->origin[1], corner[2] - c->origin[2]};
+        float z_cam = (dv[0] * c->forward[0] + dv[1] * c->forward[1]) + dv[2] * c->forward[2];
+        if (z_cam <= 0.1f) {
+            any_behind = 1;
+            continue;
+        }
+        float x_cam = (dv[0] * c->right[0] + dv[1] * c->right[1]) + dv[2] * c->right[2];
+        float y_cam = (dv[0] * c->up[0] + dv[1] * c->up[1]) + dv[2] * c->up[2];
+        float inv_z = 1.0f / (z_cam * tan_half);
+        float ndc_x = (x_cam * inv_z) / aspect;
+        float ndc_y = y_cam * inv_z;
+        int32_t px = f2i((ndc_x + 1.0f) * 0.5f * wf);
+        int32_t py = f2i((1.0f - ndc_y) * 0.5f * hf);
+        if (px < min_x) min_x = px;
+        if (py < min_y) min_y = py;
+        if (px > max_x) max_x = px;
+        if (py > max_y) max_y = py;
+        any_visible = 1;
+    }
+    if (!any_visible) return;
+    if (any_behind) {
+        min_x = 0; min_y = 0;
+        max_x = (int32_t)W - 1; max_y = (int32_t)H - 1;
+    }
+    if (max_x < 0 || max_y < 0 || min_x >= (int32_t)W || min_y >= (int32_t)H) return;
+    uint32_t tx_min = (uint32_t)(min_x > 0 ? min_x : 0) / 8u;
+    uint32_t ty_min = (uint32_t)(min_y > 0 ? min_y : 0) / 8u;
+    uint32_t tx_max = (uint32_t)(max_x < (int32_t)W - 1 ? max_x : (int32_t)W - 1) / 8u;
+    uint32_t ty_max = (uint32_t)(max_y < (int32_t)H - 1 ? max_y : (int32_t)H - 1) / 8u;
+    if (tx_max > tiles_w - 1u) tx_max = tiles_w - 1u;
+    if (ty_max > tiles_h - 1u) ty_max = tiles_h - 1u;
+    for (uint32_t ty = ty_min; ty <= ty_max; ++ty)
+        for (uint32_t tx = tx_min; tx <= tx_max; ++tx) {
+            uint32_t idx = ty * tiles_w + tx;
+            mask[idx >> 5] |= 1u << (idx & 31u);
+        }
+}
+
+/* The rotating, hash-scattered animation refresh (src/app.rs:706-725): tile
+ * (tx, ty) is refreshed when ((tx*73856093 ^ ty*19349663) * 2654435761 >> 8)
+ * % spread == phase, in 64-bit wrapping arithmetic (usize on the
+ * reference's 64-bit targets). */
+void or_refresh_tiles(uint32_t tiles_w, uint32_t tiles_h, uint32_t spread, uint32_t phase,
+                      uint32_t *mask) {
+    if (spread == 0) return;
+    for (uint32_t ti = 0; ti < tiles_w * tiles_h; ++ti) {
+        uint64_t tx = ti % tiles_w, ty = ti / tiles_w;
+        uint64_t h = ((tx * 73856093ull) ^ (ty * 19349663ull)) * 2654435761ull;
+        if ((h >> 8) % spread == phase) mask[ti >> 5] |= 1u << (ti & 31u);
+    }
+}
+
+/* ------------------------------------------------------------------ */
 /* threading                                                           */
 /* ------------------------------------------------------------------ */
 static double now_s(void) {

@@ -183,6 +183,11 @@ double or_render_frame(const OrWorld *w, const OrCamera *c, const OrParams *p,
                        OrRecord *rec, OrShadow *sh, float *beam, int nthreads,
                        OrStats *st);
 
+/* Temporal tile gating: src/temporal.rs:16-111 and src/app.rs:706-725. */
+void or_project_brick_to_tiles(const OrWorld *w, const OrCamera *c, uint32_t bi, uint32_t *mask);
+void or_refresh_tiles(uint32_t tiles_w, uint32_t tiles_h, uint32_t spread, uint32_t phase,
+                      uint32_t *mask);
+
 /* Rows offset + k*stride of a frame on nthreads threads (bounded samples). */
 double or_render_row_set(const OrWorld *w, const OrCamera *c, const OrParams *p,
                          const float *beam, uint32_t stride, uint32_t offset, OrRecord *rec,

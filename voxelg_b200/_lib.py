@@ -115,6 +115,10 @@ SIGNATURES = [
                                           _P(C.c_uint64)]),
     ("vx_render_primary_timed", C.c_int, [_vp, _P(VxCamera), _P(VxTraceParams), _vp, _vp, _vp,
                                           _P(C.c_float)]),
+    ("vx_project_dirty", C.c_int, [_vp, _P(VxCamera), _vp, C.c_size_t, _vp, _vp]),
+    ("vx_tile_refresh", C.c_int, [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, _vp, _vp]),
+    ("vx_render_primary_gated", C.c_int, [_vp, _P(VxCamera), _P(VxTraceParams), _vp, _vp, _vp,
+                                          _vp]),
     ("vx_render_primary_noalloc", C.c_int, [_P(VxWorldView), _P(VxCamera), _P(VxTraceParams),
                                             _vp, _vp, _vp]),
     ("vx_host_world_create", C.c_int, [C.c_int32, C.c_int32, C.c_int32, _P(_vp)]),

@@ -42,6 +42,8 @@ struct VxWorld {
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
     uint32_t *d_work = nullptr;      // persistent-schedule counters (self-resetting)
     cudaStream_t copy_stream = nullptr;
+    uint32_t *d_gate_idx = nullptr;  // staging of vx_project_dirty
+    size_t gate_cap = 0;
     cudaEvent_t band_ev[8] = {};
     VxTuning tuning{0, {0, 0, 0, 0, 0, 0, 0}};
 };
@@ -96,6 +98,7 @@ void free_world(VxWorld *w) {
     cudaFree(w->pick_out);
     cudaFree(w->pick_hit);
     cudaFree(w->d_work);
+    cudaFree(w->d_gate_idx);
     for (auto &e : w->ev)
         if (e) cudaEventDestroy(e);
     for (auto &e : w->band_ev)
@@ -516,6 +519,70 @@ int vx_render_primary(VxWorld *w, const VxCamera *cam, const VxTraceParams *p,
     vx::FrameArgs fa = make_frame(w, cam, p);
     fa.rec = rec_dev;
     fa.shadow = shadow_dev;
+    return run_frame(w, fa, as_stream(stream));
+}
+
+int vx_project_dirty(VxWorld *w, const VxCamera *cam, const uint32_t *brick_idx, size_t n,
+                     uint32_t *tile_mask_dev, void *stream) {
+    if (!w || !tile_mask_dev || (n > 0 && !brick_idx)) {
+        vx::set_error("vx_project_dirty: null argument");
+        return VX_ERR_INVALID;
+    }
+    int rc = check_frame(cam);
+    if (rc != VX_OK) return rc;
+    for (size_t i = 0; i < n; ++i)
+        if ((int64_t)brick_idx[i] >= w->dw.d.n_bricks) {
+            vx::set_error("vx_project_dirty: brick index out of range");
+            return VX_ERR_INVALID;
+        }
+    if (n == 0) return VX_OK;
+    rc = use_device(w);
+    if (rc != VX_OK) return rc;
+    std::lock_guard<std::mutex> lk(w->mu);
+    cudaStream_t s = as_stream(stream);
+    if (w->gate_cap < n) VX_CK(cudaStreamSynchronize(s));
+    rc = ensure(&w->d_gate_idx, &w->gate_cap, n);
+    if (rc != VX_OK) return rc;
+    VX_CK(cudaMemcpyAsync(w->d_gate_idx, brick_idx, n * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+    VX_CK(vx::launch_project_dirty(w->dw, *cam, w->d_gate_idx, n, tile_mask_dev, s));
+    // the staging buffer is reused by the next call: finish this one first
+    VX_CK(cudaStreamSynchronize(s));
+    return VX_OK;
+}
+
+int vx_tile_refresh(uint32_t width, uint32_t height, uint32_t spread, uint32_t phase,
+                    uint32_t *tile_mask_dev, void *stream) {
+    if (!tile_mask_dev || width == 0 || height == 0 || width > 32768 || height > 32768 ||
+        (spread > 0 && phase >= spread)) {
+        vx::set_error("vx_tile_refresh: invalid argument");
+        return VX_ERR_INVALID;
+    }
+    VX_CK(vx::launch_refresh_tiles((width + 7) / 8, (height + 7) / 8, spread, phase,
+                                   tile_mask_dev, as_stream(stream)));
+    return VX_OK;
+}
+
+int vx_render_primary_gated(VxWorld *w, const VxCamera *cam, const VxTraceParams *p,
+                            const uint32_t *tile_mask_dev, VxHitRecord *rec_dev,
+                            VxShadowRecord *shadow_dev, void *stream) {
+    if (!w || !rec_dev || !tile_mask_dev) {
+        vx::set_error("vx_render_primary_gated: null argument");
+        return VX_ERR_INVALID;
+    }
+    int rc = check_frame(cam);
+    if (rc == VX_OK) rc = check_params(p);
+    if (rc != VX_OK) return rc;
+    if ((reinterpret_cast<uintptr_t>(rec_dev) & 7u) || (reinterpret_cast<uintptr_t>(shadow_dev) & 7u)) {
+        vx::set_error("vx_render_primary_gated: records must be 8-byte aligned");
+        return VX_ERR_INVALID;
+    }
+    rc = use_device(w);
+    if (rc != VX_OK) return rc;
+    std::lock_guard<std::mutex> lk(w->mu);
+    vx::FrameArgs fa = make_frame(w, cam, p);
+    fa.rec = rec_dev;
+    fa.shadow = shadow_dev;
+    fa.tile_gate = tile_mask_dev;
     return run_frame(w, fa, as_stream(stream));
 }
 

@@ -67,6 +67,7 @@ struct FrameArgs {
     VxShadowRecord *shadow;
     unsigned long long *stats;  // [bytes, iters] or nullptr
     uint32_t *work;             // persistent schedule: {next tile, warps done}, or nullptr
+    const uint32_t *tile_gate;  // dirty 8x8-tile bits (cs_main gate) or nullptr = all
 };
 
 // ---- kernel launchers (vx_trace.cu / vx_world.cu) ----
@@ -77,6 +78,11 @@ cudaError_t launch_trace_rays(const TraceArgs &ta, const VxRay *rays, size_t n, 
 cudaError_t launch_raycast(const DevWorld &w, const int32_t origin[3], const float *cams,
                            const float *dirs, size_t n, VxPickHit *out, int32_t *hit,
                            cudaStream_t s);
+
+cudaError_t launch_project_dirty(const DevWorld &w, const VxCamera &cam, const uint32_t *idx,
+                                 size_t n, uint32_t *mask, cudaStream_t s);
+cudaError_t launch_refresh_tiles(uint32_t tiles_w, uint32_t tiles_h, uint32_t spread,
+                                 uint32_t phase, uint32_t *mask, cudaStream_t s);
 
 cudaError_t launch_bricks_from_aos(const DevWorld &w, const VxBrick *aos, int64_t first,
                                    int64_t count, cudaStream_t s);

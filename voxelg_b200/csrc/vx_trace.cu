@@ -27,584 +27,13 @@
 // byte the third (only on a solid voxel).
 #include <cuda_runtime.h>
 
+#include <climits>
+
 #include "vx_internal.h"
+#include "vx_walk.cuh"
 
 namespace vx {
 namespace {
-
-// ---------------------------------------------------------------- helpers
-__device__ __forceinline__ float vmin(float a, float b) { return (b < a) ? b : a; }
-__device__ __forceinline__ float vmax(float a, float b) { return (a < b) ? b : a; }
-__device__ __forceinline__ float clampf(float x, float lo, float hi) {
-    return vmin(vmax(x, lo), hi);
-}
-// f32 -> i32 toward zero, saturating (NaN -> 0), clamped to +-2^30.  The PTX
-// conversion (cvt.rzi.s32.f32) already saturates and maps NaN to 0; the clamp
-// narrows the range so later integer cell arithmetic cannot overflow.
-__device__ __forceinline__ int32_t f2i(float x) {
-    return min(max(__float2int_rz(x), -1073741824), 1073741824);
-}
-// common.wgsl:49-52
-__device__ __forceinline__ int32_t pos_mod(int32_t a, int32_t b) {
-    if (a >= 0) return a % b;
-    return (b - 1) - ((-1 - a) % b);
-}
-// v reduced into [0, n) where v is known congruent to the wanted slot; a
-// jump of a few cells needs at most two corrections, far jumps (only the
-// degenerate skip with no forward face) fall back to the division.
-__device__ __forceinline__ int32_t wrap_near(int32_t v, int32_t n) {
-    if (v < 0) {
-        v += n;
-        if (v < 0) v += n;
-    } else if (v >= n) {
-        v -= n;
-        if (v >= n) v -= n;
-    }
-    if ((uint32_t)v >= (uint32_t)n) v = pos_mod(v, n);
-    return v;
-}
-// common.wgsl:55-58
-__device__ __forceinline__ float safe_inv(float x) {
-    return (fabsf(x) < 1e-8f) ? 1e30f : 1.0f / x;
-}
-__device__ __forceinline__ int32_t sgn(float x) { return x > 0.0f ? 1 : (x < 0.0f ? -1 : 0); }
-__device__ __forceinline__ float fractf(float x) { return x - floorf(x); }
-__device__ __forceinline__ int child_bit(int lx, int ly, int lz) { return lx + lz * 4 + ly * 16; }
-__device__ __forceinline__ bool bit64(uint64_t w, int b) { return (w >> b) & 1ull; }
-
-template <typename T>
-__device__ __forceinline__ T ldg(const T *p) { return __ldg(p); }
-
-#ifndef VX_MIN_BLOCKS
-#define VX_MIN_BLOCKS 0
-#endif
-// Idle lanes a warp of the refill kernel waits for before it hands out new
-// pixels (32 = refill only when the whole warp is idle).
-#ifndef VX_REFILL_MIN
-#define VX_REFILL_MIN 16
-#endif
-#if VX_MIN_BLOCKS > 0
-#define VX_FRAME_BOUNDS __launch_bounds__(128, VX_MIN_BLOCKS)
-#else
-#define VX_FRAME_BOUNDS __launch_bounds__(128)
-#endif
-
-// Materials (src/voxel.rs:100-157, raymarch.wgsl:875-920)
-__device__ __forceinline__ bool is_water(uint32_t m) { return m >= 5u && m <= 12u; }
-__device__ __forceinline__ bool is_transparent(uint32_t m) { return is_water(m) || m == 18u; }
-__device__ __forceinline__ bool is_decoration(uint32_t m) {
-    return m == 30u || m == 31u || m == 33u || m == 34u || m == 35u || m == 36u || m == 37u;
-}
-__device__ __forceinline__ bool is_foliage(uint32_t m) {
-    return m == 14u || m == 25u || m == 26u || m == 27u || is_decoration(m);
-}
-__device__ __forceinline__ bool is_uniform_optimisable(uint32_t m) {
-    return !is_foliage(m) && !is_transparent(m);
-}
-// resolves_as_opaque_cube beyond both sub-voxel radii (raymarch.wgsl:4541)
-__device__ __forceinline__ bool resolves_cube(uint32_t m) { return !is_decoration(m); }
-// shadow_voxel_occludes far branch (raymarch.wgsl:4314-4343)
-__device__ __forceinline__ bool shadow_occludes(uint32_t m) {
-    return !(m == 33u || m == 35u || is_decoration(m));
-}
-
-// ------------------------------------------------------------- DDA state
-struct Dda {
-    float ox, oy, oz;      // origin rebased to the window corner
-    float dx, dy, dz;
-    float ix, iy, iz;      // safe_inv(dir)
-    float mx, my, mz;      // t_max
-    int32_t vx, vy, vz;    // voxel, absolute world coords
-    int32_t sx, sz;        // toroidal slot x/z (slot y == vy)
-    int32_t stx, sty, stz; // step
-};
-
-struct Ro {
-    int32_t x, y, z;
-};
-
-// dda_init, raymarch.wgsl:3369-3411.  Returns t_enter via *te.
-__device__ __forceinline__ bool dda_init(const Dims &d, Ro ro, float o0, float o1, float o2,
-                                         float d0, float d1, float d2, Dda &s, float *te) {
-    const float fx = (float)d.vx, fy = (float)d.vy, fz = (float)d.vz;
-    s.ox = o0 - (float)ro.x;
-    s.oy = o1 - (float)ro.y;
-    s.oz = o2 - (float)ro.z;
-    s.dx = d0; s.dy = d1; s.dz = d2;
-    s.ix = safe_inv(d0);
-    s.iy = safe_inv(d1);
-    s.iz = safe_inv(d2);
-    float t0x = (0.0f - s.ox) * s.ix, t1x = (fx - s.ox) * s.ix;
-    float t0y = (0.0f - s.oy) * s.iy, t1y = (fy - s.oy) * s.iy;
-    float t0z = (0.0f - s.oz) * s.iz, t1z = (fz - s.oz) * s.iz;
-    float tmnx = vmin(t0x, t1x), tmxx = vmax(t0x, t1x);
-    float tmny = vmin(t0y, t1y), tmxy = vmax(t0y, t1y);
-    float tmnz = vmin(t0z, t1z), tmxz = vmax(t0z, t1z);
-    float t_enter = vmax(vmax(tmnx, tmny), vmax(tmnz, 0.0f));
-    float t_exit = vmin(vmin(tmxx, tmxy), tmxz);
-    *te = t_enter;
-    if (t_enter >= t_exit || t_exit < 0.0f) return false;
-    const float tb = t_enter + 1e-3f;
-    float px = clampf(s.ox + d0 * tb, 0.01f, fx - 0.01f);
-    float py = clampf(s.oy + d1 * tb, 0.01f, fy - 0.01f);
-    float pz = clampf(s.oz + d2 * tb, 0.01f, fz - 0.01f);
-    s.stx = sgn(d0); s.sty = sgn(d1); s.stz = sgn(d2);
-    int32_t lx = f2i(floorf(px)), ly = f2i(floorf(py)), lz = f2i(floorf(pz));
-    s.vx = lx + ro.x; s.vy = ly + ro.y; s.vz = lz + ro.z;
-    s.mx = s.stx > 0 ? ((float)(lx + 1) - s.ox) * s.ix : ((float)lx - s.ox) * s.ix;
-    s.my = s.sty > 0 ? ((float)(ly + 1) - s.oy) * s.iy : ((float)ly - s.oy) * s.iy;
-    s.mz = s.stz > 0 ? ((float)(lz + 1) - s.oz) * s.iz : ((float)lz - s.oz) * s.iz;
-    s.sx = pos_mod(s.vx, d.vx);
-    s.sz = pos_mod(s.vz, d.vz);
-    return true;
-}
-
-// Entry axis + t when a ray hits in its very first cell (last_axis == -1):
-// recomputes tmin3/t_enter exactly as dda_init did (raymarch.wgsl:3335-3340).
-__device__ __forceinline__ void first_cell_entry(const Dims &d, const Dda &s, int *ax,
-                                                 float *t) {
-    float t0x = (0.0f - s.ox) * s.ix, t1x = ((float)d.vx - s.ox) * s.ix;
-    float t0y = (0.0f - s.oy) * s.iy, t1y = ((float)d.vy - s.oy) * s.iy;
-    float t0z = (0.0f - s.oz) * s.iz, t1z = ((float)d.vz - s.oz) * s.iz;
-    float a = vmin(t0x, t1x), b = vmin(t0y, t1y), c = vmin(t0z, t1z);
-    *t = vmax(vmax(a, b), vmax(c, 0.0f));
-    if (a >= b && a >= c) *ax = 0;
-    else if (b >= c) *ax = 1;
-    else *ax = 2;
-}
-
-// dda_step, raymarch.wgsl:3416-3448
-__device__ __forceinline__ void dda_step(const Dims &d, Dda &s, float &t_cur, int &la) {
-    if (s.mx < s.my && s.mx < s.mz) {
-        t_cur = s.mx;
-        s.vx += s.stx;
-        s.sx += s.stx;
-        if (s.sx >= d.vx) s.sx -= d.vx;
-        else if (s.sx < 0) s.sx += d.vx;
-        s.mx = s.mx + fabsf(s.ix);
-        la = 0;
-    } else if (s.my < s.mz) {
-        t_cur = s.my;
-        s.vy += s.sty;
-        s.my = s.my + fabsf(s.iy);
-        la = 1;
-    } else {
-        t_cur = s.mz;
-        s.vz += s.stz;
-        s.sz += s.stz;
-        if (s.sz >= d.vz) s.sz -= d.vz;
-        else if (s.sz < 0) s.sz += d.vz;
-        s.mz = s.mz + fabsf(s.iz);
-        la = 2;
-    }
-}
-
-// skip_to_cell, raymarch.wgsl:4807-4864.  cell is a power of two, so
-// v - pos_mod(v, cell) == v & ~(cell - 1) for every int v.
-__device__ __forceinline__ void skip_to_cell(const Dims &d, Ro ro, int32_t cell, Dda &s,
-                                             int &la) {
-    const int32_t hi = ~(cell - 1);
-    const int32_t cox = s.vx & hi, coy = s.vy & hi, coz = s.vz & hi;
-    // exit-face boundary per axis and the voxel just across it
-    const int32_t bx = s.stx > 0 ? cox + cell : cox, nbx = s.stx > 0 ? bx : cox - 1;
-    const int32_t by = s.sty > 0 ? coy + cell : coy, nby = s.sty > 0 ? by : coy - 1;
-    const int32_t bz = s.stz > 0 ? coz + cell : coz, nbz = s.stz > 0 ? bz : coz - 1;
-    const float tfx = ((float)(bx - ro.x) - s.ox) * s.ix;
-    const float tfy = ((float)(by - ro.y) - s.oy) * s.iy;
-    const float tfz = ((float)(bz - ro.z) - s.oz) * s.iz;
-    const float eps = 1e-6f;
-    float t_min = 1e30f;
-    int ax = 0;
-    if (s.stx != 0 && tfx > eps && tfx < t_min) { t_min = tfx; ax = 0; }
-    if (s.sty != 0 && tfy > eps && tfy < t_min) { t_min = tfy; ax = 1; }
-    if (s.stz != 0 && tfz > eps && tfz < t_min) { t_min = tfz; ax = 2; }
-    const float tb = t_min + 1e-3f;
-    int32_t nx = f2i(floorf(s.ox + s.dx * tb)) + ro.x;
-    int32_t ny = f2i(floorf(s.oy + s.dy * tb)) + ro.y;
-    int32_t nz = f2i(floorf(s.oz + s.dz * tb)) + ro.z;
-    nx = ax == 0 ? nbx : nx;
-    ny = ax == 1 ? nby : ny;
-    nz = ax == 2 ? nbz : nz;
-    // slot of the new voxel: old slot + displacement, folded (== pos_mod(n, dims))
-    s.sx = wrap_near(s.sx + (nx - s.vx), d.vx);
-    s.sz = wrap_near(s.sz + (nz - s.vz), d.vz);
-    s.vx = nx; s.vy = ny; s.vz = nz;
-    const int32_t lx = nx - ro.x, ly = ny - ro.y, lz = nz - ro.z;
-    s.mx = ((float)(s.stx > 0 ? lx + 1 : lx) - s.ox) * s.ix;
-    s.my = ((float)(s.sty > 0 ? ly + 1 : ly) - s.oy) * s.iy;
-    s.mz = ((float)(s.stz > 0 ? lz + 1 : lz) - s.oz) * s.iz;
-    la = ax;
-}
-
-// t of the face just crossed: t_max[la] - t_delta[la]
-__device__ __forceinline__ float crossed_t(const Dda &s, int la) {
-    return la == 0 ? s.mx - fabsf(s.ix) : (la == 1 ? s.my - fabsf(s.iy) : s.mz - fabsf(s.iz));
-}
-
-__device__ __forceinline__ bool out_of_window(const Dims &d, const Dda &s, Ro ro) {
-    return (uint32_t)(s.vx - ro.x) >= (uint32_t)d.vx || (uint32_t)(s.vy - ro.y) >= (uint32_t)d.vy ||
-           (uint32_t)(s.vz - ro.z) >= (uint32_t)d.vz;
-}
-
-struct Hit {
-    int32_t vx, vy, vz;
-    float t;
-    uint32_t steps;
-    uint32_t mat;
-    uint32_t face;    // 0xFF = miss
-    uint32_t flags;
-};
-
-__device__ __forceinline__ void set_miss(Hit &h) {
-    h.vx = h.vy = h.vz = 0;
-    h.t = 0.0f;
-    h.mat = 0;
-    h.face = 0xFFu;
-    h.flags = 0;
-}
-
-// entry_normal_and_t + last_axis_after_entry (raymarch.wgsl:3321-3342, :4800)
-__device__ __forceinline__ void set_hit(const Dims &d, const Dda &s, int la, uint32_t m,
-                                        bool early, Hit &h) {
-    int ax;
-    float t;
-    if (la >= 0) {
-        ax = la;
-        t = crossed_t(s, la);
-    } else {
-        first_cell_entry(d, s, &ax, &t);
-    }
-    const int32_t st = ax == 0 ? s.stx : (ax == 1 ? s.sty : s.stz);
-    h.vx = s.vx; h.vy = s.vy; h.vz = s.vz;
-    h.t = t;
-    h.mat = m;
-    h.face = (uint32_t)(2 * ax + (st > 0 ? 1 : 0));
-    h.flags = 1u | (early ? 2u : 0u);
-}
-
-// brick_topmost_material, raymarch.wgsl:253-295
-template <bool STATS>
-__device__ __forceinline__ uint32_t brick_topmost(const uint8_t *__restrict__ mrow, uint64_t occ,
-                                                  uint64_t &bytes) {
-    const uint32_t lo = (uint32_t)occ, hi = (uint32_t)(occ >> 32);
-    const uint32_t layer[4] = {(hi >> 16) & 0xFFFFu, hi & 0xFFFFu, (lo >> 16) & 0xFFFFu,
-                               lo & 0xFFFFu};
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        if (layer[i] != 0u) {
-            const int bit = __ffs(layer[i]) - 1;
-            const uint32_t m = ldg(mrow + (48 - 16 * i) + bit);
-            if (STATS) bytes += 1;
-            if (m != 35u) return m;
-        }
-    }
-    return (lo | hi) != 0u ? 35u : 0u;
-}
-
-// 32-bit strides of every level (all cell indices of a world that fits in
-// device memory are below 2^32; only the material row offset is widened).
-struct Geo {
-    uint32_t bx, bxy, tx, txy, cx, cxy, lx, lxy;
-};
-__device__ __forceinline__ Geo geo_of(const Dims &d) {
-    Geo g;
-    g.bx = (uint32_t)d.bx;
-    g.bxy = (uint32_t)(d.bx * d.by);
-    g.tx = (uint32_t)d.tx;
-    g.txy = (uint32_t)(d.tx * d.ty);
-    g.cx = (uint32_t)d.cx;
-    g.cxy = (uint32_t)(d.cx * d.cy);
-    g.lx = (uint32_t)d.lx;
-    g.lxy = (uint32_t)(d.lx * d.ly);
-    return g;
-}
-__device__ __forceinline__ uint32_t l4_index(const Geo &g, uint32_t sx, uint32_t sy, uint32_t sz) {
-    return (sx >> 8) + (sy >> 8) * g.lx + (sz >> 8) * g.lxy;
-}
-__device__ __forceinline__ uint32_t chunk_index(const Geo &g, uint32_t sx, uint32_t sy, uint32_t sz) {
-    return (sx >> 6) + (sy >> 6) * g.cx + (sz >> 6) * g.cxy;
-}
-__device__ __forceinline__ uint32_t tile_index(const Geo &g, uint32_t sx, uint32_t sy, uint32_t sz) {
-    return (sx >> 4) + (sy >> 4) * g.tx + (sz >> 4) * g.txy;
-}
-__device__ __forceinline__ uint32_t brick_index(const Geo &g, uint32_t bx, uint32_t by, uint32_t bz) {
-    return bx + by * g.bx + bz * g.bxy;
-}
-// child bit x + z*4 + y*16 of the level whose cell size is 1 << sh
-__device__ __forceinline__ int child_of(uint32_t sx, uint32_t sy, uint32_t sz, int sh) {
-    return (int)(((sx >> sh) & 3u) + ((sz >> sh) & 3u) * 4u + ((sy >> sh) & 3u) * 16u);
-}
-
-// ------------------------------------------------------------------ walk
-// One traversal = dda_init + repeated cascade iterations.  The three kinds
-// share the level cascade and differ only where the reference differs:
-//   KIND_TRACE    trace()           raymarch.wgsl:4600-4777 (L4 optional,
-//                                   LUT + LOD per method flags, cube rule)
-//   KIND_ANY      trace_any()       raymarch.wgsl:4345-4409 (occluder rule)
-//   KIND_NO_WATER trace_no_water()  raymarch.wgsl:3450-3532 (first
-//                                   non-transparent voxel; t_cur not
-//                                   refreshed after a skip)
-enum : uint32_t { KIND_TRACE = 0, KIND_ANY = 1, KIND_NO_WATER = 2 };
-
-struct Walk {
-    Dda s;
-    float t_cur;
-    float tmax;       // MAX_RAY_DIST / max_dist / t_cap of this ray
-    int la;           // last_axis
-    uint32_t iters;   // loop iterations begun
-    uint32_t cap;     // iteration cap (1024 / 768 / 1024)
-    uint32_t kind;
-};
-
-enum : int { WALK_CONT = 0, WALK_END = 1, WALK_HIT = 2 };
-
-__device__ __forceinline__ bool walk_init(const Dims &d, Ro ro, uint32_t kind,
-                                          const VxTraceParams &p, float o0, float o1, float o2,
-                                          float d0, float d1, float d2, float tmax, Walk &k) {
-    k.kind = kind;
-    k.tmax = tmax;
-    k.la = -1;
-    k.iters = 0;
-    k.cap = (uint32_t)(kind == KIND_ANY ? p.any_max_iters : p.max_iters);
-    return dda_init(d, ro, o0, o1, o2, d0, d1, d2, k.s, &k.t_cur);
-}
-
-// One cascade iteration.  On WALK_HIT the record fields of h are set (for
-// KIND_ANY only "occluded" matters).  FL holds VX_F_L4|VX_F_LUT|VX_F_LOD as
-// compile-time bits; KNOWN >= 0 fixes the kind at compile time.
-template <uint32_t FL, bool STATS, int KNOWN>
-__device__ __forceinline__ int walk_step(const DevWorld &w, const Geo &g, const VxTraceParams &p,
-                                         Ro ro, Walk &k, Hit &h, uint64_t &bytes) {
-    const uint32_t kind = KNOWN >= 0 ? (uint32_t)KNOWN : k.kind;
-    const bool is_trace = kind == KIND_TRACE;
-    const bool use_l4 = !is_trace || (FL & VX_F_L4) != 0u;
-    const bool f_lut = is_trace && (FL & VX_F_LUT) != 0u;
-    const bool f_lod = is_trace && (FL & VX_F_LOD) != 0u;
-    const Dims &d = w.d;
-    Dda &s = k.s;
-    if (k.iters >= k.cap) return WALK_END;
-    ++k.iters;
-    if (k.t_cur > k.tmax) return WALK_END;
-    if (out_of_window(d, s, ro)) return WALK_END;
-    const uint32_t sx = (uint32_t)s.sx, sy = (uint32_t)s.vy, sz = (uint32_t)s.sz;
-    const uint32_t ti = tile_index(g, sx, sy, sz);
-    // batch 1: every coarse word addressed by the slot coordinate
-    uint64_t lw = ~0ull;
-    if (use_l4) lw = ldg(w.l4_mask + l4_index(g, sx, sy, sz));
-    const uint64_t cw = ldg(w.chunk_mask + chunk_index(g, sx, sy, sz));
-    const uint64_t tw = ldg(w.tile_mask + ti);
-    const uint32_t tum = f_lut ? (uint32_t)ldg(w.tile_uniform + ti) : 0u;
-    int32_t cell = 0;
-    if (use_l4) {
-        if (STATS) bytes += 8;
-        if (lw == 0ull) cell = 256;
-        else if (!bit64(lw, child_of(sx, sy, sz, 6))) cell = 64;
-    }
-    if (cell == 0) {
-        if (STATS) bytes += 8;
-        if (!bit64(cw, child_of(sx, sy, sz, 4))) cell = 16;
-    }
-    if (cell == 0) {
-        // tile-level LOD (raymarch.wgsl:4672-4689)
-        if (f_lod && k.t_cur > p.tile_lod_t) {
-            if (STATS) bytes += 8;
-            uint32_t lm = 0u;
-            if (tw != 0ull) {
-                const int lin = __ffsll((long long)tw) - 1;
-                const uint32_t rbi = brick_index(g, (sx >> 4) * 4u + (uint32_t)(lin & 3),
-                                                 (sy >> 4) * 4u + (uint32_t)((lin >> 4) & 3),
-                                                 (sz >> 4) * 4u + (uint32_t)((lin >> 2) & 3));
-                if (STATS) bytes += 8;
-                lm = brick_topmost<STATS>(w.mat + (size_t)rbi * 64u, ldg(w.occ + rbi), bytes);
-            }
-            if (lm != 0u && is_uniform_optimisable(lm)) {
-                set_hit(d, s, k.la, lm, true, h);
-                return WALK_HIT;
-            }
-        }
-        if (f_lut) {
-            if (STATS) bytes += 1;
-            if (tum != 0u && is_uniform_optimisable(tum)) {
-                set_hit(d, s, k.la, tum, true, h);
-                return WALK_HIT;
-            }
-        }
-        if (STATS) bytes += 8;
-        if (!bit64(tw, child_of(sx, sy, sz, 2))) {
-            cell = 4;
-        } else {
-            const uint32_t bi = brick_index(g, sx >> 2, sy >> 2, sz >> 2);
-            // batch 2: brick occupancy + brick LUT byte
-            const uint64_t occ = ldg(w.occ + bi);
-            const uint32_t bum = f_lut ? (uint32_t)ldg(w.brick_uniform + bi) : 0u;
-            if (f_lut) {
-                if (STATS) bytes += 1;
-                if (bum != 0u && is_uniform_optimisable(bum)) {
-                    set_hit(d, s, k.la, bum, true, h);
-                    return WALK_HIT;
-                }
-            }
-            const uint8_t *mrow = w.mat + (size_t)bi * 64u;
-            bool lod_done = false;
-            if (f_lod && k.t_cur > p.lod_brick_t) {
-                if (STATS) bytes += 8;
-                if (occ == 0ull) {
-                    cell = 4;
-                    lod_done = true;
-                } else {
-                    const uint32_t m = brick_topmost<STATS>(mrow, occ, bytes);
-                    if (!is_foliage(m)) {
-                        set_hit(d, s, k.la, m, true, h);
-                        return WALK_HIT;
-                    }
-                }
-            }
-            if (!lod_done) {
-                const int vi = child_of(sx, sy, sz, 0);
-                if (STATS) bytes += 8;
-                if (bit64(occ, vi)) {
-                    // batch 3: the material byte of a solid voxel
-                    const uint32_t m = ldg(mrow + vi);
-                    if (STATS) bytes += 1;
-                    const bool stop = kind == KIND_TRACE ? resolves_cube(m)
-                                      : (kind == KIND_ANY ? shadow_occludes(m) : !is_transparent(m));
-                    if (stop) {
-                        if (kind != KIND_ANY) set_hit(d, s, k.la, m, false, h);
-                        return WALK_HIT;
-                    }
-                }
-            }
-        }
-    }
-    if (cell != 0) {
-        skip_to_cell(d, ro, cell, s, k.la);
-        if (kind != KIND_NO_WATER) k.t_cur = crossed_t(s, k.la);
-    } else {
-        dda_step(d, s, k.t_cur, k.la);
-    }
-    return WALK_CONT;
-}
-
-// trace() over one ray
-template <uint32_t FL, bool STATS>
-__device__ __forceinline__ void trace_ray(const DevWorld &w, const VxTraceParams &p, Ro ro,
-                                          float o0, float o1, float o2, float d0, float d1,
-                                          float d2, float max_dist, Hit &h, uint64_t &bytes) {
-    const Geo g = geo_of(w.d);
-    set_miss(h);
-    Walk k;
-    if (!walk_init(w.d, ro, KIND_TRACE, p, o0, o1, o2, d0, d1, d2, max_dist, k)) {
-        h.steps = 0;
-        return;
-    }
-    while (walk_step<FL, STATS, KIND_TRACE>(w, g, p, ro, k, h, bytes) == WALK_CONT) {
-    }
-    h.steps = k.iters;
-}
-
-// trace_any() over one ray: returns occluded
-template <bool STATS>
-__device__ __forceinline__ bool trace_any_ray(const DevWorld &w, const VxTraceParams &p, Ro ro,
-                                              float o0, float o1, float o2, float d0, float d1,
-                                              float d2, float max_dist, uint32_t &steps,
-                                              uint64_t &bytes) {
-    const Geo g = geo_of(w.d);
-    Walk k;
-    Hit h;
-    steps = 0;
-    if (!walk_init(w.d, ro, KIND_ANY, p, o0, o1, o2, d0, d1, d2, max_dist, k)) return false;
-    int r;
-    while ((r = walk_step<0, STATS, KIND_ANY>(w, g, p, ro, k, h, bytes)) == WALK_CONT) {
-    }
-    steps = k.iters;
-    return r == WALK_HIT;
-}
-
-// trace_no_water() over one ray
-template <bool STATS>
-__device__ __forceinline__ void trace_no_water_ray(const DevWorld &w, const VxTraceParams &p,
-                                                   Ro ro, float o0, float o1, float o2,
-                                                   float d0, float d1, float d2, float t_cap,
-                                                   Hit &h, uint64_t &bytes) {
-    const Geo g = geo_of(w.d);
-    set_miss(h);
-    Walk k;
-    if (!walk_init(w.d, ro, KIND_NO_WATER, p, o0, o1, o2, d0, d1, d2, t_cap, k)) {
-        h.steps = 0;
-        return;
-    }
-    while (walk_step<0, STATS, KIND_NO_WATER>(w, g, p, ro, k, h, bytes) == WALK_CONT) {
-    }
-    h.steps = k.iters;
-}
-
-// normalize with IEEE sqrt + divide
-__device__ __forceinline__ void normalize3(float &x, float &y, float &z) {
-    const float len = sqrtf((x * x + y * y) + z * z);
-    x = x / len;
-    y = y / len;
-    z = z / len;
-}
-
-// ray_dir_uv, raymarch.wgsl:430-438
-__device__ __forceinline__ void ray_dir_uv(const VxCamera &c, float u, float v, float &x,
-                                           float &y, float &z) {
-    const float ndc_x = u * 2.0f - 1.0f;
-    const float ndc_y = 1.0f - v * 2.0f;
-    const float aspect = c.res_x / c.res_y;
-    const float a = ndc_x * c.tan_half_fov * aspect;
-    const float b = ndc_y * c.tan_half_fov;
-    x = (c.forward[0] + c.right[0] * a) + c.up[0] * b;
-    y = (c.forward[1] + c.right[1] * a) + c.up[1] * b;
-    z = (c.forward[2] + c.right[2] * a) + c.up[2] * b;
-    normalize3(x, y, z);
-}
-
-// ign, raymarch.wgsl:394-396
-__device__ __forceinline__ float ign(float x, float y, float frame) {
-    const float a = x + frame * 5.588238f;
-    const float b = y + frame * 4.182857f;
-    return fractf(52.9829189f * fractf(0.06711056f * a + 0.00583715f * b));
-}
-
-// sin/cos by the Maclaurin series nested in x^2 (terms through x^17 / x^18),
-// evaluated in a fixed order so host and device agree bit for bit.
-__device__ __forceinline__ void sincos_series(float x, float &sn, float &cs) {
-    const float x2 = x * x;
-    float ps = 1.0f - x2 * 0.0036764706f;
-    ps = 1.0f - x2 * 0.0047619049f * ps;
-    ps = 1.0f - x2 * 0.0064102565f * ps;
-    ps = 1.0f - x2 * 0.0090909088f * ps;
-    ps = 1.0f - x2 * 0.013888889f * ps;
-    ps = 1.0f - x2 * 0.023809524f * ps;
-    ps = 1.0f - x2 * 0.050000001f * ps;
-    ps = 1.0f - x2 * 0.16666667f * ps;
-    sn = x * ps;
-    float pc = 1.0f - x2 * 0.0032679739f;
-    pc = 1.0f - x2 * 0.0041666669f * pc;
-    pc = 1.0f - x2 * 0.0054945056f * pc;
-    pc = 1.0f - x2 * 0.0075757578f * pc;
-    pc = 1.0f - x2 * 0.011111111f * pc;
-    pc = 1.0f - x2 * 0.017857144f * pc;
-    pc = 1.0f - x2 * 0.033333335f * pc;
-    pc = 1.0f - x2 * 0.083333336f * pc;
-    pc = 1.0f - x2 * 0.5f * pc;
-    cs = pc;
-}
-
-__device__ __forceinline__ void store_record(VxHitRecord *r, const Hit &h) {
-    // 24-byte record written as three 8-byte words (records are 8-aligned)
-    uint2 *q = reinterpret_cast<uint2 *>(r);
-    q[0] = make_uint2((uint32_t)h.vx, (uint32_t)h.vy);
-    q[1] = make_uint2((uint32_t)h.vz, h.face | (h.mat << 8) | (h.flags << 16));
-    q[2] = make_uint2(__float_as_uint(h.t), h.steps);
-}
-
-__device__ __forceinline__ void flush_stats(unsigned long long *stats, uint64_t bytes,
-                                            uint64_t iters) {
-    atomicAdd(stats + 0, (unsigned long long)bytes);
-    atomicAdd(stats + 1, (unsigned long long)iters);
-}
 
 // ------------------------------------------------------------------ beam
 // cs_beam + trace_first_tile, beam.wgsl:30-113 (world, non-rebased coords)
@@ -675,6 +104,13 @@ __global__ void __launch_bounds__(128) k_beam(FrameArgs fa, float *beam_out) {
     if (STATS) flush_stats(fa.stats, bytes, iters);
 }
 
+// cs_main's temporal-differential gate (raymarch.wgsl:580-587): is the 8x8
+// screen tile of this pixel marked dirty?
+__device__ __forceinline__ bool tile_dirty(const FrameArgs &fa, uint32_t px, uint32_t py) {
+    const uint32_t ti = (py >> 3) * ((fa.W + 7u) >> 3) + (px >> 3);
+    return (__ldg(fa.tile_gate + (ti >> 5)) >> (ti & 31u)) & 1u;
+}
+
 // ------------------------------------------------------------- primary
 // Per-pixel work of cs_main's traversal part (raymarch.wgsl:576-631): ray
 // through the pixel centre, beam fast-forward, trace, t re-based to the
@@ -740,6 +176,7 @@ __global__ void VX_FRAME_BOUNDS k_primary(FrameArgs fa) {
     const uint32_t px = blockIdx.x * 16u + (warp & 1u) * 8u + (lane & 7u);
     const uint32_t py = fa.y0 + blockIdx.y * 8u + (warp >> 1) * 4u + (lane >> 3);
     if (px >= fa.W || py >= fa.y1) return;
+    if (fa.tile_gate && !tile_dirty(fa, px, py)) return;  // raymarch.wgsl:580-587
     uint64_t bytes = 0, iters = 0;
     primary_pixel<FL, STATS>(fa, px, py, bytes, iters);
     if (STATS) flush_stats(fa.stats, bytes, iters);
@@ -788,7 +225,7 @@ __global__ void VX_FRAME_BOUNDS k_primary_refill(FrameArgs fa) {
                     const uint32_t tile = idx >> 5, in = idx & 31u;
                     px = (tile % tiles_x) * 8u + (in & 7u);
                     py = (tile / tiles_x) * 4u + (in >> 3);
-                    if (px < fa.W && py < fa.H) {
+                    if (px < fa.W && py < fa.H && (!fa.tile_gate || tile_dirty(fa, px, py))) {
                         item = idx;
                         float dx, dy, dz;
                         const float u = (((float)px + 0.5f) + c.jitter_x) / c.res_x;
@@ -1022,9 +459,96 @@ __global__ void __launch_bounds__(128) k_raycast(PickArgs pa, const float *__res
     hit[i] = found;
 }
 
+// ------------------------------------------------------- temporal gating
+// project_brick_to_tiles, src/temporal.rs:16-111: one thread per dirty
+// brick projects the world AABB of the brick and ORs the covered 8x8 tiles
+// into the mask.  The slot -> world fold follows the toroidal window at
+// camera.world_origin.
+__global__ void k_project_dirty(DevWorld w, VxCamera c, const uint32_t *__restrict__ idx,
+                                size_t n, uint32_t *mask) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const Dims &d = w.d;
+    const uint32_t bi = idx[i];
+    const int32_t bx = (int32_t)(bi % (uint32_t)d.bx);
+    const int32_t by = (int32_t)((bi / (uint32_t)d.bx) % (uint32_t)d.by);
+    const int32_t bz = (int32_t)(bi / ((uint32_t)d.bx * (uint32_t)d.by));
+    const float b0 = (float)(c.world_origin[0] + pos_mod(bx * 4 - c.world_origin[0], d.vx));
+    const float b1 = (float)(by * 4);
+    const float b2 = (float)(c.world_origin[2] + pos_mod(bz * 4 - c.world_origin[2], d.vz));
+    const uint32_t W = (uint32_t)c.res_x, H = (uint32_t)c.res_y;
+    const uint32_t tiles_w = (W + 7u) / 8u, tiles_h = (H + 7u) / 8u;
+    const float aspect = (float)W / (float)H;
+    const float wf = (float)W, hf = (float)H;
+    int32_t min_x = INT_MAX, min_y = INT_MAX, max_x = INT_MIN, max_y = INT_MIN;
+    bool any_visible = false, any_behind = false;
+#pragma unroll
+    for (int ci = 0; ci < 8; ++ci) {
+        const float dx = (b0 + (float)(ci & 1) * 4.0f) - c.origin[0];
+        const float dy = (b1 + (float)((ci >> 1) & 1) * 4.0f) - c.origin[1];
+        const float dz = (b2 + (float)((ci >> 2) & 1) * 4.0f) - c.origin[2];
+        const float z_cam = (dx * c.forward[0] + dy * c.forward[1]) + dz * c.forward[2];
+        if (z_cam <= 0.1f) {
+            any_behind = true;
+            continue;
+        }
+        const float x_cam = (dx * c.right[0] + dy * c.right[1]) + dz * c.right[2];
+        const float y_cam = (dx * c.up[0] + dy * c.up[1]) + dz * c.up[2];
+        const float inv_z = 1.0f / (z_cam * c.tan_half_fov);
+        const float ndc_x = (x_cam * inv_z) / aspect;
+        const float ndc_y = y_cam * inv_z;
+        const int32_t px = f2i((ndc_x + 1.0f) * 0.5f * wf);
+        const int32_t py = f2i((1.0f - ndc_y) * 0.5f * hf);
+        min_x = min(min_x, px);
+        min_y = min(min_y, py);
+        max_x = max(max_x, px);
+        max_y = max(max_y, py);
+        any_visible = true;
+    }
+    if (!any_visible) return;
+    if (any_behind) {
+        min_x = 0; min_y = 0;
+        max_x = (int32_t)W - 1; max_y = (int32_t)H - 1;
+    }
+    if (max_x < 0 || max_y < 0 || min_x >= (int32_t)W || min_y >= (int32_t)H) return;
+    const uint32_t tx0 = (uint32_t)max(min_x, 0) / 8u, ty0 = (uint32_t)max(min_y, 0) / 8u;
+    const uint32_t tx1 = min((uint32_t)min(max_x, (int32_t)W - 1) / 8u, tiles_w - 1u);
+    const uint32_t ty1 = min((uint32_t)min(max_y, (int32_t)H - 1) / 8u, tiles_h - 1u);
+    for (uint32_t ty = ty0; ty <= ty1; ++ty)
+        for (uint32_t tx = tx0; tx <= tx1; ++tx) {
+            const uint32_t t = ty * tiles_w + tx;
+            atomicOr(mask + (t >> 5), 1u << (t & 31u));
+        }
+}
+
+// Rotating hash-scattered refresh of src/app.rs:706-725 (64-bit wrapping
+// hash, as the reference's usize arithmetic on 64-bit targets).
+__global__ void k_refresh_tiles(uint32_t tiles_w, uint32_t tiles_h, uint32_t spread,
+                                uint32_t phase, uint32_t *mask) {
+    const uint32_t ti = blockIdx.x * blockDim.x + threadIdx.x;
+    if (ti >= tiles_w * tiles_h) return;
+    const uint64_t tx = ti % tiles_w, ty = ti / tiles_w;
+    const uint64_t h = ((tx * 73856093ull) ^ (ty * 19349663ull)) * 2654435761ull;
+    if ((h >> 8) % spread == phase) atomicOr(mask + (ti >> 5), 1u << (ti & 31u));
+}
+
 }  // namespace
 
 // ------------------------------------------------------------- launchers
+cudaError_t launch_project_dirty(const DevWorld &w, const VxCamera &cam, const uint32_t *idx,
+                                 size_t n, uint32_t *mask, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    k_project_dirty<<<(unsigned)((n + 127) / 128), 128, 0, s>>>(w, cam, idx, n, mask);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_refresh_tiles(uint32_t tiles_w, uint32_t tiles_h, uint32_t spread,
+                                 uint32_t phase, uint32_t *mask, cudaStream_t s) {
+    const uint32_t n = tiles_w * tiles_h;
+    if (n == 0 || spread == 0) return cudaSuccess;
+    k_refresh_tiles<<<(n + 127) / 128, 128, 0, s>>>(tiles_w, tiles_h, spread, phase, mask);
+    return cudaGetLastError();
+}
 cudaError_t launch_beam(const FrameArgs &fa, float *beam_out, cudaStream_t s) {
     dim3 block(128), grid((fa.bw + 127) / 128, fa.bh);
     if (fa.stats) k_beam<true><<<grid, block, 0, s>>>(fa, beam_out);

@@ -93,6 +93,38 @@ def render_primary(world: DeviceWorld, cam: L.VxCamera, params: L.VxTraceParams,
     return rec, shadow
 
 
+def tile_mask_words(width: int, height: int) -> int:
+    """u32 words of an 8x8-tile dirty mask (src/app.rs:643-648)."""
+    return ((width + 7) // 8 * ((height + 7) // 8) + 31) // 32
+
+
+def project_dirty(world: DeviceWorld, cam: L.VxCamera, brick_idx, mask, stream: int = 0):
+    """OR the screen tiles covered by the given slot bricks into mask (a CUDA
+    int32 tensor of tile_mask_words entries), temporal.rs:16-111."""
+    idx = np.ascontiguousarray(brick_idx, dtype=np.uint32)
+    L.check(L.load().vx_project_dirty(world.handle, C.byref(cam), C.c_void_p(L.ptr(idx)),
+                                      len(idx), C.c_void_p(mask.data_ptr()), C.c_void_p(stream)))
+    return mask
+
+
+def tile_refresh(width: int, height: int, spread: int, phase: int, mask, stream: int = 0):
+    """OR the rotating refresh set of src/app.rs:706-725 into mask."""
+    L.check(L.load().vx_tile_refresh(width, height, spread, phase, C.c_void_p(mask.data_ptr()),
+                                     C.c_void_p(stream)))
+    return mask
+
+
+def render_primary_gated(world: DeviceWorld, cam: L.VxCamera, params: L.VxTraceParams, mask,
+                         rec, shadow=None, stream: int = 0):
+    """Frame with cs_main's tile gate: only dirty tiles are re-traced into
+    rec/shadow (CUDA uint8 tensors holding the previous frame)."""
+    L.check(L.load().vx_render_primary_gated(
+        world.handle, C.byref(cam), C.byref(params), C.c_void_p(mask.data_ptr()),
+        C.c_void_p(rec.data_ptr()), C.c_void_p(shadow.data_ptr() if shadow is not None else 0),
+        C.c_void_p(stream)))
+    return rec, shadow
+
+
 def render_primary_host(world: DeviceWorld, cam: L.VxCamera, params: L.VxTraceParams,
                         rec_host: Optional[np.ndarray] = None,
                         shadow_host: Optional[np.ndarray] = None):
