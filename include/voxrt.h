@@ -230,6 +230,49 @@ int vx_render_primary_timed(VxWorld *w, const VxCamera *cam, const VxTraceParams
                             VxHitRecord *rec_dev, VxShadowRecord *shadow_dev, void *stream,
                             float ms[2]);
 
+/* ---- mixed ray queue (persistent, graph-captured, autotuned) -------------
+ * No single reference function: voxelG traces primary, shadow, GI-probe and
+ * picking rays in separate passes (raymarch.wgsl cs_main/trace_any,
+ * gi_probes.wgsl, raycast.rs).  Here one persistent launch walks a queue of
+ * VxRay of any mix of kinds (VxRay.kind low bits) and lengths (VxRay.tmax);
+ * a kind-0 ray flagged VX_RAY_SPAWN_SHADOW that hits continues with one
+ * shadow any-hit ray toward VxTraceParams.sun (jitter seeded by the ray
+ * index i: ign(i & 0xFFFF, i >> 16, frame)), recorded in shadow_dev[i].
+ * rays_dev must be 16-byte aligned; out_dev / shadow_dev 8-byte aligned; when
+ * shadow_dev is given every entry is written ({0,0} for rays without a
+ * shadow).  Records are identical for every tuning. */
+#define VX_RAY_SPAWN_SHADOW (1u << 8)
+
+typedef struct {
+    int32_t block_threads;  /* 64, 128 or 256                                  */
+    int32_t refill_min;     /* idle lanes a warp waits for before refilling, 1..32 */
+    int32_t ctas_per_sm;    /* 0 = as many as fit                              */
+    int32_t sort;           /* 1 = reorder by (kind, origin cell, direction) first */
+    int32_t reserved[4];
+} VxQueueTuning;
+
+int vx_queue_default_tuning(VxQueueTuning *t);
+int vx_queue_run(VxWorld *w, const int32_t origin[3], const VxRay *rays_dev, size_t n,
+                 const VxTraceParams *p, const VxQueueTuning *t, VxHitRecord *out_dev,
+                 VxShadowRecord *shadow_dev, void *stream);
+/* Time every candidate tuning on this queue (median of `reps` runs each),
+ * check that all give byte-identical outputs (VX_ERR_DEVICE if not), and
+ * return the fastest in *best with its time in *best_ms.  Synchronous; the
+ * outputs hold the last run's records. */
+int vx_queue_autotune(VxWorld *w, const int32_t origin[3], const VxRay *rays_dev, size_t n,
+                      const VxTraceParams *p, VxHitRecord *out_dev, VxShadowRecord *shadow_dev,
+                      int32_t reps, VxQueueTuning *best, float *best_ms);
+
+/* The queue launch captured once into a CUDA graph (scratch owned by the
+ * graph object); each vx_queue_graph_launch replays it on `stream`.  The
+ * pointers and parameters are fixed at capture. */
+typedef struct VxQueueGraph VxQueueGraph;
+int vx_queue_graph_create(VxWorld *w, const int32_t origin[3], const VxRay *rays_dev, size_t n,
+                          const VxTraceParams *p, const VxQueueTuning *t, VxHitRecord *out_dev,
+                          VxShadowRecord *shadow_dev, VxQueueGraph **out);
+int vx_queue_graph_launch(VxQueueGraph *g, void *stream);
+int vx_queue_graph_destroy(VxQueueGraph *g);
+
 /* ---- temporal differential (src/temporal.rs, src/app.rs:643-767) ------- */
 /* Screen tiles are 8x8 pixels, tiles_w = ceil(W/8); bit ti of the u32 word
  * ti/32 of a tile mask marks tile ti dirty (the tile_dirty buffer of

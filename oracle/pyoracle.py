@@ -106,7 +106,7 @@ def load():
         "or_render_row_set": (C.c_double, [P(OrWorld), P(OrCamera), P(OrParams), vp, C.c_uint32,
                                            C.c_uint32, vp, vp, C.c_int, P(OrStats)]),
         "or_trace_batch": (C.c_double, [P(OrWorld), P(C.c_int32), vp, C.c_size_t, P(OrParams),
-                                        vp, C.c_int, P(OrStats)]),
+                                        vp, vp, C.c_int, P(OrStats)]),
         "or_raycast_batch": (C.c_double, [P(OrWorld), P(C.c_int32), vp, vp, C.c_size_t, vp, vp,
                                           C.c_int]),
     }
@@ -252,14 +252,20 @@ def beam_pass(world: World, cam):
     return beam, st
 
 
-def trace_batch(world: World, rays: np.ndarray, params, origin=(0, 0, 0), threads=None):
+def trace_batch(world: World, rays: np.ndarray, params, origin=(0, 0, 0), threads=None,
+                shadows=False):
+    """The mixed queue on the CPU: (records, seconds, OrStats) or, with
+    shadows=True, (records, shadow records, seconds, OrStats)."""
     p = params_from(params)
     rays = np.ascontiguousarray(rays).view(RAY)
     out = np.zeros(len(rays), RECORD)
+    sh = np.zeros(len(rays), SHADOW) if shadows else None
     st = OrStats()
     secs = load().or_trace_batch(C.byref(world.c), i3(origin), rays.ctypes.data, len(rays),
-                                 C.byref(p), out.ctypes.data, threads or os.cpu_count() or 1,
-                                 C.byref(st))
+                                 C.byref(p), out.ctypes.data, sh.ctypes.data if shadows else None,
+                                 threads or os.cpu_count() or 1, C.byref(st))
+    if shadows:
+        return out, sh, secs, st
     return out, secs, st
 
 

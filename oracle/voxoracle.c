@@ -1115,30 +1115,60 @@ typedef struct {
     size_t a, b;
     const OrParams *p;
     OrRecord *out;
+    OrShadow *sh;
     OrStats st;
 } BatchJob;
 
+/* One queue ray: kind (low 2 bits) 1 trace_any, 2 trace_no_water, else
+ * trace; a trace ray flagged OR_RAY_SPAWN_SHADOW that hits is followed by its
+ * shadow ray (raymarch.wgsl:3953-3994) with the jitter seeded by the ray
+ * index: ign(i & 0xFFFF, i >> 16, frame). */
+static void queue_ray(const OrWorld *w, const int32_t *ro, const OrRay *r, size_t i,
+                      const OrParams *p, OrRecord *out, OrShadow *sh, OrStats *st) {
+    uint32_t kind = r->kind & 3u;
+    if (sh) memset(sh, 0, sizeof(*sh));
+    if (kind == 1u) {
+        uint32_t steps = 0;
+        int occ = or_trace_any(w, ro, r->org, r->dir, r->tmax, p, &steps, st);
+        miss_record(out);
+        out->flags = (uint8_t)(occ ? 1u : 0u);
+        out->steps = steps;
+        return;
+    }
+    if (kind == 2u) or_trace_no_water(w, ro, r->org, r->dir, r->tmax, p, out, st);
+    else or_trace(w, ro, r->org, r->dir, r->tmax, p, out, st);
+    if (sh && (r->kind & OR_RAY_SPAWN_SHADOW) && (out->flags & 1u)) {
+        int ax = out->face >> 1;
+        float nval = (out->face & 1) ? -1.0f : 1.0f;
+        float so[3], v[3], sd[3];
+        for (int k = 0; k < 3; ++k) {
+            float ph = r->org[k] + r->dir[k] * out->t;
+            so[k] = ph + ((k == ax) ? nval : 0.0f) * 0.001f;
+        }
+        float jit = or_ign((float)(uint32_t)(i & 0xFFFFu), (float)(uint32_t)(i >> 16), p->frame);
+        float theta = jit * 2.39996323f;
+        float radius = p->cone_tan * sqrtf(jit);
+        float sn, cs;
+        or_sincos(theta, &sn, &cs);
+        for (int k = 0; k < 3; ++k)
+            v[k] = p->sun[k] + (p->sun_tangent[k] * cs + p->sun_bitangent[k] * sn) * radius;
+        normalize3(v, sd);
+        uint32_t ssteps = 0;
+        sh->occluded = (uint8_t)or_trace_any(w, ro, so, sd, p->shadow_max_dist, p, &ssteps, st);
+        sh->steps = ssteps;
+        sh->traced = 1;
+    }
+}
+
 static void *batch_thread(void *arg) {
     BatchJob *j = (BatchJob *)arg;
-    for (size_t i = j->a; i < j->b; ++i) {
-        const OrRay *r = &j->rays[i];
-        if (r->kind == 1u) {
-            uint32_t steps = 0;
-            int occ = or_trace_any(j->w, j->ro, r->org, r->dir, r->tmax, j->p, &steps, &j->st);
-            miss_record(&j->out[i]);
-            j->out[i].flags = (uint8_t)(occ ? 1u : 0u);
-            j->out[i].steps = steps;
-        } else if (r->kind == 2u) {
-            or_trace_no_water(j->w, j->ro, r->org, r->dir, r->tmax, j->p, &j->out[i], &j->st);
-        } else {
-            or_trace(j->w, j->ro, r->org, r->dir, r->tmax, j->p, &j->out[i], &j->st);
-        }
-    }
+    for (size_t i = j->a; i < j->b; ++i)
+        queue_ray(j->w, j->ro, &j->rays[i], i, j->p, &j->out[i], j->sh ? &j->sh[i] : NULL, &j->st);
     return NULL;
 }
 
 double or_trace_batch(const OrWorld *w, const int32_t ro[3], const OrRay *rays, size_t n,
-                      const OrParams *p, OrRecord *out, int nthreads, OrStats *st) {
+                      const OrParams *p, OrRecord *out, OrShadow *sh, int nthreads, OrStats *st) {
     double t0 = now_s();
     if (nthreads < 1) nthreads = 1;
     if (nthreads > 256) nthreads = 256;
@@ -1150,6 +1180,7 @@ double or_trace_batch(const OrWorld *w, const int32_t ro[3], const OrRay *rays, 
         if (b <= a) continue;
         BatchJob *j = &jobs[used++];
         j->w = w; j->ro = ro; j->rays = rays; j->a = a; j->b = b; j->p = p; j->out = out;
+        j->sh = sh;
         j->st.bytes = 0; j->st.iters = 0;
     }
     for (int i = 1; i < used; ++i) pthread_create(&th[i], NULL, batch_thread, &jobs[i]);

@@ -193,8 +193,11 @@ double or_render_row_set(const OrWorld *w, const OrCamera *c, const OrParams *p,
                          const float *beam, uint32_t stride, uint32_t offset, OrRecord *rec,
                          OrShadow *sh, int nthreads, OrStats *st);
 
-/* Batched generic rays: kind 0 trace, 1 trace_any, 2 trace_no_water.
+/* Batched generic rays (the mixed queue): kind low bits 1 trace_any,
+ * 2 trace_no_water, else trace; OR_RAY_SPAWN_SHADOW on a trace ray adds its
+ * shadow ray after a hit (shadow record i; sh may be NULL).
  * Ray layout: org[3], dir[3], tmax, kind (32 bytes). */
+#define OR_RAY_SPAWN_SHADOW (1u << 8)
 typedef struct {
     float org[3];
     float dir[3];
@@ -202,7 +205,7 @@ typedef struct {
     uint32_t kind;
 } OrRay;
 double or_trace_batch(const OrWorld *w, const int32_t ro[3], const OrRay *rays,
-                      size_t n, const OrParams *p, OrRecord *out, int nthreads,
+                      size_t n, const OrParams *p, OrRecord *out, OrShadow *sh, int nthreads,
                       OrStats *st);
 double or_raycast_batch(const OrWorld *w, const int32_t origin[3], const float *cams,
                         const float *dirs, size_t n, OrPickHit *out, int32_t *hit,

@@ -27,6 +27,7 @@ VX_F_LOD = 1 << 2
 VX_F_BEAM = 1 << 3
 VX_F_SHADOW = 1 << 4
 VX_F_METHOD = VX_F_L4 | VX_F_LUT | VX_F_LOD | VX_F_BEAM
+VX_RAY_SPAWN_SHADOW = 1 << 8
 
 
 class VxError(RuntimeError):
@@ -68,6 +69,11 @@ class VxWorldView(C.Structure):
 
 class VxTuning(C.Structure):
     _fields_ = [("persistent", C.c_int32), ("reserved", C.c_int32 * 7)]
+
+
+class VxQueueTuning(C.Structure):
+    _fields_ = [("block_threads", C.c_int32), ("refill_min", C.c_int32),
+                ("ctas_per_sm", C.c_int32), ("sort", C.c_int32), ("reserved", C.c_int32 * 4)]
 
 
 class VxTerrainParams(C.Structure):
@@ -115,6 +121,15 @@ SIGNATURES = [
                                           _P(C.c_uint64)]),
     ("vx_render_primary_timed", C.c_int, [_vp, _P(VxCamera), _P(VxTraceParams), _vp, _vp, _vp,
                                           _P(C.c_float)]),
+    ("vx_queue_default_tuning", C.c_int, [_P(VxQueueTuning)]),
+    ("vx_queue_run", C.c_int, [_vp, _P(C.c_int32), _vp, C.c_size_t, _P(VxTraceParams),
+                               _P(VxQueueTuning), _vp, _vp, _vp]),
+    ("vx_queue_autotune", C.c_int, [_vp, _P(C.c_int32), _vp, C.c_size_t, _P(VxTraceParams), _vp,
+                                    _vp, C.c_int32, _P(VxQueueTuning), _P(C.c_float)]),
+    ("vx_queue_graph_create", C.c_int, [_vp, _P(C.c_int32), _vp, C.c_size_t, _P(VxTraceParams),
+                                        _P(VxQueueTuning), _vp, _vp, _P(_vp)]),
+    ("vx_queue_graph_launch", C.c_int, [_vp, _vp]),
+    ("vx_queue_graph_destroy", C.c_int, [_vp]),
     ("vx_project_dirty", C.c_int, [_vp, _P(VxCamera), _vp, C.c_size_t, _vp, _vp]),
     ("vx_tile_refresh", C.c_int, [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, _vp, _vp]),
     ("vx_render_primary_gated", C.c_int, [_vp, _P(VxCamera), _P(VxTraceParams), _vp, _vp, _vp,

@@ -34,6 +34,7 @@ SOURCES = [
     ("vx_trace.cu", EXACT),
     ("vx_world.cu", EXACT),
     ("vx_noalloc.cu", EXACT),
+    ("vx_queue.cu", EXACT),
     ("vx_api.cpp", []),
     ("vx_host_world.cpp", []),
 ]

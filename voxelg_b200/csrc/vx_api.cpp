@@ -44,6 +44,7 @@ struct VxWorld {
     cudaStream_t copy_stream = nullptr;
     uint32_t *d_gate_idx = nullptr;  // staging of vx_project_dirty
     size_t gate_cap = 0;
+    vx::QueueScratch qs;             // scratch of vx_queue_run / vx_queue_autotune
     cudaEvent_t band_ev[8] = {};
     VxTuning tuning{0, {0, 0, 0, 0, 0, 0, 0}};
 };
@@ -99,6 +100,7 @@ void free_world(VxWorld *w) {
     cudaFree(w->pick_hit);
     cudaFree(w->d_work);
     cudaFree(w->d_gate_idx);
+    w->qs.release();
     for (auto &e : w->ev)
         if (e) cudaEventDestroy(e);
     for (auto &e : w->band_ev)
@@ -522,6 +524,129 @@ int vx_render_primary(VxWorld *w, const VxCamera *cam, const VxTraceParams *p,
     return run_frame(w, fa, as_stream(stream));
 }
 
+int vx_queue_default_tuning(VxQueueTuning *t) {
+    if (!t) return VX_ERR_INVALID;
+    std::memset(t, 0, sizeof(*t));
+    t->block_threads = 128;
+    t->refill_min = 32;
+    t->ctas_per_sm = 0;
+    t->sort = 1;
+    return VX_OK;
+}
+
+namespace {
+int check_queue(const VxWorld *w, const int32_t origin[3], const VxRay *rays_dev, size_t n,
+                const VxTraceParams *p, const VxQueueTuning *t, const VxHitRecord *out_dev,
+                const VxShadowRecord *shadow_dev, const char *fn) {
+    if (!w || !origin || (n > 0 && (!rays_dev || !out_dev))) {
+        vx::set_error(std::string(fn) + ": null argument");
+        return VX_ERR_INVALID;
+    }
+    if (n >= 0xFFFFFFF0ull) {
+        vx::set_error(std::string(fn) + ": at most 2^32 - 16 rays per queue");
+        return VX_ERR_INVALID;
+    }
+    if ((reinterpret_cast<uintptr_t>(rays_dev) & 15u) || (reinterpret_cast<uintptr_t>(out_dev) & 7u) ||
+        (reinterpret_cast<uintptr_t>(shadow_dev) & 7u)) {
+        vx::set_error(std::string(fn) + ": rays must be 16-byte, records 8-byte aligned");
+        return VX_ERR_INVALID;
+    }
+    if (t && ((t->block_threads != 64 && t->block_threads != 128 && t->block_threads != 256) ||
+              t->refill_min < 1 || t->refill_min > 32 || t->ctas_per_sm < 0 ||
+              (t->sort != 0 && t->sort != 1))) {
+        vx::set_error(std::string(fn) + ": invalid VxQueueTuning");
+        return VX_ERR_INVALID;
+    }
+    return check_params(p);
+}
+
+vx::TraceArgs trace_args(const VxWorld *w, const int32_t origin[3], const VxTraceParams *p) {
+    vx::TraceArgs ta{};
+    ta.w = w->dw;
+    ta.p = *p;
+    ta.ro[0] = origin[0];
+    ta.ro[1] = origin[1];
+    ta.ro[2] = origin[2];
+    return ta;
+}
+}  // namespace
+
+int vx_queue_run(VxWorld *w, const int32_t origin[3], const VxRay *rays_dev, size_t n,
+                 const VxTraceParams *p, const VxQueueTuning *t, VxHitRecord *out_dev,
+                 VxShadowRecord *shadow_dev, void *stream) {
+    VxQueueTuning def;
+    vx_queue_default_tuning(&def);
+    if (!t) t = &def;
+    int rc = check_queue(w, origin, rays_dev, n, p, t, out_dev, shadow_dev, "vx_queue_run");
+    if (rc != VX_OK) return rc;
+    rc = use_device(w);
+    if (rc != VX_OK) return rc;
+    std::lock_guard<std::mutex> lk(w->mu);
+    cudaStream_t s = as_stream(stream);
+    if (w->qs.cap < n) VX_CK(cudaStreamSynchronize(s));
+    VX_CK(w->qs.reserve(n));
+    VX_CK(vx::launch_queue(trace_args(w, origin, p), rays_dev, n, out_dev, shadow_dev, *t, w->qs, s));
+    return VX_OK;
+}
+
+int vx_queue_autotune(VxWorld *w, const int32_t origin[3], const VxRay *rays_dev, size_t n,
+                      const VxTraceParams *p, VxHitRecord *out_dev, VxShadowRecord *shadow_dev,
+                      int32_t reps, VxQueueTuning *best, float *best_ms) {
+    int rc = check_queue(w, origin, rays_dev, n, p, nullptr, out_dev, shadow_dev,
+                         "vx_queue_autotune");
+    if (rc != VX_OK) return rc;
+    if (!best || !best_ms || reps < 1 || reps > 100) {
+        vx::set_error("vx_queue_autotune: need best, best_ms and 1 <= reps <= 100");
+        return VX_ERR_INVALID;
+    }
+    rc = use_device(w);
+    if (rc != VX_OK) return rc;
+    std::lock_guard<std::mutex> lk(w->mu);
+    cudaStream_t s = w->stream;
+    VX_CK(w->qs.reserve(n));
+    if (!w->ev[0])
+        for (int k = 0; k < 3; ++k) VX_CK(cudaEventCreate(&w->ev[k]));
+    const vx::TraceArgs ta = trace_args(w, origin, p);
+    unsigned long long ref_fp = 0;
+    bool have_ref = false;
+    float best_t = 1e30f;
+    for (int bt : {64, 128, 256})
+        for (int rm : {1, 8, 16, 24, 32})
+            for (int so : {0, 1}) {
+                VxQueueTuning t{};
+                t.block_threads = bt;
+                t.refill_min = rm;
+                t.sort = so;
+                std::vector<float> ms;
+                for (int r = 0; r < reps + 1; ++r) {  // first run warms up
+                    VX_CK(cudaEventRecord(w->ev[0], s));
+                    VX_CK(vx::launch_queue(ta, rays_dev, n, out_dev, shadow_dev, t, w->qs, s));
+                    VX_CK(cudaEventRecord(w->ev[1], s));
+                    VX_CK(cudaEventSynchronize(w->ev[1]));
+                    float m = 0.f;
+                    VX_CK(cudaEventElapsedTime(&m, w->ev[0], w->ev[1]));
+                    if (r > 0) ms.push_back(m);
+                }
+                std::sort(ms.begin(), ms.end());
+                const float med = ms[ms.size() / 2];
+                unsigned long long fp = 0;
+                VX_CK(vx::queue_fingerprint(out_dev, n, shadow_dev, w->qs, s, &fp));
+                if (!have_ref) {
+                    ref_fp = fp;
+                    have_ref = true;
+                } else if (fp != ref_fp) {
+                    vx::set_error("vx_queue_autotune: a tuning changed the records");
+                    return VX_ERR_DEVICE;
+                }
+                if (med < best_t) {
+                    best_t = med;
+                    *best = t;
+                }
+            }
+    *best_ms = best_t;
+    return VX_OK;
+}
+
 int vx_project_dirty(VxWorld *w, const VxCamera *cam, const uint32_t *brick_idx, size_t n,
                      uint32_t *tile_mask_dev, void *stream) {
     if (!w || !tile_mask_dev || (n > 0 && !brick_idx)) {
@@ -706,6 +831,80 @@ int vx_render_primary_timed(VxWorld *w, const VxCamera *cam, const VxTraceParams
     VX_CK(cudaEventSynchronize(w->ev[2]));
     VX_CK(cudaEventElapsedTime(&ms[0], w->ev[0], w->ev[1]));
     VX_CK(cudaEventElapsedTime(&ms[1], w->ev[1], w->ev[2]));
+    return VX_OK;
+}
+
+struct VxQueueGraph {
+    int device = 0;
+    vx::QueueScratch qs;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+int vx_queue_graph_create(VxWorld *w, const int32_t origin[3], const VxRay *rays_dev, size_t n,
+                          const VxTraceParams *p, const VxQueueTuning *t, VxHitRecord *out_dev,
+                          VxShadowRecord *shadow_dev, VxQueueGraph **out) {
+    VxQueueTuning def;
+    vx_queue_default_tuning(&def);
+    if (!t) t = &def;
+    int rc = check_queue(w, origin, rays_dev, n, p, t, out_dev, shadow_dev, "vx_queue_graph_create");
+    if (rc != VX_OK) return rc;
+    if (!out) return VX_ERR_INVALID;
+    rc = use_device(w);
+    if (rc != VX_OK) return rc;
+    VxQueueGraph *g = new (std::nothrow) VxQueueGraph();
+    if (!g) return VX_ERR_OOM;
+    g->device = w->device;
+    auto fail = [&](cudaError_t e) {
+        vx::set_error(std::string("vx_queue_graph_create: ") + cudaGetErrorString(e));
+        if (g->exec) cudaGraphExecDestroy(g->exec);
+        if (g->graph) cudaGraphDestroy(g->graph);
+        g->qs.release();
+        delete g;
+        return e == cudaErrorMemoryAllocation ? VX_ERR_OOM : VX_ERR_CUDA;
+    };
+    cudaError_t e = g->qs.reserve(n);
+    if (e != cudaSuccess) return fail(e);
+    cudaStream_t cs = nullptr;
+    e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return fail(e);
+    const vx::TraceArgs ta = trace_args(w, origin, p);
+    e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        // the counters reset themselves; clear them once more as a node so a
+        // replay after an interrupted one still starts from zero
+        cudaError_t e1 = cudaMemsetAsync(g->qs.work, 0, 2 * sizeof(uint32_t), cs);
+        cudaError_t e2 = e1 == cudaSuccess
+                             ? vx::launch_queue(ta, rays_dev, n, out_dev, shadow_dev, *t, g->qs, cs)
+                             : e1;
+        cudaError_t e3 = cudaStreamEndCapture(cs, &g->graph);
+        e = e2 != cudaSuccess ? e2 : e3;
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&g->exec, g->graph, 0);
+    cudaStreamDestroy(cs);
+    if (e != cudaSuccess) return fail(e);
+    *out = g;
+    return VX_OK;
+}
+
+int vx_queue_graph_launch(VxQueueGraph *g, void *stream) {
+    if (!g || !g->exec) {
+        vx::set_error("vx_queue_graph_launch: null graph");
+        return VX_ERR_INVALID;
+    }
+    VX_CK(cudaSetDevice(g->device));
+    VX_CK(cudaGraphLaunch(g->exec, as_stream(stream)));
+    return VX_OK;
+}
+
+int vx_queue_graph_destroy(VxQueueGraph *g) {
+    if (!g) return VX_OK;
+    cudaSetDevice(g->device);
+    cudaDeviceSynchronize();
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    g->qs.release();
+    delete g;
     return VX_OK;
 }
 

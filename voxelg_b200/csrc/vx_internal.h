@@ -94,6 +94,26 @@ cudaError_t launch_rebuild_pyramid(const DevWorld &w, cudaStream_t s);
 cudaError_t launch_apply_dirty(const DevWorld &w, const uint32_t *idx, const VxBrick *bricks,
                                size_t n, cudaStream_t s);
 
+// Scratch of one ray-queue configuration (owned by a world or a graph):
+// work counters, coherence-sort keys / permutation / histogram, fingerprint.
+struct QueueScratch {
+    uint32_t *work = nullptr;
+    uint32_t *keys = nullptr;
+    uint32_t *order = nullptr;
+    uint32_t *hist = nullptr;
+    unsigned long long *fp = nullptr;
+    size_t cap = 0;
+    cudaError_t reserve(size_t n);
+    void release();
+};
+
+cudaError_t launch_queue(const TraceArgs &ta, const VxRay *rays, size_t n, VxHitRecord *out,
+                         VxShadowRecord *shadow, const VxQueueTuning &t, QueueScratch &sc,
+                         cudaStream_t s);
+// order-independent fingerprint of a queue's outputs (synchronizes s)
+cudaError_t queue_fingerprint(const VxHitRecord *out, size_t n, const VxShadowRecord *shadow,
+                              QueueScratch &sc, cudaStream_t s, unsigned long long *host);
+
 // thread-local error text
 void set_error(const std::string &msg);
 
