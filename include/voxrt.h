@@ -273,6 +273,69 @@ int vx_queue_graph_create(VxWorld *w, const int32_t origin[3], const VxRay *rays
 int vx_queue_graph_launch(VxQueueGraph *g, void *stream);
 int vx_queue_graph_destroy(VxQueueGraph *g);
 
+/* ---- ray-query serving loop ---------------------------------------------
+ * The reference's headless server (src/server.rs:6-102) relays edits and
+ * poses and holds no world; picking runs client-side (src/app.rs:523-557).
+ * This is the device-resident counterpart: clients submit batches of
+ * VxRay queries (picking, line-of-sight, physics probes) against one world;
+ * a server thread forms batches continuously from whatever has arrived,
+ * admits them into a fixed set of device slots sized by the memory budget
+ * (a request waits while no slot is free), and runs each batch on its own
+ * stream, so batches that arrive while others are on the GPU overlap on the
+ * device.  World edits enter the same FIFO and are ordered against every
+ * batch before and after them.  Results are byte-identical to running each
+ * request alone through vx_trace on the same world. */
+typedef struct {
+    uint64_t mem_budget_bytes;  /* device bytes for all slots (56 B per ray) */
+    int32_t slots;              /* batches in flight at once, 1..16         */
+    int32_t max_batch_rays;     /* rays per batch; 0 = budget / slots / 56  */
+    int32_t reserved[4];
+} VxServeConfig;
+
+typedef struct {
+    uint64_t requests, rays, batches, rejected, edits, edited_bricks;
+    double p50_ms, p99_ms, mean_ms, max_ms; /* submit -> results in the caller's buffer */
+    double seconds;                         /* wall time covered (bench) */
+    double mrays_per_s;
+    uint64_t peak_inflight_rays;
+} VxServeStats;
+
+typedef struct VxServer VxServer;
+int vx_server_create(VxWorld *w, const int32_t origin[3], const VxTraceParams *p,
+                     const VxServeConfig *cfg, VxServer **out);
+/* Queue n host rays; *out (host, n records) is written before the ticket
+ * completes.  Both buffers must stay valid until then.  VX_ERR_BUSY when n
+ * exceeds a slot (max_batch_rays). */
+int vx_server_submit(VxServer *s, const VxRay *rays, size_t n, VxHitRecord *out,
+                     uint64_t *ticket);
+/* 1 done, 0 pending, VX_ERR_INVALID for an unknown ticket. */
+int vx_server_poll(VxServer *s, uint64_t ticket);
+/* Block until done (1) or timeout_s elapses (0). */
+int vx_server_wait(VxServer *s, uint64_t ticket, double timeout_s);
+/* Queue a dirty-brick update (vx_world_apply_dirty semantics, host arrays
+ * copied at the call) between the requests submitted before and after it. */
+int vx_server_edit(VxServer *s, const uint32_t *brick_idx, const VxBrick *bricks, size_t n);
+/* Latency / throughput of the requests completed since create (or reset). */
+int vx_server_stats(VxServer *s, VxServeStats *st, int32_t reset);
+int vx_server_destroy(VxServer *s);
+
+/* Built-in load generator: `clients` threads with Poisson arrivals of
+ * `rate_per_client` requests/s each for `seconds`; each request has a
+ * log-uniform size in [min_rays, max_rays] and max length log-uniform in
+ * [min_len, max_len] (kinds: first hit or line of sight), origins / directions
+ * seeded; meanwhile `edit_fraction_per_s` of all bricks per second are
+ * re-randomized through vx_server_edit.  Fills *st for this run. */
+typedef struct {
+    int32_t clients;
+    float rate_per_client;
+    float seconds;
+    int32_t min_rays, max_rays;
+    float min_len, max_len;
+    float edit_fraction_per_s;
+    uint64_t seed;
+} VxServeLoad;
+int vx_serve_bench(VxServer *s, const VxServeLoad *load, VxServeStats *st);
+
 /* ---- temporal differential (src/temporal.rs, src/app.rs:643-767) ------- */
 /* Screen tiles are 8x8 pixels, tiles_w = ceil(W/8); bit ti of the u32 word
  * ti/32 of a tile mask marks tile ti dirty (the tile_dirty buffer of

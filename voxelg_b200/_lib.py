@@ -76,6 +76,25 @@ class VxQueueTuning(C.Structure):
                 ("ctas_per_sm", C.c_int32), ("sort", C.c_int32), ("reserved", C.c_int32 * 4)]
 
 
+class VxServeConfig(C.Structure):
+    _fields_ = [("mem_budget_bytes", C.c_uint64), ("slots", C.c_int32),
+                ("max_batch_rays", C.c_int32), ("reserved", C.c_int32 * 4)]
+
+
+class VxServeStats(C.Structure):
+    _fields_ = [("requests", C.c_uint64), ("rays", C.c_uint64), ("batches", C.c_uint64),
+                ("rejected", C.c_uint64), ("edits", C.c_uint64), ("edited_bricks", C.c_uint64),
+                ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("mean_ms", C.c_double),
+                ("max_ms", C.c_double), ("seconds", C.c_double), ("mrays_per_s", C.c_double),
+                ("peak_inflight_rays", C.c_uint64)]
+
+
+class VxServeLoad(C.Structure):
+    _fields_ = [("clients", C.c_int32), ("rate_per_client", C.c_float), ("seconds", C.c_float),
+                ("min_rays", C.c_int32), ("max_rays", C.c_int32), ("min_len", C.c_float),
+                ("max_len", C.c_float), ("edit_fraction_per_s", C.c_float), ("seed", C.c_uint64)]
+
+
 class VxTerrainParams(C.Structure):
     _fields_ = [("seed", C.c_uint64), ("base_height", C.c_float), ("amplitude", C.c_float),
                 ("inv_wavelength", C.c_float), ("octaves", C.c_uint32),
@@ -130,6 +149,15 @@ SIGNATURES = [
                                         _P(VxQueueTuning), _vp, _vp, _P(_vp)]),
     ("vx_queue_graph_launch", C.c_int, [_vp, _vp]),
     ("vx_queue_graph_destroy", C.c_int, [_vp]),
+    ("vx_server_create", C.c_int, [_vp, _P(C.c_int32), _P(VxTraceParams), _P(VxServeConfig),
+                                   _P(_vp)]),
+    ("vx_server_submit", C.c_int, [_vp, _vp, C.c_size_t, _vp, _P(C.c_uint64)]),
+    ("vx_server_poll", C.c_int, [_vp, C.c_uint64]),
+    ("vx_server_wait", C.c_int, [_vp, C.c_uint64, C.c_double]),
+    ("vx_server_edit", C.c_int, [_vp, _vp, _vp, C.c_size_t]),
+    ("vx_server_stats", C.c_int, [_vp, _P(VxServeStats), C.c_int32]),
+    ("vx_server_destroy", C.c_int, [_vp]),
+    ("vx_serve_bench", C.c_int, [_vp, _P(VxServeLoad), _P(VxServeStats)]),
     ("vx_project_dirty", C.c_int, [_vp, _P(VxCamera), _vp, C.c_size_t, _vp, _vp]),
     ("vx_tile_refresh", C.c_int, [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, _vp, _vp]),
     ("vx_render_primary_gated", C.c_int, [_vp, _P(VxCamera), _P(VxTraceParams), _vp, _vp, _vp,

@@ -37,6 +37,7 @@ SOURCES = [
     ("vx_queue.cu", EXACT),
     ("vx_api.cpp", []),
     ("vx_host_world.cpp", []),
+    ("vx_serve.cpp", []),
 ]
 
 

@@ -49,6 +49,11 @@ struct VxWorld {
     VxTuning tuning{0, {0, 0, 0, 0, 0, 0, 0}};
 };
 
+namespace vx {
+DevWorld world_dev(const VxWorld *w) { return w->dw; }
+int world_device(const VxWorld *w) { return w->device; }
+}  // namespace vx
+
 namespace {
 
 #define VX_CK(call)                                                                   \

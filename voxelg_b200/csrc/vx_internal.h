@@ -114,6 +114,10 @@ cudaError_t launch_queue(const TraceArgs &ta, const VxRay *rays, size_t n, VxHit
 cudaError_t queue_fingerprint(const VxHitRecord *out, size_t n, const VxShadowRecord *shadow,
                               QueueScratch &sc, cudaStream_t s, unsigned long long *host);
 
+// accessors for library parts outside vx_api.cpp
+DevWorld world_dev(const VxWorld *w);
+int world_device(const VxWorld *w);
+
 // thread-local error text
 void set_error(const std::string &msg);
 
