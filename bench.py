@@ -50,6 +50,8 @@ def parse_args():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-seconds", type=float, default=10.0)
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the mixed-queue and serving workloads")
     ap.add_argument("--profile", action="store_true",
                     help="frames only (one counting pass, warm-up, K timed frames): the "
                          "command profiled with ncu")
@@ -230,6 +232,67 @@ def run_reference(args, cfg):
     print(json.dumps(out), flush=True)
 
 
+# ---------------------------------------------------------------- extras
+def run_extras(vg, device: int) -> dict:
+    """The other workloads on the 512x256x512 world, each a few seconds:
+    the mixed ray queue (one autotuned, graph-captured persistent launch) and
+    the ray-query serving loop (64 Poisson clients)."""
+    import torch
+
+    import voxelg_b200.queue as q
+    import voxelg_b200.serve as sv
+    from voxelg_b200 import _lib as L
+
+    out = {}
+    c1 = vg.CONFIGS["c1"]
+    dw = vg.DeviceWorld(*c1.bricks, device=device)
+    dw.generate(c1.terrain)
+    cam = vg.default_camera(dw, 1920, 1080)
+    rays, counts = q.mixed_queue(c1.bricks, cam, 1920, 1080, seed=11)
+    p = vg.default_params(L.VX_F_L4 | L.VX_F_LUT | L.VX_F_LOD, frame=7.0)
+    best, tune_ms, rt, o, sh = q.autotune(dw, rays, p, reps=3)
+    g = q.Graph(dw, rt, p, tuning=best)
+    stream = torch.cuda.current_stream().cuda_stream
+    for _ in range(3):
+        g.launch(stream)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 20
+    e0.record()
+    for _ in range(reps):
+        g.launch(stream)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    n_sh = int(vg.shadows(g.shadow)["traced"].sum())
+    out["mixed_queue"] = {
+        "workload": "512x256x512 world: 1920x1080 primary rays + their shadow rays, GI probes "
+                    "on a 16-voxel grid within 256 voxels (64 Fibonacci rays, max 256), "
+                    "10k picking rays (max 8), seeded shuffle; one graph-captured launch",
+        "rays": len(rays) + n_sh, "queue_rays": len(rays), "spawned_shadow_rays": n_sh,
+        "counts": counts, "ms_per_launch": round(ms, 4),
+        "mrays_s": round((len(rays) + n_sh) / ms / 1e3, 2),
+        "tuning": {"block_threads": best.block_threads, "refill_min": best.refill_min,
+                   "sort": best.sort}, "autotune_best_ms": round(tune_ms, 4),
+    }
+    g.close()
+    del rt, o, sh
+    srv = sv.Server(dw, p, mem_budget_bytes=1 << 30, slots=8)
+    st = srv.bench(clients=64, rate_per_client=200.0, seconds=3.0, min_rays=1, max_rays=50000,
+                   min_len=8.0, max_len=512.0, edit_fraction_per_s=0.01, seed=3)
+    srv.close()
+    out["serving"] = {
+        "workload": "64 clients, Poisson 200 req/s each, 1-50k rays per request (log-uniform), "
+                    "max length 8-512, 1% of bricks re-randomized per second",
+        "requests": st["requests"], "p50_ms": round(st["p50_ms"], 4),
+        "p99_ms": round(st["p99_ms"], 4), "max_ms": round(st["max_ms"], 4),
+        "mrays_s": round(st["mrays_per_s"], 2), "batches": st["batches"], "edits": st["edits"],
+        "seconds": round(st["seconds"], 2),
+    }
+    dw.close()
+    return out
+
+
 # ----------------------------------------------------------------- ours
 def run_ours(args, cfg):
     import numpy as np
@@ -329,6 +392,10 @@ def run_ours(args, cfg):
                          "reference traversal (the Rust reference cannot be built here)"}
         del ow, arrays
 
+    extras = {}
+    if rank == 0 and world == 1 and not args.no_extras:
+        extras = run_extras(vg, local)
+
     if rank == 0:
         out = {
             "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
@@ -360,6 +427,7 @@ def run_ours(args, cfg):
         }
         if cpu:
             out["cpu_baseline"] = cpu
+        out.update(extras)
         print(json.dumps(out), flush=True)
     dw.close()
     if world > 1:

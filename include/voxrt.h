@@ -389,6 +389,90 @@ int vx_render_primary_noalloc(const VxWorldView *world, const VxCamera *cam,
                               const VxTraceParams *p, VxHitRecord *rec_dev,
                               VxShadowRecord *shadow_dev, void *stream);
 
+/* ---- learned start-distance proposal ------------------------------------
+ * No counterpart in the reference.  A 70 -> 64 -> 64 -> 64 -> 1 MLP with
+ * GELU (tanh form) predicts log(first-hit t) of a ray from 6 ray values
+ * (origin mod 64 / 64, direction) and the 64 tile bits of the chunk that
+ * holds the origin.  Parameters: VX_MLP_FLOATS f32 in the order
+ *   W1[64][80] (columns 70..79 are padding, kept at zero), b1[64],
+ *   W2[64][64], b2[64], W3[64][64], b3[64], wo[64], bo
+ * -- 12,929 trained values.  Training runs on the device with the library's
+ * own forward / backward / Adam kernels on rays labelled by the plain DDA;
+ * inference runs on BF16 tensor cores with FP32 accumulation.
+ *
+ * vx_render_learned uses a proposal only to decide how far a verification
+ * walk checks the ray before the DDA restarts past the verified cells; the
+ * records equal vx_render_primary's with the same method flags and no beam,
+ * except `steps` (the iterations actually executed). */
+#define VX_MLP_FLOATS 13569
+#define VX_MLP_FEATURES 80
+typedef struct VxProposal VxProposal;
+
+typedef struct {
+    uint32_t poses;          /* random camera poses                            */
+    uint32_t rays_per_pose;  /* random pixel positions per pose                */
+    uint32_t steps;          /* Adam steps                                     */
+    uint32_t batch;          /* samples per step (<= 65536)                    */
+    float lr;                /* peak learning rate (cosine decay to lr/20)     */
+    float y_min, y_max;      /* camera height range (window voxels)            */
+    float pitch_min, pitch_max; /* radians                                     */
+    float fov_y;             /* radians                                        */
+    uint32_t width, height;  /* image the random pixels are drawn from         */
+    uint32_t flags;          /* method flags of the plain DDA that labels rays */
+    uint32_t held_out_poses; /* extra poses for the held-out loss              */
+    uint64_t seed;
+} VxTrainConfig;
+
+/* 200 poses x 81920 rays (16.4M pairs), 3000 steps of 16384, lr 2e-3,
+ * heights 100..200, pitch -40..+10 deg, vfov 70 deg, 1920x1080, flags
+ * L4|LUT|LOD, 8 held-out poses, seed 1. */
+int vx_proposal_default_config(VxTrainConfig *c);
+/* Random initial parameters (seeded) on the world's device. */
+int vx_proposal_create(VxWorld *w, uint64_t seed, VxProposal **out);
+int vx_proposal_destroy(VxProposal *p);
+/* Copy the f32 parameters out / in (n = VX_MLP_FLOATS); set also refreshes
+ * the BF16 inference copy and resets the Adam state. */
+int vx_proposal_get_params(VxProposal *p, float *host, size_t n);
+int vx_proposal_set_params(VxProposal *p, const float *host, size_t n);
+/* Features of n rays (n x VX_MLP_FEATURES f32, device) for a window corner. */
+int vx_proposal_features(VxProposal *p, VxWorld *w, const int32_t origin[3],
+                         const VxRay *rays_dev, size_t n, float *feats_dev, void *stream);
+/* FP32 forward + backward of one batch against targets (log t): the mean
+ * squared error and its gradient (VX_MLP_FLOATS, host).  Synchronous. */
+int vx_proposal_grad(VxProposal *p, const float *feats_dev, const float *target_dev,
+                     uint32_t batch, float *grad_host, float *loss);
+/* BF16 tensor-core inference: out_dev[i] = predicted log t.  Asynchronous. */
+int vx_proposal_infer(VxProposal *p, const float *feats_dev, size_t n, float *out_dev,
+                      void *stream);
+/* Label rays of random poses with the plain DDA on `w`, then train.
+ * loss_curve (c->steps floats, may be NULL) receives every step's batch
+ * loss, held_out (may be NULL) the loss over the held-out poses before [0]
+ * and after [1] training.  Synchronous. */
+int vx_proposal_train(VxProposal *p, VxWorld *w, const VxTrainConfig *c, float *loss_curve,
+                      float held_out[2]);
+
+typedef struct {
+    uint64_t none;       /* rays whose verification verified no cell           */
+    uint64_t partial;    /* stopped before the proposal; restarted earlier     */
+    uint64_t accepted;   /* verified up to the proposed distance               */
+    uint64_t miss;       /* verified to the window edge / max_dist: a miss     */
+    uint64_t cells;      /* verification cells stepped                         */
+    uint64_t iters;      /* DDA iterations executed                            */
+    uint64_t fallback;   /* restarts that met the iteration cap (plain re-run) */
+    uint64_t rays;
+    float infer_ms;      /* proposal inference (0 without a proposal)          */
+    float trace_ms;      /* verification + traversal                           */
+} VxLearnedStats;
+
+/* Primary frame, learned form: proposal inference (skipped when prop is
+ * NULL: the verification then runs until it fails) and the verified-restart
+ * traversal.  t_target = exp(proposal) * scale.  p->flags must not hold
+ * VX_F_BEAM or VX_F_SHADOW.  With stats != NULL the call is synchronous and
+ * fills the counters and CUDA-event times; else asynchronous on `stream`. */
+int vx_render_learned(VxWorld *w, VxProposal *prop, const VxCamera *cam,
+                      const VxTraceParams *p, float scale, VxHitRecord *rec_dev,
+                      VxLearnedStats *stats, void *stream);
+
 /* ---- host world (mirror of src/voxel.rs World, for C/C++ callers) ------ */
 int vx_host_world_create(int32_t bricks_x, int32_t bricks_y, int32_t bricks_z,
                          VxHostWorld **out);

@@ -95,6 +95,25 @@ class VxServeLoad(C.Structure):
                 ("max_len", C.c_float), ("edit_fraction_per_s", C.c_float), ("seed", C.c_uint64)]
 
 
+class VxTrainConfig(C.Structure):
+    _fields_ = [("poses", C.c_uint32), ("rays_per_pose", C.c_uint32), ("steps", C.c_uint32),
+                ("batch", C.c_uint32), ("lr", C.c_float), ("y_min", C.c_float),
+                ("y_max", C.c_float), ("pitch_min", C.c_float), ("pitch_max", C.c_float),
+                ("fov_y", C.c_float), ("width", C.c_uint32), ("height", C.c_uint32),
+                ("flags", C.c_uint32), ("held_out_poses", C.c_uint32), ("seed", C.c_uint64)]
+
+
+class VxLearnedStats(C.Structure):
+    _fields_ = [("none", C.c_uint64), ("partial", C.c_uint64), ("accepted", C.c_uint64),
+                ("miss", C.c_uint64), ("cells", C.c_uint64), ("iters", C.c_uint64),
+                ("fallback", C.c_uint64), ("rays", C.c_uint64), ("infer_ms", C.c_float),
+                ("trace_ms", C.c_float)]
+
+
+MLP_FLOATS = 13569
+MLP_FEATURES = 80
+
+
 class VxTerrainParams(C.Structure):
     _fields_ = [("seed", C.c_uint64), ("base_height", C.c_float), ("amplitude", C.c_float),
                 ("inv_wavelength", C.c_float), ("octaves", C.c_uint32),
@@ -164,6 +183,17 @@ SIGNATURES = [
                                           _vp]),
     ("vx_render_primary_noalloc", C.c_int, [_P(VxWorldView), _P(VxCamera), _P(VxTraceParams),
                                             _vp, _vp, _vp]),
+    ("vx_proposal_default_config", C.c_int, [_P(VxTrainConfig)]),
+    ("vx_proposal_create", C.c_int, [_vp, C.c_uint64, _P(_vp)]),
+    ("vx_proposal_destroy", C.c_int, [_vp]),
+    ("vx_proposal_get_params", C.c_int, [_vp, _vp, C.c_size_t]),
+    ("vx_proposal_set_params", C.c_int, [_vp, _vp, C.c_size_t]),
+    ("vx_proposal_features", C.c_int, [_vp, _vp, _P(C.c_int32), _vp, C.c_size_t, _vp, _vp]),
+    ("vx_proposal_grad", C.c_int, [_vp, _vp, _vp, C.c_uint32, _vp, _P(C.c_float)]),
+    ("vx_proposal_infer", C.c_int, [_vp, _vp, C.c_size_t, _vp, _vp]),
+    ("vx_proposal_train", C.c_int, [_vp, _vp, _P(VxTrainConfig), _vp, _vp]),
+    ("vx_render_learned", C.c_int, [_vp, _vp, _P(VxCamera), _P(VxTraceParams), C.c_float, _vp,
+                                    _P(VxLearnedStats), _vp]),
     ("vx_host_world_create", C.c_int, [C.c_int32, C.c_int32, C.c_int32, _P(_vp)]),
     ("vx_host_world_destroy", C.c_int, [_vp]),
     ("vx_host_world_arrays", C.c_int, [_vp, _P(_vp), _P(_vp), _P(_vp), _P(_vp), _P(_vp), _P(_vp)]),

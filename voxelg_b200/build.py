@@ -35,6 +35,10 @@ SOURCES = [
     ("vx_world.cu", EXACT),
     ("vx_noalloc.cu", EXACT),
     ("vx_queue.cu", EXACT),
+    ("vx_learned.cu", EXACT),
+    # the proposal network: its values only steer the verified restart
+    ("vx_mlp.cu", []),
+    ("vx_proposal.cpp", []),
     ("vx_api.cpp", []),
     ("vx_host_world.cpp", []),
     ("vx_serve.cpp", []),

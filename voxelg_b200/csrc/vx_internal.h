@@ -114,6 +114,45 @@ cudaError_t launch_queue(const TraceArgs &ta, const VxRay *rays, size_t n, VxHit
 cudaError_t queue_fingerprint(const VxHitRecord *out, size_t n, const VxShadowRecord *shadow,
                               QueueScratch &sc, cudaStream_t s, unsigned long long *host);
 
+// ---- learned start-distance proposal (vx_mlp.cu, vx_learned.cu) ----
+// MLP 70 -> 64 -> 64 -> 64 -> 1 with GELU; flat f32 parameters in the order
+// W1[64][80] (columns 70..79 zero), b1, W2[64][64], b2, W3[64][64], b3, wo, bo.
+constexpr int kMlpIn = 80, kMlpHidden = 64;
+constexpr int kMlpFloats = kMlpHidden * kMlpIn + kMlpHidden + 2 * (kMlpHidden * kMlpHidden + kMlpHidden) +
+                           kMlpHidden + 1;
+
+struct Mlp {
+    float *p = nullptr, *g = nullptr, *m = nullptr, *v = nullptr;  // params, grads, Adam moments
+    uint16_t *w16 = nullptr;   // bf16 W1 | W2 | W3 with padded rows (inference)
+    int adam_t = 0;
+    size_t cap = 0;            // training batch capacity of the activations below
+    float *z1 = nullptr, *a1 = nullptr, *z2 = nullptr, *a2 = nullptr, *z3 = nullptr, *a3 = nullptr;
+    float *y = nullptr, *dy = nullptr, *da = nullptr, *dz = nullptr, *loss = nullptr;
+};
+
+cudaError_t mlp_alloc(Mlp &m);
+void mlp_free(Mlp &m);
+cudaError_t mlp_sync_bf16(Mlp &m, cudaStream_t s);
+// forward + backward of one batch (X [B][80] f32 device, targets [B]):
+// gradients in m.g (zeroed first), mean squared error in *m.loss
+cudaError_t mlp_grad(Mlp &m, const float *X, const float *target, int B, cudaStream_t s);
+cudaError_t mlp_adam(Mlp &m, float lr, cudaStream_t s);
+cudaError_t mlp_infer_features(const Mlp &m, const float *feats, size_t n, float *out,
+                               cudaStream_t s);
+cudaError_t mlp_infer_frame(const Mlp &m, const DevWorld &w, const VxCamera &cam,
+                            const int32_t ro[3], float *out, cudaStream_t s);
+// features of rays idx(j) = ((base + j) % n) * mult % n, j < count (mult = 1: in order)
+cudaError_t mlp_features(const DevWorld &w, const int32_t ro[3], const VxRay *rays, size_t n,
+                         uint64_t base, uint64_t mult, size_t count, float *feats,
+                         const float *targets_src, float *targets_dst, cudaStream_t s);
+cudaError_t mlp_targets(const VxHitRecord *rec, size_t n, float max_dist, float *target,
+                        cudaStream_t s);
+cudaError_t mlp_pose_rays(const VxCamera &c, uint64_t seed, size_t n, VxRay *rays,
+                          float max_dist, cudaStream_t s);
+cudaError_t launch_learned(const TraceArgs &ta, const VxCamera &cam, const float *proposal,
+                           float scale, VxHitRecord *rec, unsigned long long *stats,
+                           cudaStream_t s);
+
 // accessors for library parts outside vx_api.cpp
 DevWorld world_dev(const VxWorld *w);
 int world_device(const VxWorld *w);
