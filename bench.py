@@ -20,6 +20,15 @@ roofline   the primary kernel: algorithmic bytes per launch (method loads as
            against the measured HBM copy bandwidth.
 cpu_baseline  the oracle (C restatement of the reference traversal) on all
            host threads over a bounded row sample of the same frame.
+
+Extra sections (rank 0, single GPU, a few seconds each; --no-extras skips
+them), all on the 512x256x512 world:
+mixed_queue  primary + spawned shadow + GI-probe + picking rays in one
+           autotuned, graph-captured persistent launch.
+learned    the learned start-distance proposal: on-device training, then the
+           plain DDA, the learned form and the verification without a network
+           on one 1920x1080 frame, with acceptance and iterations saved.
+serving    the ray-query server under 64 open-loop Poisson clients: p50/p99.
 """
 from __future__ import annotations
 
@@ -233,6 +242,74 @@ def run_reference(args, cfg):
 
 
 # ---------------------------------------------------------------- extras
+def run_learned(vg, dw) -> dict:
+    """Learned start-distance proposal on the 512x256x512 world at 1920x1080:
+    train on the device (16.4M plain-DDA pairs from 200 poses), then time the
+    plain DDA, the learned form and the verification without a network on
+    the same frame (primary rays, method flags L4|LUT|LOD, no beam), and
+    check that all three give the same records except steps."""
+    import numpy as np
+    import torch
+
+    from voxelg_b200 import _lib as L
+    from voxelg_b200 import learned as vl
+
+    cam = vg.default_camera(dw, 1920, 1080)
+    p = vg.default_params(L.VX_F_L4 | L.VX_F_LUT | L.VX_F_LOD)
+    n = 1920 * 1080
+    stream = torch.cuda.current_stream().cuda_stream
+    prop = vl.Proposal(dw, seed=7)
+    cfg = vl.default_config()
+    t0 = time.perf_counter()
+    curve, held_before, held_after = prop.train(dw, cfg)
+    train_s = time.perf_counter() - t0
+    plain = torch.empty(n * 24, dtype=torch.uint8, device="cuda")
+    rec = torch.empty_like(plain)
+    reps = 20
+
+    def median(xs):
+        return float(statistics.median(xs))
+
+    for _ in range(3):
+        vg.render_primary_timed(dw, cam, p, plain, stream=stream)
+    plain_ms = median([vg.render_primary_timed(dw, cam, p, plain, stream=stream)[1]
+                       for _ in range(reps)])
+    a = vg.records(plain)
+    plain_iters = int(a["steps"].astype(np.int64).sum())
+    res = {}
+    for name, pr in (("learned", prop), ("verify_only", None)):
+        for _ in range(3):
+            vl.render_learned(dw, pr, cam, p, rec, stream=stream)
+        ss = [vl.render_learned(dw, pr, cam, p, rec, stream=stream) for _ in range(reps)]
+        b = vg.records(rec)
+        fa, fb = a.copy(), b.copy()
+        fa["steps"] = 0
+        fb["steps"] = 0
+        s = ss[-1]
+        ms = median([x.infer_ms + x.trace_ms for x in ss])
+        res[name] = {
+            "ms": round(ms, 4), "infer_ms": round(median([x.infer_ms for x in ss]), 4),
+            "trace_ms": round(median([x.trace_ms for x in ss]), 4),
+            "mrays_s": round(n / ms / 1e3, 1), "speedup_vs_plain": round(plain_ms / ms, 3),
+            "iters_per_ray": round(s.iters / n, 3),
+            "steps_saved_per_ray": round((plain_iters - s.iters) / n, 3),
+            "verify_cells_per_ray": round(s.cells / n, 3),
+            "acceptance": round(s.accepted / n, 4), "partial": round(s.partial / n, 4),
+            "verified_miss": round(s.miss / n, 4), "fallback": int(s.fallback),
+            "records_equal_except_steps": bool(np.array_equal(fa.view(np.uint8),
+                                                              fb.view(np.uint8))),
+        }
+    prop.close()
+    return {
+        "workload": "512x256x512 world, 1920x1080 primary rays, method L4|LUT|LOD without the "
+                    "beam; MLP 70-64-64-64-1 GELU trained on 16.4M plain-DDA pairs (200 poses)",
+        "train_s": round(train_s, 3), "train_steps": int(cfg.steps),
+        "held_out_loss_before": round(held_before, 4), "held_out_loss_after": round(held_after, 4),
+        "plain_ms": round(plain_ms, 4), "plain_mrays_s": round(n / plain_ms / 1e3, 1),
+        "plain_iters_per_ray": round(plain_iters / n, 3), **res,
+    }
+
+
 def run_extras(vg, device: int) -> dict:
     """The other workloads on the 512x256x512 world, each a few seconds:
     the mixed ray queue (one autotuned, graph-captured persistent launch) and
@@ -277,6 +354,7 @@ def run_extras(vg, device: int) -> dict:
     }
     g.close()
     del rt, o, sh
+    out["learned"] = run_learned(vg, dw)
     srv = sv.Server(dw, p, mem_budget_bytes=1 << 30, slots=8)
     st = srv.bench(clients=64, rate_per_client=200.0, seconds=3.0, min_rays=1, max_rays=50000,
                    min_len=8.0, max_len=512.0, edit_fraction_per_s=0.01, seed=3)

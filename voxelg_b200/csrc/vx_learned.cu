@@ -182,17 +182,33 @@ __device__ __forceinline__ void verify(const DevWorld &w, const Geo &g, const Vx
         tby = exit_t(by, 4, s.sty, s.oy, s.iy);
         tbz = exit_t(bz, 4, s.stz, s.oz, s.iz);
     }
+    // Clean crossings from exit times: at a crossing at time t, axis b lies
+    // at least kClean inside its current slab of size gs iff
+    // lo_b <= e_b - t <= gs |1/d_b| - lo_b with lo_b = kClean |1/d_b| (e_b the
+    // slab's exit time).  An axis the ray does not move along is tested once
+    // on its constant coordinate (lo = -inf: always clean, +inf: never).
+    const float aix = fabsf(s.ix), aiy = fabsf(s.iy), aiz = fabsf(s.iz);
+    const float kInf = __int_as_float(0x7f800000);
+    auto lo_of = [&](int32_t st, float ai, float o) {
+        if (st != 0 && ai < 1e29f) return kClean * ai;
+        return clean_at(o, 16.0f, 0.0625f) && clean_at(o, 4.0f, 0.25f) ? -kInf : kInf;
+    };
+    const float lox = lo_of(s.stx, aix, s.ox), loy = lo_of(s.sty, aiy, s.oy),
+                loz = lo_of(s.stz, aiz, s.oz);
     float l_a = 0.f, l_b = 0.f, p_a = 0.f, p_b = 0.f;
     int l_g = 0, p_g = 0;
     bool reached = false;
     uint32_t cells = 0;
+    const float t_near = tmax - kTEps;
     for (uint32_t it = 0; it < kMaxCells; ++it) {
-        if (tin > tmax + kTEps) {
-            v.outcome = OUT_MISS;
-            v.cells = cells;
-            return;
+        if (tin > t_near) {
+            if (tin > tmax + kTEps) {
+                v.outcome = OUT_MISS;
+                v.cells = cells;
+                return;
+            }
+            break;
         }
-        if (tin > tmax - kTEps) break;
         const int gs = bricks ? 4 : 16;
         const float ex = bricks ? tbx : ttx, ey = bricks ? tby : tty, ez = bricks ? tbz : ttz;
         int ax = 0;
@@ -209,12 +225,13 @@ __device__ __forceinline__ void verify(const DevWorld &w, const Geo &g, const Vx
             break;
         }
         // the crossing point must sit clear of the faces of this level
-        const float xx = s.ox + s.dx * tout, xy = s.oy + s.dy * tout, xz = s.oz + s.dz * tout;
         {
-            const float gf = (float)gs, ig = inv_level(gs);
-            if (!((ax == 0 || clean_at(xx, gf, ig)) && (ax == 1 || clean_at(xy, gf, ig)) &&
-                  (ax == 2 || clean_at(xz, gf, ig))))
-                break;
+            const float gf = (float)gs;
+            const float qx = ex - tout, qy = ey - tout, qz = ez - tout;
+            const bool cx_ = ax == 0 || (qx >= lox && qx <= gf * aix - lox);
+            const bool cy_ = ax == 1 || (qy >= loy && qy <= gf * aiy - loy);
+            const bool cz_ = ax == 2 || (qz >= loz && qz <= gf * aiz - loz);
+            if (!(cx_ && cy_ && cz_)) break;
         }
         tin = tout;
         // step along ax; stay in the tile (brick walk) or move to the next tile
@@ -250,7 +267,10 @@ __device__ __forceinline__ void verify(const DevWorld &w, const Geo &g, const Vx
         // a non-empty tile: plain's tile LOD / uniform test happen at its entry
         if (LOD && tout > p.tile_lod_t - kTEps) break;
         if (!bricks) {
+            // entering bricks from the tile walk: the crossing must also clear
+            // the brick faces (crossing coordinates, tested directly)
             const float ig = 0.25f;
+            const float xx = s.ox + s.dx * tout, xy = s.oy + s.dy * tout, xz = s.oz + s.dz * tout;
             if (!((ax == 0 || clean_at(xx, 4.0f, ig)) && (ax == 1 || clean_at(xy, 4.0f, ig)) &&
                   (ax == 2 || clean_at(xz, 4.0f, ig))))
                 break;
@@ -293,7 +313,7 @@ struct LearnedArgs {
 };
 
 template <uint32_t FL>
-__global__ void __launch_bounds__(128) k_learned(LearnedArgs la) {
+__global__ void __launch_bounds__(128, 8) k_learned(LearnedArgs la) {
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t px = blockIdx.x * 16u + (warp & 1u) * 8u + (lane & 7u);
     const uint32_t py = blockIdx.y * 8u + (warp >> 1) * 4u + (lane >> 3);
