@@ -60,7 +60,7 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample-seconds", type=float, default=10.0)
     ap.add_argument("--no-extras", action="store_true",
-                    help="skip the mixed-queue and serving workloads")
+                    help="skip the mixed-queue, learned and serving workloads")
     ap.add_argument("--profile", action="store_true",
                     help="frames only (one counting pass, warm-up, K timed frames): the "
                          "command profiled with ncu")
@@ -164,6 +164,14 @@ def max_over_ranks(x: float, world: int, device) -> float:
     t = torch.tensor([x], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def aggregate(world: int, rays_per_step: int, steps: int, dev_ms: float, device):
+    """Whole-job throughput in Mrays/s: every rank renders rays_per_step per
+    step (weak scaling) and the job takes as long as the slowest rank's
+    device time.  Returns (max device ms over ranks, value)."""
+    dev_ms_max = max_over_ranks(dev_ms, world, device)
+    return dev_ms_max, world * rays_per_step * steps / (dev_ms_max / 1e3) / 1e6
 
 
 def frame_setup(vg, cfg, device: int):
@@ -427,8 +435,7 @@ def run_ours(args, cfg):
     wall = time.perf_counter() - t0
     clocks = sampler.stop() if sampler else None
     dev_ms = sum(beam_ms) + sum(prim_ms)
-    dev_ms_max = max_over_ranks(dev_ms, world, device)
-    value = world * rays_per_step * args.steps / (dev_ms_max / 1e3) / 1e6
+    dev_ms_max, value = aggregate(world, rays_per_step, args.steps, dev_ms, device)
 
     # end to end through the host-buffer entry point
     rec_h = torch.empty(n * 24, dtype=torch.uint8).pin_memory()
