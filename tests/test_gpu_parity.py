@@ -353,6 +353,16 @@ def test_render_host_equals_device(vg, dev_c1):
     hrec, hsh = vg.render_primary_host(dev_c1, cam, p)
     assert np.array_equal(vg.records(rec).view(np.uint8), hrec.view(np.uint8))
     assert np.array_equal(vg.shadows(sh).view(np.uint8), hsh.view(np.uint8))
+    # pinned host buffers, twice (the banded copies overwrite every byte)
+    import torch
+    n = 320 * 180
+    rp = torch.full((n * 24,), 0xAB, dtype=torch.uint8).pin_memory()
+    sp = torch.full((n * 8,), 0xAB, dtype=torch.uint8).pin_memory()
+    for _ in range(2):
+        vg.render_primary_host(dev_c1, cam, p, rp.numpy().view(vg._lib.RECORD_DTYPE),
+                               sp.numpy().view(vg._lib.SHADOW_DTYPE))
+        assert np.array_equal(vg.records(rec).view(np.uint8), rp.numpy())
+        assert np.array_equal(vg.shadows(sh).view(np.uint8), sp.numpy())
 
 
 def test_c2_full_frame_bit_exact(vg):
