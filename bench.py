@@ -29,6 +29,7 @@ learned    the learned start-distance proposal: on-device training, then the
            plain DDA, the learned form and the verification without a network
            on one 1920x1080 frame, with acceptance and iterations saved.
 serving    the ray-query server under 64 open-loop Poisson clients: p50/p99.
+ao         (on the benchmark frame) contact AO of the primary hits.
 """
 from __future__ import annotations
 
@@ -320,8 +321,9 @@ def run_learned(vg, dw) -> dict:
 
 def run_extras(vg, device: int) -> dict:
     """The other workloads on the 512x256x512 world, each a few seconds:
-    the mixed ray queue (one autotuned, graph-captured persistent launch) and
-    the ray-query serving loop (64 Poisson clients)."""
+    the mixed ray queue (one autotuned, graph-captured persistent launch),
+    the learned proposal and the ray-query serving loop (64 Poisson
+    clients)."""
     import torch
 
     import voxelg_b200.queue as q
@@ -479,7 +481,23 @@ def run_ours(args, cfg):
 
     extras = {}
     if rank == 0 and world == 1 and not args.no_extras:
-        extras = run_extras(vg, local)
+        # contact AO of the benchmark frame's primary hits (12 neighbour tests
+        # per hit within 64 voxels), timed alone on the frame's records
+        ao = torch.empty(n, dtype=torch.float32, device=device)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        for _ in range(3):
+            vg.render_ao(dw, cam, rec, ao, stream=stream)
+        e0.record()
+        for _ in range(20):
+            vg.render_ao(dw, cam, rec, ao, stream=stream)
+        e1.record()
+        torch.cuda.synchronize(device)
+        ao_ms = e0.elapsed_time(e1) / 20
+        extras["ao"] = {"workload": "contact AO of the 1920x1080 frame's primary hits "
+                                    "(vx_render_ao on the frame's records)",
+                        "ms": round(ao_ms, 4), "mpixels_s": round(n / ao_ms / 1e3, 1),
+                        "occluded_fraction": round(float((ao < 1.0).float().mean()), 4)}
+        extras.update(run_extras(vg, local))
 
     if rank == 0:
         out = {

@@ -66,7 +66,10 @@ typedef struct {
     float tan_half_fov;
     float res_x, res_y;
     float jitter_x, jitter_y;      /* sub-pixel jitter in pixels            */
-    int32_t world_origin[3];       /* loaded-window corner, world voxels    */
+    int32_t world_origin[3];       /* loaded-window corner, world voxels;
+                                      y must be 0: windows move in x/z only
+                                      (src/voxel.rs:439-445), every call
+                                      taking a window corner rejects y != 0 */
 } VxCamera;
 
 /* Method switches.  The reference method is L4|LUT|LOD|BEAM. */
@@ -212,6 +215,14 @@ int vx_trace(VxWorld *w, const int32_t origin[3], const VxRay *rays_dev, size_t 
  * VX_F_SHADOW is off.  The beam scratch is owned by the world. */
 int vx_render_primary(VxWorld *w, const VxCamera *cam, const VxTraceParams *p,
                       VxHitRecord *rec_dev, VxShadowRecord *shadow_dev, void *stream);
+/* Contact AO of the primary hits of a frame (compute_ao, raymarch.wgsl
+ * :4417-4475): for each record of rec_dev (a vx_render_primary frame of the
+ * same camera, any method flags), the hierarchical solid test of the 12
+ * neighbours of its entry-face corners, the corner rule and the bilinear
+ * mix, with the skip rule of :3862-3863 (beyond 64 voxels, leaf blocks,
+ * leaf fringe).  ao_dev[i] = 1 for misses and skipped hits. */
+int vx_render_ao(VxWorld *w, const VxCamera *cam, const VxHitRecord *rec_dev, float *ao_dev,
+                 void *stream);
 /* Same frame through host buffers: the records are copied to rec_host /
  * shadow_host (pinned memory recommended) before the call returns. */
 int vx_render_primary_host(VxWorld *w, const VxCamera *cam, const VxTraceParams *p,

@@ -102,6 +102,8 @@ def load():
         "or_render_rows": (None, [P(OrWorld), P(OrCamera), P(OrParams), vp, C.c_uint32,
                                   C.c_uint32, vp, vp, P(OrStats)]),
         "or_project_brick_to_tiles": (None, [P(OrWorld), P(OrCamera), C.c_uint32, vp]),
+        "or_compute_ao": (C.c_float, [P(OrWorld), P(OrCamera), vp, C.c_uint32, C.c_uint32]),
+        "or_render_ao": (None, [P(OrWorld), P(OrCamera), vp, vp, C.c_int]),
         "or_refresh_tiles": (None, [C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, vp]),
         "or_render_row_set": (C.c_double, [P(OrWorld), P(OrCamera), P(OrParams), vp, C.c_uint32,
                                            C.c_uint32, vp, vp, C.c_int, P(OrStats)]),
@@ -225,6 +227,17 @@ def render_row_set(world: World, cam, params, beam, stride, offset, threads=None
     rows = np.arange(offset, H, stride)
     idx = (rows[:, None] * W + np.arange(W)[None, :]).reshape(-1)
     return rec[idx], sh[idx], secs, st
+
+
+def render_ao(world: World, cam, rec: np.ndarray, threads=None) -> np.ndarray:
+    """Contact AO (compute_ao, raymarch.wgsl:4417-4453) of every primary
+    record of a frame of `cam`; 1.0 for misses and skipped hits."""
+    cam = camera_from(cam)
+    rec = np.ascontiguousarray(rec).view(RECORD)
+    ao = np.empty(len(rec), np.float32)
+    load().or_render_ao(C.byref(world.c), C.byref(cam), rec.ctypes.data, ao.ctypes.data,
+                        threads or os.cpu_count() or 1)
+    return ao
 
 
 def project_dirty(world: World, cam, brick_idx, mask=None):

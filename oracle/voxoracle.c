@@ -1056,6 +1056,135 @@ double or_render_frame(const OrWorld *w, const OrCamera *c, const OrParams *p, O
     return now_s() - t0;
 }
 
+/* ------------------------------------------------------------------ */
+/* contact AO of primary hits                                           */
+/* ------------------------------------------------------------------ */
+#define AO_DIST 64.0f /* raymarch.wgsl:4522 */
+
+static inline int is_leaf_block(uint32_t m) {  /* raymarch.wgsl:908-911 */
+    return m == 14u || m == 25u || m == 26u || m == 27u;
+}
+
+/* is_voxel_solid (raymarch.wgsl:297-322): window test, slot fold, then the
+ * chunk -> tile -> brick bits; *mat gets the voxel's material byte
+ * (voxel_material_at, :324-346) when solid. */
+static int ao_solid(const OrWorld *w, const Dims *d, const int32_t v[3], const int32_t ro[3],
+                    uint32_t *mat) {
+    int32_t rx = v[0] - ro[0], ry = v[1] - ro[1], rz = v[2] - ro[2];
+    if (rx < 0 || rx >= d->vx || ry < 0 || ry >= d->vy || rz < 0 || rz >= d->vz) return 0;
+    int32_t sx = pos_mod(v[0], d->vx), sy = v[1], sz = pos_mod(v[2], d->vz);
+    int64_t ci = chunk_idx(d, sx >> 6, sy >> 6, sz >> 6);
+    int tl = child_bit((sx >> 4) & 3, (sy >> 4) & 3, (sz >> 4) & 3);
+    if (!((w->chunk_mask[ci] >> tl) & 1ull)) return 0;
+    int64_t ti = tile_idx(d, sx >> 4, sy >> 4, sz >> 4);
+    int bl = child_bit((sx >> 2) & 3, (sy >> 2) & 3, (sz >> 2) & 3);
+    if (!((w->tile_mask[ti] >> bl) & 1ull)) return 0;
+    const OrBrick *b = &w->bricks[brick_idx(d, sx >> 2, sy >> 2, sz >> 2)];
+    int vi = child_bit(sx & 3, sy & 3, sz & 3);
+    if (!((b->occupancy >> vi) & 1ull)) return 0;
+    *mat = b->materials[vi];
+    return 1;
+}
+
+/* ao_occluder (raymarch.wgsl:4462-4465): solid and not decoration */
+static int ao_occluder(const OrWorld *w, const Dims *d, const int32_t v[3], const int32_t ro[3]) {
+    uint32_t m = 0;
+    if (!ao_solid(w, d, v, ro, &m)) return 0;
+    return !is_decoration(m);
+}
+
+/* ao_corner (raymarch.wgsl:4467-4475) */
+static float ao_corner(const OrWorld *w, const Dims *d, const int32_t base[3],
+                       const int32_t da[3], const int32_t db[3], const int32_t ro[3]) {
+    int32_t a[3], b[3], c[3];
+    for (int k = 0; k < 3; ++k) {
+        a[k] = base[k] + da[k];
+        b[k] = base[k] + db[k];
+        c[k] = base[k] + da[k] + db[k];
+    }
+    int s1 = ao_occluder(w, d, a, ro), s2 = ao_occluder(w, d, b, ro);
+    int cd = ao_occluder(w, d, c, ro);
+    if (s1 && s2) return 0.35f;
+    int cnt = s1 + s2 + cd;
+    return 1.0f - (float)cnt * 0.22f;
+}
+
+/* WGSL mix(a, b, t) = a * (1 - t) + b * t */
+static inline float mixf(float a, float b, float t) { return a * (1.0f - t) + b * t; }
+
+/* compute_ao (raymarch.wgsl:4417-4453) for pixel (px, py) of a primary
+ * frame: origin = camera origin, dir = ray_dir_uv of the pixel centre,
+ * t / voxel / entry face from its record. */
+float or_compute_ao(const OrWorld *w, const OrCamera *c, const OrRecord *rec, uint32_t px,
+                    uint32_t py) {
+    if (!(rec->flags & 1u)) return 1.0f;
+    const uint32_t m = rec->mat;
+    if (rec->t > AO_DIST || is_leaf_block(m) || m == MAT_LEAF_FRINGE) return 1.0f;
+    Dims d = dims_of(w);
+    float dir[3];
+    float u = (((float)px + 0.5f) + c->jitter_x) / c->res_x;
+    float v = (((float)py + 0.5f) + c->jitter_y) / c->res_y;
+    or_ray_dir_uv(c, u, v, dir);
+    const int na = rec->face >> 1;
+    const int32_t n_dir = (rec->face & 1u) ? -1 : 1;  /* -step[na] */
+    float lf[3];
+    for (int k = 0; k < 3; ++k) lf[k] = (c->origin[k] + dir[k] * rec->t) - (float)rec->voxel[k];
+    int32_t da[3] = {0, 0, 0}, db[3] = {0, 0, 0};
+    float fa, fb;
+    if (na == 0) { da[1] = 1; db[2] = 1; fa = lf[1]; fb = lf[2]; }
+    else if (na == 1) { da[0] = 1; db[2] = 1; fa = lf[0]; fb = lf[2]; }
+    else { da[0] = 1; db[1] = 1; fa = lf[0]; fb = lf[1]; }
+    int32_t dan[3] = {-da[0], -da[1], -da[2]}, dbn[3] = {-db[0], -db[1], -db[2]};
+    int32_t base[3] = {rec->voxel[0], rec->voxel[1], rec->voxel[2]};
+    base[na] += n_dir;
+    const int32_t *ro = c->world_origin;
+    float ao00 = ao_corner(w, &d, base, dan, dbn, ro);
+    float ao10 = ao_corner(w, &d, base, da, dbn, ro);
+    float ao01 = ao_corner(w, &d, base, dan, db, ro);
+    float ao11 = ao_corner(w, &d, base, da, db, ro);
+    float fa_c = clampf(fa, 0.0f, 1.0f), fb_c = clampf(fb, 0.0f, 1.0f);
+    float ao_x0 = mixf(ao00, ao10, fa_c);
+    float ao_x1 = mixf(ao01, ao11, fa_c);
+    return mixf(ao_x0, ao_x1, fb_c);
+}
+
+typedef struct {
+    const OrWorld *w;
+    const OrCamera *c;
+    const OrRecord *rec;
+    float *ao;
+    uint32_t y0, y1;
+} AoJob;
+
+static void *ao_thread(void *arg) {
+    AoJob *j = (AoJob *)arg;
+    uint32_t W = (uint32_t)j->c->res_x;
+    for (uint32_t y = j->y0; y < j->y1; ++y)
+        for (uint32_t x = 0; x < W; ++x)
+            j->ao[(size_t)y * W + x] = or_compute_ao(j->w, j->c, &j->rec[(size_t)y * W + x], x, y);
+    return NULL;
+}
+
+void or_render_ao(const OrWorld *w, const OrCamera *c, const OrRecord *rec, float *ao,
+                  int nthreads) {
+    if (nthreads < 1) nthreads = 1;
+    if (nthreads > 256) nthreads = 256;
+    uint32_t H = (uint32_t)c->res_y;
+    pthread_t th[256];
+    AoJob jobs[256];
+    int used = 0;
+    for (int i = 0; i < nthreads; ++i) {
+        uint32_t a = (uint32_t)((uint64_t)H * i / nthreads);
+        uint32_t b = (uint32_t)((uint64_t)H * (i + 1) / nthreads);
+        if (b <= a) continue;
+        AoJob *j = &jobs[used++];
+        j->w = w; j->c = c; j->rec = rec; j->ao = ao; j->y0 = a; j->y1 = b;
+    }
+    for (int i = 1; i < used; ++i) pthread_create(&th[i], NULL, ao_thread, &jobs[i]);
+    if (used > 0) ao_thread(&jobs[0]);
+    for (int i = 1; i < used; ++i) pthread_join(th[i], NULL);
+}
+
 typedef struct {
     const OrWorld *w;
     const OrCamera *c;

@@ -188,6 +188,14 @@ void or_project_brick_to_tiles(const OrWorld *w, const OrCamera *c, uint32_t bi,
 void or_refresh_tiles(uint32_t tiles_w, uint32_t tiles_h, uint32_t spread, uint32_t phase,
                       uint32_t *mask);
 
+/* Contact AO of primary hits: compute_ao / ao_corner / ao_occluder /
+ * is_voxel_solid (raymarch.wgsl:4417-4475, :297-322, skip rule :3862-3863).
+ * ao[i] = 1 for misses and skipped hits.  Multi-threaded over rows. */
+float or_compute_ao(const OrWorld *w, const OrCamera *c, const OrRecord *rec, uint32_t px,
+                    uint32_t py);
+void or_render_ao(const OrWorld *w, const OrCamera *c, const OrRecord *rec, float *ao,
+                  int nthreads);
+
 /* Rows offset + k*stride of a frame on nthreads threads (bounded samples). */
 double or_render_row_set(const OrWorld *w, const OrCamera *c, const OrParams *p,
                          const float *beam, uint32_t stride, uint32_t offset, OrRecord *rec,

@@ -65,6 +65,14 @@ def test_invalid_arguments_rejected_without_gpu():
     h = C.c_void_p()
     assert lib.vx_world_create(C.byref(L.VxWorldDesc(128, 60, 128, 0)), C.byref(h)) == L.VX_ERR_INVALID
     assert b"multiple" in lib.vx_last_error()
+    # a window corner with y != 0 is refused before anything touches a device
+    view = L.VxWorldView(128, 64, 128, *([16] * 7))
+    cam = vg.camera_from_pose((256.0, 140.0, 256.0), 0.0, -0.26, 1.22, 64, 36,
+                              world_origin=(0, 64, 0))
+    p = vg.default_params()
+    assert lib.vx_render_primary_noalloc(C.byref(view), C.byref(cam), C.byref(p),
+                                         C.c_void_p(16), None, None) == L.VX_ERR_INVALID
+    assert b"origin y" in lib.vx_last_error()
 
 
 def test_host_world_mirrors_voxel_rs(c1_oracle_world):

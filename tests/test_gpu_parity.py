@@ -365,6 +365,20 @@ def test_render_host_equals_device(vg, dev_c1):
         assert np.array_equal(vg.shadows(sh).view(np.uint8), sp.numpy())
 
 
+def test_window_origin_y_rejected(vg, dev_c1):
+    """Storage y is world y: a window corner with y != 0 is refused by every
+    entry point that takes one, before any kernel runs."""
+    cam = vg.camera_from_pose((256.0, 200.0, 256.0), 0.0, -0.3, 1.2, 64, 36,
+                              world_origin=(0, 64, 0))
+    for call in (lambda: vg.render_primary(dev_c1, cam, vg.default_params()),
+                 lambda: vg.render_primary_host(dev_c1, cam, vg.default_params()),
+                 lambda: vg.trace(dev_c1, np.zeros(4, po.RAY), vg.default_params(),
+                                  origin=(0, 4, 0))):
+        with pytest.raises(vg._lib.VxError) as e:
+            call()
+        assert e.value.code == vg._lib.VX_ERR_INVALID
+
+
 def test_c2_full_frame_bit_exact(vg):
     """The full benchmark workload: 2048x256x2048 world, 1920x1080 primary
     rays with beam/LUT/LOD, one shadow ray per hit."""

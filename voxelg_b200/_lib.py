@@ -155,6 +155,7 @@ SIGNATURES = [
     ("vx_trace", C.c_int, [_vp, _P(C.c_int32), _vp, C.c_size_t, _P(VxTraceParams), _vp, _vp]),
     ("vx_render_primary", C.c_int, [_vp, _P(VxCamera), _P(VxTraceParams), _vp, _vp, _vp]),
     ("vx_render_primary_host", C.c_int, [_vp, _P(VxCamera), _P(VxTraceParams), _vp, _vp]),
+    ("vx_render_ao", C.c_int, [_vp, _P(VxCamera), _vp, _vp, _vp]),
     ("vx_render_primary_stats", C.c_int, [_vp, _P(VxCamera), _P(VxTraceParams),
                                           _P(C.c_uint64)]),
     ("vx_render_primary_timed", C.c_int, [_vp, _P(VxCamera), _P(VxTraceParams), _vp, _vp, _vp,

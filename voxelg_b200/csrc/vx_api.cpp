@@ -121,6 +121,7 @@ int check_frame(const VxCamera *cam) {
         vx::set_error("camera resolution must be an integer in [1, 32768]");
         return VX_ERR_INVALID;
     }
+    if (!vx::origin_ok(cam->world_origin, "camera")) return VX_ERR_INVALID;
     return VX_OK;
 }
 
@@ -457,6 +458,7 @@ int vx_raycast(VxWorld *w, const float cam[3], const float dir[3], const int32_t
         vx::set_error("vx_raycast: null argument");
         return VX_ERR_INVALID;
     }
+    if (!vx::origin_ok(origin, "vx_raycast")) return VX_ERR_INVALID;
     int rc = use_device(w);
     if (rc != VX_OK) return rc;
     std::lock_guard<std::mutex> lk(w->mu);
@@ -478,6 +480,7 @@ int vx_raycast_batch(VxWorld *w, const int32_t origin[3], const float *cams_dev,
         vx::set_error("vx_raycast_batch: null argument");
         return VX_ERR_INVALID;
     }
+    if (!vx::origin_ok(origin, "vx_raycast_batch")) return VX_ERR_INVALID;
     int rc = use_device(w);
     if (rc != VX_OK) return rc;
     VX_CK(vx::launch_raycast(w->dw, origin, cams_dev, dirs_dev, n, out_dev, hit_dev,
@@ -491,6 +494,7 @@ int vx_trace(VxWorld *w, const int32_t origin[3], const VxRay *rays_dev, size_t 
         vx::set_error("vx_trace: null argument");
         return VX_ERR_INVALID;
     }
+    if (!vx::origin_ok(origin, "vx_trace")) return VX_ERR_INVALID;
     int rc = check_params(p);
     if (rc != VX_OK) return rc;
     if ((reinterpret_cast<uintptr_t>(rays_dev) & 15u) || (reinterpret_cast<uintptr_t>(out_dev) & 7u)) {
@@ -547,6 +551,7 @@ int check_queue(const VxWorld *w, const int32_t origin[3], const VxRay *rays_dev
         vx::set_error(std::string(fn) + ": null argument");
         return VX_ERR_INVALID;
     }
+    if (!vx::origin_ok(origin, fn)) return VX_ERR_INVALID;
     if (n >= 0xFFFFFFF0ull) {
         vx::set_error(std::string(fn) + ": at most 2^32 - 16 rays per queue");
         return VX_ERR_INVALID;
@@ -714,6 +719,24 @@ int vx_render_primary_gated(VxWorld *w, const VxCamera *cam, const VxTraceParams
     fa.shadow = shadow_dev;
     fa.tile_gate = tile_mask_dev;
     return run_frame(w, fa, as_stream(stream));
+}
+
+int vx_render_ao(VxWorld *w, const VxCamera *cam, const VxHitRecord *rec_dev, float *ao_dev,
+                 void *stream) {
+    if (!w || !rec_dev || !ao_dev) {
+        vx::set_error("vx_render_ao: null argument");
+        return VX_ERR_INVALID;
+    }
+    int rc = check_frame(cam);
+    if (rc != VX_OK) return rc;
+    if ((reinterpret_cast<uintptr_t>(rec_dev) & 7u) || (reinterpret_cast<uintptr_t>(ao_dev) & 3u)) {
+        vx::set_error("vx_render_ao: records must be 8-byte and AO 4-byte aligned");
+        return VX_ERR_INVALID;
+    }
+    rc = use_device(w);
+    if (rc != VX_OK) return rc;
+    VX_CK(vx::launch_ao(w->dw, *cam, rec_dev, ao_dev, as_stream(stream)));
+    return VX_OK;
 }
 
 int vx_render_primary_host(VxWorld *w, const VxCamera *cam, const VxTraceParams *p,

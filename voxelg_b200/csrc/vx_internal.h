@@ -79,6 +79,9 @@ cudaError_t launch_raycast(const DevWorld &w, const int32_t origin[3], const flo
                            const float *dirs, size_t n, VxPickHit *out, int32_t *hit,
                            cudaStream_t s);
 
+// contact AO of a frame's primary records (f32 per pixel)
+cudaError_t launch_ao(const DevWorld &w, const VxCamera &cam, const VxHitRecord *rec, float *ao,
+                      cudaStream_t s);
 cudaError_t launch_project_dirty(const DevWorld &w, const VxCamera &cam, const uint32_t *idx,
                                  size_t n, uint32_t *mask, cudaStream_t s);
 cudaError_t launch_refresh_tiles(uint32_t tiles_w, uint32_t tiles_h, uint32_t spread,
@@ -159,5 +162,16 @@ int world_device(const VxWorld *w);
 
 // thread-local error text
 void set_error(const std::string &msg);
+
+// The loaded window moves in x/z only (src/voxel.rs:439-445 keeps its y at
+// 0): storage y is world y, so a window corner with y != 0 would index past
+// the y extent of every level.  Entry points reject it.
+inline bool origin_ok(const int32_t o[3], const char *fn) {
+    if (o[1] != 0) {
+        set_error(std::string(fn) + ": window origin y must be 0 (windows move in x/z only)");
+        return false;
+    }
+    return true;
+}
 
 }  // namespace vx

@@ -82,6 +82,7 @@ extern "C" int vx_render_primary_noalloc(const VxWorldView *view, const VxCamera
         vx::set_error("vx_render_primary_noalloc: resolution must be an integer in [1, 32768]");
         return VX_ERR_INVALID;
     }
+    if (!vx::origin_ok(cam->world_origin, "vx_render_primary_noalloc")) return VX_ERR_INVALID;
     if (p->max_iters < 0 || p->any_max_iters < 0 || p->max_iters > (1 << 20) ||
         p->any_max_iters > (1 << 20)) {
         vx::set_error("vx_render_primary_noalloc: iteration caps outside [0, 2^20]");

@@ -261,6 +261,7 @@ int vx_proposal_features(VxProposal *p, VxWorld *w, const int32_t origin[3],
         vx::set_error("vx_proposal_features: null argument");
         return VX_ERR_INVALID;
     }
+    if (!vx::origin_ok(origin, "vx_proposal_features")) return VX_ERR_INVALID;
     VX_CK(cudaSetDevice(p->device));
     VX_CK(vx::mlp_features(vx::world_dev(w), origin, rays_dev, n, 0, 1, n, feats_dev, nullptr,
                            nullptr, as_stream(stream)));
@@ -389,6 +390,7 @@ int vx_render_learned(VxWorld *w, VxProposal *prop, const VxCamera *cam, const V
         vx::set_error("vx_render_learned: camera resolution must be an integer in [1, 32768]");
         return VX_ERR_INVALID;
     }
+    if (!vx::origin_ok(cam->world_origin, "vx_render_learned")) return VX_ERR_INVALID;
     if ((p->flags & (VX_F_BEAM | VX_F_SHADOW)) || p->max_iters < 0 || p->max_iters > (1 << 20) ||
         !(scale > 0.0f)) {
         vx::set_error("vx_render_learned: flags must not hold VX_F_BEAM / VX_F_SHADOW, "

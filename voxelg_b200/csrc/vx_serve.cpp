@@ -369,6 +369,7 @@ int vx_server_create(VxWorld *w, const int32_t origin[3], const VxTraceParams *p
         vx::set_error("vx_server_create: iteration caps outside [0, 2^20]");
         return VX_ERR_INVALID;
     }
+    if (!vx::origin_ok(origin, "vx_server_create")) return VX_ERR_INVALID;
     size_t cap = (size_t)(cfg->mem_budget_bytes / (uint64_t)cfg->slots / 56ull);
     if (cfg->max_batch_rays > 0) cap = std::min(cap, (size_t)cfg->max_batch_rays);
     if (cap < 1) {

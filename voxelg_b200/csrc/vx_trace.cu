@@ -532,9 +532,104 @@ __global__ void k_refresh_tiles(uint32_t tiles_w, uint32_t tiles_h, uint32_t spr
     if ((h >> 8) % spread == phase) atomicOr(mask + (ti >> 5), 1u << (ti & 31u));
 }
 
+// ------------------------------------------------------------------ AO
+// Contact AO of primary hits: compute_ao / ao_corner / ao_occluder /
+// is_voxel_solid (raymarch.wgsl:4417-4475, :297-322, skip rule :3862-3863,
+// AO_DIST :4522).  1.0 for misses and skipped hits.
+constexpr float kAoDist = 64.0f;
+
+__device__ __forceinline__ bool is_leaf_block(uint32_t m) {
+    return m == 14u || m == 25u || m == 26u || m == 27u;
+}
+
+// is_voxel_solid + !is_decoration_mat(voxel_material_at) at world voxel (x, y, z)
+__device__ __forceinline__ bool ao_occluder(const DevWorld &w, const Geo &g, Ro ro, int32_t x,
+                                            int32_t y, int32_t z) {
+    const Dims &d = w.d;
+    if ((uint32_t)(x - ro.x) >= (uint32_t)d.vx || (uint32_t)(y - ro.y) >= (uint32_t)d.vy ||
+        (uint32_t)(z - ro.z) >= (uint32_t)d.vz)
+        return false;
+    const uint32_t sx = (uint32_t)pos_mod(x, d.vx), sy = (uint32_t)y,
+                   sz = (uint32_t)pos_mod(z, d.vz);
+    if (!bit64(ldg(w.chunk_mask + chunk_index(g, sx, sy, sz)), child_of(sx, sy, sz, 4)))
+        return false;
+    if (!bit64(ldg(w.tile_mask + tile_index(g, sx, sy, sz)), child_of(sx, sy, sz, 2)))
+        return false;
+    const uint32_t bi = brick_index(g, sx >> 2, sy >> 2, sz >> 2);
+    const int vi = child_of(sx, sy, sz, 0);
+    if (!bit64(ldg(w.occ + bi), vi)) return false;
+    return !is_decoration((uint32_t)ldg(w.mat + (size_t)bi * 64u + vi));
+}
+
+// ao_corner: the two side voxels and the diagonal of one face corner
+__device__ __forceinline__ float ao_corner(const DevWorld &w, const Geo &g, Ro ro, int32_t bx,
+                                           int32_t by, int32_t bz, int32_t ax, int32_t ay,
+                                           int32_t az, int32_t cx, int32_t cy, int32_t cz) {
+    const bool s1 = ao_occluder(w, g, ro, bx + ax, by + ay, bz + az);
+    const bool s2 = ao_occluder(w, g, ro, bx + cx, by + cy, bz + cz);
+    const bool cd = ao_occluder(w, g, ro, bx + ax + cx, by + ay + cy, bz + az + cz);
+    if (s1 && s2) return 0.35f;
+    const int cnt = (int)s1 + (int)s2 + (int)cd;
+    return 1.0f - (float)cnt * 0.22f;
+}
+
+// WGSL mix(a, b, t) = a * (1 - t) + b * t
+__device__ __forceinline__ float mixf(float a, float b, float t) { return a * (1.0f - t) + b * t; }
+
+// one thread per pixel; origin = camera origin, dir = the pixel's ray_dir_uv
+__global__ void __launch_bounds__(128) k_ao(DevWorld w, VxCamera c,
+                                            const VxHitRecord *__restrict__ rec, uint32_t W,
+                                            uint32_t H, float *__restrict__ ao) {
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint32_t px = blockIdx.x * 16u + (warp & 1u) * 8u + (lane & 7u);
+    const uint32_t py = blockIdx.y * 8u + (warp >> 1) * 4u + (lane >> 3);
+    if (px >= W || py >= H) return;
+    const size_t idx = (size_t)py * W + px;
+    const uint2 *q = reinterpret_cast<const uint2 *>(rec + idx);
+    const uint2 q0 = q[0], q1 = q[1], q2 = q[2];
+    const uint32_t face = q1.y & 0xFFu, m = (q1.y >> 8) & 0xFFu, flags = (q1.y >> 16) & 0xFFu;
+    const float t = __uint_as_float(q2.x);
+    float r = 1.0f;
+    if ((flags & 1u) && !(t > kAoDist) && !is_leaf_block(m) && m != 33u) {
+        const Geo g = geo_of(w.d);
+        const Ro ro{c.world_origin[0], c.world_origin[1], c.world_origin[2]};
+        float dx, dy, dz;
+        const float u = (((float)px + 0.5f) + c.jitter_x) / c.res_x;
+        const float v = (((float)py + 0.5f) + c.jitter_y) / c.res_y;
+        ray_dir_uv(c, u, v, dx, dy, dz);
+        const int32_t vx = (int32_t)q0.x, vy = (int32_t)q0.y, vz = (int32_t)q1.x;
+        const float lx = (c.origin[0] + dx * t) - (float)vx;
+        const float ly = (c.origin[1] + dy * t) - (float)vy;
+        const float lz = (c.origin[2] + dz * t) - (float)vz;
+        const int na = (int)(face >> 1);
+        const int32_t nd = (face & 1u) ? -1 : 1;  // outward normal = -step
+        // face axes (da, db): (y, z) on an x face, (x, z) on y, (x, y) on z
+        const int32_t ax = na == 0 ? 0 : 1, ay = na == 0 ? 1 : 0, az = 0;
+        const int32_t cx = 0, cy = na == 2 ? 1 : 0, cz = na == 2 ? 0 : 1;
+        const float fa = na == 0 ? ly : lx, fb = na == 2 ? ly : lz;
+        const int32_t bx = vx + (na == 0 ? nd : 0), by = vy + (na == 1 ? nd : 0),
+                      bz = vz + (na == 2 ? nd : 0);
+        const float ao00 = ao_corner(w, g, ro, bx, by, bz, -ax, -ay, -az, -cx, -cy, -cz);
+        const float ao10 = ao_corner(w, g, ro, bx, by, bz, ax, ay, az, -cx, -cy, -cz);
+        const float ao01 = ao_corner(w, g, ro, bx, by, bz, -ax, -ay, -az, cx, cy, cz);
+        const float ao11 = ao_corner(w, g, ro, bx, by, bz, ax, ay, az, cx, cy, cz);
+        const float fa_c = clampf(fa, 0.0f, 1.0f), fb_c = clampf(fb, 0.0f, 1.0f);
+        r = mixf(mixf(ao00, ao10, fa_c), mixf(ao01, ao11, fa_c), fb_c);
+    }
+    ao[idx] = r;
+}
+
 }  // namespace
 
 // ------------------------------------------------------------- launchers
+cudaError_t launch_ao(const DevWorld &w, const VxCamera &cam, const VxHitRecord *rec, float *ao,
+                      cudaStream_t s) {
+    const uint32_t W = (uint32_t)cam.res_x, H = (uint32_t)cam.res_y;
+    const dim3 grid((W + 15u) / 16u, (H + 7u) / 8u);
+    k_ao<<<grid, 128, 0, s>>>(w, cam, rec, W, H, ao);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_project_dirty(const DevWorld &w, const VxCamera &cam, const uint32_t *idx,
                                  size_t n, uint32_t *mask, cudaStream_t s) {
     if (n == 0) return cudaSuccess;

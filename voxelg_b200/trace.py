@@ -140,6 +140,18 @@ def render_primary_host(world: DeviceWorld, cam: L.VxCamera, params: L.VxTracePa
     return rec_host, shadow_host
 
 
+def render_ao(world: DeviceWorld, cam: L.VxCamera, rec, ao=None, stream: int = 0):
+    """Contact AO of a frame's primary records (rec: CUDA uint8 tensor from
+    render_primary with the same camera); returns a float32 CUDA tensor."""
+    torch = _torch()
+    n = int(cam.res_x) * int(cam.res_y)
+    if ao is None:
+        ao = torch.empty(n, dtype=torch.float32, device=rec.device)
+    L.check(L.load().vx_render_ao(world.handle, C.byref(cam), C.c_void_p(rec.data_ptr()),
+                                  C.c_void_p(ao.data_ptr()), C.c_void_p(stream)))
+    return ao
+
+
 def render_stats(world: DeviceWorld, cam: L.VxCamera, params: L.VxTraceParams):
     """Algorithmic bytes and loop iterations of one frame:
     {"beam": (bytes, iters), "primary": (bytes, iters)} (primary includes
