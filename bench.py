@@ -25,6 +25,8 @@ Extra sections (rank 0, single GPU, a few seconds each; --no-extras skips
 them), all on the 512x256x512 world:
 mixed_queue  primary + spawned shadow + GI-probe + picking rays in one
            autotuned, graph-captured persistent launch.
+picking    benches/trace.rs raycast_pick rays: CPU restatement on one thread
+           (ns/ray) beside batched and single-call device picking.
 learned    the learned start-distance proposal: on-device training, then the
            plain DDA, the learned form and the verification without a network
            on one 1920x1080 frame, with acceptance and iterations saved.
@@ -251,6 +253,67 @@ def run_reference(args, cfg):
 
 
 # ---------------------------------------------------------------- extras
+def run_picking(vg, dw, n: int = 200_000) -> dict:
+    """The reference's criterion picking case (benches/trace.rs:24-40: origin
+    (256, 90, 256), dir (sin a, -0.5, cos a), a += 0.013) on the
+    512x256x512 world: the CPU baseline (the raycast restatement, one thread,
+    as criterion runs it) beside the device -- batched rays (event time) and
+    the single-ray drop-in call (wall time per call, copies and sync
+    included)."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    from oracle import pyoracle as po
+    from voxelg_b200 import _lib as L
+
+    a = (np.arange(1, n + 1, dtype=np.float32) * np.float32(0.013)).astype(np.float32)
+    dirs = np.stack([np.sin(a), np.full(n, -0.5, np.float32), np.cos(a)], 1).astype(np.float32)
+    cams = np.tile(np.array([256.0, 90.0, 256.0], np.float32), (n, 1))
+    ow = po.World(*dw.dims, arrays=dw.download())
+    want, whit, cpu_s = po.raycast_batch(ow, cams, dirs, threads=1)
+    del ow
+    dev = torch.device("cuda", dw.device)
+    c = torch.from_numpy(cams.reshape(-1)).to(dev)
+    d = torch.from_numpy(dirs.reshape(-1)).to(dev)
+    out = torch.empty(n * 24, dtype=torch.uint8, device=dev)
+    hit = torch.empty(n, dtype=torch.int32, device=dev)
+    lib = L.load()
+    stream = torch.cuda.current_stream(dev).cuda_stream
+
+    def batch():
+        L.check(lib.vx_raycast_batch(dw.handle, L.i3((0, 0, 0)), C.c_void_p(c.data_ptr()),
+                                     C.c_void_p(d.data_ptr()), n, C.c_void_p(out.data_ptr()),
+                                     C.c_void_p(hit.data_ptr()), C.c_void_p(stream)))
+    for _ in range(3):
+        batch()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(10):
+        batch()
+    e1.record()
+    torch.cuda.synchronize(dev)
+    gpu_ns = e0.elapsed_time(e1) / 10 * 1e6 / n
+    same = bool(np.array_equal(out.cpu().numpy(), want.view(np.uint8).reshape(-1)) and
+                np.array_equal(hit.cpu().numpy(), whit))
+    pick = L.VxPickHit()
+    calls = 2000
+    for i in range(20):
+        lib.vx_raycast(dw.handle, L.f3(cams[i]), L.f3(dirs[i]), L.i3((0, 0, 0)), C.byref(pick))
+    t0 = time.perf_counter()
+    for i in range(calls):
+        lib.vx_raycast(dw.handle, L.f3(cams[i]), L.f3(dirs[i]), L.i3((0, 0, 0)), C.byref(pick))
+    single_us = (time.perf_counter() - t0) / calls * 1e6
+    return {
+        "workload": f"benches/trace.rs raycast_pick rays x {n} on the 512x256x512 world",
+        "cpu_1thread_ns_per_ray": round(cpu_s * 1e9 / n, 1),
+        "gpu_batch_ns_per_ray": round(gpu_ns, 3),
+        "gpu_single_call_us": round(single_us, 2),
+        "hits": int(whit.sum()), "equal_to_cpu": same,
+    }
+
+
 def run_learned(vg, dw) -> dict:
     """Learned start-distance proposal on the 512x256x512 world at 1920x1080:
     train on the device (16.4M plain-DDA pairs from 200 poses), then time the
@@ -322,8 +385,8 @@ def run_learned(vg, dw) -> dict:
 def run_extras(vg, device: int) -> dict:
     """The other workloads on the 512x256x512 world, each a few seconds:
     the mixed ray queue (one autotuned, graph-captured persistent launch),
-    the learned proposal and the ray-query serving loop (64 Poisson
-    clients)."""
+    the criterion picking case, the learned proposal and the ray-query
+    serving loop (64 Poisson clients)."""
     import torch
 
     import voxelg_b200.queue as q
@@ -364,6 +427,7 @@ def run_extras(vg, device: int) -> dict:
     }
     g.close()
     del rt, o, sh
+    out["picking"] = run_picking(vg, dw)
     out["learned"] = run_learned(vg, dw)
     srv = sv.Server(dw, p, mem_budget_bytes=1 << 30, slots=8)
     st = srv.bench(clients=64, rate_per_client=200.0, seconds=3.0, min_rays=1, max_rays=50000,

@@ -36,9 +36,15 @@ struct VxWorld {
     size_t rec_cap = 0;
     VxShadowRecord *sh = nullptr;
     size_t sh_cap = 0;
-    float *pick_in = nullptr;        // 6 floats
-    VxPickHit *pick_out = nullptr;
-    int32_t *pick_hit = nullptr;
+    // single-ray picking: pinned, device-mapped host block that the kernel
+    // reads its ray from and writes its result to (no copies, one sync)
+    struct PickBox {
+        float in[8];
+        VxPickHit out;
+        int32_t hit;
+    };
+    PickBox *pick = nullptr;          // host address
+    PickBox *pick_dev = nullptr;      // device address of the same block
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
     uint32_t *d_work = nullptr;      // persistent-schedule counters (self-resetting)
     cudaStream_t copy_stream = nullptr;
@@ -100,9 +106,7 @@ void free_world(VxWorld *w) {
     cudaFree(w->d_stats);
     cudaFree(w->rec);
     cudaFree(w->sh);
-    cudaFree(w->pick_in);
-    cudaFree(w->pick_out);
-    cudaFree(w->pick_hit);
+    if (w->pick) cudaFreeHost(w->pick);
     cudaFree(w->d_work);
     cudaFree(w->d_gate_idx);
     w->qs.release();
@@ -279,9 +283,9 @@ int vx_world_create(const VxWorldDesc *desc, VxWorld **out) {
     VX_CKW(cudaMalloc(&w->d_stats, 4 * sizeof(unsigned long long)));
     VX_CKW(cudaMalloc(&w->d_work, 2 * sizeof(uint32_t)));
     VX_CKW(cudaMemsetAsync(w->d_work, 0, 2 * sizeof(uint32_t), w->stream));
-    VX_CKW(cudaMalloc(&w->pick_in, 8 * sizeof(float)));
-    VX_CKW(cudaMalloc(&w->pick_out, sizeof(VxPickHit)));
-    VX_CKW(cudaMalloc(&w->pick_hit, sizeof(int32_t)));
+    VX_CKW(cudaHostAlloc(reinterpret_cast<void **>(&w->pick), sizeof(VxWorld::PickBox),
+                         cudaHostAllocMapped));
+    VX_CKW(cudaHostGetDevicePointer(reinterpret_cast<void **>(&w->pick_dev), w->pick, 0));
     VX_CKW(cudaMemsetAsync(w->dw.occ, 0, d.n_bricks * sizeof(uint64_t), w->stream));
     VX_CKW(cudaMemsetAsync(w->dw.mat, 0, d.n_bricks * 64, w->stream));
     VX_CKW(cudaMemsetAsync(w->dw.tile_mask, 0, d.n_tiles * sizeof(uint64_t), w->stream));
@@ -462,15 +466,17 @@ int vx_raycast(VxWorld *w, const float cam[3], const float dir[3], const int32_t
     int rc = use_device(w);
     if (rc != VX_OK) return rc;
     std::lock_guard<std::mutex> lk(w->mu);
-    float in[6] = {cam[0], cam[1], cam[2], dir[0], dir[1], dir[2]};
-    VX_CK(cudaMemcpyAsync(w->pick_in, in, sizeof(in), cudaMemcpyHostToDevice, w->stream));
-    VX_CK(vx::launch_raycast(w->dw, origin, w->pick_in, w->pick_in + 3, 1, w->pick_out,
-                             w->pick_hit, w->stream));
-    int32_t hit = 0;
-    VX_CK(cudaMemcpyAsync(out, w->pick_out, sizeof(VxPickHit), cudaMemcpyDeviceToHost, w->stream));
-    VX_CK(cudaMemcpyAsync(&hit, w->pick_hit, sizeof(int32_t), cudaMemcpyDeviceToHost, w->stream));
+    // the ray goes in and the result comes back through the mapped block:
+    // one launch and one synchronization, no copies
+    for (int k = 0; k < 3; ++k) {
+        w->pick->in[k] = cam[k];
+        w->pick->in[3 + k] = dir[k];
+    }
+    VX_CK(vx::launch_raycast(w->dw, origin, w->pick_dev->in, w->pick_dev->in + 3, 1,
+                             &w->pick_dev->out, &w->pick_dev->hit, w->stream));
     VX_CK(cudaStreamSynchronize(w->stream));
-    return hit ? 1 : 0;
+    *out = w->pick->out;
+    return w->pick->hit ? 1 : 0;
 }
 
 int vx_raycast_batch(VxWorld *w, const int32_t origin[3], const float *cams_dev,
