@@ -479,7 +479,9 @@ typedef struct {
  * NULL: the verification then runs until it fails) and the verified-restart
  * traversal.  t_target = exp(proposal) * scale.  p->flags must not hold
  * VX_F_BEAM or VX_F_SHADOW.  With stats != NULL the call is synchronous and
- * fills the counters and CUDA-event times; else asynchronous on `stream`. */
+ * fills the counters and CUDA-event times; else asynchronous on `stream`.
+ * The per-pixel proposals live in the VxProposal: asynchronous calls with
+ * one proposal must not overlap on different streams. */
 int vx_render_learned(VxWorld *w, VxProposal *prop, const VxCamera *cam,
                       const VxTraceParams *p, float scale, VxHitRecord *rec_dev,
                       VxLearnedStats *stats, void *stream);

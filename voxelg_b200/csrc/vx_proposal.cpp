@@ -417,7 +417,6 @@ int vx_render_learned(VxWorld *w, VxProposal *prop, const VxCamera *cam, const V
     std::unique_lock<std::mutex> lk;
     unsigned long long *d_stats = nullptr;
     cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
-    bool own = false;
     if (prop) {
         lk = std::unique_lock<std::mutex>(prop->mu);
         if (prop->pred_cap < npx) {
@@ -434,18 +433,24 @@ int vx_render_learned(VxWorld *w, VxProposal *prop, const VxCamera *cam, const V
             d_stats = prop->stats;
             for (int k = 0; k < 3; ++k) ev[k] = prop->ev[k];
         }
-    } else if (stats) {
-        own = true;
-        VX_CK(cudaMalloc(&d_stats, 8 * sizeof(unsigned long long)));
-        for (auto &e : ev) VX_CK(cudaEventCreate(&e));
     }
-    auto release = [&]() {
-        if (own) {
-            cudaFree(d_stats);
-            for (auto &e : ev)
-                if (e) cudaEventDestroy(e);
+    // a statistics call without a proposal uses temporary scratch, released
+    // on every path out of this function
+    struct Temp {
+        unsigned long long *stats = nullptr;
+        cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+        ~Temp() {
+            if (stats) cudaFree(stats);
+            for (auto &x : ev)
+                if (x) cudaEventDestroy(x);
         }
-    };
+    } temp;
+    if (!prop && stats) {
+        VX_CK(cudaMalloc(&temp.stats, 8 * sizeof(unsigned long long)));
+        for (auto &x : temp.ev) VX_CK(cudaEventCreate(&x));
+        d_stats = temp.stats;
+        for (int k = 0; k < 3; ++k) ev[k] = temp.ev[k];
+    }
     cudaError_t e = cudaSuccess;
     if (stats) e = cudaMemsetAsync(d_stats, 0, 8 * sizeof(unsigned long long), s);
     if (e == cudaSuccess && stats) e = cudaEventRecord(ev[0], s);
@@ -472,7 +477,6 @@ int vx_render_learned(VxWorld *w, VxProposal *prop, const VxCamera *cam, const V
             if (!prop) stats->infer_ms = 0.0f;
         }
     }
-    release();
     if (e != cudaSuccess) {
         vx::set_error(std::string("vx_render_learned: ") + cudaGetErrorString(e));
         return e == cudaErrorMemoryAllocation ? VX_ERR_OOM : VX_ERR_CUDA;
