@@ -400,6 +400,30 @@ int vx_render_primary_noalloc(const VxWorldView *world, const VxCamera *cam,
                               const VxTraceParams *p, VxHitRecord *rec_dev,
                               VxShadowRecord *shadow_dev, void *stream);
 
+/* ---- ray-query messages in voxelG's network framing ----------------------
+ * For clients of src/net.rs: a frame is a u32 little-endian payload length
+ * (at most 16 MiB, net.rs:71-90) and a payload that bincode 1.3.3 writes
+ * for two variants appended to net.rs's `Message` (net.rs:46-67) after
+ * `Heartbeat`:
+ *   RayQuery  { id: u64, rays: Vec<WireRay> }         variant index 10
+ *   RayResult { id: u64, records: Vec<WireRecord> }   variant index 11
+ *   WireRay    { org: [f32; 3], dir: [f32; 3], tmax: f32, kind: u32 }
+ *   WireRecord { voxel: [i32; 3], face: u8, mat: u8, flags: u8, t: f32,
+ *                steps: u32 }
+ * (variant index u32, fixed-width little-endian fields, Vec as a u64 count
+ * and its elements).  The decoders reject frames whose prefix, variant or
+ * count disagrees with their length.  Host-only: no device is touched. */
+size_t vx_wire_query_bytes(size_t n);    /* whole frame, prefix included */
+size_t vx_wire_result_bytes(size_t n);
+int vx_wire_encode_query(uint64_t id, const VxRay *rays, size_t n, uint8_t *buf, size_t cap,
+                         size_t *len);
+int vx_wire_decode_query(const uint8_t *buf, size_t len, uint64_t *id, VxRay *rays, size_t cap,
+                         size_t *n);
+int vx_wire_encode_result(uint64_t id, const VxHitRecord *rec, size_t n, uint8_t *buf,
+                          size_t cap, size_t *len);
+int vx_wire_decode_result(const uint8_t *buf, size_t len, uint64_t *id, VxHitRecord *rec,
+                          size_t cap, size_t *n);
+
 /* ---- learned start-distance proposal ------------------------------------
  * No counterpart in the reference.  A 70 -> 64 -> 64 -> 64 -> 1 MLP with
  * GELU (tanh form) predicts log(first-hit t) of a ray from 6 ray values

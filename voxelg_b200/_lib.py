@@ -184,6 +184,16 @@ SIGNATURES = [
                                           _vp]),
     ("vx_render_primary_noalloc", C.c_int, [_P(VxWorldView), _P(VxCamera), _P(VxTraceParams),
                                             _vp, _vp, _vp]),
+    ("vx_wire_query_bytes", C.c_size_t, [C.c_size_t]),
+    ("vx_wire_result_bytes", C.c_size_t, [C.c_size_t]),
+    ("vx_wire_encode_query", C.c_int, [C.c_uint64, _vp, C.c_size_t, _vp, C.c_size_t,
+                                       _P(C.c_size_t)]),
+    ("vx_wire_decode_query", C.c_int, [_vp, C.c_size_t, _P(C.c_uint64), _vp, C.c_size_t,
+                                       _P(C.c_size_t)]),
+    ("vx_wire_encode_result", C.c_int, [C.c_uint64, _vp, C.c_size_t, _vp, C.c_size_t,
+                                        _P(C.c_size_t)]),
+    ("vx_wire_decode_result", C.c_int, [_vp, C.c_size_t, _P(C.c_uint64), _vp, C.c_size_t,
+                                        _P(C.c_size_t)]),
     ("vx_proposal_default_config", C.c_int, [_P(VxTrainConfig)]),
     ("vx_proposal_create", C.c_int, [_vp, C.c_uint64, _P(_vp)]),
     ("vx_proposal_destroy", C.c_int, [_vp]),

@@ -42,6 +42,7 @@ SOURCES = [
     ("vx_api.cpp", []),
     ("vx_host_world.cpp", []),
     ("vx_serve.cpp", []),
+    ("vx_wire.cpp", []),
 ]
 
 
