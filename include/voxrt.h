@@ -122,7 +122,8 @@ typedef struct {
     int32_t normal[3];
 } VxPickHit;
 
-/* Generic ray for vx_trace: kind 0 first hit (trace), 1 any hit (trace_any,
+/* Generic ray for vx_trace: kind (low two bits; higher bits ignored by
+ * vx_trace) 0 first hit (trace), 1 any hit (trace_any,
  * record.flags bit0 = occluded), 2 first non-transparent hit
  * (trace_no_water).  tmax replaces MAX_RAY_DIST / max_dist / t_cap. */
 typedef struct {

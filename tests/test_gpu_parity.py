@@ -197,6 +197,44 @@ def test_trace_kinds_bit_exact(vg, dev_c1, c1_oracle_world):
             dw_.close()
 
 
+def test_degenerate_rays_bit_exact(vg, dev_c1, c1_oracle_world):
+    """NaN / Inf / zero / denormal / huge origins and directions, Inf, NaN
+    and negative tmax, every kind and the shadow spawn bit: the device gives
+    the oracle's records (defined conversions: NaN -> 0, saturation, clamp
+    to +-2^30) through vx_trace and through the mixed queue."""
+    import voxelg_b200.queue as q
+    nan, inf = np.float32(np.nan), np.float32(np.inf)
+    origins = [(nan, 100, 100), (100, 100, 100), (inf, 100, 100), (-inf, -inf, -inf),
+               (1e30, 100, 100), (256, 300, 256), (0.0, 0.0, 0.0), (511.999, 255.999, 511.999)]
+    dirs = [(0, -1, 0), (nan, -1, 0), (0, 0, 0), (inf, -inf, 0), (1, 1, 1), (-1, 0, 0),
+            (1e-30, -1e-30, 1e-38), (1e-8, -1.0, 0.0)]
+    rays = []
+    for o in origins:
+        for d in dirs:
+            for tmax, kind in ((700.0, 0), (inf, 1), (-5.0, 2), (nan, 3), (64.0, 256),
+                               (300.0, 257), (300.0, 258)):
+                rays.append((o, d, tmax, kind))
+    r = np.zeros(len(rays), po.RAY)
+    for i, (o, d, tmax, kind) in enumerate(rays):
+        r[i]["org"], r[i]["dir"], r[i]["tmax"], r[i]["kind"] = o, d, tmax, kind
+    def canon(rec):
+        # a NaN hit distance (NaN origins) has no meaningful payload: x86 and
+        # the GPU produce different NaN bit patterns, so compare it as "NaN"
+        rec = np.ascontiguousarray(rec).view(po.RECORD).copy()
+        rec["t"][np.isnan(rec["t"])] = np.float32(np.nan)
+        return rec
+
+    p = vg.default_params(METHOD)
+    want, wsh = po.trace_batch(c1_oracle_world, r, p, shadows=True)[:2]
+    assert np.isnan(want["t"]).sum() > 0
+    got = vg.records(vg.trace(dev_c1, r, p))
+    assert_same_records(canon(got), canon(po.trace_batch(c1_oracle_world, r, p)[0]),
+                        "vx_trace degenerate")
+    _, out, sh = q.run(dev_c1, r, p)
+    assert_same_records(canon(vg.records(out)), canon(want), "queue degenerate")
+    assert np.array_equal(vg.shadows(sh).view(np.uint8), wsh.view(np.uint8))
+
+
 def test_raycast_matches_o1(vg, dev_c1, c1_oracle_world):
     rng = np.random.default_rng(5)
     n = 20000

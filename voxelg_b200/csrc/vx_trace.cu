@@ -317,7 +317,9 @@ __global__ void __launch_bounds__(128) k_trace_rays(TraceArgs ta, const VxRay *_
     if (i >= n) return;
     const float4 a = __ldg(reinterpret_cast<const float4 *>(rays + i));
     const float4 b = __ldg(reinterpret_cast<const float4 *>(rays + i) + 1);
-    const uint32_t kind = __float_as_uint(b.w);
+    // kind in the low two bits (1 any hit, 2 no water, else trace); the
+    // queue's spawn bit and other high bits are ignored here, as in the queue
+    const uint32_t kind = __float_as_uint(b.w) & 3u;
     const Ro ro{ta.ro[0], ta.ro[1], ta.ro[2]};
     uint64_t bytes = 0;
     Hit h;
