@@ -164,6 +164,41 @@ def test_shifted_window_origin(vg):
     dw.close()
 
 
+def test_non_power_of_two_world(vg):
+    """A world 768 voxels wide (192 x 32 x 128 bricks, x not a power of two)
+    under a shifted window: the general toroidal fold of the traversal gives
+    the oracle's records for frames, batched rays of every kind and the
+    queue."""
+    import voxelg_b200.queue as q
+    bricks = (192, 32, 128)
+    t = vg.TerrainParams(seed=0x5EED_0F_0DD, base_height=50.0, amplitude=24.0, water_level=30)
+    dw = vg.DeviceWorld(*bricks)
+    dw.generate(t)
+    ow = po.World(*bricks)
+    ow.generate(t)
+    got = dw.download()
+    for k in po.World.NAMES:
+        assert np.array_equal(got[k].view(np.uint8), ow.a[k].view(np.uint8)), k
+    for wo in ((0, 0, 0), (-448, 0, 320), (1216, 0, -192)):
+        cam = vg.camera_from_pose((wo[0] + 383.5, 100.0, wo[2] + 250.25), 1.3, -0.35,
+                                  math.radians(70), 200, 112, world_origin=wo)
+        for flags in (po.OR_F_L4, METHOD, METHOD | po.OR_F_BEAM | po.OR_F_SHADOW):
+            rec, sh, (wrec, wsh, _, _, _) = frame_pair(vg, dw, ow, cam, flags)
+            assert_same_records(rec, wrec, f"non-pow2 frame {wo} {flags}")
+            if sh is not None:
+                assert np.array_equal(sh.view(np.uint8), wsh.view(np.uint8))
+            assert (rec["flags"] & 1).any()
+        rng = np.random.default_rng(abs(wo[0]) + 7)
+        rays = random_rays(rng, 6000, (768, 128, 512))
+        rays["org"] += np.array(wo, np.float32)
+        p = vg.default_params(METHOD)
+        want = po.trace_batch(ow, rays, p, origin=wo)[0]
+        assert_same_records(vg.records(vg.trace(dw, rays, p, origin=wo)), want, "non-pow2 rays")
+        _, out, _ = q.run(dw, rays, p, origin=wo)
+        assert_same_records(vg.records(out), want, "non-pow2 queue")
+    dw.close()
+
+
 def random_rays(rng, n, vox, kinds=(0, 1, 2)):
     rays = np.zeros(n, po.RAY)
     lo = np.array([-40, -20, -40], np.float32)

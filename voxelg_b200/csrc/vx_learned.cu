@@ -321,9 +321,9 @@ __global__ void __launch_bounds__(128, 8) k_learned(LearnedArgs la) {
     uint32_t outcome = OUT_NONE, cells = 0, iters = 0, fallback = 0;
     if (live) {
         const DevWorld &w = la.ta.w;
-        const Geo g = geo_of(w.d);
-        const VxTraceParams &p = la.ta.p;
         const Ro ro{la.ta.ro[0], la.ta.ro[1], la.ta.ro[2]};
+        const Geo g = geo_of<FL>(w.d, ro);
+        const VxTraceParams &p = la.ta.p;
         const VxCamera &c = la.cam;
         float dx, dy, dz;
         const float u = (((float)px + 0.5f) + c.jitter_x) / c.res_x;
@@ -356,8 +356,6 @@ __global__ void __launch_bounds__(128, 8) k_learned(LearnedArgs la) {
                         s.vx = vd.r[0] + ro.x;
                         s.vy = vd.r[1] + ro.y;
                         s.vz = vd.r[2] + ro.z;
-                        s.sx = pos_mod(s.vx, w.d.vx);
-                        s.sz = pos_mod(s.vz, w.d.vz);
                         k.t_cur = vd.t_r;
                         k.la = -1;
                         k.iters = vd.good_cells;
@@ -404,6 +402,11 @@ __global__ void __launch_bounds__(128, 8) k_learned(LearnedArgs la) {
     }
 }
 
+template <uint32_t FL>
+struct LearnedK {
+    static void *fn() { return reinterpret_cast<void *>(&k_learned<FL>); }
+};
+
 }  // namespace
 
 cudaError_t launch_learned(const TraceArgs &ta, const VxCamera &cam, const float *proposal,
@@ -423,19 +426,9 @@ cudaError_t launch_learned(const TraceArgs &ta, const VxCamera &cam, const float
     la.sl.rox = ((ta.ro[0] % d.vx) + d.vx) % d.vx;
     la.sl.roz = ((ta.ro[2] % d.vz) + d.vz) % d.vz;
     const dim3 grid((la.W + 15u) / 16u, (la.H + 7u) / 8u);
-    const uint32_t fl = ta.p.flags & (VX_F_L4 | VX_F_LUT | VX_F_LOD);
+    const uint32_t fl = (ta.p.flags & (VX_F_L4 | VX_F_LUT | VX_F_LOD)) | pow2_bit(d);
     void *args[] = {&la};
-    const void *fn;
-    switch (fl) {
-        case 0: fn = (const void *)k_learned<0>; break;
-        case VX_F_L4: fn = (const void *)k_learned<VX_F_L4>; break;
-        case VX_F_LUT: fn = (const void *)k_learned<VX_F_LUT>; break;
-        case VX_F_LOD: fn = (const void *)k_learned<VX_F_LOD>; break;
-        case VX_F_L4 | VX_F_LUT: fn = (const void *)k_learned<VX_F_L4 | VX_F_LUT>; break;
-        case VX_F_L4 | VX_F_LOD: fn = (const void *)k_learned<VX_F_L4 | VX_F_LOD>; break;
-        case VX_F_LUT | VX_F_LOD: fn = (const void *)k_learned<VX_F_LUT | VX_F_LOD>; break;
-        default: fn = (const void *)k_learned<VX_F_L4 | VX_F_LUT | VX_F_LOD>; break;
-    }
+    const void *fn = pick_fl<LearnedK>(fl);
     return cudaLaunchKernel(fn, grid, dim3(128), args, 0, stream);
 }
 

@@ -53,9 +53,9 @@ __global__ void __launch_bounds__(256) k_queue(QueueArgs q) {
     constexpr uint32_t FULL = 0xFFFFFFFFu, IDLE = 0xFFFFFFFFu, DONE = 0xFFFFFFFEu;
     const uint32_t lane = threadIdx.x & 31u;
     const DevWorld &w = q.ta.w;
-    const Geo g = geo_of(w.d);
-    const VxTraceParams &p = q.ta.p;
     const Ro ro{q.ta.ro[0], q.ta.ro[1], q.ta.ro[2]};
+    const Geo g = geo_of<FL>(w.d, ro);
+    const VxTraceParams &p = q.ta.p;
     uint64_t bytes = 0;
     Walk k;
     Hit h;
@@ -236,18 +236,7 @@ struct QueueK {
     static void *fn() { return reinterpret_cast<void *>(&k_queue<FL>); }
 };
 
-void *queue_kernel(uint32_t fl) {
-    switch (fl & 7u) {
-        case 0: return QueueK<0>::fn();
-        case 1: return QueueK<1>::fn();
-        case 2: return QueueK<2>::fn();
-        case 3: return QueueK<3>::fn();
-        case 4: return QueueK<4>::fn();
-        case 5: return QueueK<5>::fn();
-        case 6: return QueueK<6>::fn();
-        default: return QueueK<7>::fn();
-    }
-}
+void *queue_kernel(uint32_t fl) { return pick_fl<QueueK>(fl); }
 
 }  // namespace
 
@@ -306,7 +295,7 @@ cudaError_t launch_queue(const TraceArgs &ta, const VxRay *rays, size_t n, VxHit
     q.shadow = shadow;
     q.work = sc.work;
     q.refill_min = (uint32_t)std::min(32, std::max(1, t.refill_min));
-    void *fn = queue_kernel(ta.p.flags);
+    void *fn = queue_kernel((ta.p.flags & 7u) | pow2_bit(ta.w.d));
     int dev = 0, sms = 0, per_sm = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);

@@ -159,7 +159,7 @@ __device__ __forceinline__ void primary_pixel(const FrameArgs &fa, uint32_t px, 
             float sdy = p.sun[1] + (p.sun_tangent[1] * cs + p.sun_bitangent[1] * sn) * radius;
             float sdz = p.sun[2] + (p.sun_tangent[2] * cs + p.sun_bitangent[2] * sn) * radius;
             normalize3(sdx, sdy, sdz);
-            occ = trace_any_ray<STATS>(fa.ta.w, p, ro, sox, soy, soz, sdx, sdy, sdz,
+            occ = trace_any_ray<FL, STATS>(fa.ta.w, p, ro, sox, soy, soz, sdx, sdy, sdz,
                                        p.shadow_max_dist, ssteps, bytes) ? 1u : 0u;
             traced = 1u;
             iters += ssteps;
@@ -194,10 +194,10 @@ __global__ void VX_FRAME_BOUNDS k_primary_refill(FrameArgs fa) {
     constexpr uint32_t FULL = 0xFFFFFFFFu, IDLE = 0xFFFFFFFFu, DONE = 0xFFFFFFFEu;
     const uint32_t lane = threadIdx.x & 31u;
     const DevWorld &w = fa.ta.w;
-    const Geo g = geo_of(w.d);
+    const Ro ro{fa.ta.ro[0], fa.ta.ro[1], fa.ta.ro[2]};
+    const Geo g = geo_of<FL>(w.d, ro);
     const VxTraceParams &p = fa.ta.p;
     const VxCamera &c = fa.cam;
-    const Ro ro{fa.ta.ro[0], fa.ta.ro[1], fa.ta.ro[2]};
     const bool beam_on = (p.flags & VX_F_BEAM) != 0u;
     const bool shadows_on = fa.shadow != nullptr && (p.flags & VX_F_SHADOW) != 0u;
     const uint32_t tiles_x = (fa.W + 7u) / 8u;
@@ -325,13 +325,13 @@ __global__ void __launch_bounds__(128) k_trace_rays(TraceArgs ta, const VxRay *_
     Hit h;
     if (kind == 1u) {
         uint32_t steps;
-        const bool occ = trace_any_ray<false>(ta.w, ta.p, ro, a.x, a.y, a.z, a.w, b.x, b.y, b.z,
+        const bool occ = trace_any_ray<FL, false>(ta.w, ta.p, ro, a.x, a.y, a.z, a.w, b.x, b.y, b.z,
                                               steps, bytes);
         set_miss(h);
         h.flags = occ ? 1u : 0u;
         h.steps = steps;
     } else if (kind == 2u) {
-        trace_no_water_ray<false>(ta.w, ta.p, ro, a.x, a.y, a.z, a.w, b.x, b.y, b.z, h, bytes);
+        trace_no_water_ray<FL, false>(ta.w, ta.p, ro, a.x, a.y, a.z, a.w, b.x, b.y, b.z, h, bytes);
     } else {
         trace_ray<FL, false>(ta.w, ta.p, ro, a.x, a.y, a.z, a.w, b.x, b.y, b.z, h, bytes);
     }
@@ -593,8 +593,8 @@ __global__ void __launch_bounds__(128) k_ao(DevWorld w, VxCamera c,
     const float t = __uint_as_float(q2.x);
     float r = 1.0f;
     if ((flags & 1u) && !(t > kAoDist) && !is_leaf_block(m) && m != 33u) {
-        const Geo g = geo_of(w.d);
         const Ro ro{c.world_origin[0], c.world_origin[1], c.world_origin[2]};
+        const Geo g = geo_of<kFlPow2>(w.d, ro);  // strides only
         float dx, dy, dz;
         const float u = (((float)px + 0.5f) + c.jitter_x) / c.res_x;
         const float v = (((float)py + 0.5f) + c.jitter_y) / c.res_y;
@@ -654,35 +654,29 @@ cudaError_t launch_beam(const FrameArgs &fa, float *beam_out, cudaStream_t s) {
 }
 
 // Method flags (L4 | LUT | LOD) -> the matching kernel instantiation.
-template <uint32_t FL, bool STATS>
+template <uint32_t FL>
 struct GridK {
-    static void *fn() { return reinterpret_cast<void *>(&k_primary<FL, STATS>); }
+    static void *fn() { return reinterpret_cast<void *>(&k_primary<FL, false>); }
 };
-template <uint32_t FL, bool STATS>
+template <uint32_t FL>
+struct GridKStats {
+    static void *fn() { return reinterpret_cast<void *>(&k_primary<FL, true>); }
+};
+template <uint32_t FL>
 struct PersistK {
-    static void *fn() { return reinterpret_cast<void *>(&k_primary_refill<FL, STATS>); }
+    static void *fn() { return reinterpret_cast<void *>(&k_primary_refill<FL, false>); }
 };
-
-template <template <uint32_t, bool> class K, bool STATS>
-void *pick_kernel(uint32_t fl) {
-    switch (fl & 7u) {
-        case 0: return K<0, STATS>::fn();
-        case 1: return K<1, STATS>::fn();
-        case 2: return K<2, STATS>::fn();
-        case 3: return K<3, STATS>::fn();
-        case 4: return K<4, STATS>::fn();
-        case 5: return K<5, STATS>::fn();
-        case 6: return K<6, STATS>::fn();
-        default: return K<7, STATS>::fn();
-    }
-}
+template <uint32_t FL>
+struct PersistKStats {
+    static void *fn() { return reinterpret_cast<void *>(&k_primary_refill<FL, true>); }
+};
 
 cudaError_t launch_primary(const FrameArgs &fa, cudaStream_t s) {
-    const uint32_t fl = fa.ta.p.flags;
+    const uint32_t fl = (fa.ta.p.flags & 7u) | pow2_bit(fa.ta.w.d);
     FrameArgs a = fa;
     void *args[] = {&a};
     if (fa.work) {
-        void *fn = fa.stats ? pick_kernel<PersistK, true>(fl) : pick_kernel<PersistK, false>(fl);
+        void *fn = fa.stats ? pick_fl<PersistKStats>(fl) : pick_fl<PersistK>(fl);
         int dev = 0, sms = 0, per_sm = 0;
         cudaError_t e = cudaGetDevice(&dev);
         if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -691,7 +685,7 @@ cudaError_t launch_primary(const FrameArgs &fa, cudaStream_t s) {
         if (per_sm < 1) per_sm = 1;
         return cudaLaunchKernel(fn, dim3((unsigned)(sms * per_sm)), dim3(128), args, 0, s);
     }
-    void *fn = fa.stats ? pick_kernel<GridK, true>(fl) : pick_kernel<GridK, false>(fl);
+    void *fn = fa.stats ? pick_fl<GridKStats>(fl) : pick_fl<GridK>(fl);
     if (fa.y1 <= fa.y0) return cudaSuccess;
     return cudaLaunchKernel(fn, dim3((fa.W + 15) / 16, (fa.y1 - fa.y0 + 7) / 8), dim3(128), args,
                             0, s);
@@ -706,17 +700,7 @@ cudaError_t launch_trace_rays(const TraceArgs &ta, const VxRay *rays, size_t n, 
                               cudaStream_t s) {
     if (n == 0) return cudaSuccess;
     const unsigned blocks = (unsigned)((n + 127) / 128);
-    void *fn;
-    switch (ta.p.flags & 7u) {
-        case 0: fn = TraceK<0>::fn(); break;
-        case 1: fn = TraceK<1>::fn(); break;
-        case 2: fn = TraceK<2>::fn(); break;
-        case 3: fn = TraceK<3>::fn(); break;
-        case 4: fn = TraceK<4>::fn(); break;
-        case 5: fn = TraceK<5>::fn(); break;
-        case 6: fn = TraceK<6>::fn(); break;
-        default: fn = TraceK<7>::fn(); break;
-    }
+    void *fn = pick_fl<TraceK>((ta.p.flags & 7u) | pow2_bit(ta.w.d));
     TraceArgs a = ta;
     const VxRay *r = rays;
     size_t nn = n;

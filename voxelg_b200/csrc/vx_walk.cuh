@@ -23,6 +23,27 @@
 namespace vx {
 namespace {
 
+// Internal template bit beside the method flags: the world's x and z voxel
+// dims are powers of two, so the toroidal slot is a mask.  Launchers set it
+// from the world's dims; callers never see it.
+constexpr uint32_t kFlPow2 = 1u << 8;
+inline uint32_t pow2_bit(const Dims &d) {
+    return ((d.vx & (d.vx - 1)) == 0 && (d.vz & (d.vz - 1)) == 0) ? kFlPow2 : 0u;
+}
+// kernel pointer K<fl>::fn() for method flags (low 3 bits) + kFlPow2
+template <template <uint32_t> class K>
+void *pick_fl(uint32_t fl) {
+    switch (fl & (7u | kFlPow2)) {
+#define VX_FL_CASE(v) \
+    case v: return K<v>::fn(); \
+    case v | kFlPow2: return K<v | kFlPow2>::fn();
+        VX_FL_CASE(0) VX_FL_CASE(1) VX_FL_CASE(2) VX_FL_CASE(3)
+        VX_FL_CASE(4) VX_FL_CASE(5) VX_FL_CASE(6) VX_FL_CASE(7)
+#undef VX_FL_CASE
+        default: return nullptr;
+    }
+}
+
 // ---------------------------------------------------------------- helpers
 __device__ __forceinline__ float vmin(float a, float b) { return (b < a) ? b : a; }
 __device__ __forceinline__ float vmax(float a, float b) { return (a < b) ? b : a; }
@@ -39,20 +60,6 @@ __device__ __forceinline__ int32_t f2i(float x) {
 __device__ __forceinline__ int32_t pos_mod(int32_t a, int32_t b) {
     if (a >= 0) return a % b;
     return (b - 1) - ((-1 - a) % b);
-}
-// v reduced into [0, n) where v is known congruent to the wanted slot; a
-// jump of a few cells needs at most two corrections, far jumps (only the
-// degenerate skip with no forward face) fall back to the division.
-__device__ __forceinline__ int32_t wrap_near(int32_t v, int32_t n) {
-    if (v < 0) {
-        v += n;
-        if (v < 0) v += n;
-    } else if (v >= n) {
-        v -= n;
-        if (v >= n) v -= n;
-    }
-    if ((uint32_t)v >= (uint32_t)n) v = pos_mod(v, n);
-    return v;
 }
 // common.wgsl:55-58
 __device__ __forceinline__ float safe_inv(float x) {
@@ -106,7 +113,6 @@ struct Dda {
     float ix, iy, iz;      // safe_inv(dir)
     float mx, my, mz;      // t_max
     int32_t vx, vy, vz;    // voxel, absolute world coords
-    int32_t sx, sz;        // toroidal slot x/z (slot y == vy)
     int32_t stx, sty, stz; // step
 };
 
@@ -145,8 +151,6 @@ __device__ __forceinline__ bool dda_init(const Dims &d, Ro ro, float o0, float o
     s.mx = s.stx > 0 ? ((float)(lx + 1) - s.ox) * s.ix : ((float)lx - s.ox) * s.ix;
     s.my = s.sty > 0 ? ((float)(ly + 1) - s.oy) * s.iy : ((float)ly - s.oy) * s.iy;
     s.mz = s.stz > 0 ? ((float)(lz + 1) - s.oz) * s.iz : ((float)lz - s.oz) * s.iz;
-    s.sx = pos_mod(s.vx, d.vx);
-    s.sz = pos_mod(s.vz, d.vz);
     return true;
 }
 
@@ -169,9 +173,6 @@ __device__ __forceinline__ void dda_step(const Dims &d, Dda &s, float &t_cur, in
     if (s.mx < s.my && s.mx < s.mz) {
         t_cur = s.mx;
         s.vx += s.stx;
-        s.sx += s.stx;
-        if (s.sx >= d.vx) s.sx -= d.vx;
-        else if (s.sx < 0) s.sx += d.vx;
         s.mx = s.mx + fabsf(s.ix);
         la = 0;
     } else if (s.my < s.mz) {
@@ -182,9 +183,6 @@ __device__ __forceinline__ void dda_step(const Dims &d, Dda &s, float &t_cur, in
     } else {
         t_cur = s.mz;
         s.vz += s.stz;
-        s.sz += s.stz;
-        if (s.sz >= d.vz) s.sz -= d.vz;
-        else if (s.sz < 0) s.sz += d.vz;
         s.mz = s.mz + fabsf(s.iz);
         la = 2;
     }
@@ -216,9 +214,6 @@ __device__ __forceinline__ void skip_to_cell(const Dims &d, Ro ro, int32_t cell,
     nx = ax == 0 ? nbx : nx;
     ny = ax == 1 ? nby : ny;
     nz = ax == 2 ? nbz : nz;
-    // slot of the new voxel: old slot + displacement, folded (== pos_mod(n, dims))
-    s.sx = wrap_near(s.sx + (nx - s.vx), d.vx);
-    s.sz = wrap_near(s.sz + (nz - s.vz), d.vz);
     s.vx = nx; s.vy = ny; s.vz = nz;
     const int32_t lx = nx - ro.x, ly = ny - ro.y, lz = nz - ro.z;
     s.mx = ((float)(s.stx > 0 ? lx + 1 : lx) - s.ox) * s.ix;
@@ -230,11 +225,6 @@ __device__ __forceinline__ void skip_to_cell(const Dims &d, Ro ro, int32_t cell,
 // t of the face just crossed: t_max[la] - t_delta[la]
 __device__ __forceinline__ float crossed_t(const Dda &s, int la) {
     return la == 0 ? s.mx - fabsf(s.ix) : (la == 1 ? s.my - fabsf(s.iy) : s.mz - fabsf(s.iz));
-}
-
-__device__ __forceinline__ bool out_of_window(const Dims &d, const Dda &s, Ro ro) {
-    return (uint32_t)(s.vx - ro.x) >= (uint32_t)d.vx || (uint32_t)(s.vy - ro.y) >= (uint32_t)d.vy ||
-           (uint32_t)(s.vz - ro.z) >= (uint32_t)d.vz;
 }
 
 struct Hit {
@@ -296,9 +286,18 @@ __device__ __forceinline__ uint32_t brick_topmost(const uint8_t *__restrict__ mr
 // device memory are below 2^32; only the material row offset is widened).
 struct Geo {
     uint32_t bx, bxy, tx, txy, cx, cxy, lx, lxy;
+    uint32_t rox, roz;  // pos_mod(window corner x / z, dims): slot of window voxel 0
 };
-__device__ __forceinline__ Geo geo_of(const Dims &d) {
+// FL's kFlPow2 bit: the slot is a mask and the window corner's fold is unused
+template <uint32_t FL>
+__device__ __forceinline__ Geo geo_of(const Dims &d, Ro ro) {
     Geo g;
+    if ((FL & kFlPow2) != 0u) {
+        g.rox = g.roz = 0u;
+    } else {
+        g.rox = (uint32_t)pos_mod(ro.x, d.vx);
+        g.roz = (uint32_t)pos_mod(ro.z, d.vz);
+    }
     g.bx = (uint32_t)d.bx;
     g.bxy = (uint32_t)(d.bx * d.by);
     g.tx = (uint32_t)d.tx;
@@ -376,8 +375,27 @@ __device__ __forceinline__ int walk_step(const DevWorld &w, const Geo &g, const 
     if (k.iters >= k.cap) return WALK_END;
     ++k.iters;
     if (k.t_cur > k.tmax) return WALK_END;
-    if (out_of_window(d, s, ro)) return WALK_END;
-    const uint32_t sx = (uint32_t)s.sx, sy = (uint32_t)s.vy, sz = (uint32_t)s.sz;
+    // window test, then the toroidal slot (world_to_slot_voxel,
+    // raymarch.wgsl:17-23) from the window-relative voxel: lx < dims and
+    // rox < dims, so one conditional subtraction folds it
+    uint32_t sx, sz;
+    if ((FL & kFlPow2) != 0u) {
+        if ((uint32_t)(s.vx - ro.x) >= (uint32_t)d.vx || (uint32_t)(s.vy - ro.y) >= (uint32_t)d.vy ||
+            (uint32_t)(s.vz - ro.z) >= (uint32_t)d.vz)
+            return WALK_END;
+        sx = (uint32_t)s.vx & (uint32_t)(d.vx - 1);
+        sz = (uint32_t)s.vz & (uint32_t)(d.vz - 1);
+    } else {
+        const uint32_t lx = (uint32_t)(s.vx - ro.x), lz = (uint32_t)(s.vz - ro.z);
+        if (lx >= (uint32_t)d.vx || (uint32_t)(s.vy - ro.y) >= (uint32_t)d.vy ||
+            lz >= (uint32_t)d.vz)
+            return WALK_END;
+        sx = lx + g.rox;
+        sz = lz + g.roz;
+        if (sx >= (uint32_t)d.vx) sx -= (uint32_t)d.vx;
+        if (sz >= (uint32_t)d.vz) sz -= (uint32_t)d.vz;
+    }
+    const uint32_t sy = (uint32_t)s.vy;
     const uint32_t ti = tile_index(g, sx, sy, sz);
     // batch 1: every coarse word addressed by the slot coordinate
     uint64_t lw = ~0ull;
@@ -481,7 +499,7 @@ template <uint32_t FL, bool STATS>
 __device__ __forceinline__ void trace_ray(const DevWorld &w, const VxTraceParams &p, Ro ro,
                                           float o0, float o1, float o2, float d0, float d1,
                                           float d2, float max_dist, Hit &h, uint64_t &bytes) {
-    const Geo g = geo_of(w.d);
+    const Geo g = geo_of<FL>(w.d, ro);
     set_miss(h);
     Walk k;
     if (!walk_init(w.d, ro, KIND_TRACE, p, o0, o1, o2, d0, d1, d2, max_dist, k)) {
@@ -493,38 +511,38 @@ __device__ __forceinline__ void trace_ray(const DevWorld &w, const VxTraceParams
     h.steps = k.iters;
 }
 
-// trace_any() over one ray: returns occluded
-template <bool STATS>
+// trace_any() over one ray: returns occluded (FLP carries kFlPow2 only)
+template <uint32_t FLP, bool STATS>
 __device__ __forceinline__ bool trace_any_ray(const DevWorld &w, const VxTraceParams &p, Ro ro,
                                               float o0, float o1, float o2, float d0, float d1,
                                               float d2, float max_dist, uint32_t &steps,
                                               uint64_t &bytes) {
-    const Geo g = geo_of(w.d);
+    const Geo g = geo_of<FLP>(w.d, ro);
     Walk k;
     Hit h;
     steps = 0;
     if (!walk_init(w.d, ro, KIND_ANY, p, o0, o1, o2, d0, d1, d2, max_dist, k)) return false;
     int r;
-    while ((r = walk_step<0, STATS, KIND_ANY>(w, g, p, ro, k, h, bytes)) == WALK_CONT) {
+    while ((r = walk_step<FLP & kFlPow2, STATS, KIND_ANY>(w, g, p, ro, k, h, bytes)) == WALK_CONT) {
     }
     steps = k.iters;
     return r == WALK_HIT;
 }
 
-// trace_no_water() over one ray
-template <bool STATS>
+// trace_no_water() over one ray (FLP carries kFlPow2 only)
+template <uint32_t FLP, bool STATS>
 __device__ __forceinline__ void trace_no_water_ray(const DevWorld &w, const VxTraceParams &p,
                                                    Ro ro, float o0, float o1, float o2,
                                                    float d0, float d1, float d2, float t_cap,
                                                    Hit &h, uint64_t &bytes) {
-    const Geo g = geo_of(w.d);
+    const Geo g = geo_of<FLP>(w.d, ro);
     set_miss(h);
     Walk k;
     if (!walk_init(w.d, ro, KIND_NO_WATER, p, o0, o1, o2, d0, d1, d2, t_cap, k)) {
         h.steps = 0;
         return;
     }
-    while (walk_step<0, STATS, KIND_NO_WATER>(w, g, p, ro, k, h, bytes) == WALK_CONT) {
+    while (walk_step<FLP & kFlPow2, STATS, KIND_NO_WATER>(w, g, p, ro, k, h, bytes) == WALK_CONT) {
     }
     h.steps = k.iters;
 }
