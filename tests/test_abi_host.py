@@ -111,3 +111,23 @@ def test_host_world_dirty_tracking():
     # a device sync clears all_dirty; emulate via the ABI contract: after
     # rebuild everything is dirty, so dirty_count reports every brick
     assert hw.dirty_count() == 64 * 16 * 64
+
+
+def test_header_compiles_as_c99_and_links(tmp_path):
+    """include/voxrt.h is plain C: a strict C99 caller compiles against it,
+    links libvoxrt.so and drives the host-only entry points without a GPU."""
+    import shutil
+    import subprocess
+    from voxelg_b200 import _lib as L
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    exe = tmp_path / "abi_smoke"
+    libdir = str(L.LIB_PATH.parent)
+    subprocess.run([cc, "-std=c99", "-Wall", "-Wextra", "-Werror", "-pedantic",
+                    f"-I{ROOT / 'include'}", str(ROOT / "tests" / "c" / "abi_smoke.c"),
+                    "-o", str(exe), f"-L{libdir}", "-lvoxrt", f"-Wl,-rpath,{libdir}", "-lm"],
+                   check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, out.stderr
+    assert "c abi ok" in out.stdout
