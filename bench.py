@@ -67,6 +67,10 @@ def parse_args():
     ap.add_argument("--profile", action="store_true",
                     help="frames only (one counting pass, warm-up, K timed frames): the "
                          "command profiled with ncu")
+    ap.add_argument("--profile-learned", action="store_true",
+                    help="the learned-form frames only (a short training, then K plain, "
+                         "learned and verification-only frames): the command profiled "
+                         "with ncu")
     return ap.parse_args()
 
 
@@ -602,10 +606,39 @@ def run_ours(args, cfg):
         dist.destroy_process_group()
 
 
+def profile_learned(args):
+    """K frames of each form on the 512x256x512 world at 1920x1080 after a
+    short training (20 poses, 200 steps): the launches ncu captures."""
+    import torch
+
+    import voxelg_b200 as vg
+    from voxelg_b200 import learned as vl
+    c1 = vg.CONFIGS["c1"]
+    dw = vg.DeviceWorld(*c1.bricks)
+    dw.generate(c1.terrain)
+    cam = vg.default_camera(dw, 1920, 1080)
+    p = vg.default_params(7)
+    prop = vl.Proposal(dw, seed=7)
+    prop.train(dw, vl.default_config(poses=20, rays_per_pose=16384, steps=200,
+                                     held_out_poses=0))
+    rec = torch.empty(1920 * 1080 * 24, dtype=torch.uint8, device="cuda")
+    for _ in range(args.steps):
+        vg.render_primary(dw, cam, p, rec)
+        vl.render_learned(dw, prop, cam, p, rec, stats=False)
+        vl.render_learned(dw, None, cam, p, rec, stats=False)
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_learned_frames": args.steps}), flush=True)
+    prop.close()
+    dw.close()
+
+
 def main():
     args = parse_args()
     import voxelg_b200.configs as configs
     cfg = configs.CONFIGS[CONFIG_NAME]
+    if args.profile_learned:
+        profile_learned(args)
+        return
     if args.impl == "reference":
         run_reference(args, cfg)
     else:
