@@ -8,7 +8,7 @@
 // its shadow ray (raymarch.wgsl:3953-3994).  Lanes of a warp refill together
 // once `refill_min` of them are idle (a lone refill would stall 31 lanes
 // through a ray set-up).  Optionally the queue is first reordered by a
-// coherence key (kind, coarse origin cell, direction on a 16x16 octahedral
+// coherence key (kind, window half in x and z, direction on a 64x64 octahedral
 // grid) with a counting sort, so that a warp's rays start near each other
 // and head the same way.  Results do not depend on
 // any of these choices; the autotuner checks that and keeps the fastest.
@@ -152,9 +152,18 @@ __global__ void __launch_bounds__(256) k_queue(QueueArgs q) {
 }
 
 // ---- coherence reorder: 16-bit key = kind(2) | origin cell(6) | direction(8)
-__device__ __forceinline__ uint32_t spread3(uint32_t v) {  // 4 bits -> every third bit
-    v &= 0xFu;
-    return (v & 1u) | ((v & 2u) << 2) | ((v & 4u) << 4) | ((v & 8u) << 6);
+
+// atomicAdd(base + key, 1) for every active lane, one atomic per distinct
+// key in the warp; returns this lane's slot among the lanes sharing its key
+__device__ __forceinline__ uint32_t warp_count(uint32_t *base, uint32_t key) {
+    const unsigned active = __activemask();
+    const unsigned peers = __match_any_sync(active, key);
+    const int leader = __ffs(peers) - 1;
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t off = 0;
+    if ((int)lane == leader) off = atomicAdd(base + key, (uint32_t)__popc(peers));
+    off = __shfl_sync(peers, off, leader);
+    return off + (uint32_t)__popc(peers & ((1u << lane) - 1u));
 }
 
 __global__ void k_sort_keys(const VxRay *rays, uint32_t n, int32_t rox, int32_t roy, int32_t roz,
@@ -164,7 +173,7 @@ __global__ void k_sort_keys(const VxRay *rays, uint32_t n, int32_t rox, int32_t 
     float ox, oy, oz, dx, dy, dz, tmax;
     uint32_t kind;
     load_ray(rays, i, ox, oy, oz, dx, dy, dz, tmax, kind);
-    // direction on a 16x16 octahedral grid (rays sharing an origin -- the
+    // direction on a 64x64 octahedral grid (rays sharing an origin -- the
     // primaries -- then group by screen region)
     const float l1 = fabsf(dx) + fabsf(dy) + fabsf(dz);
     float u = l1 > 0.f ? dx / l1 : 0.f, v = l1 > 0.f ? dz / l1 : 0.f;
@@ -173,17 +182,17 @@ __global__ void k_sort_keys(const VxRay *rays, uint32_t n, int32_t rox, int32_t 
         v = (1.f - fabsf(u)) * (v < 0.f ? -1.f : 1.f);
         u = uu;
     }
-    const uint32_t qu = (uint32_t)min(15, max(0, (int32_t)((u + 1.f) * 8.f)));
-    const uint32_t qv = (uint32_t)min(15, max(0, (int32_t)((v + 1.f) * 8.f)));
-    // origin on a coarse Morton grid (2 bits per axis)
+    const uint32_t qu = (uint32_t)min(63, max(0, (int32_t)((u + 1.f) * 32.f)));
+    const uint32_t qv = (uint32_t)min(63, max(0, (int32_t)((v + 1.f) * 32.f)));
+    // origin: which half of the window in x and in z (the window split in
+    // quarters by `shift`, then halved)
     const int32_t cx = max(0, (int32_t)floorf(ox) - rox) >> shift;
-    const int32_t cy = max(0, (int32_t)floorf(oy) - roy) >> shift;
     const int32_t cz = max(0, (int32_t)floorf(oz) - roz) >> shift;
-    const uint32_t cell = (spread3((uint32_t)cx & 3u) | (spread3((uint32_t)cy & 3u) << 1) |
-                           (spread3((uint32_t)cz & 3u) << 2)) & 0x3Fu;
-    const uint32_t key = ((kind & 3u) << 14) | (cell << 8) | (qv << 4) | qu;
+    (void)roy;
+    const uint32_t cell = ((uint32_t)(cx >> 1) & 1u) | (((uint32_t)(cz >> 1) & 1u) << 1);
+    const uint32_t key = ((kind & 3u) << 14) | (cell << 12) | (qv << 6) | qu;
     keys[i] = key;
-    atomicAdd(hist + key, 1u);
+    warp_count(hist, key);
 }
 
 // exclusive scan of the 65536-bin histogram in one 1024-thread CTA
@@ -212,7 +221,7 @@ __global__ void __launch_bounds__(1024) k_scan_bins(uint32_t *hist) {
 __global__ void k_scatter(const uint32_t *keys, uint32_t n, uint32_t *cursor, uint32_t *order) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    order[atomicAdd(cursor + keys[i], 1u)] = i;
+    order[warp_count(cursor, keys[i])] = i;
 }
 
 // order-independent fingerprint of the outputs (autotuner consistency check)
