@@ -36,72 +36,132 @@ namespace vx {
 namespace {
 
 // ------------------------------------------------------------------ beam
-// cs_beam + trace_first_tile, beam.wgsl:30-113 (world, non-rebased coords)
-template <bool STATS>
+// Chunk masks staged in shared memory for the beam walk when they fit.
+// 40 KB keeps dynamic plus static shared memory under the default 48 KB.
+constexpr uint32_t kBeamSmemBytes = 40u * 1024u;
+constexpr uint32_t kWaitLimit = 1u << 20;   // mbarrier polls before giving up
+
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0u;
+}
+
+// cs_beam + trace_first_tile, beam.wgsl:30-113 (world, non-rebased coords).
+// SMEM: the whole chunk-mask array is brought into shared memory by one bulk
+// TMA copy (cp.async.bulk completing on an mbarrier) before the walk, so each
+// of the up to 80 dependent steps reads shared memory.  The wait is bounded:
+// on a timeout the CTA reads global memory instead (same values, same
+// records) and waits, again bounded, for the copy to land before it exits.
+template <bool STATS, bool SMEM>
 __global__ void __launch_bounds__(128) k_beam(FrameArgs fa, float *beam_out) {
+    extern __shared__ __align__(16) uint64_t s_chunk[];
+    __shared__ __align__(8) uint64_t s_bar;
+    const Dims &d = fa.ta.w.d;
+    bool staged = false;
+    uint32_t bar = 0;
+    if (SMEM) {
+        bar = (uint32_t)__cvta_generic_to_shared(&s_bar);
+        const uint32_t bytes = (uint32_t)d.n_chunks * 8u;  // launcher: 16-byte multiple
+        if (threadIdx.x == 0) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+                         "r"(bytes)
+                         : "memory");
+            asm volatile(
+                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], "
+                "%2, [%3];" ::"r"((uint32_t)__cvta_generic_to_shared(s_chunk)),
+                "l"(fa.ta.w.chunk_mask), "r"(bytes), "r"(bar)
+                : "memory");
+        }
+        for (uint32_t it = 0; it < kWaitLimit && !staged; ++it) staged = mbar_try_wait(bar, 0u);
+    }
     const uint32_t gx = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t gy = blockIdx.y;
-    if (gx >= fa.bw || gy >= fa.bh) return;
-    const VxCamera &c = fa.cam;
-    const Dims &d = fa.ta.w.d;
-    uint64_t bytes = 0, iters = 0;
-    float dx, dy, dz;
-    ray_dir_uv(c, ((float)gx * 8.0f + 4.0f) / c.res_x, ((float)gy * 8.0f + 4.0f) / c.res_y, dx,
-               dy, dz);
-    float result = 1e9f;
-    const float ix = safe_inv(dx), iy = safe_inv(dy), iz = safe_inv(dz);
-    const float wminx = (float)c.world_origin[0], wminy = (float)c.world_origin[1],
-                wminz = (float)c.world_origin[2];
-    const float wmaxx = wminx + (float)d.vx, wmaxy = wminy + (float)d.vy,
-                wmaxz = wminz + (float)d.vz;
-    const float t0x = (wminx - c.origin[0]) * ix, t1x = (wmaxx - c.origin[0]) * ix;
-    const float t0y = (wminy - c.origin[1]) * iy, t1y = (wmaxy - c.origin[1]) * iy;
-    const float t0z = (wminz - c.origin[2]) * iz, t1z = (wmaxz - c.origin[2]) * iz;
-    const float t_enter = vmax(vmax(vmin(t0x, t1x), vmin(t0y, t1y)), vmax(vmin(t0z, t1z), 0.0f));
-    const float t_exit = vmin(vmin(vmax(t0x, t1x), vmax(t0y, t1y)), vmax(t0z, t1z));
-    if (!(t_enter >= t_exit || t_exit < 0.0f)) {
-        const float tb = t_enter + 0.05f;
-        const float px = clampf(c.origin[0] + dx * tb, wminx + 0.01f, wmaxx - 0.01f);
-        const float py = clampf(c.origin[1] + dy * tb, wminy + 0.01f, wmaxy - 0.01f);
-        const float pz = clampf(c.origin[2] + dz * tb, wminz + 0.01f, wmaxz - 0.01f);
-        int32_t tx = f2i(floorf(px / 16.0f)), ty = f2i(floorf(py / 16.0f)),
-                tz = f2i(floorf(pz / 16.0f));
-        const int32_t sx = sgn(dx), sy = sgn(dy), sz = sgn(dz);
-        const float tdx = fabsf(ix) * 16.0f, tdy = fabsf(iy) * 16.0f, tdz = fabsf(iz) * 16.0f;
-        float mx = sx > 0 ? ((float)((tx + 1) * 16) - c.origin[0]) * ix
-                          : ((float)(tx * 16) - c.origin[0]) * ix;
-        float my = sy > 0 ? ((float)((ty + 1) * 16) - c.origin[1]) * iy
-                          : ((float)(ty * 16) - c.origin[1]) * iy;
-        float mz = sz > 0 ? ((float)((tz + 1) * 16) - c.origin[2]) * iz
-                          : ((float)(tz * 16) - c.origin[2]) * iz;
-        const int32_t otx = c.world_origin[0] / 16, oty = c.world_origin[1] / 16,
-                      otz = c.world_origin[2] / 16;
-        float t_cur = t_enter;
-        for (int s = 0; s < 80; ++s) {
-            ++iters;
-            if ((uint32_t)(tx - otx) >= (uint32_t)d.tx || (uint32_t)(ty - oty) >= (uint32_t)d.ty ||
-                (uint32_t)(tz - otz) >= (uint32_t)d.tz)
-                break;
-            const int32_t stx = pos_mod(tx, d.tx), sty = ty, stz = pos_mod(tz, d.tz);
-            const int64_t ci = (int64_t)(stx / 4) + (int64_t)(sty / 4) * d.cx +
-                               (int64_t)(stz / 4) * d.cx * d.cy;
-            const int lin = (stx & 3) + (stz & 3) * 4 + (sty & 3) * 16;
-            if (STATS) bytes += 8;
-            if (bit64(ldg(fa.ta.w.chunk_mask + ci), lin)) {
-                result = t_cur;
-                break;
-            }
-            if (mx < my && mx < mz) {
-                tx += sx; t_cur = mx; mx = mx + tdx;
-            } else if (my < mz) {
-                ty += sy; t_cur = my; my = my + tdy;
-            } else {
-                tz += sz; t_cur = mz; mz = mz + tdz;
+    if (gx < fa.bw && gy < fa.bh) {
+        const VxCamera &c = fa.cam;
+        uint64_t bytes = 0, iters = 0;
+        float dx, dy, dz;
+        ray_dir_uv(c, ((float)gx * 8.0f + 4.0f) / c.res_x, ((float)gy * 8.0f + 4.0f) / c.res_y,
+                   dx, dy, dz);
+        float result = 1e9f;
+        const float ix = safe_inv(dx), iy = safe_inv(dy), iz = safe_inv(dz);
+        const float wminx = (float)c.world_origin[0], wminy = (float)c.world_origin[1],
+                    wminz = (float)c.world_origin[2];
+        const float wmaxx = wminx + (float)d.vx, wmaxy = wminy + (float)d.vy,
+                    wmaxz = wminz + (float)d.vz;
+        const float t0x = (wminx - c.origin[0]) * ix, t1x = (wmaxx - c.origin[0]) * ix;
+        const float t0y = (wminy - c.origin[1]) * iy, t1y = (wmaxy - c.origin[1]) * iy;
+        const float t0z = (wminz - c.origin[2]) * iz, t1z = (wmaxz - c.origin[2]) * iz;
+        const float t_enter =
+            vmax(vmax(vmin(t0x, t1x), vmin(t0y, t1y)), vmax(vmin(t0z, t1z), 0.0f));
+        const float t_exit = vmin(vmin(vmax(t0x, t1x), vmax(t0y, t1y)), vmax(t0z, t1z));
+        if (!(t_enter >= t_exit || t_exit < 0.0f)) {
+            const float tb = t_enter + 0.05f;
+            const float px = clampf(c.origin[0] + dx * tb, wminx + 0.01f, wmaxx - 0.01f);
+            const float py = clampf(c.origin[1] + dy * tb, wminy + 0.01f, wmaxy - 0.01f);
+            const float pz = clampf(c.origin[2] + dz * tb, wminz + 0.01f, wmaxz - 0.01f);
+            int32_t tx = f2i(floorf(px / 16.0f)), ty = f2i(floorf(py / 16.0f)),
+                    tz = f2i(floorf(pz / 16.0f));
+            const int32_t sx = sgn(dx), sy = sgn(dy), sz = sgn(dz);
+            const float tdx = fabsf(ix) * 16.0f, tdy = fabsf(iy) * 16.0f, tdz = fabsf(iz) * 16.0f;
+            float mx = sx > 0 ? ((float)((tx + 1) * 16) - c.origin[0]) * ix
+                              : ((float)(tx * 16) - c.origin[0]) * ix;
+            float my = sy > 0 ? ((float)((ty + 1) * 16) - c.origin[1]) * iy
+                              : ((float)(ty * 16) - c.origin[1]) * iy;
+            float mz = sz > 0 ? ((float)((tz + 1) * 16) - c.origin[2]) * iz
+                              : ((float)(tz * 16) - c.origin[2]) * iz;
+            const int32_t otx = c.world_origin[0] / 16, oty = c.world_origin[1] / 16,
+                          otz = c.world_origin[2] / 16;
+            // slot of window tile 0; inside the window the slot of tile t is
+            // (t - ot) + slot0, folded once (== pos_mod(t, tiles))
+            const uint32_t sox = (uint32_t)pos_mod(otx, d.tx), soz = (uint32_t)pos_mod(otz, d.tz);
+            float t_cur = t_enter;
+            for (int s = 0; s < 80; ++s) {
+                ++iters;
+                const uint32_t rx = (uint32_t)(tx - otx), rz = (uint32_t)(tz - otz);
+                if (rx >= (uint32_t)d.tx || (uint32_t)(ty - oty) >= (uint32_t)d.ty ||
+                    rz >= (uint32_t)d.tz)
+                    break;
+                uint32_t stx = rx + sox, stz = rz + soz;
+                if (stx >= (uint32_t)d.tx) stx -= (uint32_t)d.tx;
+                if (stz >= (uint32_t)d.tz) stz -= (uint32_t)d.tz;
+                const uint32_t sty = (uint32_t)ty;
+                const uint32_t ci = (stx >> 2) + (sty >> 2) * (uint32_t)d.cx +
+                                    (stz >> 2) * (uint32_t)(d.cx * d.cy);
+                const int lin = (int)((stx & 3u) + (stz & 3u) * 4u + (sty & 3u) * 16u);
+                if (STATS) bytes += 8;
+                const uint64_t cw = (SMEM && staged) ? s_chunk[ci] : ldg(fa.ta.w.chunk_mask + ci);
+                if (bit64(cw, lin)) {
+                    result = t_cur;
+                    break;
+                }
+                if (mx < my && mx < mz) {
+                    tx += sx; t_cur = mx; mx = mx + tdx;
+                } else if (my < mz) {
+                    ty += sy; t_cur = my; my = my + tdy;
+                } else {
+                    tz += sz; t_cur = mz; mz = mz + tdz;
+                }
             }
         }
+        beam_out[(size_t)gy * fa.bw + gx] = result;
+        if (STATS) flush_stats(fa.stats, bytes, iters);
     }
-    beam_out[(size_t)gy * fa.bw + gx] = result;
-    if (STATS) flush_stats(fa.stats, bytes, iters);
+    if (SMEM && !staged) {
+        // the copy still targets this CTA's shared memory: let it land (bounded)
+        bool done = false;
+        for (uint32_t it = 0; it < kWaitLimit && !done; ++it) done = mbar_try_wait(bar, 0u);
+    }
 }
 
 // cs_main's temporal-differential gate (raymarch.wgsl:580-587): is the 8x8
@@ -648,8 +708,16 @@ cudaError_t launch_refresh_tiles(uint32_t tiles_w, uint32_t tiles_h, uint32_t sp
 }
 cudaError_t launch_beam(const FrameArgs &fa, float *beam_out, cudaStream_t s) {
     dim3 block(128), grid((fa.bw + 127) / 128, fa.bh);
-    if (fa.stats) k_beam<true><<<grid, block, 0, s>>>(fa, beam_out);
-    else k_beam<false><<<grid, block, 0, s>>>(fa, beam_out);
+    const uint64_t bytes = (uint64_t)fa.ta.w.d.n_chunks * 8u;
+    const bool smem = bytes <= kBeamSmemBytes && (bytes % 16u) == 0u &&
+                      (reinterpret_cast<uintptr_t>(fa.ta.w.chunk_mask) & 15u) == 0u;
+    if (smem) {
+        if (fa.stats) k_beam<true, true><<<grid, block, (size_t)bytes, s>>>(fa, beam_out);
+        else k_beam<false, true><<<grid, block, (size_t)bytes, s>>>(fa, beam_out);
+    } else {
+        if (fa.stats) k_beam<true, false><<<grid, block, 0, s>>>(fa, beam_out);
+        else k_beam<false, false><<<grid, block, 0, s>>>(fa, beam_out);
+    }
     return cudaGetLastError();
 }
 
