@@ -22,11 +22,15 @@ cpu_baseline  the oracle (C restatement of the reference traversal) on all
            host threads over a bounded row sample of the same frame.
 
 Extra sections (rank 0, single GPU, a few seconds each; --no-extras skips
-them), all on the 512x256x512 world:
+them), on 512x256x512 worlds:
 mixed_queue  primary + spawned shadow + GI-probe + picking rays in one
            autotuned, graph-captured persistent launch.
-picking    benches/trace.rs raycast_pick rays: CPU restatement on one thread
-           (ns/ray) beside batched and single-call device picking.
+worldgen   the reference's chunk generator gen_slot_bricks: the criterion
+           chunks on one CPU thread beside the device, and whole windows
+           (the demo world, a 2048x256x2048 window) on the device.
+picking    benches/trace.rs raycast_pick rays on the reference's demo world:
+           CPU restatement on one thread (ns/ray) beside batched and
+           single-call device picking.
 learned    the learned start-distance proposal: on-device training, then the
            plain DDA, the learned form and the verification without a network
            on one 1920x1080 frame, with acceptance and iterations saved.
@@ -67,6 +71,9 @@ def parse_args():
     ap.add_argument("--profile", action="store_true",
                     help="frames only (one counting pass, warm-up, K timed frames): the "
                          "command profiled with ncu")
+    ap.add_argument("--profile-worldgen", action="store_true",
+                    help="the chunk generator only (the 512x256x512 demo world once, then K "
+                         "fills of the 2048x256x2048 window): the command profiled with ncu")
     ap.add_argument("--profile-learned", action="store_true",
                     help="the learned-form frames only (a short training, then K plain, "
                          "learned and verification-only frames): the command profiled "
@@ -259,8 +266,9 @@ def run_reference(args, cfg):
 # ---------------------------------------------------------------- extras
 def run_picking(vg, dw, n: int = 200_000) -> dict:
     """The reference's criterion picking case (benches/trace.rs:24-40: origin
-    (256, 90, 256), dir (sin a, -0.5, cos a), a += 0.013) on the
-    512x256x512 world: the CPU baseline (the raycast restatement, one thread,
+    (256, 90, 256), dir (sin a, -0.5, cos a), a += 0.013) on the world it
+    picks in, World::new + fill_demo_terrain (seed 0xC0FFEE_F00D_BEEF,
+    512x256x512): the CPU baseline (the raycast restatement, one thread,
     as criterion runs it) beside the device -- batched rays (event time) and
     the single-ray drop-in call (wall time per call, copies and sync
     included)."""
@@ -310,7 +318,8 @@ def run_picking(vg, dw, n: int = 200_000) -> dict:
         lib.vx_raycast(dw.handle, L.f3(cams[i]), L.f3(dirs[i]), L.i3((0, 0, 0)), C.byref(pick))
     single_us = (time.perf_counter() - t0) / calls * 1e6
     return {
-        "workload": f"benches/trace.rs raycast_pick rays x {n} on the 512x256x512 world",
+        "workload": f"benches/trace.rs raycast_pick rays x {n} on the reference's demo world "
+                    "(fill_demo_terrain, seed 0xC0FFEE_F00D_BEEF, 512x256x512)",
         "cpu_1thread_ns_per_ray": round(cpu_s * 1e9 / n, 1),
         "gpu_batch_ns_per_ray": round(gpu_ns, 3),
         "gpu_single_call_us": round(single_us, 2),
@@ -386,6 +395,56 @@ def run_learned(vg, dw) -> dict:
     }
 
 
+def run_worldgen(vg, device: int) -> tuple:
+    """The reference's chunk generator gen_slot_bricks (src/voxel.rs:1322-1500).
+    The criterion case (benches/trace.rs:11-22: chunks (i & 7, 0, (i >> 3) & 7),
+    seed 0xC0FFEE_F00D_BEEF) runs on one CPU thread through the oracle
+    restatement, as criterion runs it, and on the device as one batch;
+    whole windows are the 512x256x512 demo world (fill_demo_terrain, 2048
+    chunks) and a 2048x256x2048 window (32768 chunks).  Device figures are
+    wall times of the synchronous call: job upload, generation and pyramid
+    rebuild.  Returns (result, the demo world for the picking case)."""
+    import numpy as np
+
+    from oracle import pyoracle as po
+
+    seed = 0xC0FFEE_F00D_BEEF
+    chunks = [(i & 7, 0, (i >> 3) & 7) for i in range(1, 65)]
+    t0 = time.perf_counter()
+    want = [po.gen_slot_bricks(*c, seed) for c in chunks for _ in range(2)][::2]
+    cpu_ns = (time.perf_counter() - t0) / (2 * len(chunks)) * 1e9
+    demo = vg.DeviceWorld(128, 64, 128, device=device)
+
+    def wall(fn, reps):
+        fn()
+        t = time.perf_counter()
+        for _ in range(reps):
+            fn()
+        return (time.perf_counter() - t) / reps
+
+    # the criterion chunks: slots (x, 0, z) of the demo window, x, z < 8
+    batch_s = wall(lambda: demo.gen_chunks(seed, chunks), 10)
+    got = demo.download()["bricks"].reshape(128, 64, 128)   # (z, y, x) bricks
+    same = all(np.array_equal(
+        np.ascontiguousarray(got[cz * 8:cz * 8 + 8, 0:8, cx * 8:cx * 8 + 8]).reshape(-1)
+        .view(np.uint8), w.reshape(-1).view(np.uint8)) for (cx, _, cz), w in zip(chunks, want))
+    demo_s = wall(lambda: demo.fill_window(seed, 0, 0), 5)
+    big = vg.DeviceWorld(512, 64, 512, device=device)
+    big_s = wall(lambda: big.fill_window(seed, 0, 0), 3)
+    big.close()
+    return {
+        "workload": "gen_slot_bricks (terrain, biomes, ores, decoration, trees), seed "
+                    "0xC0FFEE_F00D_BEEF",
+        "criterion_case": {"chunks": len(chunks), "cpu_1thread_us_per_chunk":
+                           round(cpu_ns / 1e3, 1), "gpu_us_per_chunk":
+                           round(batch_s * 1e6 / len(chunks), 2), "equal_to_cpu": same},
+        "demo_world_512x256x512": {"chunks": 2048, "ms": round(demo_s * 1e3, 3),
+                                   "chunks_per_s": round(2048 / demo_s)},
+        "window_2048x256x2048": {"chunks": 32768, "ms": round(big_s * 1e3, 3),
+                                 "chunks_per_s": round(32768 / big_s)},
+    }, demo
+
+
 def run_extras(vg, device: int) -> dict:
     """The other workloads on the 512x256x512 world, each a few seconds:
     the mixed ray queue (one autotuned, graph-captured persistent launch),
@@ -431,7 +490,9 @@ def run_extras(vg, device: int) -> dict:
     }
     g.close()
     del rt, o, sh
-    out["picking"] = run_picking(vg, dw)
+    out["worldgen"], demo = run_worldgen(vg, device)
+    out["picking"] = run_picking(vg, demo)
+    demo.close()
     out["learned"] = run_learned(vg, dw)
     srv = sv.Server(dw, p, mem_budget_bytes=1 << 30, slots=8)
     st = srv.bench(clients=64, rate_per_client=200.0, seconds=3.0, min_rays=1, max_rays=50000,
@@ -632,12 +693,31 @@ def profile_learned(args):
     dw.close()
 
 
+def profile_worldgen(args):
+    """The chunk generator's launches for ncu: the 512x256x512 demo world
+    (2048 chunks) once, then K fills of the 2048x256x2048 window (32768
+    chunks), seed 0xC0FFEE_F00D_BEEF."""
+    import voxelg_b200 as vg
+    seed = 0xC0FFEE_F00D_BEEF
+    demo = vg.DeviceWorld(128, 64, 128)
+    demo.fill_window(seed, 0, 0)
+    demo.close()
+    big = vg.DeviceWorld(512, 64, 512)
+    for _ in range(args.steps):
+        big.fill_window(seed, 0, 0)
+    big.close()
+    print(json.dumps({"profile_worldgen_fills": args.steps}), flush=True)
+
+
 def main():
     args = parse_args()
     import voxelg_b200.configs as configs
     cfg = configs.CONFIGS[CONFIG_NAME]
     if args.profile_learned:
         profile_learned(args)
+        return
+    if args.profile_worldgen:
+        profile_worldgen(args)
         return
     if args.impl == "reference":
         run_reference(args, cfg)

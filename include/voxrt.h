@@ -178,6 +178,29 @@ int vx_world_download(VxWorld *w, VxBrick *bricks, uint64_t *tile_mask, uint64_t
 /* Generate the seeded synthetic terrain on the device and build masks and
  * uniform LUTs there (src/voxel.rs:946-1000 semantics). */
 int vx_world_generate(VxWorld *w, const VxTerrainParams *t);
+
+/* The reference's storage-chunk generator gen_slot_bricks
+ * (src/voxel.rs:1322-1500: terrain, biomes, ores, decoration, trees) on the
+ * device.  A storage chunk is 8x8x8 bricks (32^3 voxels); world chunk
+ * (cx, cy, cz) lives in slot (pos_mod(cx, bricks_x/8), cy,
+ * pos_mod(cz, bricks_z/8)), the toroidal mapping of shift_origin
+ * (src/voxel.rs:507-537).  Masks and LUTs are rebuilt afterwards.  All three
+ * calls are synchronous.
+ *
+ * vx_world_gen_chunks: generate the n world chunks of `chunks` (n x, y, z
+ * triples, host memory; 0 <= y < bricks_y/8, |x|, |z| < 2^24) into their
+ * slots; of two chunks for one slot the later wins. */
+int vx_world_gen_chunks(VxWorld *w, uint64_t seed, const int32_t *chunks, uint32_t n);
+/* fill_demo_terrain (src/voxel.rs:1005-1060) for a window whose lower corner
+ * is world chunk (origin_cx, 0, origin_cz): every slot generated.  The
+ * camera's world_origin for this window is (32*origin_cx, 0, 32*origin_cz). */
+int vx_world_fill_window(VxWorld *w, uint64_t seed, int32_t origin_cx, int32_t origin_cz);
+/* shift_origin (src/voxel.rs:507-537) after vx_world_fill_window: only the
+ * slots whose world chunk changes are regenerated, with the fill's seed;
+ * their count goes to *n_regenerated when non-null.  Edits are not
+ * replayed (apply them with vx_world_apply_dirty). */
+int vx_world_shift_origin(VxWorld *w, int32_t origin_cx, int32_t origin_cz,
+                          uint32_t *n_regenerated);
 /* Incremental update from dirty bricks (renderer.rs:1345-1394): writes the
  * given bricks and recomputes the touched tile/chunk/L4 masks and uniform
  * LUT entries on the device (voxel.rs:879-946 semantics).  brick_idx and

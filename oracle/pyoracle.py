@@ -85,6 +85,10 @@ def load():
         "or_rebuild_all_uniform": (None, [P(OrWorld)]),
         "or_set_voxel": (C.c_int64, [P(OrWorld), C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint8]),
         "or_generate_terrain": (None, [P(OrWorld), P(OrTerrain), C.c_int]),
+        "or_sample_terrain": (C.c_int32, [C.c_float, C.c_float, C.c_uint64, P(C.c_int32)]),
+        "or_trees_for_chunk": (C.c_int, [C.c_int32, C.c_int32, C.c_uint64, vp]),
+        "or_gen_slot_bricks": (None, [C.c_int32, C.c_int32, C.c_int32, C.c_uint64, vp]),
+        "or_fill_window": (None, [P(OrWorld), C.c_uint64, C.c_int32, C.c_int32, C.c_int]),
         "or_fbm_2d": (C.c_float, [C.c_float, C.c_float, C.c_uint32]),
         "or_value_noise_3d": (C.c_float, [C.c_float, C.c_float, C.c_float]),
         "or_ray_dir_uv": (None, [P(OrCamera), C.c_float, C.c_float, P(C.c_float)]),
@@ -161,6 +165,38 @@ class World:
                       terrain.cave_inv_wavelength, terrain.cave_threshold, terrain.dirt_depth)
         load().or_generate_terrain(C.byref(self.c), C.byref(t), threads or os.cpu_count() or 1)
         self.rebuild()
+
+
+TREE = np.dtype([("base", "<i4", 3), ("ttype", "<u4"), ("hash", "<u4")])
+
+
+def gen_slot_bricks(cx, cy, cz, seed):
+    """The reference's chunk generator for world chunk (cx, cy, cz): 512
+    bricks in scratch order x + y*8 + z*64 (voxel.rs:1322-1500)."""
+    out = np.zeros(512, BRICK)
+    load().or_gen_slot_bricks(cx, cy, cz, C.c_uint64(seed & (2**64 - 1)), out.ctypes.data)
+    return out
+
+
+def sample_terrain(wx, wz, seed):
+    """(height, water_top) of one column (voxel.rs:1244-1316)."""
+    wt = C.c_int32()
+    h = load().or_sample_terrain(float(np.float32(wx)), float(np.float32(wz)),
+                                 C.c_uint64(seed & (2**64 - 1)), C.byref(wt))
+    return h, wt.value
+
+
+def trees_for_chunk(cx, cz, seed):
+    out = np.zeros(12, TREE)
+    n = load().or_trees_for_chunk(cx, cz, C.c_uint64(seed & (2**64 - 1)), out.ctypes.data)
+    return out[:n]
+
+
+def fill_window(world: "World", seed, ox=0, oz=0, threads=None):
+    """fill_demo_terrain for a window whose lower corner is world chunk
+    (ox, 0, oz): every slot generated by gen_slot_bricks, masks rebuilt."""
+    load().or_fill_window(C.byref(world.c), C.c_uint64(seed & (2**64 - 1)), ox, oz,
+                          threads or os.cpu_count() or 1)
 
 
 def params_from(p) -> OrParams:

@@ -378,6 +378,454 @@ void or_generate_terrain(const OrWorld *w, const OrTerrain *t, int nthreads) {
 }
 
 /* ------------------------------------------------------------------ */
+/* gen_slot_bricks: the reference's own chunk generator                */
+/* (voxel.rs:1244-1500 terrain/biomes/ores/decoration, :1500-1811      */
+/* trees, :1822-1997 biome tables).  Rivers and ravines are disabled   */
+/* in the reference (voxel.rs:1267-1306) and are absent here too.      */
+/* powf / cosf / sinf are the C library's, the functions the           */
+/* reference's f32::powf / cos / sin call on Linux.                    */
+/* ------------------------------------------------------------------ */
+enum { SG_SEA = 64, SG_WORLD_Y = 256, SG_CV = 32 };
+enum { SG_SAND = 1, SG_WOOD = 13, SG_LEAVES = 14, SG_SNOW = 15, SG_COAL = 19, SG_IRON = 20,
+       SG_GOLD = 21, SG_DIAMOND = 22, SG_WOOD_BIRCH = 23, SG_WOOD_PINE = 24,
+       SG_LEAVES_BIRCH = 25, SG_LEAVES_PINE = 26, SG_LEAVES_AUTUMN = 27, SG_FLOWER = 30,
+       SG_TALL_GRASS = 31, SG_CACTUS = 32, SG_GRASS_DRY = 34, SG_BUSH = 36 };
+/* Biome (voxel.rs:1810-1820) */
+enum { B_TUNDRA, B_PLAINS, B_FOREST, B_JUNGLE, B_SAVANNA, B_DESERT, B_BEACH, B_MOUNTAIN };
+
+static inline float fmaxr(float a, float b) { return a < b ? b : a; }  /* f32::max, no NaN here */
+static inline float fminr(float a, float b) { return b < a ? b : a; }
+
+/* sample_terrain, voxel.rs:1244-1316 (ravine_cut 0, rivers off) */
+int32_t or_sample_terrain(float wx, float wz, uint64_t seed, int32_t *water_top) {
+    float off[2];
+    or_seed_offset_xz(seed, off);
+    float px = wx + off[0], pz = wz + off[1];
+    float warp_x = or_fbm_2d(px * 0.005f, pz * 0.005f, 2) * 8.0f;
+    float warp_z = or_fbm_2d(px * 0.005f + 50.0f, pz * 0.005f + 50.0f, 2) * 8.0f;
+    float wpx = px + warp_x, wpz = pz + warp_z;
+    float base = or_fbm_2d(wpx * 0.012f, wpz * 0.012f, 4) * 22.0f;
+    float mountain_mask = fmaxr(or_fbm_2d(wpx * 0.0028f, wpz * 0.0028f, 2) + 0.2f, 0.0f);
+    float mountain_amp = fminr(mountain_mask, 1.0f);
+    float mountain_h =
+        powf(fmaxr(or_fbm_2d(wpx * 0.009f, wpz * 0.009f, 5), 0.0f), 1.15f) * mountain_amp * 110.0f;
+    float base_h = 64.0f + 8.0f + base + mountain_h - 0.0f;
+    float h = base_h < 2.0f ? 2.0f : (base_h > 255.0f ? 255.0f : base_h);
+    int32_t h_i = f2i(h);
+    if (water_top) *water_top = h_i < SG_SEA ? SG_SEA : 0;
+    return h_i;
+}
+
+/* pick_biome, voxel.rs:1822-1832 */
+static int pick_biome(float temp, float humid, uint32_t h, uint32_t sea) {
+    if (h > sea + 36) return B_MOUNTAIN;
+    if (h <= sea + 1) return B_BEACH;
+    if (temp < -0.20f) return B_TUNDRA;
+    if (temp > 0.25f && humid < -0.05f) return B_DESERT;
+    if (temp > 0.15f && humid > 0.25f) return B_JUNGLE;
+    if (temp > 0.10f && humid < 0.10f) return B_SAVANNA;
+    if (humid > 0.20f) return B_FOREST;
+    return B_PLAINS;
+}
+/* Biome::top_block / subsoil / tree_type / flora_probs / tree_density,
+ * voxel.rs:1834-1903 */
+static uint8_t top_block(int b, uint32_t h) {
+    switch (b) {
+    case B_TUNDRA: return SG_SNOW;
+    case B_DESERT: case B_BEACH: case B_SAVANNA: return SG_SAND;
+    case B_MOUNTAIN: return h > SG_SEA + 55 ? SG_SNOW : MAT_STONE;
+    default: return MAT_GRASS;
+    }
+}
+static uint8_t subsoil(int b) {
+    switch (b) {
+    case B_DESERT: case B_BEACH: return SG_SAND;
+    case B_MOUNTAIN: return MAT_STONE;
+    default: return MAT_DIRT;
+    }
+}
+static uint32_t tree_type(int b, uint32_t hash) {
+    switch (b) {
+    case B_TUNDRA: case B_MOUNTAIN: return 2;
+    case B_PLAINS: return hash % 3 == 0 ? 1 : 0;
+    case B_FOREST: { uint32_t k = hash % 4; return k == 0 ? 1 : (k == 1 ? 3 : 0); }
+    case B_JUNGLE: return hash % 4 == 0 ? 3 : 0;
+    default: return 0;
+    }
+}
+static void flora_probs(int b, float *fp, float *gp) {
+    switch (b) {
+    case B_PLAINS: *fp = 0.020f; *gp = 0.08f; break;
+    case B_FOREST: *fp = 0.010f; *gp = 0.065f; break;
+    case B_JUNGLE: *fp = 0.012f; *gp = 0.09f; break;
+    default: *fp = 0.015f; *gp = 0.065f; break;
+    }
+}
+static float tree_density(int b) {
+    switch (b) {
+    case B_JUNGLE: return 1.2f;
+    case B_FOREST: return 0.55f;
+    case B_TUNDRA: return 0.30f;
+    case B_PLAINS: return 0.20f;
+    case B_MOUNTAIN: return 0.14f;
+    case B_DESERT: return 0.20f;
+    default: return 0.0f;
+    }
+}
+
+/* stone_or_ore, voxel.rs:1906-1916 */
+static uint8_t stone_or_ore(float x, float y, float z, uint32_t h) {
+    float depth = fmaxr((float)h - y, 0.0f);
+    float n1 = or_value_noise_3d(x * 0.27f, y * 0.27f, z * 0.27f);
+    float n2 = or_value_noise_3d(x * 0.55f, y * 0.55f, z * 0.55f);
+    float combined = n1 + n2 * 0.30f;
+    if (depth > 30.0f && combined > 0.50f) return SG_DIAMOND;
+    if (depth > 20.0f && combined > 0.36f) return SG_GOLD;
+    if (depth > 10.0f && combined > 0.24f) return SG_IRON;
+    if (combined > 0.32f) return SG_COAL;
+    return MAT_STONE;
+}
+
+/* Brick::set (voxel.rs:315-325) on the chunk scratch, x + y*8 + z*64 */
+static void sg_set(OrBrick *s, uint32_t dx, uint32_t dy, uint32_t dz, uint8_t mat) {
+    OrBrick *b = &s[(dx / 4) + (dy / 4) * 8 + (dz / 4) * 64];
+    int vi = child_bit((int32_t)(dx % 4), (int32_t)(dy % 4), (int32_t)(dz % 4));
+    if (mat == 0) {
+        b->occupancy &= ~(1ull << vi);
+        b->materials[vi] = 0;
+    } else {
+        b->occupancy |= 1ull << vi;
+        b->materials[vi] = mat;
+    }
+}
+
+/* trees_for_chunk, voxel.rs:1537-1591 */
+int or_trees_for_chunk(int32_t cx, int32_t cz, uint64_t seed, OrTree out[12]) {
+    float off[2];
+    or_seed_offset_xz(seed, off);
+    float ccx = ((float)cx + 0.5f) * 32.0f;
+    float ccz = ((float)cz + 0.5f) * 32.0f;
+    float temperature = or_fbm_2d((ccx + off[0]) * 0.0006f, (ccz + off[1]) * 0.0006f, 3);
+    float humidity =
+        or_fbm_2d((ccx + off[0]) * 0.0008f + 100.0f, (ccz + off[1]) * 0.0008f + 100.0f, 3);
+    int biome = pick_biome(temperature, humidity, SG_SEA + 10, SG_SEA);
+    uint32_t n_cand = (uint32_t)f2i(roundf(tree_density(biome) * 5.0f));
+    if (n_cand == 0) return 0;
+    float patch_mul = 1.0f;
+    if (biome != B_DESERT) {
+        float patch_raw = or_fbm_2d(ccx * 0.0035f, ccz * 0.0035f, 2);
+        patch_mul = fminr(fmaxr(patch_raw + 0.4f, 0.0f) * 1.6f, 2.0f);
+    }
+    uint32_t n = (uint32_t)f2i((float)n_cand * patch_mul);
+    /* hash_chunk, voxel.rs:1593-1601 */
+    uint32_t s = (uint32_t)seed ^ (uint32_t)(seed >> 32);
+    uint32_t ch = (uint32_t)cx * 0x9E3779B1u;
+    ch = ch + (uint32_t)cz * 0x85EBCA77u;
+    ch = ch + s * 0xC2B2AE3Du;
+    ch = ch ^ (ch >> 16);
+    ch = ch * 0xD2B74407u;
+    ch = ch ^ (ch >> 13);
+    int k = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        uint32_t h = ch * 2654435761u + i * 7919u;
+        int32_t wx = cx * 32 + (int32_t)(h & 31u);
+        int32_t wz = cz * 32 + (int32_t)((h >> 5) & 31u);
+        int32_t th = or_sample_terrain((float)wx, (float)wz, seed, NULL);
+        if ((uint32_t)th <= SG_SEA + 1) continue;
+        if (th + 22 >= SG_WORLD_Y) continue;
+        float lt = or_fbm_2d(((float)wx + off[0]) * 0.0006f, ((float)wz + off[1]) * 0.0006f, 3);
+        float lh = or_fbm_2d(((float)wx + off[0]) * 0.0008f + 100.0f,
+                             ((float)wz + off[1]) * 0.0008f + 100.0f, 3);
+        int lb = pick_biome(lt, lh, (uint32_t)th, SG_SEA);
+        uint32_t tt;
+        if (lb == B_BEACH || lb == B_SAVANNA) continue;
+        tt = lb == B_DESERT ? 4u : tree_type(lb, h);
+        out[k].base[0] = wx; out[k].base[1] = th + 1; out[k].base[2] = wz;
+        out[k].ttype = tt; out[k].hash = h;
+        ++k;
+    }
+    return k;
+}
+
+typedef struct {
+    OrBrick *s;
+    int32_t mn[3], mx[3];
+} SgChunk;
+
+/* try_write_tree_voxel, voxel.rs:1500-1525 */
+static void sg_tree_voxel(const SgChunk *c, int32_t x, int32_t y, int32_t z, uint8_t mat) {
+    if (x < c->mn[0] || x >= c->mx[0]) return;
+    if (y < c->mn[1] || y >= c->mx[1]) return;
+    if (z < c->mn[2] || z >= c->mx[2]) return;
+    uint32_t dx = (uint32_t)(x - c->mn[0]), dy = (uint32_t)(y - c->mn[1]), dz = (uint32_t)(z - c->mn[2]);
+    const OrBrick *b = &c->s[(dx / 4) + (dy / 4) * 8 + (dz / 4) * 64];
+    int vi = child_bit((int32_t)(dx % 4), (int32_t)(dy % 4), (int32_t)(dz % 4));
+    int occupied = (b->occupancy >> vi) & 1u;
+    int fringe = occupied && b->materials[vi] == MAT_LEAF_FRINGE;
+    if (!occupied || (fringe && mat != MAT_LEAF_FRINGE)) sg_set(c->s, dx, dy, dz, mat);
+}
+
+/* paint_line with thickness 0, voxel.rs:1744-1776 */
+static void sg_line(const SgChunk *c, const int32_t a[3], const int32_t b[3], uint8_t mat) {
+    int32_t d0 = b[0] - a[0], d1 = b[1] - a[1], d2 = b[2] - a[2];
+    float len = sqrtf((float)(d0 * d0 + d1 * d1 + d2 * d2));
+    int32_t steps = f2i(ceilf(len * 1.5f));
+    if (steps <= 0) {
+        sg_tree_voxel(c, a[0], a[1], a[2], mat);
+        return;
+    }
+    for (int32_t s = 0; s <= steps; ++s) {
+        float t = (float)s / (float)steps;
+        int32_t x = f2i(roundf((float)a[0] + (float)d0 * t));
+        int32_t y = f2i(roundf((float)a[1] + (float)d1 * t));
+        int32_t z = f2i(roundf((float)a[2] + (float)d2 * t));
+        sg_tree_voxel(c, x, y, z, mat);
+    }
+}
+/* paint_fringe_shell + paint_sphere = paint_canopy, voxel.rs:1715-1742, :1778-1789 */
+static void sg_canopy(const SgChunk *c, const int32_t ctr[3], int32_t r, uint8_t mat) {
+    int32_t rf = r + 1, r2 = rf * rf;
+    for (int32_t dy = -rf; dy <= rf; ++dy)
+        for (int32_t dx = -(rf + 1); dx <= rf + 1; ++dx)
+            for (int32_t dz = -(rf + 1); dz <= rf + 1; ++dz) {
+                int32_t hx = abs(dx) - 1, hz = abs(dz) - 1;
+                if (hx < 0) hx = 0;
+                if (hz < 0) hz = 0;
+                if (hx * hx + dy * dy + hz * hz > r2) continue;
+                sg_tree_voxel(c, ctr[0] + dx, ctr[1] + dy, ctr[2] + dz, MAT_LEAF_FRINGE);
+            }
+    r2 = r * r;
+    for (int32_t dy = -r; dy <= r; ++dy)
+        for (int32_t dx = -r; dx <= r; ++dx)
+            for (int32_t dz = -r; dz <= r; ++dz) {
+                if (dx * dx + dy * dy + dz * dz > r2) continue;
+                sg_tree_voxel(c, ctr[0] + dx, ctr[1] + dy, ctr[2] + dz, mat);
+            }
+}
+/* branch_jitter, voxel.rs:1791-1797 */
+static float branch_jitter(uint32_t hash, uint32_t b, uint32_t salt) {
+    uint32_t h = hash * 0x9E3779B1u + b * 2654435761u + salt * 40503u;
+    return ((float)(h & 0xFFFFu) / 65535.0f) * 2.0f - 1.0f;
+}
+
+/* paint_tree, voxel.rs:1605-1710 */
+static void sg_paint_tree(const SgChunk *c, const OrTree *t) {
+    const float tau = 6.28318548202514648f; /* std::f32::consts::TAU */
+    const int32_t *base = t->base;
+    uint32_t h = t->hash;
+    if (t->ttype == 2) {
+        int32_t trunk_h = 10 + (int32_t)(h % 6);
+        int32_t top[3] = {base[0], base[1] + trunk_h, base[2]};
+        sg_line(c, base, top, SG_WOOD_PINE);
+        for (int32_t i = 0; i < 6; ++i) {
+            float tf = (float)i / 6.0f;
+            int32_t y = base[1] + f2i((float)trunk_h * (0.35f + tf * 0.78f));
+            int32_t r = f2i(powf(1.0f - tf, 0.85f) * 3.5f + 1.0f);
+            int32_t ctr[3] = {base[0], y, base[2]};
+            sg_canopy(c, ctr, r, SG_LEAVES_PINE);
+        }
+    } else if (t->ttype == 1) {
+        int32_t trunk_h = 8 + (int32_t)(h % 5);
+        int32_t top[3] = {base[0], base[1] + trunk_h, base[2]};
+        sg_line(c, base, top, SG_WOOD_BIRCH);
+        int32_t n = 2 + (int32_t)(h % 2);
+        for (int32_t b = 0; b < n; ++b) {
+            float angle = ((float)b / (float)n) * tau + branch_jitter(h, (uint32_t)b, 0) * 0.5f;
+            int32_t len = 2 + (int32_t)((h * ((uint32_t)b + 1u)) % 3u);
+            int32_t sy = base[1] + f2i((float)trunk_h * 0.7f);
+            int32_t from[3] = {base[0], sy, base[2]};
+            int32_t end[3] = {base[0] + f2i(cosf(angle) * (float)len), sy + 1,
+                              base[2] + f2i(sinf(angle) * (float)len)};
+            sg_line(c, from, end, SG_WOOD_BIRCH);
+            sg_canopy(c, end, 2, SG_LEAVES_BIRCH);
+        }
+        sg_canopy(c, top, 3, SG_LEAVES_BIRCH);
+    } else if (t->ttype == 4) {
+        static const int32_t sets[4][2][2] = {{{1, 0}, {0, 1}}, {{-1, 0}, {0, -1}},
+                                              {{0, 1}, {-1, 0}}, {{0, -1}, {1, 0}}};
+        int32_t col_h = 3 + (int32_t)(h % 6);
+        int32_t top[3] = {base[0], base[1] + col_h, base[2]};
+        sg_line(c, base, top, SG_CACTUS);
+        int32_t n_arms = (int32_t)(h % 3);
+        const int32_t(*set)[2] = sets[h & 3u];
+        for (int32_t a = 0; a < n_arms; ++a) {
+            int32_t dx = set[a % 2][0], dz = set[a % 2][1];
+            int32_t sy = base[1] + f2i((float)col_h * 0.4f);
+            int32_t arm_top = base[1] + f2i((float)col_h * 0.9f);
+            int32_t ax = base[0] + dx * 2, az = base[2] + dz * 2;
+            int32_t p0[3] = {base[0], sy, base[2]}, p1[3] = {ax, sy, az}, p2[3] = {ax, arm_top, az};
+            sg_line(c, p0, p1, SG_CACTUS);
+            sg_line(c, p1, p2, SG_CACTUS);
+        }
+    } else {
+        uint8_t leaf = t->ttype == 3 ? SG_LEAVES_AUTUMN : SG_LEAVES;
+        int32_t trunk_h = 8 + (int32_t)(h % 5);
+        int32_t top[3] = {base[0], base[1] + trunk_h, base[2]};
+        sg_line(c, base, top, SG_WOOD);
+        int32_t n = 3 + (int32_t)(h % 2);
+        for (int32_t b = 0; b < n; ++b) {
+            float angle = ((float)b / (float)n) * tau + branch_jitter(h, (uint32_t)b, 0) * 0.6f;
+            int32_t len = 3 + (int32_t)((h * ((uint32_t)b + 7u)) % 3u);
+            int32_t sy = base[1] + f2i((float)trunk_h * 0.65f);
+            int32_t from[3] = {base[0], sy, base[2]};
+            int32_t end[3] = {base[0] + f2i(cosf(angle) * (float)len), sy + f2i((float)len * 0.5f),
+                              base[2] + f2i(sinf(angle) * (float)len)};
+            sg_line(c, from, end, SG_WOOD);
+            sg_canopy(c, end, 3, leaf);
+        }
+        sg_canopy(c, top, 4, leaf);
+    }
+}
+
+/* gen_slot_bricks, voxel.rs:1322-1500 */
+void or_gen_slot_bricks(int32_t cx, int32_t cy, int32_t cz, uint64_t seed, OrBrick *out) {
+    memset(out, 0, sizeof(OrBrick) * 512);
+    float off[2];
+    or_seed_offset_xz(seed, off);
+    const int32_t x0 = cx * SG_CV, y0 = cy * SG_CV, z0 = cz * SG_CV;
+    for (int32_t dz = 0; dz < SG_CV; ++dz) {
+        for (int32_t dx = 0; dx < SG_CV; ++dx) {
+            const int32_t wxi = x0 + dx, wzi = z0 + dz;
+            const float wx = (float)wxi, wz = (float)wzi;
+            int32_t water_top;
+            const int32_t h = or_sample_terrain(wx, wz, seed, &water_top);
+            const uint32_t hu = (uint32_t)h;
+            const int32_t col_top = h > water_top ? h : water_top;
+            if (col_top < y0 || 0 >= y0 + SG_CV) continue;
+            float temperature = or_fbm_2d((wx + off[0]) * 0.0006f, (wz + off[1]) * 0.0006f, 3);
+            float humidity = or_fbm_2d((wx + off[0]) * 0.0008f + 100.0f,
+                                       (wz + off[1]) * 0.0008f + 100.0f, 3);
+            int biome = pick_biome(temperature, humidity, hu, SG_SEA);
+            const int32_t ys = y0 > 0 ? y0 : 0;
+            const int32_t ye = (y0 + SG_CV) < SG_WORLD_Y ? (y0 + SG_CV) : SG_WORLD_Y;
+            const int32_t seal = water_top > h ? h - 5 : INT32_MIN;
+            for (int32_t y = ys; y < ye; ++y) {
+                if (y > h) break;
+                if (!(y >= seal)) {
+                    float cn = or_value_noise_3d(wx * 0.045f, (float)y * 0.085f, wz * 0.045f);
+                    float cn2 = or_value_noise_3d(wx * 0.110f, (float)y * 0.060f, wz * 0.110f);
+                    if (y > 4 && y + 3 < h && (cn + cn2 * 0.6f) > 0.30f) continue;
+                }
+                uint8_t mat;
+                if ((uint32_t)y >= hu) mat = top_block(biome, hu);
+                else if ((uint32_t)y + 4u >= hu) mat = subsoil(biome);
+                else mat = stone_or_ore(wx, (float)y, wz, hu);
+                sg_set(out, (uint32_t)dx, (uint32_t)(y - y0), (uint32_t)dz, mat);
+            }
+            if (water_top > h) {
+                int32_t fb = h + 1 > y0 ? h + 1 : y0;
+                int32_t fe = water_top < y0 + SG_CV - 1 ? water_top : y0 + SG_CV - 1;
+                for (int32_t wy = fb; wy <= fe; ++wy)
+                    sg_set(out, (uint32_t)dx, (uint32_t)(wy - y0), (uint32_t)dz, MAT_WATER);
+            }
+            if (water_top == 0 && hu < SG_WORLD_Y - 1) {
+                uint8_t surface = top_block(biome, hu);
+                int32_t dec_y = h + 1;
+                if (dec_y >= y0 && dec_y < y0 + SG_CV) {
+                    float v = hash3(wxi, dec_y, wzi) * 0.5f + 0.5f;
+                    uint8_t dec = 0;
+                    const int32_t ax = wxi & ~1, az = wzi & ~1;
+                    if (surface == MAT_GRASS) {
+                        float fp, gp;
+                        flora_probs(biome, &fp, &gp);
+                        if (or_fbm_2d((float)wxi * 0.02f + 7.0f, (float)wzi * 0.02f - 3.0f, 2) > 0.30f) {
+                            fp *= 3.0f;
+                            gp *= 12.0f;
+                        }
+                        if (v > 1.0f - fp) dec = SG_FLOWER;
+                        else if (v > 1.0f - fp - gp) dec = SG_TALL_GRASS;
+                        else if (hash3(ax, 977, az) * 0.5f + 0.5f > 0.9955f) dec = SG_BUSH;
+                        else if (v > 1.0f - fp - gp - 0.004f) dec = SG_BUSH;
+                    } else if (surface == SG_SAND && (biome == B_DESERT || biome == B_SAVANNA)) {
+                        if (v > 0.99f) dec = SG_GRASS_DRY;
+                    } else if (surface == SG_SNOW && biome == B_TUNDRA) {
+                        if (v > 0.995f) dec = SG_GRASS_DRY;
+                    }
+                    if (dec != 0) {
+                        uint32_t dy = (uint32_t)(dec_y - y0);
+                        sg_set(out, (uint32_t)dx, dy, (uint32_t)dz, dec);
+                        if (dec == SG_BUSH) {
+                            int big = hash3(ax, 977, az) * 0.5f + 0.5f > 0.9955f;
+                            if (big && dec_y + 1 >= y0 && dec_y + 1 < y0 + SG_CV)
+                                sg_set(out, (uint32_t)dx, dy + 1, (uint32_t)dz, SG_BUSH);
+                        }
+                    }
+                }
+            }
+        }
+    }
+    /* tree pass: trees based in this chunk's column or its 8 xz neighbours */
+    SgChunk c;
+    c.s = out;
+    c.mn[0] = x0; c.mn[1] = y0; c.mn[2] = z0;
+    c.mx[0] = x0 + SG_CV; c.mx[1] = y0 + SG_CV; c.mx[2] = z0 + SG_CV;
+    for (int32_t ncz = -1; ncz <= 1; ++ncz)
+        for (int32_t ncx = -1; ncx <= 1; ++ncx) {
+            OrTree trees[12];
+            int n = or_trees_for_chunk(cx + ncx, cz + ncz, seed, trees);
+            for (int i = 0; i < n; ++i) {
+                if (trees[i].base[1] > c.mx[1] || trees[i].base[1] + 22 < c.mn[1]) continue;
+                sg_paint_tree(&c, &trees[i]);
+            }
+        }
+}
+
+/* fill_demo_terrain (voxel.rs:1005-1060) generalised to a window whose
+ * lower corner is world chunk (ox, 0, oz): the slot (sx, sy, sz) holds the
+ * world chunk shift_origin assigns it (voxel.rs:507-537), then the masks
+ * and LUTs are rebuilt. */
+typedef struct {
+    const OrWorld *w;
+    uint64_t seed;
+    int32_t ox, oz;
+    int64_t j0, j1;
+} SlotJob;
+
+static void *slot_thread(void *arg) {
+    SlotJob *j = (SlotJob *)arg;
+    Dims d = dims_of(j->w);
+    const int32_t sx_n = d.bx / 8, sy_n = d.by / 8, sz_n = d.bz / 8;
+    OrBrick *scratch = (OrBrick *)malloc(sizeof(OrBrick) * 512);
+    if (!scratch) return NULL;
+    for (int64_t k = j->j0; k < j->j1; ++k) {
+        int32_t sx = (int32_t)(k % sx_n), sy = (int32_t)((k / sx_n) % sy_n),
+                sz = (int32_t)(k / ((int64_t)sx_n * sy_n));
+        int32_t wcx = j->ox + pos_mod(sx - j->ox, sx_n);
+        int32_t wcz = j->oz + pos_mod(sz - j->oz, sz_n);
+        or_gen_slot_bricks(wcx, sy, wcz, j->seed, scratch);
+        for (int32_t bz = 0; bz < 8; ++bz)
+            for (int32_t by = 0; by < 8; ++by)
+                for (int32_t bx = 0; bx < 8; ++bx)
+                    j->w->bricks[brick_idx(&d, sx * 8 + bx, sy * 8 + by, sz * 8 + bz)] =
+                        scratch[bx + by * 8 + bz * 64];
+    }
+    free(scratch);
+    return NULL;
+}
+
+void or_fill_window(const OrWorld *w, uint64_t seed, int32_t ox, int32_t oz, int nthreads) {
+    Dims d = dims_of(w);
+    const int64_t n = (int64_t)(d.bx / 8) * (d.by / 8) * (d.bz / 8);
+    if (nthreads < 1) nthreads = 1;
+    if (nthreads > 256) nthreads = 256;
+    pthread_t th[256];
+    SlotJob jobs[256];
+    int used = 0;
+    for (int i = 0; i < nthreads; ++i) {
+        int64_t a = n * i / nthreads, b = n * (i + 1) / nthreads;
+        if (b <= a) continue;
+        jobs[used].w = w; jobs[used].seed = seed; jobs[used].ox = ox; jobs[used].oz = oz;
+        jobs[used].j0 = a; jobs[used].j1 = b;
+        used++;
+    }
+    for (int i = 1; i < used; ++i) pthread_create(&th[i], NULL, slot_thread, &jobs[i]);
+    if (used > 0) slot_thread(&jobs[0]);
+    for (int i = 1; i < used; ++i) pthread_join(th[i], NULL);
+    or_rebuild_all_masks(w);
+    or_rebuild_all_uniform(w);
+}
+
+/* ------------------------------------------------------------------ */
 /* ray generation                                                      */
 /* ------------------------------------------------------------------ */
 static inline void normalize3(const float v[3], float out[3]) {

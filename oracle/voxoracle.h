@@ -146,6 +146,23 @@ typedef struct {
 /* Fill bricks (not masks) with the seeded terrain; columns [x0,x1). */
 void or_generate_terrain(const OrWorld *w, const OrTerrain *t, int nthreads);
 
+/* ---- the reference's chunk generator gen_slot_bricks (voxel.rs:1322-1500) ---- */
+typedef struct {
+    int32_t base[3];
+    uint32_t ttype;   /* 0 oak, 1 birch, 2 pine, 3 autumn, 4 cactus */
+    uint32_t hash;
+} OrTree;
+/* sample_terrain (voxel.rs:1244-1316): column height; *water_top if non-null */
+int32_t or_sample_terrain(float wx, float wz, uint64_t seed, int32_t *water_top);
+/* trees_for_chunk (voxel.rs:1537-1591): up to 12 trees, returns the count */
+int or_trees_for_chunk(int32_t cx, int32_t cz, uint64_t seed, OrTree out[12]);
+/* one storage chunk: 512 bricks, index x + y*8 + z*64 */
+void or_gen_slot_bricks(int32_t cx, int32_t cy, int32_t cz, uint64_t seed, OrBrick *out);
+/* every slot of a window whose lower corner is world chunk (ox, 0, oz), in
+ * the toroidal slot shift_origin assigns (voxel.rs:507-537); then masks and
+ * LUTs rebuilt.  World dims must be multiples of 8 bricks. */
+void or_fill_window(const OrWorld *w, uint64_t seed, int32_t ox, int32_t oz, int nthreads);
+
 /* ---- rays ---- */
 void or_ray_dir_uv(const OrCamera *c, float u, float v, float out[3]);
 void or_sincos(float x, float *s, float *c);

@@ -33,6 +33,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-O2,-ffp-contra
 SOURCES = [
     ("vx_trace.cu", EXACT),
     ("vx_world.cu", EXACT),
+    ("vx_slotgen.cu", EXACT),
     ("vx_noalloc.cu", EXACT),
     ("vx_queue.cu", EXACT),
     ("vx_learned.cu", EXACT),

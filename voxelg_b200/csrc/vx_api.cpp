@@ -53,6 +53,11 @@ struct VxWorld {
     vx::QueueScratch qs;             // scratch of vx_queue_run / vx_queue_autotune
     cudaEvent_t band_ev[8] = {};
     VxTuning tuning{0, {0, 0, 0, 0, 0, 0, 0}};
+    // chunk generator state: the world chunk each storage-chunk slot holds
+    // (3 ints per slot, empty until a window is filled), its seed and origin
+    std::vector<int32_t> slot_chunk;
+    uint64_t gen_seed = 0;
+    int32_t gen_origin[2] = {0, 0};
 };
 
 namespace vx {
@@ -406,6 +411,146 @@ int vx_world_generate(VxWorld *w, const VxTerrainParams *t) {
     cudaFreeAsync(heights, w->stream);
     VX_CK(e);
     VX_CK(cudaStreamSynchronize(w->stream));
+    return VX_OK;
+}
+
+namespace {
+// Generates the listed world chunks (x, y, z triples) into their toroidal
+// slots: slot = (pos_mod(x, SX), y, pos_mod(z, SZ)), SX/SY/SZ the window in
+// storage chunks (voxel.rs:507-537).  Caller holds w->mu.
+int gen_chunks_locked(VxWorld *w, uint64_t seed, const int32_t *chunks, uint32_t n,
+                      const char *fn) {
+    const vx::Dims &d = w->dw.d;
+    const int32_t sx_n = d.bx / 8, sy_n = d.by / 8, sz_n = d.bz / 8;
+    // one job per slot: a later chunk for the same slot replaces an earlier
+    // one, as a later install does in the reference
+    std::vector<int64_t> last((size_t)sx_n * sy_n * sz_n, -1);
+    for (uint32_t i = 0; i < n; ++i) {
+        const int32_t cx = chunks[3 * i], cy = chunks[3 * i + 1], cz = chunks[3 * i + 2];
+        if (cy < 0 || cy >= sy_n || cx < -(1 << 24) || cx >= (1 << 24) || cz < -(1 << 24) ||
+            cz >= (1 << 24)) {
+            vx::set_error(std::string(fn) + ": chunk y outside the window or x/z beyond +-2^24");
+            return VX_ERR_INVALID;
+        }
+        const int32_t sx = ((cx % sx_n) + sx_n) % sx_n, sz = ((cz % sz_n) + sz_n) % sz_n;
+        last[(size_t)sx + (size_t)cy * sx_n + (size_t)sz * sx_n * sy_n] = i;
+    }
+    std::vector<int32_t> jobs;
+    jobs.reserve((size_t)n * 6);
+    for (uint32_t i = 0; i < n; ++i) {
+        const int32_t cx = chunks[3 * i], cy = chunks[3 * i + 1], cz = chunks[3 * i + 2];
+        const int32_t sx = ((cx % sx_n) + sx_n) % sx_n, sz = ((cz % sz_n) + sz_n) % sz_n;
+        if (last[(size_t)sx + (size_t)cy * sx_n + (size_t)sz * sx_n * sy_n] != (int64_t)i) continue;
+        const int32_t j[6] = {cx, cy, cz, sx, cy, sz};
+        jobs.insert(jobs.end(), j, j + 6);
+    }
+    n = (uint32_t)(jobs.size() / 6);
+    if (w->slot_chunk.empty()) w->slot_chunk.assign((size_t)sx_n * sy_n * sz_n * 3, INT32_MIN);
+    if (n == 0) return VX_OK;
+    int32_t *d_jobs = nullptr;
+    VX_CK(cudaMallocAsync(&d_jobs, jobs.size() * sizeof(int32_t), w->stream));
+    cudaError_t e = cudaMemcpyAsync(d_jobs, jobs.data(), jobs.size() * sizeof(int32_t),
+                                    cudaMemcpyHostToDevice, w->stream);
+    if (e == cudaSuccess) e = vx::launch_gen_slots(w->dw, seed, d_jobs, n, w->stream);
+    cudaFreeAsync(d_jobs, w->stream);
+    VX_CK(e);
+    VX_CK(cudaStreamSynchronize(w->stream));
+    for (uint32_t i = 0; i < n; ++i) {
+        const int32_t *j = &jobs[(size_t)i * 6];
+        const size_t slot = (size_t)j[3] + (size_t)j[4] * sx_n + (size_t)j[5] * sx_n * sy_n;
+        w->slot_chunk[slot * 3] = j[0];
+        w->slot_chunk[slot * 3 + 1] = j[1];
+        w->slot_chunk[slot * 3 + 2] = j[2];
+    }
+    return VX_OK;
+}
+
+// The world chunk shift_origin assigns slot (sx, sy, sz) for a window
+// whose lower corner is chunk (ox, oz) (voxel.rs:515-521).
+inline void wanted_chunk(const vx::Dims &d, int32_t ox, int32_t oz, int32_t sx, int32_t sy,
+                         int32_t sz, int32_t out[3]) {
+    const int32_t sx_n = d.bx / 8, sz_n = d.bz / 8;
+    out[0] = ox + (((sx - ox) % sx_n) + sx_n) % sx_n;
+    out[1] = sy;
+    out[2] = oz + (((sz - oz) % sz_n) + sz_n) % sz_n;
+}
+
+bool origin_in_range(int32_t ox, int32_t oz) {
+    return ox > -(1 << 23) && ox < (1 << 23) && oz > -(1 << 23) && oz < (1 << 23);
+}
+}  // namespace
+
+int vx_world_gen_chunks(VxWorld *w, uint64_t seed, const int32_t *chunks, uint32_t n) {
+    if (!w || (n > 0 && !chunks)) {
+        vx::set_error("vx_world_gen_chunks: null argument");
+        return VX_ERR_INVALID;
+    }
+    int rc = use_device(w);
+    if (rc != VX_OK) return rc;
+    std::lock_guard<std::mutex> lk(w->mu);
+    return gen_chunks_locked(w, seed, chunks, n, "vx_world_gen_chunks");
+}
+
+int vx_world_fill_window(VxWorld *w, uint64_t seed, int32_t origin_cx, int32_t origin_cz) {
+    if (!w || !origin_in_range(origin_cx, origin_cz)) {
+        vx::set_error("vx_world_fill_window: null world or origin beyond +-2^23 chunks");
+        return VX_ERR_INVALID;
+    }
+    int rc = use_device(w);
+    if (rc != VX_OK) return rc;
+    std::lock_guard<std::mutex> lk(w->mu);
+    const vx::Dims &d = w->dw.d;
+    const int32_t sx_n = d.bx / 8, sy_n = d.by / 8, sz_n = d.bz / 8;
+    std::vector<int32_t> chunks;
+    chunks.reserve((size_t)sx_n * sy_n * sz_n * 3);
+    for (int32_t sz = 0; sz < sz_n; ++sz)
+        for (int32_t sy = 0; sy < sy_n; ++sy)
+            for (int32_t sx = 0; sx < sx_n; ++sx) {
+                int32_t c[3];
+                wanted_chunk(d, origin_cx, origin_cz, sx, sy, sz, c);
+                chunks.insert(chunks.end(), c, c + 3);
+            }
+    rc = gen_chunks_locked(w, seed, chunks.data(), (uint32_t)(chunks.size() / 3),
+                           "vx_world_fill_window");
+    if (rc != VX_OK) return rc;
+    w->gen_seed = seed;
+    w->gen_origin[0] = origin_cx;
+    w->gen_origin[1] = origin_cz;
+    return VX_OK;
+}
+
+int vx_world_shift_origin(VxWorld *w, int32_t origin_cx, int32_t origin_cz,
+                          uint32_t *n_regenerated) {
+    if (!w || !origin_in_range(origin_cx, origin_cz)) {
+        vx::set_error("vx_world_shift_origin: null world or origin beyond +-2^23 chunks");
+        return VX_ERR_INVALID;
+    }
+    int rc = use_device(w);
+    if (rc != VX_OK) return rc;
+    std::lock_guard<std::mutex> lk(w->mu);
+    if (w->slot_chunk.empty()) {
+        vx::set_error("vx_world_shift_origin: no window generated yet (vx_world_fill_window)");
+        return VX_ERR_INVALID;
+    }
+    const vx::Dims &d = w->dw.d;
+    const int32_t sx_n = d.bx / 8, sy_n = d.by / 8, sz_n = d.bz / 8;
+    std::vector<int32_t> chunks;
+    for (int32_t sz = 0; sz < sz_n; ++sz)
+        for (int32_t sy = 0; sy < sy_n; ++sy)
+            for (int32_t sx = 0; sx < sx_n; ++sx) {
+                int32_t c[3];
+                wanted_chunk(d, origin_cx, origin_cz, sx, sy, sz, c);
+                const size_t slot = (size_t)sx + (size_t)sy * sx_n + (size_t)sz * sx_n * sy_n;
+                const int32_t *have = &w->slot_chunk[slot * 3];
+                if (have[0] != c[0] || have[1] != c[1] || have[2] != c[2])
+                    chunks.insert(chunks.end(), c, c + 3);
+            }
+    rc = gen_chunks_locked(w, w->gen_seed, chunks.data(), (uint32_t)(chunks.size() / 3),
+                           "vx_world_shift_origin");
+    if (rc != VX_OK) return rc;
+    w->gen_origin[0] = origin_cx;
+    w->gen_origin[1] = origin_cz;
+    if (n_regenerated) *n_regenerated = (uint32_t)(chunks.size() / 3);
     return VX_OK;
 }
 

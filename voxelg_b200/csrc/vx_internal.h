@@ -91,6 +91,10 @@ cudaError_t launch_bricks_from_aos(const DevWorld &w, const VxBrick *aos, int64_
                                    int64_t count, cudaStream_t s);
 cudaError_t launch_bricks_to_aos(const DevWorld &w, VxBrick *aos, int64_t first, int64_t count,
                                  cudaStream_t s);
+// gen_slot_bricks on the device: d_jobs holds 6 ints per job (world chunk
+// x, y, z, slot x, y, z); the pyramid is rebuilt afterwards.
+cudaError_t launch_gen_slots(const DevWorld &w, uint64_t seed, const int32_t *d_jobs,
+                             uint32_t n_jobs, cudaStream_t s);
 cudaError_t launch_generate(const DevWorld &w, const VxTerrainParams &t, int16_t *heights,
                             cudaStream_t s);
 cudaError_t launch_rebuild_pyramid(const DevWorld &w, cudaStream_t s);

@@ -117,6 +117,26 @@ class DeviceWorld:
         t = terrain.to_c()
         L.check(self._lib.vx_world_generate(self.handle, C.byref(t)))
 
+    def fill_window(self, seed: int, origin_cx: int = 0, origin_cz: int = 0):
+        """The reference's chunk generator (gen_slot_bricks) over every
+        storage-chunk slot of a window whose lower corner is world chunk
+        (origin_cx, 0, origin_cz); origin 0 is fill_demo_terrain."""
+        L.check(self._lib.vx_world_fill_window(self.handle, C.c_uint64(seed & (2**64 - 1)),
+                                               origin_cx, origin_cz))
+
+    def shift_origin(self, origin_cx: int, origin_cz: int) -> int:
+        """Slide the window (shift_origin): regenerates the slots whose
+        world chunk changes and returns how many."""
+        n = C.c_uint32()
+        L.check(self._lib.vx_world_shift_origin(self.handle, origin_cx, origin_cz, C.byref(n)))
+        return n.value
+
+    def gen_chunks(self, seed: int, chunks):
+        """Generate the given world chunks ((x, y, z) rows) into their slots."""
+        c = np.ascontiguousarray(np.asarray(chunks, dtype=np.int32).reshape(-1, 3))
+        L.check(self._lib.vx_world_gen_chunks(self.handle, C.c_uint64(seed & (2**64 - 1)),
+                                              L.ptr(c), len(c)))
+
     def apply_dirty(self, brick_idx: np.ndarray, bricks: np.ndarray, stream: int = 0):
         idx = np.ascontiguousarray(brick_idx, dtype=np.uint32)
         b = np.ascontiguousarray(bricks).view(L.BRICK_DTYPE)
