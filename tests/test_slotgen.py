@@ -274,3 +274,14 @@ def test_frame_on_reference_world():
         mats = set(np.unique(got["mat"][(got["flags"] & 1) == 1]).tolist())
         assert mats & {14, 25, 26, 27, 33}, mats   # foliage was hit
     dw.close()
+
+
+def test_hash_normalisation_without_division():
+    """The device noise computes hash2/hash3's (h & 0xFFFFFF) / 16777215.0
+    (voxel.rs:1180, :1192) as float(u) * 2^-24 with its bit pattern plus
+    one: equal to the IEEE binary32 quotient for every u < 2^24."""
+    u = np.arange(1 << 24, dtype=np.uint32)
+    q = u.astype(np.float32) / np.float32(16777215.0)
+    p = (u.astype(np.float32) * np.float32(2.0 ** -24)).view(np.uint32)
+    r = np.where(u != 0, p + np.uint32(1), np.uint32(0)).view(np.float32)
+    assert np.array_equal(q.view(np.uint32), r.view(np.uint32))

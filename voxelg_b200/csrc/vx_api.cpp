@@ -58,6 +58,10 @@ struct VxWorld {
     std::vector<int32_t> slot_chunk;
     uint64_t gen_seed = 0;
     int32_t gen_origin[2] = {0, 0};
+    void *d_gen = nullptr;           // chunk generator scratch: plan, column words, trees
+    size_t gen_cap = 0;              // bytes
+    void *h_gen = nullptr;           // pinned staging of the generator's plan
+    size_t h_gen_cap = 0;            // bytes
 };
 
 namespace vx {
@@ -114,6 +118,8 @@ void free_world(VxWorld *w) {
     if (w->pick) cudaFreeHost(w->pick);
     cudaFree(w->d_work);
     cudaFree(w->d_gate_idx);
+    cudaFree(w->d_gen);
+    if (w->h_gen) cudaFreeHost(w->h_gen);
     w->qs.release();
     for (auto &e : w->ev)
         if (e) cudaEventDestroy(e);
@@ -415,6 +421,52 @@ int vx_world_generate(VxWorld *w, const VxTerrainParams *t) {
 }
 
 namespace {
+// pos_mod(a, n) for n > 0; a mask when n is a power of two
+inline int32_t wrap(int32_t a, int32_t n) {
+    return (n & (n - 1)) == 0 ? (a & (n - 1)) : ((a % n) + n) % n;
+}
+
+// Lays out the generator's scratch -- the plan's ints (explicit plans),
+// column words, tree headers and primitives -- uploads the ints through the
+// pinned staging buffer, runs the kernels and waits.  Caller holds w->mu.
+int run_gen_plan(VxWorld *w, uint64_t seed, vx::GenPlan &plan, const std::vector<int32_t> &ints) {
+    auto up16 = [](size_t b) { return (b + 15) & ~(size_t)15; };
+    const size_t plan_bytes = ints.size() * sizeof(int32_t);
+    const size_t off_colw = up16(plan_bytes);
+    const size_t off_hdr = off_colw + up16((size_t)plan.n_cols * 1024 * sizeof(uint32_t));
+    const size_t off_prim = off_hdr + up16((size_t)plan.n_srcs * 12 * sizeof(int32_t));
+    const size_t bytes = off_prim + (size_t)plan.n_srcs * vx::gen_prim_bytes_per_src();
+    if (bytes > w->gen_cap) {
+        VX_CK(cudaStreamSynchronize(w->stream));
+        cudaFree(w->d_gen);
+        w->d_gen = nullptr;
+        w->gen_cap = 0;
+        VX_CK(cudaMalloc(&w->d_gen, bytes));
+        w->gen_cap = bytes;
+    }
+    uint8_t *base = static_cast<uint8_t *>(w->d_gen);
+    if (plan_bytes > 0) {
+        if (plan_bytes > w->h_gen_cap) {
+            if (w->h_gen) cudaFreeHost(w->h_gen);
+            w->h_gen = nullptr;
+            w->h_gen_cap = 0;
+            VX_CK(cudaHostAlloc(&w->h_gen, plan_bytes, cudaHostAllocDefault));
+            w->h_gen_cap = plan_bytes;
+        }
+        std::memcpy(w->h_gen, ints.data(), plan_bytes);   // the previous call synchronized
+        VX_CK(cudaMemcpyAsync(base, w->h_gen, plan_bytes, cudaMemcpyHostToDevice, w->stream));
+        plan.jobs = reinterpret_cast<const int32_t *>(base);
+        plan.cols = plan.jobs + (size_t)plan.n_jobs * vx::kGenJobInts;
+        plan.srcs = plan.cols + (size_t)plan.n_cols * 2;
+    }
+    plan.colw = reinterpret_cast<uint32_t *>(base + off_colw);
+    plan.hdr = reinterpret_cast<int32_t *>(base + off_hdr);
+    plan.prims = base + off_prim;
+    VX_CK(vx::launch_gen_slots(w->dw, seed, plan, w->stream));
+    VX_CK(cudaStreamSynchronize(w->stream));
+    return VX_OK;
+}
+
 // Generates the listed world chunks (x, y, z triples) into their toroidal
 // slots: slot = (pos_mod(x, SX), y, pos_mod(z, SZ)), SX/SY/SZ the window in
 // storage chunks (voxel.rs:507-537).  Caller holds w->mu.
@@ -425,6 +477,7 @@ int gen_chunks_locked(VxWorld *w, uint64_t seed, const int32_t *chunks, uint32_t
     // one job per slot: a later chunk for the same slot replaces an earlier
     // one, as a later install does in the reference
     std::vector<int64_t> last((size_t)sx_n * sy_n * sz_n, -1);
+    std::vector<uint32_t> slot_of(n);
     for (uint32_t i = 0; i < n; ++i) {
         const int32_t cx = chunks[3 * i], cy = chunks[3 * i + 1], cz = chunks[3 * i + 2];
         if (cy < 0 || cy >= sy_n || cx < -(1 << 24) || cx >= (1 << 24) || cz < -(1 << 24) ||
@@ -432,31 +485,67 @@ int gen_chunks_locked(VxWorld *w, uint64_t seed, const int32_t *chunks, uint32_t
             vx::set_error(std::string(fn) + ": chunk y outside the window or x/z beyond +-2^24");
             return VX_ERR_INVALID;
         }
-        const int32_t sx = ((cx % sx_n) + sx_n) % sx_n, sz = ((cz % sz_n) + sz_n) % sz_n;
-        last[(size_t)sx + (size_t)cy * sx_n + (size_t)sz * sx_n * sy_n] = i;
+        slot_of[i] = (uint32_t)wrap(cx, sx_n) + (uint32_t)cy * (uint32_t)sx_n +
+                     (uint32_t)wrap(cz, sz_n) * (uint32_t)(sx_n * sy_n);
+        last[slot_of[i]] = i;
     }
-    std::vector<int32_t> jobs;
-    jobs.reserve((size_t)n * 6);
+    // distinct xz chunks (terrain columns) and 3x3 source chunks (trees),
+    // numbered through a dense grid over the jobs' bounding box (widened by
+    // the neighbour ring) when it is small, else through a hash map
+    int32_t x0 = INT32_MAX, x1 = INT32_MIN, z0 = INT32_MAX, z1 = INT32_MIN;
+    for (uint32_t i = 0; i < n; ++i) {
+        x0 = std::min(x0, chunks[3 * i] - 1);
+        x1 = std::max(x1, chunks[3 * i] + 1);
+        z0 = std::min(z0, chunks[3 * i + 2] - 1);
+        z1 = std::max(z1, chunks[3 * i + 2] + 1);
+    }
+    const int64_t gw = n ? (int64_t)x1 - x0 + 1 : 0, gh = n ? (int64_t)z1 - z0 + 1 : 0;
+    const bool dense = gw * gh <= std::max<int64_t>(1 << 16, (int64_t)n * 16);
+    std::vector<int32_t> col_grid(dense ? gw * gh : 0, -1), src_grid(dense ? gw * gh : 0, -1);
+    std::unordered_map<uint64_t, int32_t> col_map, src_map;
+    std::vector<int32_t> jobs, cols, srcs;
+    auto index = [&](std::vector<int32_t> &grid, std::unordered_map<uint64_t, int32_t> &m,
+                     std::vector<int32_t> &v, int32_t x, int32_t z) {
+        int32_t *slot;
+        if (dense) {
+            slot = &grid[(size_t)(z - z0) * gw + (size_t)(x - x0)];
+        } else {
+            slot = &m.emplace(((uint64_t)(uint32_t)x << 32) | (uint32_t)z, -1).first->second;
+        }
+        if (*slot < 0) {
+            *slot = (int32_t)(v.size() / 2);
+            v.push_back(x);
+            v.push_back(z);
+        }
+        return *slot;
+    };
+    jobs.reserve((size_t)n * vx::kGenJobInts);
     for (uint32_t i = 0; i < n; ++i) {
         const int32_t cx = chunks[3 * i], cy = chunks[3 * i + 1], cz = chunks[3 * i + 2];
-        const int32_t sx = ((cx % sx_n) + sx_n) % sx_n, sz = ((cz % sz_n) + sz_n) % sz_n;
-        if (last[(size_t)sx + (size_t)cy * sx_n + (size_t)sz * sx_n * sy_n] != (int64_t)i) continue;
-        const int32_t j[6] = {cx, cy, cz, sx, cy, sz};
-        jobs.insert(jobs.end(), j, j + 6);
+        if (last[slot_of[i]] != (int64_t)i) continue;
+        const int32_t sx = wrap(cx, sx_n), sz = wrap(cz, sz_n);
+        int32_t j[vx::kGenJobInts] = {cx, cy, cz, sx, cy, sz,
+                                      index(col_grid, col_map, cols, cx, cz)};
+        for (int k = 0; k < 9; ++k)
+            j[7 + k] = index(src_grid, src_map, srcs, cx + k % 3 - 1, cz + k / 3 - 1);
+        jobs.insert(jobs.end(), j, j + vx::kGenJobInts);
     }
-    n = (uint32_t)(jobs.size() / 6);
+    n = (uint32_t)(jobs.size() / vx::kGenJobInts);
     if (w->slot_chunk.empty()) w->slot_chunk.assign((size_t)sx_n * sy_n * sz_n * 3, INT32_MIN);
     if (n == 0) return VX_OK;
-    int32_t *d_jobs = nullptr;
-    VX_CK(cudaMallocAsync(&d_jobs, jobs.size() * sizeof(int32_t), w->stream));
-    cudaError_t e = cudaMemcpyAsync(d_jobs, jobs.data(), jobs.size() * sizeof(int32_t),
-                                    cudaMemcpyHostToDevice, w->stream);
-    if (e == cudaSuccess) e = vx::launch_gen_slots(w->dw, seed, d_jobs, n, w->stream);
-    cudaFreeAsync(d_jobs, w->stream);
-    VX_CK(e);
-    VX_CK(cudaStreamSynchronize(w->stream));
+    // [jobs | cols | srcs] ints, then column words, headers, primitives
+    std::vector<int32_t> ints(jobs);
+    ints.insert(ints.end(), cols.begin(), cols.end());
+    ints.insert(ints.end(), srcs.begin(), srcs.end());
+    vx::GenPlan plan{};
+    plan.window = false;
+    plan.n_jobs = n;
+    plan.n_cols = (uint32_t)(cols.size() / 2);
+    plan.n_srcs = (uint32_t)(srcs.size() / 2);
+    int rc = run_gen_plan(w, seed, plan, ints);
+    if (rc != VX_OK) return rc;
     for (uint32_t i = 0; i < n; ++i) {
-        const int32_t *j = &jobs[(size_t)i * 6];
+        const int32_t *j = &jobs[(size_t)i * vx::kGenJobInts];
         const size_t slot = (size_t)j[3] + (size_t)j[4] * sx_n + (size_t)j[5] * sx_n * sy_n;
         w->slot_chunk[slot * 3] = j[0];
         w->slot_chunk[slot * 3 + 1] = j[1];
@@ -469,10 +558,9 @@ int gen_chunks_locked(VxWorld *w, uint64_t seed, const int32_t *chunks, uint32_t
 // whose lower corner is chunk (ox, oz) (voxel.rs:515-521).
 inline void wanted_chunk(const vx::Dims &d, int32_t ox, int32_t oz, int32_t sx, int32_t sy,
                          int32_t sz, int32_t out[3]) {
-    const int32_t sx_n = d.bx / 8, sz_n = d.bz / 8;
-    out[0] = ox + (((sx - ox) % sx_n) + sx_n) % sx_n;
+    out[0] = ox + wrap(sx - ox, d.bx / 8);
     out[1] = sy;
-    out[2] = oz + (((sz - oz) % sz_n) + sz_n) % sz_n;
+    out[2] = oz + wrap(sz - oz, d.bz / 8);
 }
 
 bool origin_in_range(int32_t ox, int32_t oz) {
@@ -501,18 +589,22 @@ int vx_world_fill_window(VxWorld *w, uint64_t seed, int32_t origin_cx, int32_t o
     std::lock_guard<std::mutex> lk(w->mu);
     const vx::Dims &d = w->dw.d;
     const int32_t sx_n = d.bx / 8, sy_n = d.by / 8, sz_n = d.bz / 8;
-    std::vector<int32_t> chunks;
-    chunks.reserve((size_t)sx_n * sy_n * sz_n * 3);
+    vx::GenPlan plan{};
+    plan.window = true;
+    plan.ox = origin_cx;
+    plan.oz = origin_cz;
+    plan.n_jobs = (uint32_t)(sx_n * sy_n * sz_n);
+    plan.n_cols = (uint32_t)(sx_n * sz_n);
+    plan.n_srcs = (uint32_t)((sx_n + 2) * (sz_n + 2));
+    rc = run_gen_plan(w, seed, plan, {});
+    if (rc != VX_OK) return rc;
+    w->slot_chunk.resize((size_t)sx_n * sy_n * sz_n * 3);
     for (int32_t sz = 0; sz < sz_n; ++sz)
         for (int32_t sy = 0; sy < sy_n; ++sy)
             for (int32_t sx = 0; sx < sx_n; ++sx) {
-                int32_t c[3];
-                wanted_chunk(d, origin_cx, origin_cz, sx, sy, sz, c);
-                chunks.insert(chunks.end(), c, c + 3);
+                const size_t slot = (size_t)sx + (size_t)sy * sx_n + (size_t)sz * sx_n * sy_n;
+                wanted_chunk(d, origin_cx, origin_cz, sx, sy, sz, &w->slot_chunk[slot * 3]);
             }
-    rc = gen_chunks_locked(w, seed, chunks.data(), (uint32_t)(chunks.size() / 3),
-                           "vx_world_fill_window");
-    if (rc != VX_OK) return rc;
     w->gen_seed = seed;
     w->gen_origin[0] = origin_cx;
     w->gen_origin[1] = origin_cz;

@@ -91,10 +91,33 @@ cudaError_t launch_bricks_from_aos(const DevWorld &w, const VxBrick *aos, int64_
                                    int64_t count, cudaStream_t s);
 cudaError_t launch_bricks_to_aos(const DevWorld &w, VxBrick *aos, int64_t first, int64_t count,
                                  cudaStream_t s);
-// gen_slot_bricks on the device: d_jobs holds 6 ints per job (world chunk
-// x, y, z, slot x, y, z); the pyramid is rebuilt afterwards.
-cudaError_t launch_gen_slots(const DevWorld &w, uint64_t seed, const int32_t *d_jobs,
-                             uint32_t n_jobs, cudaStream_t s);
+// gen_slot_bricks on the device.  Explicit plans (window == false) list
+// their jobs: kGenJobInts ints each -- world chunk x, y, z; slot x, y, z;
+// the index of its xz chunk in `cols`; the indices in `srcs` of its 3x3
+// source chunks in (z, x) order; cols / srcs hold (x, z) pairs.  A window
+// plan (window == true) generates every slot of the window whose lower
+// corner is world chunk (ox, 0, oz) and derives all of that on the device:
+// job b is slot (b % SX, b / SX % SY, b / (SX SY)), column k the slot column
+// (k % SX, k / SX), source k world chunk (ox - 1 + k % (SX + 2),
+// oz - 1 + k / (SX + 2)).  colw has 1024 words per column chunk, prims
+// gen_prim_bytes_per_src() bytes and hdr 12 ints per source chunk.  The
+// pyramid is rebuilt afterwards.
+constexpr int kGenJobInts = 16;
+struct GenPlan {
+    bool window;
+    int32_t ox, oz;            // window plans
+    const int32_t *jobs;       // explicit plans
+    uint32_t n_jobs;
+    const int32_t *cols;       // explicit plans
+    uint32_t n_cols;
+    const int32_t *srcs;       // explicit plans
+    uint32_t n_srcs;
+    uint32_t *colw;
+    void *prims;
+    int32_t *hdr;
+};
+size_t gen_prim_bytes_per_src();
+cudaError_t launch_gen_slots(const DevWorld &w, uint64_t seed, const GenPlan &p, cudaStream_t s);
 cudaError_t launch_generate(const DevWorld &w, const VxTerrainParams &t, int16_t *heights,
                             cudaStream_t s);
 cudaError_t launch_rebuild_pyramid(const DevWorld &w, cudaStream_t s);

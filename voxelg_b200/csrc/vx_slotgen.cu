@@ -4,21 +4,27 @@
 // neighbours, written straight into the world's toroidal slots.  Compiled
 // with --fmad=false so every binary32 operation rounds as the CPU's does.
 //
-// One 1024-thread CTA generates one storage chunk (32^3 voxels, 512 bricks)
-// in shared memory:
-//   1. thread (dx, dz) runs its column (voxel.rs:1333-1461);
-//   2. threads 0..107 each take one tree candidate of the 3x3 source chunks
-//      (trees_for_chunk, voxel.rs:1537-1591) and expand it into its paint
-//      primitives (paint_tree, :1605-1710), keeping those whose box meets
-//      the chunk;
-//   3. the CTA paints the primitives in the reference's order -- source
-//      chunk (z, x), tree, primitive -- one primitive at a time with a
-//      barrier between, its voxels spread over all threads.  Every write of
-//      one primitive carries the same material, so the order among them
-//      cannot change what try_write_tree_voxel (:1500-1525) leaves;
-//   4. the 512 bricks, their occupancy words (occupancy == material != 0,
-//      the invariant Brick::set keeps, :315-325) and uniform bytes are
-//      written to the slot's bricks.
+// The reference recomputes, for every storage chunk, the terrain of its
+// 32x32 columns and the trees of its 3x3 neighbourhood.  Both depend only on
+// x and z, so a batch of chunks is generated by three kernels:
+//   k_gen_columns  one thread per column of each distinct xz chunk:
+//                  sample_terrain (:1244-1316), the biome (:1342-1344) and
+//                  the surface decoration (:1394-1459) packed in one word;
+//   k_gen_trees    one thread per tree candidate of each distinct source
+//                  chunk (trees_for_chunk, :1537-1591), expanded into its
+//                  paint primitives (paint_tree, :1605-1710);
+//   k_gen_slot     one 256-thread CTA per storage chunk, four per SM: the
+//                  voxels of its columns (cave and ore noise per voxel) in
+//                  shared memory, then the primitives of the 3x3 source
+//                  chunks in the reference's order -- source chunk (z, x),
+//                  tree, primitive -- one primitive at a time with a
+//                  barrier between, skipping primitives whose box misses
+//                  the chunk.  Every write of one primitive carries one
+//                  material, so the order among its voxels cannot change
+//                  what try_write_tree_voxel (:1500-1525) leaves.  Last the
+//                  512 bricks, their occupancy words (occupancy == material
+//                  != 0, the invariant Brick::set keeps, :315-325) and
+//                  uniform bytes go to the slot's bricks.
 // pow, cos and sin are evaluated in double precision and rounded to float.
 #include <cuda_runtime.h>
 
@@ -38,7 +44,6 @@ constexpr int kWorldY = 256;     // WORLD_VOXELS_Y the generator is written for
 constexpr int kCand = 12;        // trees_for_chunk yields at most round(1.2*5)*2
 constexpr int kTrees = 9 * kCand;
 constexpr int kPrims = 16;       // primitives of one tree (oak: 1 + 4*3 + 2)
-constexpr int kThreads = 1024;
 
 enum : uint8_t {
     M_SAND = 1, M_GRASS = 2, M_DIRT = 3, M_STONE = 4, M_WATER = 12, M_WOOD = 13,
@@ -61,9 +66,7 @@ __device__ __forceinline__ float pow_f(float x, float y) { return (float)pow((do
 __device__ __forceinline__ float cos_f(float x) { return (float)cos((double)x); }
 __device__ __forceinline__ float sin_f(float x) { return (float)sin((double)x); }
 
-struct SlotGen {
-    DevWorld w;
-    const int32_t *jobs;   // per job: world chunk x, y, z, slot x, y, z
+struct Seed {
     uint64_t seed;
     float offx, offz;      // seed_offset_xz, voxel.rs:1163-1167
 };
@@ -130,19 +133,6 @@ __device__ __forceinline__ float tree_density(int b) {
     }
 }
 
-// stone_or_ore, voxel.rs:1906-1916
-__device__ __forceinline__ uint8_t stone_or_ore(float x, float y, float z, uint32_t h) {
-    const float depth = fmaxr((float)h - y, 0.0f);
-    const float n1 = value_noise_3d(x * 0.27f, y * 0.27f, z * 0.27f);
-    const float n2 = value_noise_3d(x * 0.55f, y * 0.55f, z * 0.55f);
-    const float combined = n1 + n2 * 0.30f;
-    if (depth > 30.0f && combined > 0.50f) return M_DIAMOND;
-    if (depth > 20.0f && combined > 0.36f) return M_GOLD;
-    if (depth > 10.0f && combined > 0.24f) return M_IRON;
-    if (combined > 0.32f) return M_COAL;
-    return M_STONE;
-}
-
 // shared-memory chunk: brick (x + y*8 + z*64) * 64 + x + z*4 + y*16
 __device__ __forceinline__ uint32_t vox(uint32_t dx, uint32_t dy, uint32_t dz) {
     return (((dx >> 2) + (dy >> 2) * 8u + (dz >> 2) * 64u) << 6) +
@@ -157,7 +147,7 @@ struct Tree {
 
 // candidate i of trees_for_chunk(cx, cz) (voxel.rs:1537-1591); false when
 // the reference's loop yields no tree for it
-__device__ bool tree_candidate(int32_t cx, int32_t cz, uint32_t i, const SlotGen &g, Tree &t) {
+__device__ bool tree_candidate(int32_t cx, int32_t cz, uint32_t i, const Seed &g, Tree &t) {
     const float ccx = ((float)cx + 0.5f) * 32.0f, ccz = ((float)cz + 0.5f) * 32.0f;
     const float temperature = fbm_2d((ccx + g.offx) * 0.0006f, (ccz + g.offz) * 0.0006f, 3);
     const float humidity =
@@ -205,22 +195,13 @@ struct Prim {
     int32_t steps;   // line: ceil(len * 1.5)
 };
 
-// Appends a tree's primitives (paint_tree order) that can write into the
-// chunk [lo, lo + 32).
+// Appends a tree's primitives in paint_tree order.
 struct Emit {
     Prim *out;
     int n;
-    int32_t lo[3];
-    __device__ bool meets(int32_t x0, int32_t x1, int32_t y0, int32_t y1, int32_t z0,
-                          int32_t z1) const {
-        return x1 >= lo[0] && x0 < lo[0] + kCV && y1 >= lo[1] && y0 < lo[1] + kCV &&
-               z1 >= lo[2] && z0 < lo[2] + kCV;
-    }
     // paint_line with thickness 0, voxel.rs:1744-1776
     __device__ void line(int32_t ax, int32_t ay, int32_t az, int32_t bx, int32_t by, int32_t bz,
                          uint8_t mat) {
-        if (!meets(min(ax, bx), max(ax, bx), min(ay, by), max(ay, by), min(az, bz), max(az, bz)))
-            return;
         const int32_t d0 = bx - ax, d1 = by - ay, d2 = bz - az;
         const float len = sqrtf((float)(d0 * d0 + d1 * d1 + d2 * d2));
         Prim &p = out[n++];
@@ -232,23 +213,40 @@ struct Emit {
     // paint_fringe_shell(c, r + 1) then paint_sphere(c, r): paint_canopy,
     // voxel.rs:1715-1742, :1778-1789
     __device__ void canopy(int32_t cx, int32_t cy, int32_t cz, int32_t r, uint8_t mat) {
-        const int32_t rf = r + 1;
-        if (meets(cx - rf - 1, cx + rf + 1, cy - rf, cy + rf, cz - rf - 1, cz + rf + 1)) {
-            Prim &p = out[n++];
-            p.a[0] = cx; p.a[1] = cy; p.a[2] = cz;
-            p.b[0] = rf; p.b[1] = p.b[2] = 0;
-            p.kind_mat = (PR_SHELL << 8) | M_FRINGE;
-            p.steps = 0;
-        }
-        if (meets(cx - r, cx + r, cy - r, cy + r, cz - r, cz + r)) {
-            Prim &p = out[n++];
-            p.a[0] = cx; p.a[1] = cy; p.a[2] = cz;
-            p.b[0] = r; p.b[1] = p.b[2] = 0;
-            p.kind_mat = (PR_SPHERE << 8) | mat;
-            p.steps = 0;
-        }
+        Prim &f = out[n++];
+        f.a[0] = cx; f.a[1] = cy; f.a[2] = cz;
+        f.b[0] = r + 1; f.b[1] = f.b[2] = 0;
+        f.kind_mat = (PR_SHELL << 8) | M_FRINGE;
+        f.steps = 0;
+        Prim &p = out[n++];
+        p.a[0] = cx; p.a[1] = cy; p.a[2] = cz;
+        p.b[0] = r; p.b[1] = p.b[2] = 0;
+        p.kind_mat = (PR_SPHERE << 8) | mat;
+        p.steps = 0;
     }
 };
+
+// Whether a primitive can write into the chunk [lo, lo + 32): its voxels
+// lie in the box of the segment (rounding a + d t with t in [0, 1] stays
+// between the ends), in c +- (r + 1, r, r + 1) for a shell, c +- r for a
+// sphere.
+__device__ __forceinline__ bool prim_meets(const Prim &p, const int32_t lo[3]) {
+    const uint32_t kind = p.kind_mat >> 8;
+    int32_t mn[3], mx[3];
+    if (kind == PR_LINE) {
+        for (int k = 0; k < 3; ++k) {
+            mn[k] = min(p.a[k], p.b[k]);
+            mx[k] = max(p.a[k], p.b[k]);
+        }
+    } else {
+        const int32_t r = p.b[0], rh = kind == PR_SHELL ? r + 1 : r;
+        mn[0] = p.a[0] - rh; mx[0] = p.a[0] + rh;
+        mn[1] = p.a[1] - r;  mx[1] = p.a[1] + r;
+        mn[2] = p.a[2] - rh; mx[2] = p.a[2] + rh;
+    }
+    return mx[0] >= lo[0] && mn[0] < lo[0] + kCV && mx[1] >= lo[1] && mn[1] < lo[1] + kCV &&
+           mx[2] >= lo[2] && mn[2] < lo[2] + kCV;
+}
 
 // branch_jitter, voxel.rs:1791-1797
 __device__ __forceinline__ float branch_jitter(uint32_t hash, uint32_t b) {
@@ -329,7 +327,7 @@ __device__ __forceinline__ void tree_voxel(uint8_t *s_mat, const int32_t lo[3], 
 }
 
 // Voxel k of a primitive (any order: one primitive writes one material).
-__device__ void paint_prim(uint8_t *s_mat, const int32_t lo[3], const Prim &p) {
+__device__ void paint_prim(uint8_t *s_mat, const int32_t lo[3], const Prim &p, int nthr) {
     const uint32_t kind = p.kind_mat >> 8;
     const uint8_t mat = (uint8_t)(p.kind_mat & 0xFFu);
     if (kind == PR_LINE) {
@@ -338,7 +336,7 @@ __device__ void paint_prim(uint8_t *s_mat, const int32_t lo[3], const Prim &p) {
             return;
         }
         const int32_t d0 = p.b[0] - p.a[0], d1 = p.b[1] - p.a[1], d2 = p.b[2] - p.a[2];
-        for (int32_t s = (int32_t)threadIdx.x; s <= p.steps; s += kThreads) {
+        for (int32_t s = (int32_t)threadIdx.x; s <= p.steps; s += nthr) {
             const float t = (float)s / (float)p.steps;
             const int32_t x = f2i(roundf((float)p.a[0] + (float)d0 * t));
             const int32_t y = f2i(roundf((float)p.a[1] + (float)d1 * t));
@@ -347,7 +345,7 @@ __device__ void paint_prim(uint8_t *s_mat, const int32_t lo[3], const Prim &p) {
         }
     } else if (kind == PR_SHELL) {
         const int32_t r = p.b[0], r2 = r * r, wxz = 2 * r + 3, n = (2 * r + 1) * wxz * wxz;
-        for (int32_t k = (int32_t)threadIdx.x; k < n; k += kThreads) {
+        for (int32_t k = (int32_t)threadIdx.x; k < n; k += nthr) {
             const int32_t dz = k % wxz - (r + 1), dx = (k / wxz) % wxz - (r + 1),
                           dy = k / (wxz * wxz) - r;
             const int32_t hx = max(abs(dx) - 1, 0), hz = max(abs(dz) - 1, 0);
@@ -356,7 +354,7 @@ __device__ void paint_prim(uint8_t *s_mat, const int32_t lo[3], const Prim &p) {
         }
     } else {
         const int32_t r = p.b[0], r2 = r * r, wd = 2 * r + 1, n = wd * wd * wd;
-        for (int32_t k = (int32_t)threadIdx.x; k < n; k += kThreads) {
+        for (int32_t k = (int32_t)threadIdx.x; k < n; k += nthr) {
             const int32_t dz = k % wd - r, dx = (k / wd) % wd - r, dy = k / (wd * wd) - r;
             if (dx * dx + dy * dy + dz * dz > r2) continue;
             tree_voxel(s_mat, lo, p.a[0] + dx, p.a[1] + dy, p.a[2] + dz, mat);
@@ -364,152 +362,251 @@ __device__ void paint_prim(uint8_t *s_mat, const int32_t lo[3], const Prim &p) {
     }
 }
 
-constexpr size_t kSmemMat = (size_t)kCV * kCV * kCV;
-constexpr size_t kSmemPrim = sizeof(Prim) * kTrees * kPrims;
-constexpr size_t kSmemBytes = kSmemMat + kSmemPrim + 512;
+// ------------------------------------------------------------------ columns
+// Column word: bits 0-7 h, 8 water (water_top = sea level), 9-11 biome,
+// 12-17 decoration material (0: none), 18 the decoration is a big bush.
+// pos_mod(a, n), n > 0
+__device__ __forceinline__ int32_t wrap(int32_t a, int32_t n) { return ((a % n) + n) % n; }
 
-__global__ void __launch_bounds__(kThreads, 1) k_gen_slot(SlotGen g) {
-    extern __shared__ __align__(16) uint8_t smem[];
-    uint8_t *s_mat = smem;
-    Prim *s_prim = reinterpret_cast<Prim *>(smem + kSmemMat);
-    int32_t *s_nprim = reinterpret_cast<int32_t *>(smem + kSmemMat + kSmemPrim);
-    const int32_t *job = g.jobs + (size_t)blockIdx.x * 6;
-    const int32_t cx = job[0], cy = job[1], cz = job[2];
-    const int32_t lo[3] = {cx * kCV, cy * kCV, cz * kCV};
+// The world chunk (x, z) of column chunk k / source chunk k of a plan.
+__device__ __forceinline__ void col_chunk(const GenPlan &p, const Dims &d, uint32_t k,
+                                          int32_t &cx, int32_t &cz) {
+    if (p.window) {
+        const int32_t sxn = d.bx / 8, szn = d.bz / 8;
+        const int32_t sx = (int32_t)k % sxn, sz = (int32_t)k / sxn;
+        cx = p.ox + wrap(sx - p.ox, sxn);
+        cz = p.oz + wrap(sz - p.oz, szn);
+    } else {
+        cx = p.cols[2 * k];
+        cz = p.cols[2 * k + 1];
+    }
+}
+__device__ __forceinline__ void src_chunk(const GenPlan &p, const Dims &d, uint32_t k,
+                                          int32_t &cx, int32_t &cz) {
+    if (p.window) {
+        const int32_t w = d.bx / 8 + 2;
+        cx = p.ox - 1 + (int32_t)k % w;
+        cz = p.oz - 1 + (int32_t)k / w;
+    } else {
+        cx = p.srcs[2 * k];
+        cz = p.srcs[2 * k + 1];
+    }
+}
+
+__global__ void __launch_bounds__(256) k_gen_columns(GenPlan p, Dims d, Seed g) {
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= p.n_cols * (uint32_t)(kCV * kCV)) return;
+    const uint32_t k = c >> 10, col = c & 1023u;
+    int32_t ccx, ccz;
+    col_chunk(p, d, k, ccx, ccz);
+    const int32_t wxi = ccx * kCV + (int32_t)(col & 31u);
+    const int32_t wzi = ccz * kCV + (int32_t)(col >> 5);
+    const float wx = (float)wxi, wz = (float)wzi;
+    int32_t water_top;
+    const int32_t h = sample_terrain(wx, wz, g.offx, g.offz, &water_top);
+    const uint32_t hu = (uint32_t)h;
+    const float temperature = fbm_2d((wx + g.offx) * 0.0006f, (wz + g.offz) * 0.0006f, 3);
+    const float humidity =
+        fbm_2d((wx + g.offx) * 0.0008f + 100.0f, (wz + g.offz) * 0.0008f + 100.0f, 3);
+    const int biome = pick_biome(temperature, humidity, hu);
+    uint32_t dec = 0, big = 0;
+    if (water_top == 0 && hu < (uint32_t)(kWorldY - 1)) {
+        const uint8_t surface = top_block(biome, hu);
+        const int32_t dec_y = h + 1;
+        const float v = hash3(wxi, dec_y, wzi) * 0.5f + 0.5f;
+        const bool big_lattice = hash3(wxi & ~1, 977, wzi & ~1) * 0.5f + 0.5f > 0.9955f;
+        if (surface == M_GRASS) {
+            float fp, gp;
+            if (biome == B_PLAINS) { fp = 0.020f; gp = 0.08f; }
+            else if (biome == B_FOREST) { fp = 0.010f; gp = 0.065f; }
+            else if (biome == B_JUNGLE) { fp = 0.012f; gp = 0.09f; }
+            else { fp = 0.015f; gp = 0.065f; }
+            if (fbm_2d((float)wxi * 0.02f + 7.0f, (float)wzi * 0.02f - 3.0f, 2) > 0.30f) {
+                fp *= 3.0f;
+                gp *= 12.0f;
+            }
+            if (v > 1.0f - fp) dec = M_FLOWER;
+            else if (v > 1.0f - fp - gp) dec = M_TALL_GRASS;
+            else if (big_lattice) dec = M_BUSH;
+            else if (v > 1.0f - fp - gp - 0.004f) dec = M_BUSH;
+        } else if (surface == M_SAND && (biome == B_DESERT || biome == B_SAVANNA)) {
+            if (v > 0.99f) dec = M_GRASS_DRY;
+        } else if (surface == M_SNOW && biome == B_TUNDRA) {
+            if (v > 0.995f) dec = M_GRASS_DRY;
+        }
+        big = (dec == M_BUSH && big_lattice) ? 1u : 0u;
+    }
+    p.colw[c] = hu | ((water_top != 0 ? 1u : 0u) << 8) | ((uint32_t)biome << 9) | (dec << 12) |
+             (big << 18);
+}
+
+// ------------------------------------------------------------------ trees
+// Per source chunk: kCand headers (primitive count | base y << 8, 0 when the
+// candidate yields no tree) and kCand x kPrims primitives.
+__global__ void __launch_bounds__(128) k_gen_trees(GenPlan p, Dims d, Seed g) {
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= p.n_srcs * (uint32_t)kCand) return;
+    const uint32_t k = c / kCand, i = c % kCand;
+    int32_t scx, scz;
+    src_chunk(p, d, k, scx, scz);
+    Tree t;
+    int32_t h = 0;
+    if (tree_candidate(scx, scz, i, g, t)) {
+        Emit e;
+        e.out = reinterpret_cast<Prim *>(p.prims) + (size_t)c * kPrims;
+        e.n = 0;
+        tree_prims(t, e);
+        h = e.n | (t.y << 8);
+    }
+    p.hdr[c] = h;
+}
+
+// ------------------------------------------------------------------ chunks
+constexpr int kSlotThreads = 256;   // four CTAs per SM overlap each other's barriers
+static_assert(kTrees <= 9 * kCand && (512 % kSlotThreads) == 0, "write-out covers 512 bricks");
+
+// Job b of a plan (kGenJobInts ints, the layout of explicit plans).
+__device__ __forceinline__ void job_of(const GenPlan &p, const Dims &d, uint32_t b,
+                                      int32_t job[kGenJobInts]) {
+    if (!p.window) {
+#pragma unroll
+        for (int k = 0; k < kGenJobInts; ++k) job[k] = p.jobs[(size_t)b * kGenJobInts + k];
+        return;
+    }
+    const int32_t sxn = d.bx / 8, syn = d.by / 8, szn = d.bz / 8;
+    const int32_t sx = (int32_t)b % sxn, sy = ((int32_t)b / sxn) % syn,
+                  sz = (int32_t)b / (sxn * syn);
+    const int32_t cx = p.ox + wrap(sx - p.ox, sxn), cz = p.oz + wrap(sz - p.oz, szn);
+    job[0] = cx; job[1] = sy; job[2] = cz;
+    job[3] = sx; job[4] = sy; job[5] = sz;
+    job[6] = sx + sz * sxn;
+#pragma unroll
+    for (int k = 0; k < 9; ++k)
+        job[7 + k] = (cx + k % 3 - 1 - (p.ox - 1)) + (cz + k / 3 - 1 - (p.oz - 1)) * (sxn + 2);
+}
+
+__global__ void __launch_bounds__(kSlotThreads, 4) k_gen_slot(DevWorld w, GenPlan pl) {
+    __shared__ __align__(16) uint8_t s_mat[kCV * kCV * kCV];
+    __shared__ int32_t s_job[kGenJobInts];
+    if (threadIdx.x == 0) {
+        int32_t j[kGenJobInts];
+        job_of(pl, w.d, blockIdx.x, j);
+#pragma unroll
+        for (int k = 0; k < kGenJobInts; ++k) s_job[k] = j[k];
+    }
     const uint32_t tid = threadIdx.x;
+    const Prim *prims = reinterpret_cast<const Prim *>(pl.prims);
 
     uint4 *z4 = reinterpret_cast<uint4 *>(s_mat);
-    for (uint32_t i = tid; i < kSmemMat / 16; i += kThreads) z4[i] = make_uint4(0, 0, 0, 0);
+    for (uint32_t i = tid; i < (uint32_t)(kCV * kCV * kCV / 16); i += kSlotThreads)
+        z4[i] = make_uint4(0, 0, 0, 0);
     __syncthreads();
+    const int32_t *job = s_job;
+    const int32_t lo[3] = {job[0] * kCV, job[1] * kCV, job[2] * kCV};
+    const uint32_t *colw = pl.colw + (size_t)job[6] * (kCV * kCV);
 
-    // ---- 1. the column (dx, dz), voxel.rs:1333-1461
-    {
-        const int32_t dx = (int32_t)(tid & 31u), dz = (int32_t)(tid >> 5);
-        const int32_t wxi = lo[0] + dx, wzi = lo[2] + dz, y0 = lo[1];
-        const float wx = (float)wxi, wz = (float)wzi;
-        int32_t water_top;
-        const int32_t h = sample_terrain(wx, wz, g.offx, g.offz, &water_top);
+    // ---- the columns (dx, dz), voxel.rs:1333-1461
+    const int32_t y0 = lo[1];
+    for (uint32_t col = tid; col < (uint32_t)(kCV * kCV); col += kSlotThreads) {
+        const uint32_t word = colw[col];
+        const int32_t h = (int32_t)(word & 0xFFu);
         const uint32_t hu = (uint32_t)h;
-        const int32_t col_top = max(h, water_top);
-        if (!(col_top < y0 || 0 >= y0 + kCV)) {
-            const float temperature = fbm_2d((wx + g.offx) * 0.0006f, (wz + g.offz) * 0.0006f, 3);
-            const float humidity = fbm_2d((wx + g.offx) * 0.0008f + 100.0f,
-                                          (wz + g.offz) * 0.0008f + 100.0f, 3);
-            const int biome = pick_biome(temperature, humidity, hu);
-            const int32_t ys = max(y0, 0), ye = min(y0 + kCV, kWorldY);
-            const int32_t seal = water_top > h ? h - 5 : INT32_MIN;
-            for (int32_t y = ys; y < ye; ++y) {
-                if (y > h) break;
-                if (!(y >= seal) && y > 4 && y + 3 < h) {
-                    const float cn = value_noise_3d(wx * 0.045f, (float)y * 0.085f, wz * 0.045f);
-                    const float cn2 = value_noise_3d(wx * 0.110f, (float)y * 0.060f, wz * 0.110f);
-                    if ((cn + cn2 * 0.6f) > 0.30f) continue;
-                }
-                uint8_t mat;
-                if ((uint32_t)y >= hu) mat = top_block(biome, hu);
-                else if ((uint32_t)y + 4u >= hu) mat = subsoil(biome);
-                else mat = stone_or_ore(wx, (float)y, wz, hu);
-                s_mat[vox((uint32_t)dx, (uint32_t)(y - y0), (uint32_t)dz)] = mat;
+        const int32_t water_top = (word >> 8) & 1u ? kSea : 0;
+        const int col_top = max(h, water_top);
+        if (col_top < y0 || 0 >= y0 + kCV) continue;
+        const int biome = (int)((word >> 9) & 7u);
+        const uint32_t dx = col & 31u, dz = col >> 5;
+        const float wx = (float)(lo[0] + (int32_t)dx), wz = (float)(lo[2] + (int32_t)dz);
+        const int32_t ys = max(y0, 0), ye = min(y0 + kCV, kWorldY);
+        const int32_t seal = water_top > h ? h - 5 : INT32_MIN;
+        // stone_or_ore's two noises (voxel.rs:1906-1916) along this column
+        // and the two cave noises (:1361-1366)
+        noise::ColumnNoise3 ore1, ore2, cave1, cave2;
+        ore1.init(wx * 0.27f, wz * 0.27f);
+        ore2.init(wx * 0.55f, wz * 0.55f);
+        cave1.init(wx * 0.045f, wz * 0.045f);
+        cave2.init(wx * 0.110f, wz * 0.110f);
+        for (int32_t y = ys; y < ye; ++y) {
+            if (y > h) break;
+            if (!(y >= seal) && y > 4 && y + 3 < h) {
+                const float cn = cave1.eval((float)y * 0.085f);
+                const float cn2 = cave2.eval((float)y * 0.060f);
+                if ((cn + cn2 * 0.6f) > 0.30f) continue;
             }
-            if (water_top > h) {
-                const int32_t fb = max(h + 1, y0), fe = min(water_top, y0 + kCV - 1);
-                for (int32_t wy = fb; wy <= fe; ++wy)
-                    s_mat[vox((uint32_t)dx, (uint32_t)(wy - y0), (uint32_t)dz)] = M_WATER;
+            uint8_t mat;
+            if ((uint32_t)y >= hu) {
+                mat = top_block(biome, hu);
+            } else if ((uint32_t)y + 4u >= hu) {
+                mat = subsoil(biome);
+            } else {
+                const float fy = (float)y;
+                const float depth = fmaxr((float)hu - fy, 0.0f);
+                const float n1 = ore1.eval(fy * 0.27f);
+                const float n2 = ore2.eval(fy * 0.55f);
+                const float combined = n1 + n2 * 0.30f;
+                if (depth > 30.0f && combined > 0.50f) mat = M_DIAMOND;
+                else if (depth > 20.0f && combined > 0.36f) mat = M_GOLD;
+                else if (depth > 10.0f && combined > 0.24f) mat = M_IRON;
+                else if (combined > 0.32f) mat = M_COAL;
+                else mat = M_STONE;
             }
-            if (water_top == 0 && hu < (uint32_t)(kWorldY - 1)) {
-                const uint8_t surface = top_block(biome, hu);
-                const int32_t dec_y = h + 1;
-                if (dec_y >= y0 && dec_y < y0 + kCV) {
-                    const float v = hash3(wxi, dec_y, wzi) * 0.5f + 0.5f;
-                    const int32_t ax = wxi & ~1, az = wzi & ~1;
-                    uint8_t dec = 0;
-                    if (surface == M_GRASS) {
-                        float fp, gp;
-                        if (biome == B_PLAINS) { fp = 0.020f; gp = 0.08f; }
-                        else if (biome == B_FOREST) { fp = 0.010f; gp = 0.065f; }
-                        else if (biome == B_JUNGLE) { fp = 0.012f; gp = 0.09f; }
-                        else { fp = 0.015f; gp = 0.065f; }
-                        if (fbm_2d((float)wxi * 0.02f + 7.0f, (float)wzi * 0.02f - 3.0f, 2) > 0.30f) {
-                            fp *= 3.0f;
-                            gp *= 12.0f;
-                        }
-                        if (v > 1.0f - fp) dec = M_FLOWER;
-                        else if (v > 1.0f - fp - gp) dec = M_TALL_GRASS;
-                        else if (hash3(ax, 977, az) * 0.5f + 0.5f > 0.9955f) dec = M_BUSH;
-                        else if (v > 1.0f - fp - gp - 0.004f) dec = M_BUSH;
-                    } else if (surface == M_SAND && (biome == B_DESERT || biome == B_SAVANNA)) {
-                        if (v > 0.99f) dec = M_GRASS_DRY;
-                    } else if (surface == M_SNOW && biome == B_TUNDRA) {
-                        if (v > 0.995f) dec = M_GRASS_DRY;
-                    }
-                    if (dec != 0) {
-                        const uint32_t dy = (uint32_t)(dec_y - y0);
-                        s_mat[vox((uint32_t)dx, dy, (uint32_t)dz)] = dec;
-                        if (dec == M_BUSH && hash3(ax, 977, az) * 0.5f + 0.5f > 0.9955f &&
-                            dec_y + 1 >= y0 && dec_y + 1 < y0 + kCV)
-                            s_mat[vox((uint32_t)dx, dy + 1u, (uint32_t)dz)] = M_BUSH;
-                    }
-                }
-            }
+            s_mat[vox(dx, (uint32_t)(y - y0), dz)] = mat;
         }
-    }
-
-    // ---- 2. tree candidates of the 3x3 source chunks, expanded to primitives
-    if (tid < (uint32_t)kTrees) {
-        const int32_t src = (int32_t)tid / kCand, i = (int32_t)tid % kCand;
-        const int32_t ncz = src / 3 - 1, ncx = src % 3 - 1;
-        Tree t;
-        int np = 0;
-        if (tree_candidate(cx + ncx, cz + ncz, (uint32_t)i, g, t) &&
-            !(t.y > lo[1] + kCV || t.y + 22 < lo[1])) {
-            Emit e;
-            e.out = s_prim + tid * kPrims;
-            e.n = 0;
-            e.lo[0] = lo[0]; e.lo[1] = lo[1]; e.lo[2] = lo[2];
-            tree_prims(t, e);
-            np = e.n;
+        if (water_top > h) {
+            const int32_t fb = max(h + 1, y0), fe = min(water_top, y0 + kCV - 1);
+            for (int32_t wy = fb; wy <= fe; ++wy) s_mat[vox(dx, (uint32_t)(wy - y0), dz)] = M_WATER;
         }
-        s_nprim[tid] = np;
+        const uint32_t dec = (word >> 12) & 63u;
+        const int32_t dec_y = h + 1;
+        if (dec != 0u && dec_y >= y0 && dec_y < y0 + kCV) {
+            const uint32_t dy = (uint32_t)(dec_y - y0);
+            s_mat[vox(dx, dy, dz)] = (uint8_t)dec;
+            if (((word >> 18) & 1u) && dec_y + 1 < y0 + kCV) s_mat[vox(dx, dy + 1u, dz)] = M_BUSH;
+        }
     }
     __syncthreads();
 
-    // ---- 3. paint in the reference's order, one primitive per barrier
-    for (int t = 0; t < kTrees; ++t) {
-        const int np = s_nprim[t];
-        for (int p = 0; p < np; ++p) {
-            paint_prim(s_mat, lo, s_prim[t * kPrims + p]);
-            __syncthreads();
+    // ---- trees of the 3x3 source chunks in the reference's order
+    for (int k = 0; k < 9; ++k) {
+        const int32_t src = job[7 + k];
+        for (int i = 0; i < kCand; ++i) {
+            const int32_t hd = pl.hdr[(size_t)src * kCand + i];
+            const int np = hd & 0xFF;
+            const int32_t base_y = hd >> 8;
+            if (np == 0 || base_y > lo[1] + kCV || base_y + 22 < lo[1]) continue;
+            const Prim *tp = prims + ((size_t)src * kCand + i) * kPrims;
+            for (int p = 0; p < np; ++p) {
+                const Prim pr = tp[p];
+                if (!prim_meets(pr, lo)) continue;
+                paint_prim(s_mat, lo, pr, kSlotThreads);
+                __syncthreads();
+            }
         }
     }
 
-    // ---- 4. bricks out: material rows, occupancy words, uniform bytes
-    const DevWorld &w = g.w;
+    // ---- bricks out: material rows, occupancy words, uniform bytes
     const uint32_t sbx = (uint32_t)job[3] * 8u, sby = (uint32_t)job[4] * 8u,
                    sbz = (uint32_t)job[5] * 8u;
-    {
-        const uint32_t b = tid >> 1, half = tid & 1u;
+    for (uint32_t b = tid; b < 512u; b += kSlotThreads) {
         const uint32_t gbi = (sbx + (b & 7u)) + (sby + ((b >> 3) & 7u)) * (uint32_t)w.d.bx +
                              (sbz + (b >> 6)) * (uint32_t)(w.d.bx * w.d.by);
-        const uint4 *src = reinterpret_cast<const uint4 *>(s_mat + b * 64u + half * 32u);
-        uint4 *dst = reinterpret_cast<uint4 *>(w.mat + (size_t)gbi * 64u + half * 32u);
-        dst[0] = src[0];
-        dst[1] = src[1];
-    }
-    if (tid < 512u) {
-        const uint32_t b = tid;
-        const uint32_t gbi = (sbx + (b & 7u)) + (sby + ((b >> 3) & 7u)) * (uint32_t)w.d.bx +
-                             (sbz + (b >> 6)) * (uint32_t)(w.d.bx * w.d.by);
-        const uint32_t *row = reinterpret_cast<const uint32_t *>(s_mat + b * 64u);
+        const uint4 *src = reinterpret_cast<const uint4 *>(s_mat + b * 64u);
+        uint4 *dst = reinterpret_cast<uint4 *>(w.mat + (size_t)gbi * 64u);
         uint64_t occ = 0;
-        const uint32_t m0 = row[0] & 0xFFu, rep = 0x01010101u * m0;
+        const uint32_t m0 = s_mat[b * 64u], rep = 0x01010101u * m0;
         bool same = m0 != 0u;
 #pragma unroll
-        for (int k = 0; k < 16; ++k) {
-            const uint32_t q = row[k];
-            same = same && q == rep;
+        for (int q4 = 0; q4 < 4; ++q4) {
+            const uint4 q = src[q4];
+            dst[q4] = q;
+            const uint32_t qs[4] = {q.x, q.y, q.z, q.w};
 #pragma unroll
-            for (int j = 0; j < 4; ++j)
-                if ((q >> (8 * j)) & 0xFFu) occ |= 1ull << (4 * k + j);
+            for (int m = 0; m < 4; ++m) {
+                same = same && qs[m] == rep;
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    if ((qs[m] >> (8 * j)) & 0xFFu) occ |= 1ull << (16 * q4 + 4 * m + j);
+            }
         }
         w.occ[gbi] = occ;
         w.brick_uniform[gbi] = (occ == ~0ull && same) ? (uint8_t)m0 : (uint8_t)0;
@@ -518,20 +615,20 @@ __global__ void __launch_bounds__(kThreads, 1) k_gen_slot(SlotGen g) {
 
 }  // namespace
 
-cudaError_t launch_gen_slots(const DevWorld &w, uint64_t seed, const int32_t *d_jobs,
-                             uint32_t n_jobs, cudaStream_t s) {
-    if (n_jobs == 0) return cudaSuccess;
-    cudaError_t attr = cudaFuncSetAttribute(k_gen_slot, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)kSmemBytes);
-    if (attr != cudaSuccess) return attr;
-    SlotGen g;
-    g.w = w;
-    g.jobs = d_jobs;
+size_t gen_prim_bytes_per_src() { return sizeof(Prim) * kCand * kPrims; }
+
+cudaError_t launch_gen_slots(const DevWorld &w, uint64_t seed, const GenPlan &p, cudaStream_t s) {
+    if (p.n_jobs == 0) return cudaSuccess;
+    Seed g;
     g.seed = seed;
     // seed_offset_xz, voxel.rs:1163-1167
     g.offx = (float)(int32_t)(uint32_t)(seed >> 32) * 0.01734f;
     g.offz = (float)(int32_t)(uint32_t)(seed & 0xFFFFFFFFull) * 0.02153f;
-    k_gen_slot<<<n_jobs, kThreads, kSmemBytes, s>>>(g);
+    const uint32_t n_col_threads = p.n_cols * (uint32_t)(kCV * kCV);
+    k_gen_columns<<<(n_col_threads + 255) / 256, 256, 0, s>>>(p, w.d, g);
+    const uint32_t n_tree_threads = p.n_srcs * (uint32_t)kCand;
+    k_gen_trees<<<(n_tree_threads + 127) / 128, 128, 0, s>>>(p, w.d, g);
+    k_gen_slot<<<p.n_jobs, kSlotThreads, 0, s>>>(w, p);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     return launch_rebuild_pyramid(w, s);
