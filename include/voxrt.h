@@ -198,7 +198,8 @@ int vx_world_fill_window(VxWorld *w, uint64_t seed, int32_t origin_cx, int32_t o
 /* shift_origin (src/voxel.rs:507-537) after vx_world_fill_window: only the
  * slots whose world chunk changes are regenerated, with the fill's seed;
  * their count goes to *n_regenerated when non-null.  Edits are not
- * replayed (apply them with vx_world_apply_dirty). */
+ * replayed (apply them with vx_world_apply_dirty).  VX_ERR_INVALID when no
+ * window was filled, or vx_world_upload / vx_world_generate replaced it. */
 int vx_world_shift_origin(VxWorld *w, int32_t origin_cx, int32_t origin_cz,
                           uint32_t *n_regenerated);
 /* Incremental update from dirty bricks (renderer.rs:1345-1394): writes the

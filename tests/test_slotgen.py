@@ -245,6 +245,61 @@ def test_device_gen_rejects_bad_chunks():
         assert e.value.code == L.VX_ERR_INVALID
     with pytest.raises(L.VxError):
         dw.shift_origin(1, 1)      # no window generated yet
+    dw.gen_chunks(SEED, [(0, 2, 0)])
+    with pytest.raises(L.VxError):
+        dw.shift_origin(1, 1)      # a list of chunks is not a window
+    dw.fill_window(SEED, 0, 0)
+    assert dw.shift_origin(1, 0) == 8 * 16
+    c1 = vg.CONFIGS["c1"]
+    dw.generate(c1.terrain)        # replaces the world: the slot table is void
+    with pytest.raises(L.VxError):
+        dw.shift_origin(2, 0)
+    dw.close()
+
+
+@pytest.mark.gpu
+def test_device_full_size_window_sampled():
+    """The 2048x256x2048 window (32768 chunks, the bench's size): 256
+    random slots byte-equal to the oracle's gen_slot_bricks, and the masks
+    consistent with the bricks (every occupied brick's tile bit set)."""
+    _gpu()
+    import voxelg_b200 as vg
+    dims = (512, 64, 512)
+    ox, oz = -5, 9
+    dw = vg.DeviceWorld(*dims)
+    dw.fill_window(SEED, ox, oz)
+    got = dw.download()
+    bricks = got["bricks"].reshape(dims[2], dims[1], dims[0])
+    rng = np.random.default_rng(3)
+    for sx, sy, sz in zip(rng.integers(0, 64, 256), rng.integers(0, 8, 256),
+                          rng.integers(0, 64, 256)):
+        cx, cz = ox + (sx - ox) % 64, oz + (sz - oz) % 64
+        blk = np.ascontiguousarray(bricks[sz * 8:sz * 8 + 8, sy * 8:sy * 8 + 8,
+                                          sx * 8:sx * 8 + 8]).reshape(-1)
+        assert np.array_equal(blk.view(np.uint8), po.gen_slot_bricks(cx, sy, cz, SEED)
+                              .view(np.uint8)), (sx, sy, sz)
+    occ = (bricks["occupancy"] != 0).reshape(dims[2] // 4, 4, dims[1] // 4, 4, dims[0] // 4, 4)
+    tiles = got["tile_mask"].reshape(dims[2] // 4, dims[1] // 4, dims[0] // 4)
+    assert np.array_equal(occ.any(axis=(1, 3, 5)), tiles != 0)
+    dw.close()
+
+
+@pytest.mark.gpu
+def test_device_far_chunks():
+    """Chunks far from the origin (|x|, |z| up to 2^20 chunks, 2^25 voxels,
+    where float coordinates lose their low bits) equal the oracle's."""
+    _gpu()
+    import voxelg_b200 as vg
+    dw = vg.DeviceWorld(*DEMO)
+    far = [(1 << 20, 2, -(1 << 20) + 3), (-777777, 1, 654321), (123457, 2, -98765)]
+    dw.gen_chunks(SEED, far)
+    got = dw.download()["bricks"].reshape(128, 64, 128)
+    for cx, cy, cz in far:
+        sx, sz = cx % 16, cz % 16
+        blk = np.ascontiguousarray(got[sz * 8:sz * 8 + 8, cy * 8:cy * 8 + 8,
+                                       sx * 8:sx * 8 + 8]).reshape(-1)
+        assert np.array_equal(blk.view(np.uint8), po.gen_slot_bricks(cx, cy, cz, SEED)
+                              .view(np.uint8)), (cx, cy, cz)
     dw.close()
 
 

@@ -58,6 +58,7 @@ struct VxWorld {
     std::vector<int32_t> slot_chunk;
     uint64_t gen_seed = 0;
     int32_t gen_origin[2] = {0, 0};
+    bool gen_window = false;         // a window fill made the slot table whole
     void *d_gen = nullptr;           // chunk generator scratch: plan, column words, trees
     size_t gen_cap = 0;              // bytes
     void *h_gen = nullptr;           // pinned staging of the generator's plan
@@ -127,6 +128,13 @@ void free_world(VxWorld *w) {
         if (e) cudaEventDestroy(e);
     if (w->copy_stream) cudaStreamDestroy(w->copy_stream);
     if (w->stream) cudaStreamDestroy(w->stream);
+}
+
+// The whole world is replaced: the chunk generator's slot table no longer
+// describes it.  Caller holds w->mu.
+void forget_generated(VxWorld *w) {
+    w->slot_chunk.clear();
+    w->gen_window = false;
 }
 
 int check_frame(const VxCamera *cam) {
@@ -354,6 +362,7 @@ int vx_world_upload(VxWorld *w, const VxBrick *bricks, const uint64_t *tile_mask
     int rc = use_device(w);
     if (rc != VX_OK) return rc;
     std::lock_guard<std::mutex> lk(w->mu);
+    forget_generated(w);
     const vx::Dims &d = w->dw.d;
     const size_t chunk = (size_t)1 << 20;  // bricks per staging round (72 MiB)
     rc = ensure(&w->d_bricks, &w->bricks_cap, std::min<size_t>(chunk, (size_t)d.n_bricks));
@@ -410,6 +419,7 @@ int vx_world_generate(VxWorld *w, const VxTerrainParams *t) {
     int rc = use_device(w);
     if (rc != VX_OK) return rc;
     std::lock_guard<std::mutex> lk(w->mu);
+    forget_generated(w);
     const vx::Dims &d = w->dw.d;
     int16_t *heights = nullptr;
     VX_CK(cudaMallocAsync(&heights, (size_t)d.vx * d.vz * sizeof(int16_t), w->stream));
@@ -608,6 +618,7 @@ int vx_world_fill_window(VxWorld *w, uint64_t seed, int32_t origin_cx, int32_t o
     w->gen_seed = seed;
     w->gen_origin[0] = origin_cx;
     w->gen_origin[1] = origin_cz;
+    w->gen_window = true;
     return VX_OK;
 }
 
@@ -620,8 +631,9 @@ int vx_world_shift_origin(VxWorld *w, int32_t origin_cx, int32_t origin_cz,
     int rc = use_device(w);
     if (rc != VX_OK) return rc;
     std::lock_guard<std::mutex> lk(w->mu);
-    if (w->slot_chunk.empty()) {
-        vx::set_error("vx_world_shift_origin: no window generated yet (vx_world_fill_window)");
+    if (!w->gen_window) {
+        vx::set_error("vx_world_shift_origin: the world is not a generated window "
+                      "(vx_world_fill_window first; uploads and vx_world_generate replace it)");
         return VX_ERR_INVALID;
     }
     const vx::Dims &d = w->dw.d;
