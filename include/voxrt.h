@@ -252,6 +252,17 @@ int vx_render_ao(VxWorld *w, const VxCamera *cam, const VxHitRecord *rec_dev, fl
  * shadow_host (pinned memory recommended) before the call returns. */
 int vx_render_primary_host(VxWorld *w, const VxCamera *cam, const VxTraceParams *p,
                            VxHitRecord *rec_host, VxShadowRecord *shadow_host);
+/* The same, for frame pipelines: enqueues the frame and returns.  Its
+ * records are in rec_host / shadow_host once vx_render_host_wait(w) returns;
+ * until then the caller must neither read nor free those buffers (pinned
+ * memory, for the copies to overlap).  Frames alternate between two device
+ * buffers, so frame N+1's traversal overlaps frame N's copies to the host,
+ * and the copies of successive frames land in call order. */
+int vx_render_primary_host_async(VxWorld *w, const VxCamera *cam, const VxTraceParams *p,
+                                 VxHitRecord *rec_host, VxShadowRecord *shadow_host);
+/* Waits until every frame enqueued by vx_render_primary_host_async has
+ * landed in its host buffers. */
+int vx_render_host_wait(VxWorld *w);
 /* The frame of vx_render_primary, run once more with algorithmic load
  * counters on: bytes the method reads (8 per mask word / occupancy, 1 per
  * LUT or material byte) and loop iterations, summed over all rays.

@@ -494,3 +494,25 @@ def test_invalid_calls_fail_loudly(vg, dev_c1):
     idx = np.array([10 ** 9], np.uint32)
     with pytest.raises(L.VxError):
         dev_c1.apply_dirty(idx, np.zeros(1, po.BRICK))
+
+
+def test_host_frame_pipeline_bit_exact(vg, dev_c1, c1_oracle_world):
+    """vx_render_primary_host_async: three frames of different cameras in
+    flight into three host buffer pairs (two device buffers alternate), each
+    equal to its own oracle frame after vx_render_host_wait."""
+    import torch
+    cfg = vg.CONFIGS["c1"]
+    p = vg.default_params(METHOD | po.OR_F_SHADOW)
+    cams = [vg.camera_from_pose((256.0 + 40 * i, 140.0, 256.0 - 30 * i), 0.3 * i, -0.26, 1.22,
+                                cfg.width, cfg.height, (0, 0, 0)) for i in range(3)]
+    n = cfg.width * cfg.height
+    bufs = [(torch.empty(n * 24, dtype=torch.uint8).pin_memory(),
+             torch.empty(n * 8, dtype=torch.uint8).pin_memory()) for _ in cams]
+    for cam, (r, s) in zip(cams, bufs):
+        vg.render_primary_host_async(dev_c1, cam, p, r.numpy().view(po.RECORD),
+                                     s.numpy().view(po.SHADOW))
+    vg.render_host_wait(dev_c1)
+    for cam, (r, s) in zip(cams, bufs):
+        wrec, wsh, _, _, _ = po.render_frame(c1_oracle_world, cam, p)
+        assert_same_records(r.numpy().view(po.RECORD), wrec, "pipelined host frame")
+        assert np.array_equal(s.numpy(), wsh.view(np.uint8))

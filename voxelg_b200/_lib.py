@@ -158,6 +158,8 @@ SIGNATURES = [
     ("vx_trace", C.c_int, [_vp, _P(C.c_int32), _vp, C.c_size_t, _P(VxTraceParams), _vp, _vp]),
     ("vx_render_primary", C.c_int, [_vp, _P(VxCamera), _P(VxTraceParams), _vp, _vp, _vp]),
     ("vx_render_primary_host", C.c_int, [_vp, _P(VxCamera), _P(VxTraceParams), _vp, _vp]),
+    ("vx_render_primary_host_async", C.c_int, [_vp, _P(VxCamera), _P(VxTraceParams), _vp, _vp]),
+    ("vx_render_host_wait", C.c_int, [_vp]),
     ("vx_render_ao", C.c_int, [_vp, _P(VxCamera), _vp, _vp, _vp]),
     ("vx_render_primary_stats", C.c_int, [_vp, _P(VxCamera), _P(VxTraceParams),
                                           _P(C.c_uint64)]),

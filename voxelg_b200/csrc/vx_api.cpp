@@ -59,6 +59,13 @@ struct VxWorld {
     uint64_t gen_seed = 0;
     int32_t gen_origin[2] = {0, 0};
     bool gen_window = false;         // a window fill made the slot table whole
+    // host-buffer frames: ping-pong device records, and per buffer the event
+    // after its last copy to the host (frame N+1 renders while N copies)
+    VxHitRecord *hrec[2] = {nullptr, nullptr};
+    VxShadowRecord *hsh[2] = {nullptr, nullptr};
+    size_t hrec_cap[2] = {0, 0}, hsh_cap[2] = {0, 0};
+    cudaEvent_t copy_done[2] = {nullptr, nullptr};
+    uint64_t host_frames = 0;
     void *d_gen = nullptr;           // chunk generator scratch: plan, column words, trees
     size_t gen_cap = 0;              // bytes
     void *h_gen = nullptr;           // pinned staging of the generator's plan
@@ -121,6 +128,12 @@ void free_world(VxWorld *w) {
     cudaFree(w->d_gate_idx);
     cudaFree(w->d_gen);
     if (w->h_gen) cudaFreeHost(w->h_gen);
+    if (w->copy_stream) cudaStreamSynchronize(w->copy_stream);
+    for (int i = 0; i < 2; ++i) {
+        cudaFree(w->hrec[i]);
+        cudaFree(w->hsh[i]);
+        if (w->copy_done[i]) cudaEventDestroy(w->copy_done[i]);
+    }
     w->qs.release();
     for (auto &e : w->ev)
         if (e) cudaEventDestroy(e);
@@ -994,35 +1007,38 @@ int vx_render_ao(VxWorld *w, const VxCamera *cam, const VxHitRecord *rec_dev, fl
     return VX_OK;
 }
 
-int vx_render_primary_host(VxWorld *w, const VxCamera *cam, const VxTraceParams *p,
-                           VxHitRecord *rec_host, VxShadowRecord *shadow_host) {
-    if (!w || !rec_host) {
-        vx::set_error("vx_render_primary_host: null argument");
-        return VX_ERR_INVALID;
-    }
-    int rc = check_frame(cam);
-    if (rc == VX_OK) rc = check_params(p);
-    if (rc != VX_OK) return rc;
-    rc = use_device(w);
-    if (rc != VX_OK) return rc;
-    std::lock_guard<std::mutex> lk(w->mu);
+namespace {
+// Enqueues one host-buffer frame: beam, then row bands whose copies to the
+// host (copy stream) overlap the next band's traversal.  Frames alternate
+// between two device buffers; a frame first waits, on the device, for the
+// copies of the frame two calls back that used its buffer.  Caller holds
+// w->mu.
+int enqueue_host_frame(VxWorld *w, const VxCamera *cam, const VxTraceParams *p,
+                       VxHitRecord *rec_host, VxShadowRecord *shadow_host) {
     vx::FrameArgs fa = make_frame(w, cam, p);
     const size_t n = (size_t)fa.W * fa.H;
-    rc = ensure(&w->rec, &w->rec_cap, n);
-    if (rc == VX_OK) rc = ensure(&w->sh, &w->sh_cap, n);
-    if (rc != VX_OK) return rc;
-    fa.rec = w->rec;
-    fa.shadow = shadow_host ? w->sh : nullptr;
+    const int buf = (int)(w->host_frames & 1u);
     if (!w->copy_stream) {
         VX_CK(cudaStreamCreateWithFlags(&w->copy_stream, cudaStreamNonBlocking));
         for (auto &e : w->band_ev) VX_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     }
-    // Bands of rows: the copy of band b to the host overlaps the traversal of
-    // band b+1 (the grid form only; the persistent form renders in one go).
+    if (!w->copy_done[0]) {
+        for (auto &e : w->copy_done) VX_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    if (w->hrec_cap[buf] < n || w->hsh_cap[buf] < n) {
+        VX_CK(cudaStreamSynchronize(w->copy_stream));   // no copy may read a freed buffer
+        int rc = ensure(&w->hrec[buf], &w->hrec_cap[buf], n);
+        if (rc == VX_OK) rc = ensure(&w->hsh[buf], &w->hsh_cap[buf], n);
+        if (rc != VX_OK) return rc;
+    }
+    fa.rec = w->hrec[buf];
+    fa.shadow = shadow_host ? w->hsh[buf] : nullptr;
+    VX_CK(cudaStreamWaitEvent(w->stream, w->copy_done[buf], 0));
+    // bands of rows (the grid form only; the persistent form renders in one go)
     const uint32_t nb = fa.work ? 1u : kBands;
     const uint32_t band = ((fa.H + nb - 1) / nb + 7u) & ~7u;
     if (fa.ta.p.flags & VX_F_BEAM) {
-        rc = ensure(&w->beam, &w->beam_cap, (size_t)fa.bw * fa.bh);
+        int rc = ensure(&w->beam, &w->beam_cap, (size_t)fa.bw * fa.bh);
         if (rc != VX_OK) return rc;
         fa.beam = w->beam;
         VX_CK(vx::launch_beam(fa, w->beam, w->stream));
@@ -1036,13 +1052,59 @@ int vx_render_primary_host(VxWorld *w, const VxCamera *cam, const VxTraceParams 
         VX_CK(cudaEventRecord(w->band_ev[b], w->stream));
         VX_CK(cudaStreamWaitEvent(w->copy_stream, w->band_ev[b], 0));
         const size_t r0 = (size_t)fa.y0 * fa.W, rn = (size_t)(fa.y1 - fa.y0) * fa.W;
-        VX_CK(cudaMemcpyAsync(rec_host + r0, w->rec + r0, rn * sizeof(VxHitRecord),
+        VX_CK(cudaMemcpyAsync(rec_host + r0, fa.rec + r0, rn * sizeof(VxHitRecord),
                               cudaMemcpyDeviceToHost, w->copy_stream));
         if (shadow_host)
-            VX_CK(cudaMemcpyAsync(shadow_host + r0, w->sh + r0, rn * sizeof(VxShadowRecord),
+            VX_CK(cudaMemcpyAsync(shadow_host + r0, fa.shadow + r0, rn * sizeof(VxShadowRecord),
                                   cudaMemcpyDeviceToHost, w->copy_stream));
     }
+    VX_CK(cudaEventRecord(w->copy_done[buf], w->copy_stream));
+    ++w->host_frames;
+    return VX_OK;
+}
+
+int host_frame_args(VxWorld *w, const VxCamera *cam, const VxTraceParams *p,
+                    VxHitRecord *rec_host, const char *fn) {
+    if (!w || !rec_host) {
+        vx::set_error(std::string(fn) + ": null argument");
+        return VX_ERR_INVALID;
+    }
+    int rc = check_frame(cam);
+    if (rc == VX_OK) rc = check_params(p);
+    if (rc == VX_OK) rc = use_device(w);
+    return rc;
+}
+}  // namespace
+
+int vx_render_primary_host(VxWorld *w, const VxCamera *cam, const VxTraceParams *p,
+                           VxHitRecord *rec_host, VxShadowRecord *shadow_host) {
+    int rc = host_frame_args(w, cam, p, rec_host, "vx_render_primary_host");
+    if (rc != VX_OK) return rc;
+    std::lock_guard<std::mutex> lk(w->mu);
+    rc = enqueue_host_frame(w, cam, p, rec_host, shadow_host);
+    if (rc != VX_OK) return rc;
     VX_CK(cudaStreamSynchronize(w->copy_stream));
+    VX_CK(cudaStreamSynchronize(w->stream));
+    return VX_OK;
+}
+
+int vx_render_primary_host_async(VxWorld *w, const VxCamera *cam, const VxTraceParams *p,
+                                 VxHitRecord *rec_host, VxShadowRecord *shadow_host) {
+    int rc = host_frame_args(w, cam, p, rec_host, "vx_render_primary_host_async");
+    if (rc != VX_OK) return rc;
+    std::lock_guard<std::mutex> lk(w->mu);
+    return enqueue_host_frame(w, cam, p, rec_host, shadow_host);
+}
+
+int vx_render_host_wait(VxWorld *w) {
+    if (!w) {
+        vx::set_error("vx_render_host_wait: null world");
+        return VX_ERR_INVALID;
+    }
+    int rc = use_device(w);
+    if (rc != VX_OK) return rc;
+    std::lock_guard<std::mutex> lk(w->mu);
+    if (w->copy_stream) VX_CK(cudaStreamSynchronize(w->copy_stream));
     VX_CK(cudaStreamSynchronize(w->stream));
     return VX_OK;
 }

@@ -140,6 +140,21 @@ def render_primary_host(world: DeviceWorld, cam: L.VxCamera, params: L.VxTracePa
     return rec_host, shadow_host
 
 
+def render_primary_host_async(world: DeviceWorld, cam: L.VxCamera, params: L.VxTraceParams,
+                              rec_host: np.ndarray, shadow_host: Optional[np.ndarray] = None):
+    """Enqueue a frame into host buffers (pinned) and return at once; the
+    records are there after render_host_wait(world).  Successive frames
+    overlap: one renders while the previous one copies."""
+    L.check(L.load().vx_render_primary_host_async(
+        world.handle, C.byref(cam), C.byref(params), C.c_void_p(L.ptr(rec_host)),
+        C.c_void_p(L.ptr(shadow_host) if shadow_host is not None else 0)))
+
+
+def render_host_wait(world: DeviceWorld):
+    """Wait until every enqueued host-buffer frame has landed."""
+    L.check(L.load().vx_render_host_wait(world.handle))
+
+
 def render_ao(world: DeviceWorld, cam: L.VxCamera, rec, ao=None, stream: int = 0):
     """Contact AO of a frame's primary records (rec: CUDA uint8 tensor from
     render_primary with the same camera); returns a float32 CUDA tensor."""
