@@ -76,6 +76,10 @@ def parse_args():
     ap.add_argument("--profile-worldgen", action="store_true",
                     help="the chunk generator only (the 512x256x512 demo world once, then K "
                          "fills of the 2048x256x2048 window): the command profiled with ncu")
+    ap.add_argument("--profile-queue", action="store_true",
+                    help="the mixed ray queue only (512x256x512 world, 4.4M rays, the "
+                         "tuning 256 threads / refill at 8 idle lanes / no sort, K graph "
+                         "launches): the command profiled with ncu")
     ap.add_argument("--profile-learned", action="store_true",
                     help="the learned-form frames only (a short training, then K plain, "
                          "learned and verification-only frames): the command profiled "
@@ -710,6 +714,32 @@ def profile_learned(args):
     dw.close()
 
 
+def profile_queue(args):
+    """The mixed ray queue's launches for ncu: the workload of the
+    mixed_queue section, captured once in a graph and launched K times."""
+    import torch
+
+    import voxelg_b200 as vg
+    import voxelg_b200.queue as q
+    from voxelg_b200 import _lib as L
+    c1 = vg.CONFIGS["c1"]
+    dw = vg.DeviceWorld(*c1.bricks)
+    dw.generate(c1.terrain)
+    cam = vg.default_camera(dw, 1920, 1080)
+    rays, _ = q.mixed_queue(c1.bricks, cam, 1920, 1080, seed=11)
+    p = vg.default_params(L.VX_F_L4 | L.VX_F_LUT | L.VX_F_LOD, frame=7.0)
+    t = q.default_tuning()
+    t.block_threads, t.refill_min, t.ctas_per_sm, t.sort = 256, 8, 0, 0
+    g = q.Graph(dw, rays, p, tuning=t)
+    stream = torch.cuda.current_stream().cuda_stream
+    for _ in range(args.steps):
+        g.launch(stream)
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_queue_launches": args.steps}), flush=True)
+    g.close()
+    dw.close()
+
+
 def profile_worldgen(args):
     """The chunk generator's launches for ncu: the 512x256x512 demo world
     (2048 chunks) once, then K fills of the 2048x256x2048 window (32768
@@ -735,6 +765,9 @@ def main():
         return
     if args.profile_worldgen:
         profile_worldgen(args)
+        return
+    if args.profile_queue:
+        profile_queue(args)
         return
     if args.impl == "reference":
         run_reference(args, cfg)
