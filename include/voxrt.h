@@ -196,12 +196,24 @@ int vx_world_gen_chunks(VxWorld *w, uint64_t seed, const int32_t *chunks, uint32
  * camera's world_origin for this window is (32*origin_cx, 0, 32*origin_cz). */
 int vx_world_fill_window(VxWorld *w, uint64_t seed, int32_t origin_cx, int32_t origin_cz);
 /* shift_origin (src/voxel.rs:507-537) after vx_world_fill_window: only the
- * slots whose world chunk changes are regenerated, with the fill's seed;
- * their count goes to *n_regenerated when non-null.  Edits are not
- * replayed (apply them with vx_world_apply_dirty).  VX_ERR_INVALID when no
+ * slots whose world chunk changes are regenerated, with the fill's seed,
+ * and get the recorded edits inside them (vx_world_apply_edit); their count
+ * goes to *n_regenerated when non-null.  VX_ERR_INVALID when no
  * window was filled, or vx_world_upload / vx_world_generate replaced it. */
 int vx_world_shift_origin(VxWorld *w, int32_t origin_cx, int32_t origin_cz,
                           uint32_t *n_regenerated);
+/* apply_edit (src/voxel.rs:448-474): a persistent edit at world voxel
+ * (wx, wy, wz), |wx|, |wz| < 2^29.  It is kept in the world's edit log (a
+ * later edit of the same voxel replaces it) and written on the device now
+ * when it lies inside the window -- the one of the last vx_world_fill_window
+ * or vx_world_shift_origin, else the window at origin 0.  Every chunk that a
+ * later vx_world_fill_window, vx_world_shift_origin or vx_world_gen_chunks
+ * generates gets the edits inside it written again (replay_edits_for_chunk,
+ * src/voxel.rs:571-603), so edits survive streaming.  mat 0 clears the voxel
+ * (Brick::set).  Masks and LUTs are updated.  Synchronous. */
+int vx_world_apply_edit(VxWorld *w, int32_t wx, int32_t wy, int32_t wz, uint8_t mat);
+/* Forget every recorded edit (the device world is left as it is). */
+int vx_world_clear_edits(VxWorld *w);
 /* Incremental update from dirty bricks (renderer.rs:1345-1394): writes the
  * given bricks and recomputes the touched tile/chunk/L4 masks and uniform
  * LUT entries on the device (voxel.rs:879-946 semantics).  brick_idx and

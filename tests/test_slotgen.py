@@ -340,3 +340,75 @@ def test_hash_normalisation_without_division():
     p = (u.astype(np.float32) * np.float32(2.0 ** -24)).view(np.uint32)
     r = np.where(u != 0, p + np.uint32(1), np.uint32(0)).view(np.float32)
     assert np.array_equal(q.view(np.uint32), r.view(np.uint32))
+
+
+MAT_GLASS = 18
+
+
+def _material_at_world(dw, origin_c, wx, wy, wz):
+    """World::material_at_world for the device window at chunk origin_c."""
+    ox, oz = origin_c[0] * 32, origin_c[1] * 32
+    vx, vy, vz = dw.dims[0] * 4, dw.dims[1] * 4, dw.dims[2] * 4
+    assert ox <= wx < ox + vx and 0 <= wy < vy and oz <= wz < oz + vz
+    x, z = wx % vx, wz % vz
+    b = dw.download()["bricks"].reshape(dw.dims[2], dw.dims[1], dw.dims[0])[z // 4, wy // 4, x // 4]
+    return int(b["materials"][(x & 3) + (z & 3) * 4 + (wy & 3) * 16])
+
+
+def _oracle_with_edits(seed, origin_c, edits):
+    ow = _oracle_window(DEMO, seed, *origin_c)
+    vx, vz = DEMO[0] * 4, DEMO[2] * 4
+    for (x, y, z), m in edits.items():
+        if origin_c[0] * 32 <= x < origin_c[0] * 32 + vx and \
+                origin_c[1] * 32 <= z < origin_c[1] * 32 + vz and 0 <= y < DEMO[1] * 4:
+            ow.set_voxel(x % vx, y, z % vz, m)
+    return ow
+
+
+@pytest.mark.gpu
+def test_device_edits_survive_streaming_round_trip():
+    """tests/worldgen.rs:47-81: edits applied in the window survive a shift of
+    the whole window away and back (every slot unloaded and regenerated,
+    the edit log replayed), and the world equals the oracle's with the same
+    edits set."""
+    _gpu()
+    import voxelg_b200 as vg
+    seed = 0xABCD_1234_5678_9999
+    dw = vg.DeviceWorld(*DEMO)
+    dw.fill_window(seed, 0, 0)
+    edits = {(10, 100, 10): MAT_GLASS, (40, 70, 80): MAT_GLASS, (200, 64, 130): MAT_GLASS}
+    for (x, y, z), m in edits.items():
+        dw.apply_edit(x, y, z, m)
+        assert _material_at_world(dw, (0, 0), x, y, z) == MAT_GLASS
+    _assert_world_equal(dw, _oracle_with_edits(seed, (0, 0), edits))
+    assert dw.shift_origin(16, 16) == 16 * 8 * 16
+    assert dw.shift_origin(0, 0) == 16 * 8 * 16
+    for (x, y, z) in edits:
+        assert _material_at_world(dw, (0, 0), x, y, z) == MAT_GLASS
+    _assert_world_equal(dw, _oracle_with_edits(seed, (0, 0), edits))
+    dw.close()
+
+
+@pytest.mark.gpu
+def test_device_edits_replayed_when_streamed_in():
+    """An edit recorded outside the window is not written, and appears when
+    a shift brings its chunk into the window; a clearing edit (material 0)
+    empties a terrain voxel and its masks follow."""
+    _gpu()
+    import voxelg_b200 as vg
+    dw = vg.DeviceWorld(*DEMO)
+    dw.fill_window(SEED, 0, 0)
+    edits = {(600, 90, 20): MAT_GLASS, (100, 10, 100): 0, (-3, 80, 7): MAT_GLASS}
+    for (x, y, z), m in edits.items():
+        dw.apply_edit(x, y, z, m)
+    assert _material_at_world(dw, (0, 0), 100, 10, 100) == 0
+    _assert_world_equal(dw, _oracle_with_edits(SEED, (0, 0), edits))
+    dw.shift_origin(4, -1)                  # x in [128, 640), z in [-32, 480)
+    assert _material_at_world(dw, (4, -1), 600, 90, 20) == MAT_GLASS
+    _assert_world_equal(dw, _oracle_with_edits(SEED, (4, -1), edits))
+    dw.clear_edits()
+    dw.shift_origin(0, 0)
+    dw.shift_origin(4, -1)                  # regenerated without the log
+    assert _material_at_world(dw, (4, -1), 600, 90, 20) != MAT_GLASS
+    _assert_world_equal(dw, _oracle_window(DEMO, SEED, 4, -1))
+    dw.close()

@@ -3,8 +3,10 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <new>
 #include <string>
@@ -59,6 +61,10 @@ struct VxWorld {
     uint64_t gen_seed = 0;
     int32_t gen_origin[2] = {0, 0};
     bool gen_window = false;         // a window fill made the slot table whole
+    // persistent edits by world voxel, replayed into regenerated chunks
+    std::map<std::array<int32_t, 3>, uint8_t> edits;
+    uint2 *d_edits = nullptr;
+    size_t edits_cap = 0;
     // host-buffer frames: ping-pong device records, and per buffer the event
     // after its last copy to the host (frame N+1 renders while N copies)
     VxHitRecord *hrec[2] = {nullptr, nullptr};
@@ -127,6 +133,7 @@ void free_world(VxWorld *w) {
     cudaFree(w->d_work);
     cudaFree(w->d_gate_idx);
     cudaFree(w->d_gen);
+    cudaFree(w->d_edits);
     if (w->h_gen) cudaFreeHost(w->h_gen);
     if (w->copy_stream) cudaStreamSynchronize(w->copy_stream);
     for (int i = 0; i < 2; ++i) {
@@ -449,6 +456,47 @@ inline int32_t wrap(int32_t a, int32_t n) {
     return (n & (n - 1)) == 0 ? (a & (n - 1)) : ((a % n) + n) % n;
 }
 
+// pos_mod / div_euclid by a chunk's 32 voxels
+inline int32_t chunk_of(int32_t v) { return v >= 0 ? v / 32 : -((-v + 31) / 32); }
+
+// Writes edits (world voxel + material) into their slot voxels
+// (pos_mod(x, VX), y, pos_mod(z, VZ)) on the device and refreshes the
+// touched bricks' uniform bytes and parent masks.  Caller holds w->mu.
+int write_edits_locked(VxWorld *w, const std::vector<std::array<int32_t, 4>> &list) {
+    if (list.empty()) return VX_OK;
+    const vx::Dims &d = w->dw.d;
+    std::vector<uint2> ed;
+    std::vector<uint32_t> bricks;
+    ed.reserve(list.size());
+    for (const auto &e : list) {
+        const uint32_t x = (uint32_t)wrap(e[0], d.vx), y = (uint32_t)e[1],
+                       z = (uint32_t)wrap(e[2], d.vz);
+        const uint32_t bi = (x >> 2) + (y >> 2) * (uint32_t)d.bx + (z >> 2) * (uint32_t)(d.bx * d.by);
+        const uint32_t vi = (x & 3u) + (z & 3u) * 4u + (y & 3u) * 16u;
+        ed.push_back(make_uint2(bi, vi | ((uint32_t)e[3] << 8)));
+        bricks.push_back(bi);
+    }
+    std::sort(bricks.begin(), bricks.end());
+    bricks.erase(std::unique(bricks.begin(), bricks.end()), bricks.end());
+    int rc = ensure(&w->d_edits, &w->edits_cap, ed.size());
+    if (rc == VX_OK) rc = ensure(&w->d_idx, &w->idx_cap, bricks.size());
+    if (rc != VX_OK) return rc;
+    VX_CK(cudaMemcpyAsync(w->d_edits, ed.data(), ed.size() * sizeof(uint2), cudaMemcpyHostToDevice,
+                          w->stream));
+    VX_CK(cudaMemcpyAsync(w->d_idx, bricks.data(), bricks.size() * sizeof(uint32_t),
+                          cudaMemcpyHostToDevice, w->stream));
+    VX_CK(vx::launch_edits(w->dw, w->d_edits, ed.size(), w->d_idx, bricks.size(), w->stream));
+    VX_CK(cudaStreamSynchronize(w->stream));
+    return VX_OK;
+}
+
+// The window's lower corner in world voxels: that of the last window fill or
+// shift, else 0 (World::world_origin_voxel, voxel.rs:439-445).
+inline void window_corner(const VxWorld *w, int32_t &ox, int32_t &oz) {
+    ox = w->gen_window ? w->gen_origin[0] * 32 : 0;
+    oz = w->gen_window ? w->gen_origin[1] * 32 : 0;
+}
+
 // Lays out the generator's scratch -- the plan's ints (explicit plans),
 // column words, tree headers and primitives -- uploads the ints through the
 // pinned staging buffer, runs the kernels and waits.  Caller holds w->mu.
@@ -567,6 +615,29 @@ int gen_chunks_locked(VxWorld *w, uint64_t seed, const int32_t *chunks, uint32_t
     plan.n_srcs = (uint32_t)(srcs.size() / 2);
     int rc = run_gen_plan(w, seed, plan, ints);
     if (rc != VX_OK) return rc;
+    // replay_edits_for_chunk (voxel.rs:571-603) for every generated chunk
+    if (!w->edits.empty()) {
+        std::vector<char> generated((size_t)sx_n * sy_n * sz_n, 0);
+        std::vector<std::array<int32_t, 3>> gen_chunk((size_t)sx_n * sy_n * sz_n);
+        for (uint32_t i = 0; i < n; ++i) {
+            const int32_t *j = &jobs[(size_t)i * vx::kGenJobInts];
+            const size_t slot = (size_t)j[3] + (size_t)j[4] * sx_n + (size_t)j[5] * sx_n * sy_n;
+            generated[slot] = 1;
+            gen_chunk[slot] = {j[0], j[1], j[2]};
+        }
+        std::vector<std::array<int32_t, 4>> replay;
+        for (const auto &e : w->edits) {
+            const int32_t cx = chunk_of(e.first[0]), cy = chunk_of(e.first[1]),
+                          cz = chunk_of(e.first[2]);
+            if (cy < 0 || cy >= sy_n) continue;
+            const size_t slot = (size_t)wrap(cx, sx_n) + (size_t)cy * sx_n +
+                                (size_t)wrap(cz, sz_n) * sx_n * sy_n;
+            if (generated[slot] && gen_chunk[slot] == std::array<int32_t, 3>{cx, cy, cz})
+                replay.push_back({e.first[0], e.first[1], e.first[2], e.second});
+        }
+        rc = write_edits_locked(w, replay);
+        if (rc != VX_OK) return rc;
+    }
     for (uint32_t i = 0; i < n; ++i) {
         const int32_t *j = &jobs[(size_t)i * vx::kGenJobInts];
         const size_t slot = (size_t)j[3] + (size_t)j[4] * sx_n + (size_t)j[5] * sx_n * sy_n;
@@ -621,6 +692,16 @@ int vx_world_fill_window(VxWorld *w, uint64_t seed, int32_t origin_cx, int32_t o
     plan.n_srcs = (uint32_t)((sx_n + 2) * (sz_n + 2));
     rc = run_gen_plan(w, seed, plan, {});
     if (rc != VX_OK) return rc;
+    // replay_edits_for_chunk (voxel.rs:571-603) over the whole window
+    std::vector<std::array<int32_t, 4>> replay;
+    for (const auto &e : w->edits) {
+        const int64_t rx = (int64_t)e.first[0] - (int64_t)origin_cx * 32,
+                      rz = (int64_t)e.first[2] - (int64_t)origin_cz * 32;
+        if (rx >= 0 && rx < d.vx && e.first[1] >= 0 && e.first[1] < d.vy && rz >= 0 && rz < d.vz)
+            replay.push_back({e.first[0], e.first[1], e.first[2], e.second});
+    }
+    rc = write_edits_locked(w, replay);
+    if (rc != VX_OK) return rc;
     w->slot_chunk.resize((size_t)sx_n * sy_n * sz_n * 3);
     for (int32_t sz = 0; sz < sz_n; ++sz)
         for (int32_t sy = 0; sy < sy_n; ++sy)
@@ -668,6 +749,33 @@ int vx_world_shift_origin(VxWorld *w, int32_t origin_cx, int32_t origin_cz,
     w->gen_origin[0] = origin_cx;
     w->gen_origin[1] = origin_cz;
     if (n_regenerated) *n_regenerated = (uint32_t)(chunks.size() / 3);
+    return VX_OK;
+}
+
+int vx_world_apply_edit(VxWorld *w, int32_t wx, int32_t wy, int32_t wz, uint8_t mat) {
+    if (!w || wx <= -(1 << 29) || wx >= (1 << 29) || wz <= -(1 << 29) || wz >= (1 << 29)) {
+        vx::set_error("vx_world_apply_edit: null world or x/z beyond +-2^29");
+        return VX_ERR_INVALID;
+    }
+    int rc = use_device(w);
+    if (rc != VX_OK) return rc;
+    std::lock_guard<std::mutex> lk(w->mu);
+    w->edits[{wx, wy, wz}] = mat;
+    int32_t ox, oz;
+    window_corner(w, ox, oz);
+    const vx::Dims &d = w->dw.d;
+    const int64_t rx = (int64_t)wx - ox, rz = (int64_t)wz - oz;
+    if (rx < 0 || rx >= d.vx || wy < 0 || wy >= d.vy || rz < 0 || rz >= d.vz) return VX_OK;
+    return write_edits_locked(w, {{wx, wy, wz, (int32_t)mat}});
+}
+
+int vx_world_clear_edits(VxWorld *w) {
+    if (!w) {
+        vx::set_error("vx_world_clear_edits: null world");
+        return VX_ERR_INVALID;
+    }
+    std::lock_guard<std::mutex> lk(w->mu);
+    w->edits.clear();
     return VX_OK;
 }
 

@@ -121,6 +121,10 @@ cudaError_t launch_gen_slots(const DevWorld &w, uint64_t seed, const GenPlan &p,
 cudaError_t launch_generate(const DevWorld &w, const VxTerrainParams &t, int16_t *heights,
                             cudaStream_t s);
 cudaError_t launch_rebuild_pyramid(const DevWorld &w, cudaStream_t s);
+// Persistent edits: ed[i] = {brick, voxel | material << 8}, distinct voxels;
+// idx the distinct bricks they touch (uniform bytes and masks refreshed).
+cudaError_t launch_edits(const DevWorld &w, const uint2 *ed, size_t n_edits, const uint32_t *idx,
+                         size_t n_bricks, cudaStream_t s);
 cudaError_t launch_apply_dirty(const DevWorld &w, const uint32_t *idx, const VxBrick *bricks,
                                size_t n, cudaStream_t s);
 

@@ -266,9 +266,44 @@ __global__ void k_dirty_l4(DevWorld w, const uint32_t *__restrict__ idx, size_t 
     build_l4(w, (bx / 64) + (int64_t)(by / 64) * d.lx + (int64_t)(bz / 64) * d.lx * d.ly);
 }
 
+// Persistent edits (apply_edit / replay_edits_for_chunk, voxel.rs:448-474,
+// :571-603): edit i sets voxel (ed[i].y & 63) of brick ed[i].x to material
+// ed[i].y >> 8, Brick::set semantics (voxel.rs:315-325: material 0 clears the
+// occupancy bit).  The edits of one batch name distinct voxels; several may
+// share a brick, so the occupancy word is updated atomically.
+__global__ void k_edit_voxels(DevWorld w, const uint2 *__restrict__ ed, size_t n) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint2 e = ed[i];
+    const uint32_t vi = e.y & 63u, mat = e.y >> 8;
+    w.mat[(size_t)e.x * 64u + vi] = (uint8_t)mat;
+    unsigned long long *occ = reinterpret_cast<unsigned long long *>(w.occ + e.x);
+    if (mat != 0u) atomicOr(occ, 1ull << vi);
+    else atomicAnd(occ, ~(1ull << vi));
+}
+// the uniform byte of each edited brick, once all its voxels are written
+__global__ void k_edit_uniform(DevWorld w, const uint32_t *__restrict__ idx, size_t n) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int64_t bi = idx[i];
+    w.brick_uniform[bi] = uniform_of(w.occ[bi], w.mat + bi * 64);
+}
+
 inline unsigned blocks_for(int64_t n, int t) { return (unsigned)((n + t - 1) / t); }
 
 }  // namespace
+
+cudaError_t launch_edits(const DevWorld &w, const uint2 *ed, size_t n_edits, const uint32_t *idx,
+                         size_t n_bricks, cudaStream_t s) {
+    if (n_edits == 0) return cudaSuccess;
+    k_edit_voxels<<<blocks_for((int64_t)n_edits, 128), 128, 0, s>>>(w, ed, n_edits);
+    const unsigned b = blocks_for((int64_t)n_bricks, 128);
+    k_edit_uniform<<<b, 128, 0, s>>>(w, idx, n_bricks);
+    k_dirty_tiles<<<b, 128, 0, s>>>(w, idx, n_bricks);
+    k_dirty_chunks<<<b, 128, 0, s>>>(w, idx, n_bricks);
+    k_dirty_l4<<<b, 128, 0, s>>>(w, idx, n_bricks);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_bricks_from_aos(const DevWorld &w, const VxBrick *aos, int64_t first,
                                    int64_t count, cudaStream_t s) {

@@ -131,6 +131,14 @@ class DeviceWorld:
         L.check(self._lib.vx_world_shift_origin(self.handle, origin_cx, origin_cz, C.byref(n)))
         return n.value
 
+    def apply_edit(self, wx: int, wy: int, wz: int, mat: int):
+        """A persistent edit at a world voxel (apply_edit): written now when
+        inside the window, and replayed into every chunk generated later."""
+        L.check(self._lib.vx_world_apply_edit(self.handle, wx, wy, wz, mat))
+
+    def clear_edits(self):
+        L.check(self._lib.vx_world_clear_edits(self.handle))
+
     def gen_chunks(self, seed: int, chunks):
         """Generate the given world chunks ((x, y, z) rows) into their slots."""
         c = np.ascontiguousarray(np.asarray(chunks, dtype=np.int32).reshape(-1, 3))
