@@ -78,8 +78,8 @@ def parse_args():
                          "fills of the 2048x256x2048 window): the command profiled with ncu")
     ap.add_argument("--profile-queue", action="store_true",
                     help="the mixed ray queue only (512x256x512 world, 4.4M rays, the "
-                         "tuning 256 threads / refill at 8 idle lanes / no sort, K graph "
-                         "launches): the command profiled with ncu")
+                         "tuning 256 threads / refill at 32 idle lanes / coherence sort, K "
+                         "graph launches): the command profiled with ncu")
     ap.add_argument("--profile-learned", action="store_true",
                     help="the learned-form frames only (a short training, then K plain, "
                          "learned and verification-only frames): the command profiled "
@@ -729,7 +729,7 @@ def profile_queue(args):
     rays, _ = q.mixed_queue(c1.bricks, cam, 1920, 1080, seed=11)
     p = vg.default_params(L.VX_F_L4 | L.VX_F_LUT | L.VX_F_LOD, frame=7.0)
     t = q.default_tuning()
-    t.block_threads, t.refill_min, t.ctas_per_sm, t.sort = 256, 8, 0, 0
+    t.block_threads, t.refill_min, t.ctas_per_sm, t.sort = 256, 32, 0, 1
     g = q.Graph(dw, rays, p, tuning=t)
     stream = torch.cuda.current_stream().cuda_stream
     for _ in range(args.steps):

@@ -132,9 +132,11 @@ cudaError_t launch_apply_dirty(const DevWorld &w, const uint32_t *idx, const VxB
 // work counters, coherence-sort keys / permutation / histogram, fingerprint.
 struct QueueScratch {
     uint32_t *work = nullptr;
-    uint32_t *keys = nullptr;
-    uint32_t *order = nullptr;
-    uint32_t *hist = nullptr;
+    uint32_t *keys = nullptr;     // coherence sort: keys and permutation,
+    uint32_t *order = nullptr;    // with their ping-pong partners
+    uint32_t *keys2 = nullptr;
+    uint32_t *order2 = nullptr;
+    uint32_t *hist = nullptr;     // per-tile digit counts
     unsigned long long *fp = nullptr;
     size_t cap = 0;
     cudaError_t reserve(size_t n);

@@ -7,11 +7,13 @@
 // that hits and carries VX_RAY_SPAWN_SHADOW continues in the same lane with
 // its shadow ray (raymarch.wgsl:3953-3994).  Lanes of a warp refill together
 // once `refill_min` of them are idle (a lone refill would stall 31 lanes
-// through a ray set-up).  Optionally the queue is first reordered by a
-// coherence key (kind, window half in x and z, direction on a 64x64 octahedral
-// grid) with a counting sort, so that a warp's rays start near each other
-// and head the same way.  Results do not depend on
-// any of these choices; the autotuner checks that and keeps the fastest.
+// through a ray set-up).  Optionally the queue is first reordered by a 32-bit
+// coherence key -- kind, then the direction on a 512x512 octahedral grid in
+// Morton order, then the 64-voxel origin cell -- with a stable LSD radix sort
+// (four 8-bit passes), so that a warp's rays head the same way from nearby
+// origins: rays of one camera fall into pixel-sized direction cells, the
+// rays of one probe site stay together.  Results do not depend on any of
+// these choices; the autotuner checks that and keeps the fastest.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -26,7 +28,7 @@
 namespace vx {
 namespace {
 
-constexpr uint32_t kSortBins = 1u << 16;
+constexpr uint32_t kTileItems = 2048;   // radix sort: items per warp-tile
 
 struct QueueArgs {
     TraceArgs ta;
@@ -151,30 +153,26 @@ __global__ void __launch_bounds__(256) k_queue(QueueArgs q) {
     }
 }
 
-// ---- coherence reorder: 16-bit key = kind(2) | origin cell(6) | direction(8)
+// ---- coherence reorder: stable LSD radix sort of a 32-bit key
+// key = kind(2) | Morton(octahedral direction, 9+9 bits) | origin cell(12)
 
-// atomicAdd(base + key, 1) for every active lane, one atomic per distinct
-// key in the warp; returns this lane's slot among the lanes sharing its key
-__device__ __forceinline__ uint32_t warp_count(uint32_t *base, uint32_t key) {
-    const unsigned active = __activemask();
-    const unsigned peers = __match_any_sync(active, key);
-    const int leader = __ffs(peers) - 1;
-    const uint32_t lane = threadIdx.x & 31u;
-    uint32_t off = 0;
-    if ((int)lane == leader) off = atomicAdd(base + key, (uint32_t)__popc(peers));
-    off = __shfl_sync(peers, off, leader);
-    return off + (uint32_t)__popc(peers & ((1u << lane) - 1u));
+__device__ __forceinline__ uint32_t spread_bits(uint32_t x) {   // 9 bits -> even bits
+    x &= 0x1FFu;
+    x = (x | (x << 8)) & 0x00FF00FFu;
+    x = (x | (x << 4)) & 0x0F0F0F0Fu;
+    x = (x | (x << 2)) & 0x33333333u;
+    x = (x | (x << 1)) & 0x55555555u;
+    return x;
 }
 
-__global__ void k_sort_keys(const VxRay *rays, uint32_t n, int32_t rox, int32_t roy, int32_t roz,
-                            uint32_t shift, uint32_t *keys, uint32_t *hist) {
+__global__ void k_radix_keys(const VxRay *rays, uint32_t n, int32_t rox, int32_t roz,
+                             uint32_t *keys, uint32_t *vals) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float ox, oy, oz, dx, dy, dz, tmax;
     uint32_t kind;
     load_ray(rays, i, ox, oy, oz, dx, dy, dz, tmax, kind);
-    // direction on a 64x64 octahedral grid (rays sharing an origin -- the
-    // primaries -- then group by screen region)
+    // direction on the octahedral map, lower hemisphere folded out
     const float l1 = fabsf(dx) + fabsf(dy) + fabsf(dz);
     float u = l1 > 0.f ? dx / l1 : 0.f, v = l1 > 0.f ? dz / l1 : 0.f;
     if (dy < 0.f) {
@@ -182,46 +180,104 @@ __global__ void k_sort_keys(const VxRay *rays, uint32_t n, int32_t rox, int32_t 
         v = (1.f - fabsf(u)) * (v < 0.f ? -1.f : 1.f);
         u = uu;
     }
-    const uint32_t qu = (uint32_t)min(63, max(0, (int32_t)((u + 1.f) * 32.f)));
-    const uint32_t qv = (uint32_t)min(63, max(0, (int32_t)((v + 1.f) * 32.f)));
-    // origin: which half of the window in x and in z (the window split in
-    // quarters by `shift`, then halved)
-    const int32_t cx = max(0, (int32_t)floorf(ox) - rox) >> shift;
-    const int32_t cz = max(0, (int32_t)floorf(oz) - roz) >> shift;
-    (void)roy;
-    const uint32_t cell = ((uint32_t)(cx >> 1) & 1u) | (((uint32_t)(cz >> 1) & 1u) << 1);
-    const uint32_t key = ((kind & 3u) << 14) | (cell << 12) | (qv << 6) | qu;
-    keys[i] = key;
-    warp_count(hist, key);
+    const uint32_t qu = (uint32_t)min(511, max(0, (int32_t)((u + 1.f) * 256.f)));
+    const uint32_t qv = (uint32_t)min(511, max(0, (int32_t)((v + 1.f) * 256.f)));
+    const uint32_t morton = spread_bits(qu) | (spread_bits(qv) << 1);
+    // origin cell of 64 voxels relative to the window corner (x, z) and in y
+    auto cell = [](float o, int32_t corner) -> uint32_t {
+        const float f = floorf(o);
+        const int32_t c = f != f ? 0 : (int32_t)fminf(fmaxf(f - (float)corner, 0.f), 1e9f);
+        return ((uint32_t)c >> 6) & 15u;
+    };
+    const uint32_t oc = cell(ox, rox) | (cell(oz, roz) << 4) | (cell(oy, 0) << 8);
+    keys[i] = ((kind & 3u) << 30) | (morton << 12) | oc;
+    vals[i] = i;
 }
 
-// exclusive scan of the 65536-bin histogram in one 1024-thread CTA
-__global__ void __launch_bounds__(1024) k_scan_bins(uint32_t *hist) {
-    __shared__ uint32_t part[1024];
-    const uint32_t t = threadIdx.x;
-    const uint32_t per = kSortBins / 1024u;
+// Per warp-tile histogram of one 8-bit digit: counts[digit * tiles + tile].
+__global__ void __launch_bounds__(128) k_radix_hist(const uint32_t *keys, uint32_t n,
+                                                    uint32_t shift, uint32_t tiles,
+                                                    uint32_t *counts) {
+    __shared__ uint32_t h[4][256];
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    for (uint32_t d = lane; d < 256u; d += 32u) h[warp][d] = 0u;
+    __syncwarp();
+    const uint32_t tile = blockIdx.x * 4u + warp;
+    if (tile < tiles) {
+        const uint32_t end = min(n, (tile + 1u) * kTileItems);
+        for (uint32_t i = tile * kTileItems + lane; i < end; i += 32u)
+            atomicAdd(&h[warp][(keys[i] >> shift) & 255u], 1u);
+        __syncwarp();
+        for (uint32_t d = lane; d < 256u; d += 32u) counts[d * tiles + tile] = h[warp][d];
+    }
+}
+
+// Exclusive scan of the digit-major counts, one warp per digit row: first
+// the row totals, then each row scanned from its digit's base (the totals
+// of the smaller digits), 32 entries at a time.
+__global__ void __launch_bounds__(256) k_radix_rowsum(const uint32_t *counts, uint32_t tiles,
+                                                      uint32_t *rowsum) {
+    const uint32_t d = blockIdx.x * 8u + (threadIdx.x >> 5), lane = threadIdx.x & 31u;
+    const uint32_t *row = counts + (size_t)d * tiles;
     uint32_t sum = 0;
-    for (uint32_t j = 0; j < per; ++j) sum += hist[t * per + j];
-    part[t] = sum;
-    __syncthreads();
-    for (uint32_t off = 1; off < 1024u; off <<= 1) {
-        const uint32_t v = t >= off ? part[t - off] : 0u;
-        __syncthreads();
-        part[t] += v;
-        __syncthreads();
-    }
-    uint32_t run = part[t] - sum;
-    for (uint32_t j = 0; j < per; ++j) {
-        const uint32_t c = hist[t * per + j];
-        hist[t * per + j] = run;
-        run += c;
+    for (uint32_t t = lane; t < tiles; t += 32u) sum += row[t];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xFFFFFFFFu, sum, o);
+    if (lane == 0) rowsum[d] = sum;
+}
+
+__global__ void __launch_bounds__(256) k_radix_rowscan(uint32_t *counts, uint32_t tiles,
+                                                       const uint32_t *rowsum) {
+    const uint32_t d = blockIdx.x * 8u + (threadIdx.x >> 5), lane = threadIdx.x & 31u;
+    uint32_t base = 0;
+    for (uint32_t k = lane; k < d; k += 32u) base += rowsum[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) base += __shfl_xor_sync(0xFFFFFFFFu, base, o);
+    uint32_t *row = counts + (size_t)d * tiles;
+    for (uint32_t t0 = 0; t0 < tiles; t0 += 32u) {
+        const uint32_t t = t0 + lane;
+        const uint32_t c = t < tiles ? row[t] : 0u;
+        uint32_t inc = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, inc, o);
+            if ((int)lane >= o) inc += v;
+        }
+        if (t < tiles) row[t] = base + inc - c;
+        base += __shfl_sync(0xFFFFFFFFu, inc, 31);
     }
 }
 
-__global__ void k_scatter(const uint32_t *keys, uint32_t n, uint32_t *cursor, uint32_t *order) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    order[warp_count(cursor, keys[i])] = i;
+// Stable scatter: each warp walks its tile in index order, 32 items a round;
+// lanes sharing a digit take consecutive slots in lane order.
+__global__ void __launch_bounds__(128) k_radix_scatter(const uint32_t *keys_in,
+                                                       const uint32_t *vals_in, uint32_t n,
+                                                       uint32_t shift, uint32_t tiles,
+                                                       const uint32_t *counts, uint32_t *keys_out,
+                                                       uint32_t *vals_out) {
+    __shared__ uint32_t off[4][256];
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    const uint32_t tile = blockIdx.x * 4u + warp;
+    if (tile >= tiles) return;
+    for (uint32_t d = lane; d < 256u; d += 32u) off[warp][d] = counts[d * tiles + tile];
+    __syncwarp();
+    const uint32_t begin = tile * kTileItems, end = min(n, begin + kTileItems);
+    for (uint32_t r = begin; r < end; r += 32u) {
+        const uint32_t i = r + lane;
+        const unsigned valid = __ballot_sync(0xFFFFFFFFu, i < end);
+        if (i < end) {
+            const uint32_t key = keys_in[i];
+            const uint32_t dg = (key >> shift) & 255u;
+            const unsigned peers = __match_any_sync(valid, dg);
+            const uint32_t base = off[warp][dg];
+            const uint32_t dst = base + (uint32_t)__popc(peers & ((1u << lane) - 1u));
+            keys_out[dst] = key;
+            vals_out[dst] = vals_in[i];
+            __syncwarp(valid);
+            if ((uint32_t)(__ffs(peers) - 1) == lane) off[warp][dg] = base + (uint32_t)__popc(peers);
+        }
+        __syncwarp();
+    }
 }
 
 // order-independent fingerprint of the outputs (autotuner consistency check)
@@ -253,17 +309,21 @@ cudaError_t QueueScratch::reserve(size_t n) {
     if (!work) {
         cudaError_t e = cudaMalloc(&work, 2 * sizeof(uint32_t));
         if (e == cudaSuccess) e = cudaMemset(work, 0, 2 * sizeof(uint32_t));
-        if (e == cudaSuccess) e = cudaMalloc(&hist, kSortBins * sizeof(uint32_t));
         if (e == cudaSuccess) e = cudaMalloc(&fp, sizeof(unsigned long long));
         if (e != cudaSuccess) return e;
     }
     if (cap >= n && keys) return cudaSuccess;
-    cudaFree(keys);
-    cudaFree(order);
-    keys = order = nullptr;
+    uint32_t **bufs[] = {&keys, &order, &keys2, &order2, &hist};
+    for (uint32_t **b : bufs) {
+        cudaFree(*b);
+        *b = nullptr;
+    }
     cap = 0;
-    cudaError_t e = cudaMalloc(&keys, std::max<size_t>(n, 1) * sizeof(uint32_t));
-    if (e == cudaSuccess) e = cudaMalloc(&order, std::max<size_t>(n, 1) * sizeof(uint32_t));
+    const size_t m = std::max<size_t>(n, 1);
+    const size_t tiles = (m + kTileItems - 1) / kTileItems;
+    cudaError_t e = cudaSuccess;
+    for (int k = 0; k < 4 && e == cudaSuccess; ++k) e = cudaMalloc(bufs[k], m * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&hist, (tiles + 1) * 256 * sizeof(uint32_t));
     if (e == cudaSuccess) cap = n;
     return e;
 }
@@ -272,6 +332,8 @@ void QueueScratch::release() {
     cudaFree(work);
     cudaFree(keys);
     cudaFree(order);
+    cudaFree(keys2);
+    cudaFree(order2);
     cudaFree(hist);
     cudaFree(fp);
     *this = QueueScratch();
@@ -284,16 +346,20 @@ cudaError_t launch_queue(const TraceArgs &ta, const VxRay *rays, size_t n, VxHit
     const uint32_t nn = (uint32_t)n;
     const uint32_t *order = nullptr;
     if (t.sort) {
-        // origin cells: 4 per horizontal axis across the window
-        uint32_t shift = 6;
-        while (((uint32_t)std::max(ta.w.d.vx, ta.w.d.vz) >> shift) > 4u) ++shift;
-        cudaError_t e = cudaMemsetAsync(sc.hist, 0, kSortBins * sizeof(uint32_t), s);
-        if (e != cudaSuccess) return e;
-        k_sort_keys<<<(nn + 255) / 256, 256, 0, s>>>(rays, nn, ta.ro[0], ta.ro[1], ta.ro[2], shift,
-                                                     sc.keys, sc.hist);
-        k_scan_bins<<<1, 1024, 0, s>>>(sc.hist);
-        k_scatter<<<(nn + 255) / 256, 256, 0, s>>>(sc.keys, nn, sc.hist, sc.order);
-        order = sc.order;
+        const uint32_t tiles = (nn + kTileItems - 1) / kTileItems;
+        const unsigned tb = (tiles + 3) / 4;
+        k_radix_keys<<<(nn + 255) / 256, 256, 0, s>>>(rays, nn, ta.ro[0], ta.ro[2], sc.keys,
+                                                      sc.order);
+        uint32_t *kin = sc.keys, *vin = sc.order, *kout = sc.keys2, *vout = sc.order2;
+        for (uint32_t shift = 0; shift < 32u; shift += 8u) {
+            k_radix_hist<<<tb, 128, 0, s>>>(kin, nn, shift, tiles, sc.hist);
+            k_radix_rowsum<<<32, 256, 0, s>>>(sc.hist, tiles, sc.hist + (size_t)tiles * 256u);
+            k_radix_rowscan<<<32, 256, 0, s>>>(sc.hist, tiles, sc.hist + (size_t)tiles * 256u);
+            k_radix_scatter<<<tb, 128, 0, s>>>(kin, vin, nn, shift, tiles, sc.hist, kout, vout);
+            std::swap(kin, kout);
+            std::swap(vin, vout);
+        }
+        order = vin;   // four passes: back in sc.order
     }
     QueueArgs q;
     q.ta = ta;
