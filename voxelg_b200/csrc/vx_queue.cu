@@ -248,31 +248,50 @@ __global__ void __launch_bounds__(256) k_radix_rowscan(uint32_t *counts, uint32_
     }
 }
 
-// Stable scatter: each warp walks its tile in index order, 32 items a round;
-// lanes sharing a digit take consecutive slots in lane order.
-__global__ void __launch_bounds__(128) k_radix_scatter(const uint32_t *keys_in,
-                                                       const uint32_t *vals_in, uint32_t n,
-                                                       uint32_t shift, uint32_t tiles,
-                                                       const uint32_t *counts, uint32_t *keys_out,
-                                                       uint32_t *vals_out) {
-    __shared__ uint32_t off[4][256];
+// Stable scatter: each warp stages its tile's keys and values in shared
+// memory (coalesced 16-byte loads), then walks the tile in index order, 32
+// items a round; lanes sharing a digit take consecutive slots in lane order.
+constexpr uint32_t kScatterWarps = 2;
+__global__ void __launch_bounds__(32 * kScatterWarps) k_radix_scatter(
+    const uint32_t *keys_in, const uint32_t *vals_in, uint32_t n, uint32_t shift, uint32_t tiles,
+    const uint32_t *counts, uint32_t *keys_out, uint32_t *vals_out) {
+    __shared__ __align__(16) uint32_t sk[kScatterWarps][kTileItems];
+    __shared__ __align__(16) uint32_t sv[kScatterWarps][kTileItems];
+    __shared__ uint32_t off[kScatterWarps][256];
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
-    const uint32_t tile = blockIdx.x * 4u + warp;
+    const uint32_t tile = blockIdx.x * kScatterWarps + warp;
     if (tile >= tiles) return;
     for (uint32_t d = lane; d < 256u; d += 32u) off[warp][d] = counts[d * tiles + tile];
-    __syncwarp();
     const uint32_t begin = tile * kTileItems, end = min(n, begin + kTileItems);
-    for (uint32_t r = begin; r < end; r += 32u) {
+    const uint32_t cnt = end - begin;
+    if (cnt == kTileItems) {
+        // begin is a multiple of 2048 items: 16-byte aligned
+        const uint4 *k4 = reinterpret_cast<const uint4 *>(keys_in + begin);
+        const uint4 *v4 = reinterpret_cast<const uint4 *>(vals_in + begin);
+        uint4 *sk4 = reinterpret_cast<uint4 *>(sk[warp]), *sv4 = reinterpret_cast<uint4 *>(sv[warp]);
+#pragma unroll 4
+        for (uint32_t q = lane; q < kTileItems / 4u; q += 32u) {
+            sk4[q] = k4[q];
+            sv4[q] = v4[q];
+        }
+    } else {
+        for (uint32_t q = lane; q < cnt; q += 32u) {
+            sk[warp][q] = keys_in[begin + q];
+            sv[warp][q] = vals_in[begin + q];
+        }
+    }
+    __syncwarp();
+    for (uint32_t r = 0; r < cnt; r += 32u) {
         const uint32_t i = r + lane;
-        const unsigned valid = __ballot_sync(0xFFFFFFFFu, i < end);
-        if (i < end) {
-            const uint32_t key = keys_in[i];
+        const unsigned valid = __ballot_sync(0xFFFFFFFFu, i < cnt);
+        if (i < cnt) {
+            const uint32_t key = sk[warp][i];
             const uint32_t dg = (key >> shift) & 255u;
             const unsigned peers = __match_any_sync(valid, dg);
             const uint32_t base = off[warp][dg];
             const uint32_t dst = base + (uint32_t)__popc(peers & ((1u << lane) - 1u));
             keys_out[dst] = key;
-            vals_out[dst] = vals_in[i];
+            vals_out[dst] = sv[warp][i];
             __syncwarp(valid);
             if ((uint32_t)(__ffs(peers) - 1) == lane) off[warp][dg] = base + (uint32_t)__popc(peers);
         }
@@ -355,7 +374,8 @@ cudaError_t launch_queue(const TraceArgs &ta, const VxRay *rays, size_t n, VxHit
             k_radix_hist<<<tb, 128, 0, s>>>(kin, nn, shift, tiles, sc.hist);
             k_radix_rowsum<<<32, 256, 0, s>>>(sc.hist, tiles, sc.hist + (size_t)tiles * 256u);
             k_radix_rowscan<<<32, 256, 0, s>>>(sc.hist, tiles, sc.hist + (size_t)tiles * 256u);
-            k_radix_scatter<<<tb, 128, 0, s>>>(kin, vin, nn, shift, tiles, sc.hist, kout, vout);
+            k_radix_scatter<<<(tiles + kScatterWarps - 1) / kScatterWarps, 32 * kScatterWarps, 0,
+                              s>>>(kin, vin, nn, shift, tiles, sc.hist, kout, vout);
             std::swap(kin, kout);
             std::swap(vin, vout);
         }
