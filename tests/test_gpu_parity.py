@@ -516,3 +516,60 @@ def test_host_frame_pipeline_bit_exact(vg, dev_c1, c1_oracle_world):
         wrec, wsh, _, _, _ = po.render_frame(c1_oracle_world, cam, p)
         assert_same_records(r.numpy().view(po.RECORD), wrec, "pipelined host frame")
         assert np.array_equal(s.numpy(), wsh.view(np.uint8))
+
+
+def _pattern_world(kind, seed=0):
+    """Smallest legal window (64x16x64 bricks = 256x64x256 voxels) filled
+    with a pattern: 'full' stone, a 3D 'checker' of alternating voxels, or
+    'sparse' random voxels (5 %) of every material class."""
+    bx, by, bz = 64, 16, 64
+    x, y, z = np.meshgrid(np.arange(bx * 4), np.arange(by * 4), np.arange(bz * 4), indexing="ij")
+    if kind == "full":
+        m = np.full(x.shape, 4, np.uint8)
+    elif kind == "checker":
+        m = np.where((x + y + z) % 2 == 0, 2, 0).astype(np.uint8)
+    else:
+        rng = np.random.default_rng(seed)
+        classes = np.array([1, 2, 3, 4, 12, 14, 18, 25, 30, 31, 33, 35, 36], np.uint8)
+        m = np.where(rng.random(x.shape) < 0.05, rng.choice(classes, x.shape), 0).astype(np.uint8)
+    w = po.World(bx, by, bz)
+    vi = (x & 3) + (z & 3) * 4 + (y & 3) * 16
+    bi = (x >> 2) + (y >> 2) * bx + (z >> 2) * bx * by
+    mats = w.a["bricks"]["materials"]
+    mats[bi.ravel(), vi.ravel()] = m.ravel()
+    occ = (mats != 0).astype(np.uint64) << np.arange(64, dtype=np.uint64)
+    w.a["bricks"]["occupancy"] = np.bitwise_or.reduce(occ, axis=1)
+    w.rebuild()
+    return w
+
+
+@pytest.mark.parametrize("kind", ["full", "checker", "sparse"])
+def test_pattern_worlds_bit_exact(vg, kind):
+    """Extreme worlds: every level uniform (full), the densest voxel-level
+    stepping (checker), and every material class scattered (sparse), with
+    the camera inside the world; frames under two flag sets and 4k random
+    rays of each kind against the oracle."""
+    ow = _pattern_world(kind)
+    dw = upload_oracle(vg, ow)
+    for pose in [((128.5, 30.2, 128.5), 0.4, -0.3), ((3.0, 63.0, 250.0), 2.2, -0.9)]:
+        cam = vg.camera_from_pose(pose[0], pose[1], pose[2], 1.2, 96, 54)
+        for flags in (METHOD | po.OR_F_SHADOW, po.OR_F_L4):
+            rec, sh, (wrec, wsh, _, _, _) = frame_pair(vg, dw, ow, cam, flags)
+            assert_same_records(rec, wrec, f"{kind} flags={flags}")
+            if sh is not None:
+                assert np.array_equal(sh.view(np.uint8), wsh.view(np.uint8))
+    rng = np.random.default_rng(7)
+    n = 4000
+    rays = np.zeros(n, po.RAY)
+    rays["org"] = rng.uniform([-20, -10, -20], [276, 74, 276], (n, 3)).astype(np.float32)
+    d = rng.normal(size=(n, 3)).astype(np.float32)
+    d /= np.sqrt((d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1]) + d[:, 2] * d[:, 2])[:, None]
+    rays["dir"] = d
+    rays["tmax"] = rng.uniform(1, 400, n).astype(np.float32)
+    for kind_id in (0, 1, 2):
+        rays["kind"] = kind_id
+        p = vg.default_params(METHOD)
+        got = vg.records(vg.trace(dw, rays, p))
+        want = po.trace_batch(ow, rays, p)[0]
+        assert_same_records(got, want, f"{kind} ray kind {kind_id}")
+    dw.close()
