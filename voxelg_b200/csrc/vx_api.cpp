@@ -375,6 +375,7 @@ int vx_world_counts(const VxWorld *w, uint64_t counts[4]) {
 int vx_world_upload(VxWorld *w, const VxBrick *bricks, const uint64_t *tile_mask,
                     const uint64_t *chunk_mask, const uint64_t *l4_mask,
                     const uint8_t *brick_uniform, const uint8_t *tile_uniform) {
+    vx::Range nvtx_range("vx_world_upload");
     if (!w || !bricks || !tile_mask || !chunk_mask || !l4_mask || !brick_uniform || !tile_uniform) {
         vx::set_error("vx_world_upload: null argument");
         return VX_ERR_INVALID;
@@ -432,6 +433,7 @@ int vx_world_download(VxWorld *w, VxBrick *bricks, uint64_t *tile_mask, uint64_t
 }
 
 int vx_world_generate(VxWorld *w, const VxTerrainParams *t) {
+    vx::Range nvtx_range("vx_world_generate");
     if (!w || !t || t->octaves > 32) {
         vx::set_error("vx_world_generate: null argument or octaves > 32");
         return VX_ERR_INVALID;
@@ -663,6 +665,7 @@ bool origin_in_range(int32_t ox, int32_t oz) {
 }  // namespace
 
 int vx_world_gen_chunks(VxWorld *w, uint64_t seed, const int32_t *chunks, uint32_t n) {
+    vx::Range nvtx_range("vx_world_gen_chunks");
     if (!w || (n > 0 && !chunks)) {
         vx::set_error("vx_world_gen_chunks: null argument");
         return VX_ERR_INVALID;
@@ -674,6 +677,7 @@ int vx_world_gen_chunks(VxWorld *w, uint64_t seed, const int32_t *chunks, uint32
 }
 
 int vx_world_fill_window(VxWorld *w, uint64_t seed, int32_t origin_cx, int32_t origin_cz) {
+    vx::Range nvtx_range("vx_world_fill_window");
     if (!w || !origin_in_range(origin_cx, origin_cz)) {
         vx::set_error("vx_world_fill_window: null world or origin beyond +-2^23 chunks");
         return VX_ERR_INVALID;
@@ -718,6 +722,7 @@ int vx_world_fill_window(VxWorld *w, uint64_t seed, int32_t origin_cx, int32_t o
 
 int vx_world_shift_origin(VxWorld *w, int32_t origin_cx, int32_t origin_cz,
                           uint32_t *n_regenerated) {
+    vx::Range nvtx_range("vx_world_shift_origin");
     if (!w || !origin_in_range(origin_cx, origin_cz)) {
         vx::set_error("vx_world_shift_origin: null world or origin beyond +-2^23 chunks");
         return VX_ERR_INVALID;
@@ -753,6 +758,7 @@ int vx_world_shift_origin(VxWorld *w, int32_t origin_cx, int32_t origin_cz,
 }
 
 int vx_world_apply_edit(VxWorld *w, int32_t wx, int32_t wy, int32_t wz, uint8_t mat) {
+    vx::Range nvtx_range("vx_world_apply_edit");
     if (!w || wx <= -(1 << 29) || wx >= (1 << 29) || wz <= -(1 << 29) || wz >= (1 << 29)) {
         vx::set_error("vx_world_apply_edit: null world or x/z beyond +-2^29");
         return VX_ERR_INVALID;
@@ -781,6 +787,7 @@ int vx_world_clear_edits(VxWorld *w) {
 
 int vx_world_apply_dirty(VxWorld *w, const uint32_t *brick_idx, const VxBrick *bricks, size_t n,
                          void *stream) {
+    vx::Range nvtx_range("vx_world_apply_dirty");
     if (!w || (n > 0 && (!brick_idx || !bricks))) {
         vx::set_error("vx_world_apply_dirty: null argument");
         return VX_ERR_INVALID;
@@ -852,6 +859,7 @@ int vx_raycast(VxWorld *w, const float cam[3], const float dir[3], const int32_t
 int vx_raycast_batch(VxWorld *w, const int32_t origin[3], const float *cams_dev,
                      const float *dirs_dev, size_t n, VxPickHit *out_dev, int32_t *hit_dev,
                      void *stream) {
+    vx::Range nvtx_range("vx_raycast_batch");
     if (!w || !origin || (n > 0 && (!cams_dev || !dirs_dev || !out_dev || !hit_dev))) {
         vx::set_error("vx_raycast_batch: null argument");
         return VX_ERR_INVALID;
@@ -866,6 +874,7 @@ int vx_raycast_batch(VxWorld *w, const int32_t origin[3], const float *cams_dev,
 
 int vx_trace(VxWorld *w, const int32_t origin[3], const VxRay *rays_dev, size_t n,
              const VxTraceParams *p, VxHitRecord *out_dev, void *stream) {
+    vx::Range nvtx_range("vx_trace");
     if (!w || !origin || (n > 0 && (!rays_dev || !out_dev))) {
         vx::set_error("vx_trace: null argument");
         return VX_ERR_INVALID;
@@ -889,6 +898,7 @@ int vx_trace(VxWorld *w, const int32_t origin[3], const VxRay *rays_dev, size_t 
 
 int vx_render_primary(VxWorld *w, const VxCamera *cam, const VxTraceParams *p,
                       VxHitRecord *rec_dev, VxShadowRecord *shadow_dev, void *stream) {
+    vx::Range nvtx_range("vx_render_primary");
     if (!w || !rec_dev) {
         vx::set_error("vx_render_primary: null argument");
         return VX_ERR_INVALID;
@@ -960,6 +970,7 @@ vx::TraceArgs trace_args(const VxWorld *w, const int32_t origin[3], const VxTrac
 int vx_queue_run(VxWorld *w, const int32_t origin[3], const VxRay *rays_dev, size_t n,
                  const VxTraceParams *p, const VxQueueTuning *t, VxHitRecord *out_dev,
                  VxShadowRecord *shadow_dev, void *stream) {
+    vx::Range nvtx_range("vx_queue_run");
     VxQueueTuning def;
     vx_queue_default_tuning(&def);
     if (!t) t = &def;
@@ -1099,6 +1110,7 @@ int vx_render_primary_gated(VxWorld *w, const VxCamera *cam, const VxTraceParams
 
 int vx_render_ao(VxWorld *w, const VxCamera *cam, const VxHitRecord *rec_dev, float *ao_dev,
                  void *stream) {
+    vx::Range nvtx_range("vx_render_ao");
     if (!w || !rec_dev || !ao_dev) {
         vx::set_error("vx_render_ao: null argument");
         return VX_ERR_INVALID;
@@ -1186,6 +1198,7 @@ int host_frame_args(VxWorld *w, const VxCamera *cam, const VxTraceParams *p,
 
 int vx_render_primary_host(VxWorld *w, const VxCamera *cam, const VxTraceParams *p,
                            VxHitRecord *rec_host, VxShadowRecord *shadow_host) {
+    vx::Range nvtx_range("vx_render_primary_host");
     int rc = host_frame_args(w, cam, p, rec_host, "vx_render_primary_host");
     if (rc != VX_OK) return rc;
     std::lock_guard<std::mutex> lk(w->mu);
@@ -1198,6 +1211,7 @@ int vx_render_primary_host(VxWorld *w, const VxCamera *cam, const VxTraceParams 
 
 int vx_render_primary_host_async(VxWorld *w, const VxCamera *cam, const VxTraceParams *p,
                                  VxHitRecord *rec_host, VxShadowRecord *shadow_host) {
+    vx::Range nvtx_range("vx_render_primary_host_async");
     int rc = host_frame_args(w, cam, p, rec_host, "vx_render_primary_host_async");
     if (rc != VX_OK) return rc;
     std::lock_guard<std::mutex> lk(w->mu);

@@ -9,7 +9,18 @@
 
 #include "voxrt.h"
 
+#include <nvtx3/nvToolsExt.h>
+
 namespace vx {
+
+// Names one library call on a profiler's timeline (an NVTX range); it costs
+// nothing when no tool is attached.
+struct Range {
+    explicit Range(const char *name) { nvtxRangePushA(name); }
+    ~Range() { nvtxRangePop(); }
+    Range(const Range &) = delete;
+    Range &operator=(const Range &) = delete;
+};
 
 // World dimensions; the derived counts follow src/world_dims.rs:12-37.
 struct Dims {

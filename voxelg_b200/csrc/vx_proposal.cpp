@@ -305,6 +305,7 @@ int vx_proposal_infer(VxProposal *p, const float *feats_dev, size_t n, float *ou
 
 int vx_proposal_train(VxProposal *p, VxWorld *w, const VxTrainConfig *c, float *loss_curve,
                       float held_out[2]) {
+    vx::Range nvtx_range("vx_proposal_train");
     int rc = check_prop(p, "vx_proposal_train");
     if (rc != VX_OK) return rc;
     if (!w || !c || c->poses == 0 || c->rays_per_pose == 0 || c->batch == 0 ||
@@ -380,6 +381,7 @@ int vx_proposal_train(VxProposal *p, VxWorld *w, const VxTrainConfig *c, float *
 
 int vx_render_learned(VxWorld *w, VxProposal *prop, const VxCamera *cam, const VxTraceParams *p,
                       float scale, VxHitRecord *rec_dev, VxLearnedStats *stats, void *stream) {
+    vx::Range nvtx_range("vx_render_learned");
     if (!w || !cam || !p || !rec_dev) {
         vx::set_error("vx_render_learned: null argument");
         return VX_ERR_INVALID;
