@@ -412,3 +412,31 @@ def test_device_edits_replayed_when_streamed_in():
     assert _material_at_world(dw, (4, -1), 600, 90, 20) != MAT_GLASS
     _assert_world_equal(dw, _oracle_window(DEMO, SEED, 4, -1))
     dw.close()
+
+
+@pytest.mark.gpu
+def test_full_size_generated_window_frame_bit_exact():
+    """The 2048x256x2048 window generated by the reference's generator
+    (32768 chunks): every byte of the world equals the oracle's, and a
+    1920x1080 frame with beam/LUT/LOD and shadow rays over it is bit-exact."""
+    _gpu()
+    import torch
+
+    import voxelg_b200 as vg
+    dims = (512, 64, 512)
+    dw = vg.DeviceWorld(*dims)
+    dw.fill_window(SEED, 0, 0)
+    ow = po.World(*dims)
+    po.fill_window(ow, SEED, 0, 0)
+    _assert_world_equal(dw, ow)
+    cam = vg.camera_from_pose((1024.0, 150.0, 1024.0), 0.7, -0.3, 1.22, 1920, 1080)
+    flags = po.OR_F_L4 | po.OR_F_LUT | po.OR_F_LOD | po.OR_F_BEAM | po.OR_F_SHADOW
+    p = vg.default_params(flags)
+    rec, sh = vg.render_primary(dw, cam, p)
+    torch.cuda.synchronize()
+    wrec, wsh, _, _, _ = po.render_frame(ow, cam, p)
+    got = vg.records(rec)
+    assert np.array_equal(got.view(np.uint8), wrec.view(np.uint8))
+    assert np.array_equal(vg.shadows(sh).view(np.uint8), wsh.view(np.uint8))
+    assert (got["flags"] & 1).mean() > 0.3
+    dw.close()
