@@ -143,10 +143,8 @@ cudaError_t launch_apply_dirty(const DevWorld &w, const uint32_t *idx, const VxB
 // work counters, coherence-sort keys / permutation / histogram, fingerprint.
 struct QueueScratch {
     uint32_t *work = nullptr;
-    uint32_t *keys = nullptr;     // coherence sort: keys and permutation,
-    uint32_t *order = nullptr;    // with their ping-pong partners
-    uint32_t *keys2 = nullptr;
-    uint32_t *order2 = nullptr;
+    uint2 *kv = nullptr;          // coherence sort: (key, ray) pairs
+    uint2 *kv2 = nullptr;         // and their ping-pong partner
     uint32_t *hist = nullptr;     // per-tile digit counts
     unsigned long long *fp = nullptr;
     size_t cap = 0;

@@ -33,7 +33,7 @@ constexpr uint32_t kTileItems = 2048;   // radix sort: items per warp-tile
 struct QueueArgs {
     TraceArgs ta;
     const VxRay *rays;
-    const uint32_t *order;    // coherence permutation or nullptr (identity)
+    const uint2 *order;       // sorted (key, ray) pairs or nullptr (identity order)
     uint32_t n;
     VxHitRecord *out;
     VxShadowRecord *shadow;   // shadow records of spawning rays, or nullptr
@@ -80,7 +80,7 @@ __global__ void __launch_bounds__(256) k_queue(QueueArgs q) {
                     item = DONE;
                 } else {
                     item = slot;
-                    ray = q.order ? __ldg(q.order + slot) : slot;
+                    ray = q.order ? __ldg(q.order + slot).y : slot;
                     float dx, dy, dz, tmax;
                     load_ray(q.rays, ray, ox, oy, oz, dx, dy, dz, tmax, rkind);
                     shadow_phase = false;
@@ -166,7 +166,7 @@ __device__ __forceinline__ uint32_t spread_bits(uint32_t x) {   // 9 bits -> eve
 }
 
 __global__ void k_radix_keys(const VxRay *rays, uint32_t n, int32_t rox, int32_t roz,
-                             uint32_t *keys, uint32_t *vals) {
+                             uint2 *kv) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float ox, oy, oz, dx, dy, dz, tmax;
@@ -190,12 +190,11 @@ __global__ void k_radix_keys(const VxRay *rays, uint32_t n, int32_t rox, int32_t
         return ((uint32_t)c >> 6) & 15u;
     };
     const uint32_t oc = cell(ox, rox) | (cell(oz, roz) << 4) | (cell(oy, 0) << 8);
-    keys[i] = ((kind & 3u) << 30) | (morton << 12) | oc;
-    vals[i] = i;
+    kv[i] = make_uint2(((kind & 3u) << 30) | (morton << 12) | oc, i);
 }
 
 // Per warp-tile histogram of one 8-bit digit: counts[digit * tiles + tile].
-__global__ void __launch_bounds__(128) k_radix_hist(const uint32_t *keys, uint32_t n,
+__global__ void __launch_bounds__(128) k_radix_hist(const uint2 *kv, uint32_t n,
                                                     uint32_t shift, uint32_t tiles,
                                                     uint32_t *counts) {
     __shared__ uint32_t h[4][256];
@@ -206,7 +205,7 @@ __global__ void __launch_bounds__(128) k_radix_hist(const uint32_t *keys, uint32
     if (tile < tiles) {
         const uint32_t end = min(n, (tile + 1u) * kTileItems);
         for (uint32_t i = tile * kTileItems + lane; i < end; i += 32u)
-            atomicAdd(&h[warp][(keys[i] >> shift) & 255u], 1u);
+            atomicAdd(&h[warp][(kv[i].x >> shift) & 255u], 1u);
         __syncwarp();
         for (uint32_t d = lane; d < 256u; d += 32u) counts[d * tiles + tile] = h[warp][d];
     }
@@ -248,15 +247,15 @@ __global__ void __launch_bounds__(256) k_radix_rowscan(uint32_t *counts, uint32_
     }
 }
 
-// Stable scatter: each warp stages its tile's keys and values in shared
+// Stable scatter: each warp stages its tile's (key, ray) pairs in shared
 // memory (coalesced 16-byte loads), then walks the tile in index order, 32
 // items a round; lanes sharing a digit take consecutive slots in lane order.
+// A pair is stored as one 8-byte word, so each item dirties one sector.
 constexpr uint32_t kScatterWarps = 2;
 __global__ void __launch_bounds__(32 * kScatterWarps) k_radix_scatter(
-    const uint32_t *keys_in, const uint32_t *vals_in, uint32_t n, uint32_t shift, uint32_t tiles,
-    const uint32_t *counts, uint32_t *keys_out, uint32_t *vals_out) {
-    __shared__ __align__(16) uint32_t sk[kScatterWarps][kTileItems];
-    __shared__ __align__(16) uint32_t sv[kScatterWarps][kTileItems];
+    const uint2 *in, uint32_t n, uint32_t shift, uint32_t tiles, const uint32_t *counts,
+    uint2 *out) {
+    __shared__ __align__(16) uint2 st[kScatterWarps][kTileItems];
     __shared__ uint32_t off[kScatterWarps][256];
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
     const uint32_t tile = blockIdx.x * kScatterWarps + warp;
@@ -265,33 +264,24 @@ __global__ void __launch_bounds__(32 * kScatterWarps) k_radix_scatter(
     const uint32_t begin = tile * kTileItems, end = min(n, begin + kTileItems);
     const uint32_t cnt = end - begin;
     if (cnt == kTileItems) {
-        // begin is a multiple of 2048 items: 16-byte aligned
-        const uint4 *k4 = reinterpret_cast<const uint4 *>(keys_in + begin);
-        const uint4 *v4 = reinterpret_cast<const uint4 *>(vals_in + begin);
-        uint4 *sk4 = reinterpret_cast<uint4 *>(sk[warp]), *sv4 = reinterpret_cast<uint4 *>(sv[warp]);
+        // begin is a multiple of 2048 pairs: 16-byte aligned
+        const uint4 *src = reinterpret_cast<const uint4 *>(in + begin);
+        uint4 *dst = reinterpret_cast<uint4 *>(st[warp]);
 #pragma unroll 4
-        for (uint32_t q = lane; q < kTileItems / 4u; q += 32u) {
-            sk4[q] = k4[q];
-            sv4[q] = v4[q];
-        }
+        for (uint32_t q = lane; q < kTileItems / 2u; q += 32u) dst[q] = src[q];
     } else {
-        for (uint32_t q = lane; q < cnt; q += 32u) {
-            sk[warp][q] = keys_in[begin + q];
-            sv[warp][q] = vals_in[begin + q];
-        }
+        for (uint32_t q = lane; q < cnt; q += 32u) st[warp][q] = in[begin + q];
     }
     __syncwarp();
     for (uint32_t r = 0; r < cnt; r += 32u) {
         const uint32_t i = r + lane;
         const unsigned valid = __ballot_sync(0xFFFFFFFFu, i < cnt);
         if (i < cnt) {
-            const uint32_t key = sk[warp][i];
-            const uint32_t dg = (key >> shift) & 255u;
+            const uint2 item = st[warp][i];
+            const uint32_t dg = (item.x >> shift) & 255u;
             const unsigned peers = __match_any_sync(valid, dg);
             const uint32_t base = off[warp][dg];
-            const uint32_t dst = base + (uint32_t)__popc(peers & ((1u << lane) - 1u));
-            keys_out[dst] = key;
-            vals_out[dst] = sv[warp][i];
+            out[base + (uint32_t)__popc(peers & ((1u << lane) - 1u))] = item;
             __syncwarp(valid);
             if ((uint32_t)(__ffs(peers) - 1) == lane) off[warp][dg] = base + (uint32_t)__popc(peers);
         }
@@ -331,17 +321,17 @@ cudaError_t QueueScratch::reserve(size_t n) {
         if (e == cudaSuccess) e = cudaMalloc(&fp, sizeof(unsigned long long));
         if (e != cudaSuccess) return e;
     }
-    if (cap >= n && keys) return cudaSuccess;
-    uint32_t **bufs[] = {&keys, &order, &keys2, &order2, &hist};
-    for (uint32_t **b : bufs) {
-        cudaFree(*b);
-        *b = nullptr;
-    }
+    if (cap >= n && kv) return cudaSuccess;
+    cudaFree(kv);
+    cudaFree(kv2);
+    cudaFree(hist);
+    kv = kv2 = nullptr;
+    hist = nullptr;
     cap = 0;
     const size_t m = std::max<size_t>(n, 1);
     const size_t tiles = (m + kTileItems - 1) / kTileItems;
-    cudaError_t e = cudaSuccess;
-    for (int k = 0; k < 4 && e == cudaSuccess; ++k) e = cudaMalloc(bufs[k], m * sizeof(uint32_t));
+    cudaError_t e = cudaMalloc(&kv, m * sizeof(uint2));
+    if (e == cudaSuccess) e = cudaMalloc(&kv2, m * sizeof(uint2));
     if (e == cudaSuccess) e = cudaMalloc(&hist, (tiles + 1) * 256 * sizeof(uint32_t));
     if (e == cudaSuccess) cap = n;
     return e;
@@ -349,10 +339,8 @@ cudaError_t QueueScratch::reserve(size_t n) {
 
 void QueueScratch::release() {
     cudaFree(work);
-    cudaFree(keys);
-    cudaFree(order);
-    cudaFree(keys2);
-    cudaFree(order2);
+    cudaFree(kv);
+    cudaFree(kv2);
     cudaFree(hist);
     cudaFree(fp);
     *this = QueueScratch();
@@ -363,23 +351,21 @@ cudaError_t launch_queue(const TraceArgs &ta, const VxRay *rays, size_t n, VxHit
                          cudaStream_t s) {
     if (n == 0) return cudaSuccess;
     const uint32_t nn = (uint32_t)n;
-    const uint32_t *order = nullptr;
+    const uint2 *order = nullptr;
     if (t.sort) {
         const uint32_t tiles = (nn + kTileItems - 1) / kTileItems;
         const unsigned tb = (tiles + 3) / 4;
-        k_radix_keys<<<(nn + 255) / 256, 256, 0, s>>>(rays, nn, ta.ro[0], ta.ro[2], sc.keys,
-                                                      sc.order);
-        uint32_t *kin = sc.keys, *vin = sc.order, *kout = sc.keys2, *vout = sc.order2;
+        k_radix_keys<<<(nn + 255) / 256, 256, 0, s>>>(rays, nn, ta.ro[0], ta.ro[2], sc.kv);
+        uint2 *in = sc.kv, *out = sc.kv2;
         for (uint32_t shift = 0; shift < 32u; shift += 8u) {
-            k_radix_hist<<<tb, 128, 0, s>>>(kin, nn, shift, tiles, sc.hist);
+            k_radix_hist<<<tb, 128, 0, s>>>(in, nn, shift, tiles, sc.hist);
             k_radix_rowsum<<<32, 256, 0, s>>>(sc.hist, tiles, sc.hist + (size_t)tiles * 256u);
             k_radix_rowscan<<<32, 256, 0, s>>>(sc.hist, tiles, sc.hist + (size_t)tiles * 256u);
             k_radix_scatter<<<(tiles + kScatterWarps - 1) / kScatterWarps, 32 * kScatterWarps, 0,
-                              s>>>(kin, vin, nn, shift, tiles, sc.hist, kout, vout);
-            std::swap(kin, kout);
-            std::swap(vin, vout);
+                              s>>>(in, nn, shift, tiles, sc.hist, out);
+            std::swap(in, out);
         }
-        order = vin;   // four passes: back in sc.order
+        order = in;
     }
     QueueArgs q;
     q.ta = ta;
