@@ -8,7 +8,7 @@
 // its shadow ray (raymarch.wgsl:3953-3994).  Lanes of a warp refill together
 // once `refill_min` of them are idle (a lone refill would stall 31 lanes
 // through a ray set-up).  Optionally the queue is first reordered by a 32-bit
-// coherence key -- kind, then the direction on a 512x512 octahedral grid in
+// coherence key -- kind, then the direction on a 1024x1024 octahedral grid in
 // Morton order, then the 64-voxel origin cell -- with a stable LSD radix sort
 // (four 8-bit passes), so that a warp's rays head the same way from nearby
 // origins: rays of one camera fall into pixel-sized direction cells, the
@@ -154,10 +154,11 @@ __global__ void __launch_bounds__(256) k_queue(QueueArgs q) {
 }
 
 // ---- coherence reorder: stable LSD radix sort of a 32-bit key
-// key = kind(2) | Morton(octahedral direction, 9+9 bits) | origin cell(12)
+// key = kind(2) | Morton(octahedral direction, 10+10 bits) | origin cell(10:
+// 64-voxel cells, 4 bits each in x and z, 2 in y)
 
-__device__ __forceinline__ uint32_t spread_bits(uint32_t x) {   // 9 bits -> even bits
-    x &= 0x1FFu;
+__device__ __forceinline__ uint32_t spread_bits(uint32_t x) {   // 10 bits -> even bits
+    x &= 0x3FFu;
     x = (x | (x << 8)) & 0x00FF00FFu;
     x = (x | (x << 4)) & 0x0F0F0F0Fu;
     x = (x | (x << 2)) & 0x33333333u;
@@ -180,8 +181,8 @@ __global__ void k_radix_keys(const VxRay *rays, uint32_t n, int32_t rox, int32_t
         v = (1.f - fabsf(u)) * (v < 0.f ? -1.f : 1.f);
         u = uu;
     }
-    const uint32_t qu = (uint32_t)min(511, max(0, (int32_t)((u + 1.f) * 256.f)));
-    const uint32_t qv = (uint32_t)min(511, max(0, (int32_t)((v + 1.f) * 256.f)));
+    const uint32_t qu = (uint32_t)min(1023, max(0, (int32_t)((u + 1.f) * 512.f)));
+    const uint32_t qv = (uint32_t)min(1023, max(0, (int32_t)((v + 1.f) * 512.f)));
     const uint32_t morton = spread_bits(qu) | (spread_bits(qv) << 1);
     // origin cell of 64 voxels relative to the window corner (x, z) and in y
     auto cell = [](float o, int32_t corner) -> uint32_t {
@@ -189,8 +190,8 @@ __global__ void k_radix_keys(const VxRay *rays, uint32_t n, int32_t rox, int32_t
         const int32_t c = f != f ? 0 : (int32_t)fminf(fmaxf(f - (float)corner, 0.f), 1e9f);
         return ((uint32_t)c >> 6) & 15u;
     };
-    const uint32_t oc = cell(ox, rox) | (cell(oz, roz) << 4) | (cell(oy, 0) << 8);
-    kv[i] = make_uint2(((kind & 3u) << 30) | (morton << 12) | oc, i);
+    const uint32_t oc = cell(ox, rox) | (cell(oz, roz) << 4) | ((cell(oy, 0) & 3u) << 8);
+    kv[i] = make_uint2(((kind & 3u) << 30) | (morton << 10) | oc, i);
 }
 
 // Per warp-tile histogram of one 8-bit digit: counts[digit * tiles + tile].
