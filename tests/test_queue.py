@@ -128,7 +128,36 @@ def test_queue_edge_rays(gpu, c1_oracle_world):
     rays["kind"] = rng.choice(np.array([0, 1, 2, 256, 257, 258, 3], np.uint32), n)
     p = vg.default_params(po.OR_F_L4 | po.OR_F_LUT | po.OR_F_LOD)
     want, wsh, _, _ = po.trace_batch(c1_oracle_world, rays, p, shadows=True)
-    _, out, sh = q.run(dw, rays, p)
+    for so in (0, 1):
+        t = q.default_tuning()
+        t.block_threads, t.refill_min, t.sort = 256, 32, so
+        _, out, sh = q.run(dw, rays, p, tuning=t)
+        torch.cuda.synchronize()
+        assert np.array_equal(out.cpu().numpy(), want.view(np.uint8)), so
+        assert np.array_equal(sh.cpu().numpy(), wsh.view(np.uint8)), so
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [1, 31, 33, 2047, 2048, 2049, 6149])
+def test_queue_sorted_sizes(gpu, c1_oracle_world, n):
+    """The radix-sorted queue at sizes around its 2048-ray tiles and the
+    32-lane packets: every record equals the oracle's."""
+    import torch
+    import voxelg_b200.queue as q
+    vg, dw = gpu
+    rng = np.random.default_rng(n)
+    rays = np.zeros(n, po.RAY)
+    rays["org"] = rng.uniform([0, 60, 0], [512, 220, 512], size=(n, 3)).astype(np.float32)
+    d = rng.normal(size=(n, 3)).astype(np.float32)
+    d /= np.sqrt((d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1]) + d[:, 2] * d[:, 2])[:, None]
+    rays["dir"] = d
+    rays["tmax"] = 300.0
+    rays["kind"] = rng.choice(np.array([0, 1, 2, 256], np.uint32), n)
+    p = vg.default_params(po.OR_F_L4 | po.OR_F_LUT | po.OR_F_LOD)
+    want, wsh, _, _ = po.trace_batch(c1_oracle_world, rays, p, shadows=True)
+    t = q.default_tuning()
+    t.block_threads, t.refill_min, t.sort = 128, 32, 1
+    _, out, sh = q.run(dw, rays, p, tuning=t)
     torch.cuda.synchronize()
     assert np.array_equal(out.cpu().numpy(), want.view(np.uint8))
     assert np.array_equal(sh.cpu().numpy(), wsh.view(np.uint8))
