@@ -573,3 +573,35 @@ def test_pattern_worlds_bit_exact(vg, kind):
         want = po.trace_batch(ow, rays, p)[0]
         assert_same_records(got, want, f"{kind} ray kind {kind_id}")
     dw.close()
+
+
+def test_single_call_pick_matches_o1(vg, dev_c1, c1_oracle_world):
+    """The single-ray drop-in (one warp walks one ray 32 voxels at a time):
+    3000 calls -- random starts in and around the window (inside terrain,
+    in the air, outside), zero, denormal and axis-aligned directions, long
+    grazing rays and the criterion picking rays -- each equal to O1."""
+    rng = np.random.default_rng(11)
+    vox = c1_oracle_world.voxels
+    n = 2600
+    cams = rng.uniform([-40, -10, -40], [vox[0] + 40, 260, vox[2] + 40], size=(n, 3))
+    dirs = rng.normal(size=(n, 3))
+    dirs[::13] = 0.0
+    dirs[1::29] *= 1e-20
+    dirs[2::31] = (1.0, 0.0, 0.0)
+    dirs[3::37] = (0.0, -1.0, 0.0)
+    dirs[4::41] = (0.0, 0.0, -1.0)
+    dirs[5::7, 1] = 1e-3                     # nearly horizontal: long walks
+    a = (np.arange(1, 401) * np.float32(0.013)).astype(np.float32)
+    bench_dirs = np.stack([np.sin(a), np.full(400, -0.5, np.float32), np.cos(a)], 1)
+    cams = np.concatenate([cams, np.tile([256.0, 90.0, 256.0], (400, 1))]).astype(np.float32)
+    dirs = np.concatenate([dirs, bench_dirs]).astype(np.float32)
+    want, whit, _ = po.raycast_batch(c1_oracle_world, cams, dirs)
+    long_walks = 0
+    for i in range(len(cams)):
+        h = vg.raycast(cams[i], dirs[i], dev_c1)
+        assert (h is not None) == bool(whit[i]), i
+        if h is not None:
+            assert h.voxel == tuple(want[i]["voxel"]) and h.normal == tuple(want[i]["normal"]), i
+        if whit[i] and np.abs(np.array(want[i]["voxel"], np.float64) - cams[i]).sum() > 64:
+            long_walks += 1
+    assert 0.2 < whit.mean() < 0.95 and long_walks > 50

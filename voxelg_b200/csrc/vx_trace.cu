@@ -427,6 +427,73 @@ __device__ __forceinline__ bool o1_in_solid(const DevWorld &w, const int32_t v[3
     return ldg(w.mat + bi * 64 + vi) != 33u;
 }
 
+// The walk of raycast(): direction normalised as glam 0.29.3's
+// normalize_or_zero (self * (1 / sqrt(dot))), window clip, start voxel
+// (raycast.rs:21-90).  False when the ray has no walk (zero direction,
+// misses the window).
+struct O1State {
+    int32_t voxel[3], step[3];
+    float tdel[3], tm[3];
+};
+
+__device__ __forceinline__ bool o1_start(const Dims &d, const int32_t o[3], const float cam[3],
+                                         const float din[3], O1State &s) {
+    const float len = sqrtf((din[0] * din[0] + din[1] * din[1]) + din[2] * din[2]);
+    const float rcp = 1.0f / len;
+    if (!(isfinite(rcp) && rcp > 0.0f)) return false;
+    const float dir[3] = {din[0] * rcp, din[1] * rcp, din[2] * rcp};
+    if (dir[0] == 0.0f && dir[1] == 0.0f && dir[2] == 0.0f) return false;
+    const float dims[3] = {(float)d.vx, (float)d.vy, (float)d.vz};
+    float wmin[3], wmax[3], inv[3], tmn[3], tmx[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        wmin[k] = (float)o[k];
+        wmax[k] = wmin[k] + dims[k];
+        inv[k] = safe_inv(dir[k]);
+        const float t0 = (wmin[k] - cam[k]) * inv[k];
+        const float t1 = (wmax[k] - cam[k]) * inv[k];
+        tmn[k] = vmin(t0, t1);
+        tmx[k] = vmax(t0, t1);
+    }
+    const float t_enter = vmax(vmax(tmn[0], vmax(tmn[1], tmn[2])), 0.0f);
+    const float t_exit = vmin(tmx[0], vmin(tmx[1], tmx[2]));
+    if (t_enter >= t_exit || t_exit < 0.0f) return false;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        float pk = cam[k] + dir[k] * (t_enter + 1e-3f);
+        pk = vmin(vmax(pk, wmin[k] + 1e-3f), wmax[k] - 1e-3f);
+        s.voxel[k] = f2i(floorf(pk));
+        s.step[k] = sgn(dir[k]);
+        s.tdel[k] = fabsf(inv[k]);
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float nxt = s.step[k] > 0 ? (float)(s.voxel[k] + 1) : (float)s.voxel[k];
+        s.tm[k] = (nxt - cam[k]) * inv[k];
+    }
+    return true;
+}
+
+// argmin_step, raycast.rs:92-103 (ties go to the lowest axis); -1: no axis
+__device__ __forceinline__ int o1_argmin_step(O1State &s) {
+    int a = -1;
+    float m = __int_as_float(0x7f800000);
+    if (s.step[0] != 0 && s.tm[0] < m) { a = 0; m = s.tm[0]; }
+    if (s.step[1] != 0 && s.tm[1] < m) { a = 1; m = s.tm[1]; }
+    if (s.step[2] != 0 && s.tm[2] < m) { a = 2; m = s.tm[2]; }
+    if (a == 0) { s.voxel[0] += s.step[0]; s.tm[0] += s.tdel[0]; }
+    else if (a == 1) { s.voxel[1] += s.step[1]; s.tm[1] += s.tdel[1]; }
+    else if (a == 2) { s.voxel[2] += s.step[2]; s.tm[2] += s.tdel[2]; }
+    return a;
+}
+
+__device__ __forceinline__ void o1_normal(const O1State &s, int last_axis, VxPickHit &res) {
+    const int sa = last_axis == 0 ? s.step[0] : (last_axis == 1 ? s.step[1] : s.step[2]);
+    if (last_axis == 0) res.normal[0] = -sa;
+    else if (last_axis == 1) res.normal[1] = -sa;
+    else if (last_axis == 2) res.normal[2] = -sa;
+}
+
 __global__ void __launch_bounds__(128) k_raycast(PickArgs pa, const float *__restrict__ cams,
                                                  const float *__restrict__ dirs, size_t n,
                                                  VxPickHit *out, int32_t *hit) {
@@ -440,78 +507,31 @@ __global__ void __launch_bounds__(128) k_raycast(PickArgs pa, const float *__res
     int32_t found = 0;
     const float cam[3] = {cams[3 * i], cams[3 * i + 1], cams[3 * i + 2]};
     const float din[3] = {dirs[3 * i], dirs[3 * i + 1], dirs[3 * i + 2]};
-    // glam 0.29.3 normalize_or_zero: self * (1 / sqrt(dot(self, self)))
-    const float len = sqrtf((din[0] * din[0] + din[1] * din[1]) + din[2] * din[2]);
-    const float rcp = 1.0f / len;
+    O1State s;
     do {
-        if (!(isfinite(rcp) && rcp > 0.0f)) break;
-        float dir[3] = {din[0] * rcp, din[1] * rcp, din[2] * rcp};
-        if (dir[0] == 0.0f && dir[1] == 0.0f && dir[2] == 0.0f) break;
-        const float dims[3] = {(float)d.vx, (float)d.vy, (float)d.vz};
-        float wmin[3], wmax[3], inv[3], tmn[3], tmx[3];
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            wmin[k] = (float)o[k];
-            wmax[k] = wmin[k] + dims[k];
-            inv[k] = safe_inv(dir[k]);
-            const float t0 = (wmin[k] - cam[k]) * inv[k];
-            const float t1 = (wmax[k] - cam[k]) * inv[k];
-            tmn[k] = vmin(t0, t1);
-            tmx[k] = vmax(t0, t1);
-        }
-        const float t_enter = vmax(vmax(tmn[0], vmax(tmn[1], tmn[2])), 0.0f);
-        const float t_exit = vmin(tmx[0], vmin(tmx[1], tmx[2]));
-        if (t_enter >= t_exit || t_exit < 0.0f) break;
-        int32_t voxel[3], step[3];
-        float tdel[3], tm[3];
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            float pk = cam[k] + dir[k] * (t_enter + 1e-3f);
-            pk = vmin(vmax(pk, wmin[k] + 1e-3f), wmax[k] - 1e-3f);
-            voxel[k] = f2i(floorf(pk));
-            step[k] = sgn(dir[k]);
-            tdel[k] = fabsf(inv[k]);
-        }
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            const float nxt = step[k] > 0 ? (float)(voxel[k] + 1) : (float)voxel[k];
-            tm[k] = (nxt - cam[k]) * inv[k];
-        }
+        if (!o1_start(d, o, cam, din, s)) break;
         int last_axis = -1;
         int steps_left = 4096;
         bool dead = false;
-        // argmin_step, raycast.rs:92-103 (ties go to the lowest axis)
-        auto argmin_step = [&]() -> int {
-            int a = -1;
-            float m = __int_as_float(0x7f800000);
-            if (step[0] != 0 && tm[0] < m) { a = 0; m = tm[0]; }
-            if (step[1] != 0 && tm[1] < m) { a = 1; m = tm[1]; }
-            if (step[2] != 0 && tm[2] < m) { a = 2; m = tm[2]; }
-            if (a == 0) { voxel[0] += step[0]; tm[0] += tdel[0]; }
-            else if (a == 1) { voxel[1] += step[1]; tm[1] += tdel[1]; }
-            else if (a == 2) { voxel[2] += step[2]; tm[2] += tdel[2]; }
-            return a;
-        };
-        while (steps_left > 0 && o1_in_solid(pa.w, voxel, o)) {
-            const int ax = argmin_step();
+        // phase 1: leave the solids the start voxel is in
+        while (steps_left > 0 && o1_in_solid(pa.w, s.voxel, o)) {
+            const int ax = o1_argmin_step(s);
             if (ax < 0) { dead = true; break; }
             last_axis = ax;
             steps_left--;
-            if (!o1_in_window(d, voxel, o)) { dead = true; break; }
+            if (!o1_in_window(d, s.voxel, o)) { dead = true; break; }
         }
         if (dead) break;
+        // phase 2: the first solid non-fringe voxel
         while (steps_left > 0) {
-            if (!o1_in_window(d, voxel, o)) break;
-            if (o1_in_solid(pa.w, voxel, o)) {
-                res.voxel[0] = voxel[0]; res.voxel[1] = voxel[1]; res.voxel[2] = voxel[2];
-                const int sa = last_axis == 0 ? step[0] : (last_axis == 1 ? step[1] : step[2]);
-                if (last_axis == 0) res.normal[0] = -sa;
-                else if (last_axis == 1) res.normal[1] = -sa;
-                else if (last_axis == 2) res.normal[2] = -sa;
+            if (!o1_in_window(d, s.voxel, o)) break;
+            if (o1_in_solid(pa.w, s.voxel, o)) {
+                res.voxel[0] = s.voxel[0]; res.voxel[1] = s.voxel[1]; res.voxel[2] = s.voxel[2];
+                o1_normal(s, last_axis, res);
                 found = 1;
                 break;
             }
-            const int ax = argmin_step();
+            const int ax = o1_argmin_step(s);
             if (ax < 0) break;
             last_axis = ax;
             steps_left--;
@@ -519,6 +539,95 @@ __global__ void __launch_bounds__(128) k_raycast(PickArgs pa, const float *__res
     } while (0);
     out[i] = res;
     hit[i] = found;
+}
+
+// One ray with a whole warp (the single-call pick, where one thread's chain
+// of dependent voxel loads is the latency).  The voxel sequence of the walk
+// depends on arithmetic only, so lane 0 emits the next 32 voxels with the
+// same argmin steps, every lane tests its voxel (window, solid) at once, and
+// lane 0 runs raycast.rs's two phases over the resulting bits: element k of
+// the walk is examined with 4096 - k steps left, a phase-1 step is followed
+// by the window test of the voxel it reaches.  At most 129 rounds.
+__global__ void __launch_bounds__(32) k_raycast_warp(PickArgs pa, const float *__restrict__ cams,
+                                                     const float *__restrict__ dirs, VxPickHit *out,
+                                                     int32_t *hit) {
+    constexpr unsigned FULL = 0xFFFFFFFFu;
+    __shared__ int32_t sv[32][4];   // voxel, axis of the step into it
+    const uint32_t lane = threadIdx.x;
+    const Dims &d = pa.w.d;
+    const int32_t *o = pa.origin;
+    const float cam[3] = {cams[0], cams[1], cams[2]};
+    const float din[3] = {dirs[0], dirs[1], dirs[2]};
+    VxPickHit res;
+    res.voxel[0] = res.voxel[1] = res.voxel[2] = 0;
+    res.normal[0] = res.normal[1] = res.normal[2] = 0;
+    int32_t found = 0;
+    O1State s;
+    if (o1_start(d, o, cam, din, s)) {   // same on every lane
+        bool alive = true;               // lane 0: the walk can still step
+        int la_next = -1;                // lane 0: axis of the step into the next voxel
+        int phase = 1;
+        bool post_check = false, done = false;
+        for (int32_t base = 0; base <= 4096 && !done; base += 32) {
+            uint32_t exist = 0;
+            if (lane == 0) {
+                for (int j = 0; j < 32 && alive; ++j) {
+                    sv[j][0] = s.voxel[0]; sv[j][1] = s.voxel[1]; sv[j][2] = s.voxel[2];
+                    sv[j][3] = la_next;
+                    exist |= 1u << j;
+                    const int ax = o1_argmin_step(s);
+                    if (ax < 0) alive = false;
+                    else la_next = ax;
+                }
+            }
+            exist = __shfl_sync(FULL, exist, 0);
+            __syncwarp();
+            bool inwin = false, solid = false;
+            if ((exist >> lane) & 1u) {
+                const int32_t v[3] = {sv[lane][0], sv[lane][1], sv[lane][2]};
+                inwin = o1_in_window(d, v, o);
+                solid = o1_in_solid(pa.w, v, o);
+            }
+            const unsigned win = __ballot_sync(FULL, inwin), sol = __ballot_sync(FULL, solid);
+            if (lane == 0) {
+                int j = 0;
+                while (j < 32 && !done) {
+                    const int32_t left = 4096 - (base + j);
+                    const bool next = j + 1 < 32 ? ((exist >> (j + 1)) & 1u) != 0u : alive;
+                    if (post_check) {
+                        post_check = false;
+                        if (!((win >> j) & 1u)) { done = true; break; }   // phase-1 step left the window
+                    }
+                    const bool is_solid = (sol >> j) & 1u;
+                    if (phase == 1) {
+                        if (left > 0 && is_solid) {
+                            if (!next) { done = true; break; }
+                            post_check = true;
+                            ++j;
+                            continue;
+                        }
+                        phase = 2;
+                    }
+                    if (left <= 0 || !((win >> j) & 1u)) { done = true; break; }
+                    if (is_solid) {
+                        res.voxel[0] = sv[j][0]; res.voxel[1] = sv[j][1]; res.voxel[2] = sv[j][2];
+                        o1_normal(s, sv[j][3], res);
+                        found = 1;
+                        done = true;
+                        break;
+                    }
+                    if (!next) { done = true; break; }
+                    ++j;
+                }
+            }
+            done = __shfl_sync(FULL, done ? 1 : 0, 0) != 0;
+            __syncwarp();
+        }
+    }
+    if (lane == 0) {
+        *out = res;
+        *hit = found;
+    }
 }
 
 // ------------------------------------------------------- temporal gating
@@ -784,6 +893,10 @@ cudaError_t launch_raycast(const DevWorld &w, const int32_t origin[3], const flo
     PickArgs pa;
     pa.w = w;
     pa.origin[0] = origin[0]; pa.origin[1] = origin[1]; pa.origin[2] = origin[2];
+    if (n == 1) {
+        k_raycast_warp<<<1, 32, 0, s>>>(pa, cams, dirs, out, hit);
+        return cudaGetLastError();
+    }
     const unsigned blocks = (unsigned)((n + 127) / 128);
     k_raycast<<<blocks, 128, 0, s>>>(pa, cams, dirs, n, out, hit);
     return cudaGetLastError();
