@@ -214,6 +214,14 @@ int vx_world_shift_origin(VxWorld *w, int32_t origin_cx, int32_t origin_cz,
 int vx_world_apply_edit(VxWorld *w, int32_t wx, int32_t wy, int32_t wz, uint8_t mat);
 /* Forget every recorded edit (the device world is left as it is). */
 int vx_world_clear_edits(VxWorld *w);
+/* Checkpoint of a device world in a .vxw file: the six arrays in voxelG's
+ * host layout, the edit log and the chunk generator's window state.  The
+ * reference keeps its world only as (seed, edit log); this dump restores a
+ * device world exactly, for debugging and resume.  vx_world_load requires
+ * a world of the same dims (VX_ERR_INVALID otherwise, and on a truncated
+ * or foreign file).  Both synchronous. */
+int vx_world_save(VxWorld *w, const char *path);
+int vx_world_load(VxWorld *w, const char *path);
 /* Incremental update from dirty bricks (renderer.rs:1345-1394): writes the
  * given bricks and recomputes the touched tile/chunk/L4 masks and uniform
  * LUT entries on the device (voxel.rs:879-946 semantics).  brick_idx and

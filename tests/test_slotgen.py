@@ -440,3 +440,42 @@ def test_full_size_generated_window_frame_bit_exact():
     assert np.array_equal(vg.shadows(sh).view(np.uint8), wsh.view(np.uint8))
     assert (got["flags"] & 1).mean() > 0.3
     dw.close()
+
+
+@pytest.mark.gpu
+def test_world_checkpoint_round_trip(tmp_path):
+    """vx_world_save / vx_world_load: a streamed, edited window restored into
+    a fresh world equals the original, and both stream on identically (edit
+    log and slot table come back too); wrong dims and truncated files are
+    rejected."""
+    _gpu()
+    import voxelg_b200 as vg
+    from voxelg_b200 import _lib as L
+    a = vg.DeviceWorld(*DEMO)
+    a.fill_window(SEED, 2, -1)
+    a.apply_edit(100, 90, 40, MAT_GLASS)
+    a.apply_edit(700, 95, 60, MAT_GLASS)    # outside the window for now
+    path = tmp_path / "w.vxw"
+    a.save(path)
+    b = vg.DeviceWorld(*DEMO)
+    b.load(path)
+
+    def same(x, y):
+        gx, gy = x.download(), y.download()
+        for k in po.World.NAMES:
+            assert np.array_equal(np.ascontiguousarray(gx[k]).view(np.uint8),
+                                  np.ascontiguousarray(gy[k]).view(np.uint8)), k
+    same(a, b)
+    assert a.shift_origin(8, 0) == b.shift_origin(8, 0) > 0
+    same(a, b)
+    assert _material_at_world(b, (8, 0), 700, 95, 60) == MAT_GLASS
+    small = vg.DeviceWorld(64, 64, 64)
+    with pytest.raises(L.VxError) as e:
+        small.load(path)
+    assert e.value.code == L.VX_ERR_INVALID
+    cut = tmp_path / "cut.vxw"
+    cut.write_bytes(path.read_bytes()[:100000])
+    with pytest.raises(L.VxError):
+        b.load(cut)
+    for w in (a, b, small):
+        w.close()

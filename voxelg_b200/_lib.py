@@ -151,6 +151,8 @@ SIGNATURES = [
     ("vx_world_shift_origin", C.c_int, [_vp, C.c_int32, C.c_int32, _P(C.c_uint32)]),
     ("vx_world_apply_edit", C.c_int, [_vp, C.c_int32, C.c_int32, C.c_int32, C.c_uint8]),
     ("vx_world_clear_edits", C.c_int, [_vp]),
+    ("vx_world_save", C.c_int, [_vp, C.c_char_p]),
+    ("vx_world_load", C.c_int, [_vp, C.c_char_p]),
     ("vx_world_apply_dirty", C.c_int, [_vp, _vp, _vp, C.c_size_t, _vp]),
     ("vx_world_counts", C.c_int, [_vp, _P(C.c_uint64)]),
     ("vx_world_set_tuning", C.c_int, [_vp, _P(VxTuning)]),

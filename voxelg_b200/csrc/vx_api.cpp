@@ -5,6 +5,7 @@
 #include <algorithm>
 #include <array>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -782,6 +783,133 @@ int vx_world_clear_edits(VxWorld *w) {
     }
     std::lock_guard<std::mutex> lk(w->mu);
     w->edits.clear();
+    return VX_OK;
+}
+
+namespace {
+// .vxw: "VXW1", u32 version, i32 dims[3], u64 counts[4], the six arrays in
+// voxelG's host layout, the edit log (u64 n, then i32 x, y, z + u8 mat each),
+// the chunk generator's state (u8 window, u64 seed, i32 origin[2], u64 n,
+// then n ints of the slot table).
+constexpr char kVxwMagic[4] = {'V', 'X', 'W', '1'};
+constexpr uint32_t kVxwVersion = 1;
+
+struct File {
+    FILE *f = nullptr;
+    ~File() {
+        if (f) fclose(f);
+    }
+};
+bool put(FILE *f, const void *p, size_t n) { return n == 0 || fwrite(p, 1, n, f) == n; }
+bool get(FILE *f, void *p, size_t n) { return n == 0 || fread(p, 1, n, f) == n; }
+}  // namespace
+
+int vx_world_save(VxWorld *w, const char *path) {
+    if (!w || !path) {
+        vx::set_error("vx_world_save: null argument");
+        return VX_ERR_INVALID;
+    }
+    const vx::Dims d = w->dw.d;
+    std::vector<VxBrick> bricks((size_t)d.n_bricks);
+    std::vector<uint64_t> tm((size_t)d.n_tiles), cm((size_t)d.n_chunks), lm((size_t)d.n_l4);
+    std::vector<uint8_t> bu((size_t)d.n_bricks), tu((size_t)d.n_tiles);
+    int rc = vx_world_download(w, bricks.data(), tm.data(), cm.data(), lm.data(), bu.data(),
+                               tu.data());
+    if (rc != VX_OK) return rc;
+    std::lock_guard<std::mutex> lk(w->mu);
+    File out;
+    out.f = fopen(path, "wb");
+    if (!out.f) {
+        vx::set_error(std::string("vx_world_save: cannot open ") + path);
+        return VX_ERR_INVALID;
+    }
+    const int32_t dims[3] = {d.bx, d.by, d.bz};
+    const uint64_t counts[4] = {(uint64_t)d.n_bricks, (uint64_t)d.n_tiles, (uint64_t)d.n_chunks,
+                                (uint64_t)d.n_l4};
+    bool ok = put(out.f, kVxwMagic, 4) && put(out.f, &kVxwVersion, 4) && put(out.f, dims, 12) &&
+              put(out.f, counts, 32) && put(out.f, bricks.data(), bricks.size() * sizeof(VxBrick)) &&
+              put(out.f, tm.data(), tm.size() * 8) && put(out.f, cm.data(), cm.size() * 8) &&
+              put(out.f, lm.data(), lm.size() * 8) && put(out.f, bu.data(), bu.size()) &&
+              put(out.f, tu.data(), tu.size());
+    const uint64_t ne = w->edits.size();
+    ok = ok && put(out.f, &ne, 8);
+    for (const auto &e : w->edits) ok = ok && put(out.f, e.first.data(), 12) && put(out.f, &e.second, 1);
+    const uint8_t win = w->gen_window ? 1 : 0;
+    const uint64_t ns = w->slot_chunk.size();
+    ok = ok && put(out.f, &win, 1) && put(out.f, &w->gen_seed, 8) && put(out.f, w->gen_origin, 8) &&
+         put(out.f, &ns, 8) && put(out.f, w->slot_chunk.data(), ns * 4);
+    ok = ok && fflush(out.f) == 0;
+    if (!ok) {
+        vx::set_error(std::string("vx_world_save: write failed: ") + path);
+        return VX_ERR_INVALID;
+    }
+    return VX_OK;
+}
+
+int vx_world_load(VxWorld *w, const char *path) {
+    if (!w || !path) {
+        vx::set_error("vx_world_load: null argument");
+        return VX_ERR_INVALID;
+    }
+    const vx::Dims d = w->dw.d;
+    File in;
+    in.f = fopen(path, "rb");
+    if (!in.f) {
+        vx::set_error(std::string("vx_world_load: cannot open ") + path);
+        return VX_ERR_INVALID;
+    }
+    char magic[4];
+    uint32_t version = 0;
+    int32_t dims[3];
+    uint64_t counts[4];
+    if (!get(in.f, magic, 4) || std::memcmp(magic, kVxwMagic, 4) != 0 || !get(in.f, &version, 4) ||
+        version != kVxwVersion || !get(in.f, dims, 12) || !get(in.f, counts, 32)) {
+        vx::set_error(std::string("vx_world_load: not a .vxw file of this version: ") + path);
+        return VX_ERR_INVALID;
+    }
+    if (dims[0] != d.bx || dims[1] != d.by || dims[2] != d.bz ||
+        counts[0] != (uint64_t)d.n_bricks || counts[1] != (uint64_t)d.n_tiles ||
+        counts[2] != (uint64_t)d.n_chunks || counts[3] != (uint64_t)d.n_l4) {
+        vx::set_error("vx_world_load: the file's world dims differ from this world's");
+        return VX_ERR_INVALID;
+    }
+    std::vector<VxBrick> bricks((size_t)d.n_bricks);
+    std::vector<uint64_t> tm((size_t)d.n_tiles), cm((size_t)d.n_chunks), lm((size_t)d.n_l4);
+    std::vector<uint8_t> bu((size_t)d.n_bricks), tu((size_t)d.n_tiles);
+    bool ok = get(in.f, bricks.data(), bricks.size() * sizeof(VxBrick)) &&
+              get(in.f, tm.data(), tm.size() * 8) && get(in.f, cm.data(), cm.size() * 8) &&
+              get(in.f, lm.data(), lm.size() * 8) && get(in.f, bu.data(), bu.size()) &&
+              get(in.f, tu.data(), tu.size());
+    uint64_t ne = 0;
+    ok = ok && get(in.f, &ne, 8) && ne <= ((uint64_t)1 << 32);
+    std::map<std::array<int32_t, 3>, uint8_t> edits;
+    for (uint64_t i = 0; ok && i < ne; ++i) {
+        std::array<int32_t, 3> k;
+        uint8_t m = 0;
+        ok = get(in.f, k.data(), 12) && get(in.f, &m, 1);
+        edits[k] = m;
+    }
+    uint8_t win = 0;
+    uint64_t seed = 0, ns = 0;
+    int32_t origin[2] = {0, 0};
+    ok = ok && get(in.f, &win, 1) && get(in.f, &seed, 8) && get(in.f, origin, 8) &&
+         get(in.f, &ns, 8) && (ns == 0 || ns == (uint64_t)(d.bx / 8) * (d.by / 8) * (d.bz / 8) * 3);
+    std::vector<int32_t> slots((size_t)(ok ? ns : 0));
+    ok = ok && get(in.f, slots.data(), slots.size() * 4);
+    if (!ok) {
+        vx::set_error(std::string("vx_world_load: truncated or inconsistent file: ") + path);
+        return VX_ERR_INVALID;
+    }
+    int rc = vx_world_upload(w, bricks.data(), tm.data(), cm.data(), lm.data(), bu.data(),
+                             tu.data());
+    if (rc != VX_OK) return rc;
+    std::lock_guard<std::mutex> lk(w->mu);
+    w->edits = std::move(edits);
+    w->gen_window = win != 0;
+    w->gen_seed = seed;
+    w->gen_origin[0] = origin[0];
+    w->gen_origin[1] = origin[1];
+    w->slot_chunk = std::move(slots);
     return VX_OK;
 }
 

@@ -139,6 +139,15 @@ class DeviceWorld:
     def clear_edits(self):
         L.check(self._lib.vx_world_clear_edits(self.handle))
 
+    def save(self, path):
+        """Checkpoint the device world (arrays, edit log, window state) to a
+        .vxw file."""
+        L.check(self._lib.vx_world_save(self.handle, str(path).encode()))
+
+    def load(self, path):
+        """Restore a .vxw checkpoint into this world (same dims)."""
+        L.check(self._lib.vx_world_load(self.handle, str(path).encode()))
+
     def gen_chunks(self, seed: int, chunks):
         """Generate the given world chunks ((x, y, z) rows) into their slots."""
         c = np.ascontiguousarray(np.asarray(chunks, dtype=np.int32).reshape(-1, 3))
