@@ -605,3 +605,72 @@ def test_single_call_pick_matches_o1(vg, dev_c1, c1_oracle_world):
         if whit[i] and np.abs(np.array(want[i]["voxel"], np.float64) - cams[i]).sum() > 64:
             long_walks += 1
     assert 0.2 < whit.mean() < 0.95 and long_walks > 50
+
+
+def test_rebuild_in_place_grow_shrink_stream(vg):
+    """accel.rs:761-835 (accel_rebuild_in_place_matches_cpu): a 3x3 pillar
+    raised on the flat floor through the edit path, removed again, then a
+    streamed window origin.  After each in-place update the device arrays
+    equal the oracle's, the probe rays' records and picks equal the
+    oracle's, and the removed pillar leaves nothing behind."""
+    from scenes import MAT_STONE, flat_floor, normalize
+    ow = flat_floor(8, 8, 56)
+    dw = upload_oracle(vg, ow)
+    p = vg.default_params(METHOD)
+
+    def probe(world, eyes, d, wo=(0, 0, 0)):
+        rays = np.zeros(len(eyes), po.RAY)
+        rays["org"] = np.asarray(eyes, np.float32) + np.asarray(wo, np.float32)
+        rays["dir"] = d
+        rays["tmax"] = 700.0
+        got = vg.records(vg.trace(dw, rays, p, origin=wo))
+        assert_same_records(got, po.trace_batch(world, rays, p, origin=wo)[0])
+        dirs = np.tile(np.asarray(d, np.float32), (len(eyes), 1))
+        picks, hits = vg.raycast_batch(dw, rays["org"], dirs, origin=wo)
+        wpicks, whits, _ = po.raycast_batch(world, rays["org"], dirs, origin=wo)
+        assert np.array_equal(hits, whits)
+        assert np.array_equal(picks.view(np.uint8), wpicks.view(np.uint8))
+        return got, picks, hits
+
+    def world_equal(world):
+        got = dw.download()
+        for k in po.World.NAMES:
+            assert np.array_equal(got[k].view(np.uint8), world.a[k].view(np.uint8)), k
+
+    pillar = [(30 + dx, y, 30 + dz) for y in range(61, 75) for dz in range(3) for dx in range(3)]
+    eyes = [(20.0, 70.0, 31.5), (20.0, 62.5, 30.2), (20.0, 74.9, 32.9), (20.0, 75.1, 31.0)]
+    # grow in place
+    for x, y, z in pillar:
+        dw.apply_edit(x, y, z, MAT_STONE)
+        ow.set_voxel(x, y, z, MAT_STONE)
+    world_equal(ow)
+    rec, picks, hits = probe(ow, eyes, (1.0, 0.0, 0.0))
+    assert hits[:3].all() and not hits[3]
+    assert tuple(picks[0]["voxel"]) == (30, 70, 31) and tuple(picks[0]["normal"]) == (-1, 0, 0)
+    assert (rec["flags"][:3] & 1).all()
+    # shrink in place: the same rays sail over the floor and miss
+    for x, y, z in pillar:
+        dw.apply_edit(x, y, z, 0)
+        ow.set_voxel(x, y, z, 0)
+    world_equal(ow)
+    rec, picks, hits = probe(ow, eyes, (1.0, 0.0, 0.0))
+    assert not hits.any() and not (rec["flags"] & 1).any()
+    # streamed: a generated window shifted by (2, 3) chunks
+    dw.clear_edits()
+    seed = 0xC0FFEE_F00D_BEEF
+    dw.fill_window(seed, 0, 0)
+    dw.shift_origin(2, 3)
+    sw = po.World(*ow.dims)
+    po.fill_window(sw, seed, 2, 3)
+    world_equal(sw)
+    wo = (64, 0, 96)
+    rng = np.random.default_rng(3)
+    eyes = np.concatenate([[(40.0, 140.0, 40.0)],
+                           rng.uniform([8, 100, 8], [500, 200, 500], (63, 3))]).astype(np.float32)
+    rec, picks, hits = probe(sw, eyes, normalize((0.001, -1.0, 0.001)), wo)
+    assert hits.mean() > 0.9
+    cam = vg.camera_from_pose((200.0 + wo[0], 150.0, 300.0 + wo[2]), 0.7, -0.5, 1.2, 96, 54,
+                              world_origin=wo)
+    got = vg.render_primary(dw, cam, p)[0]
+    assert_same_records(vg.records(got), po.render_frame(sw, cam, p)[0], "streamed")
+    dw.close()
