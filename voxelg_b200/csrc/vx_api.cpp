@@ -124,6 +124,7 @@ void free_world(VxWorld *w) {
     cudaFree(w->dw.l4_mask);
     cudaFree(w->dw.brick_uniform);
     cudaFree(w->dw.tile_uniform);
+    cudaFree(w->dw.tile_meta);
     cudaFree(w->beam);
     cudaFree(w->d_idx);
     cudaFree(w->d_bricks);
@@ -320,6 +321,7 @@ int vx_world_create(const VxWorldDesc *desc, VxWorld **out) {
     VX_CKW(cudaMalloc(&w->dw.l4_mask, d.n_l4 * sizeof(uint64_t)));
     VX_CKW(cudaMalloc(&w->dw.brick_uniform, d.n_bricks));
     VX_CKW(cudaMalloc(&w->dw.tile_uniform, d.n_tiles));
+    VX_CKW(cudaMalloc(&w->dw.tile_meta, d.n_tiles * sizeof(uint16_t)));
     VX_CKW(cudaMalloc(&w->d_stats, 4 * sizeof(unsigned long long)));
     VX_CKW(cudaMalloc(&w->d_work, 2 * sizeof(uint32_t)));
     VX_CKW(cudaMemsetAsync(w->d_work, 0, 2 * sizeof(uint32_t), w->stream));
@@ -333,6 +335,7 @@ int vx_world_create(const VxWorldDesc *desc, VxWorld **out) {
     VX_CKW(cudaMemsetAsync(w->dw.l4_mask, 0, d.n_l4 * sizeof(uint64_t), w->stream));
     VX_CKW(cudaMemsetAsync(w->dw.brick_uniform, 0, d.n_bricks, w->stream));
     VX_CKW(cudaMemsetAsync(w->dw.tile_uniform, 0, d.n_tiles, w->stream));
+    VX_CKW(vx::launch_tile_meta(w->dw, w->stream));
     VX_CKW(cudaStreamSynchronize(w->stream));
 #undef VX_CKW
     *out = w;
@@ -400,6 +403,7 @@ int vx_world_upload(VxWorld *w, const VxBrick *bricks, const uint64_t *tile_mask
     VX_CK(cudaMemcpyAsync(w->dw.l4_mask, l4_mask, d.n_l4 * 8, cudaMemcpyHostToDevice, w->stream));
     VX_CK(cudaMemcpyAsync(w->dw.brick_uniform, brick_uniform, d.n_bricks, cudaMemcpyHostToDevice, w->stream));
     VX_CK(cudaMemcpyAsync(w->dw.tile_uniform, tile_uniform, d.n_tiles, cudaMemcpyHostToDevice, w->stream));
+    VX_CK(vx::launch_tile_meta(w->dw, w->stream));
     VX_CK(cudaStreamSynchronize(w->stream));
     return VX_OK;
 }

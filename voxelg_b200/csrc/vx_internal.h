@@ -59,6 +59,11 @@ struct DevWorld {
     uint64_t *l4_mask;        // n_l4
     uint8_t *brick_uniform;   // n_bricks
     uint8_t *tile_uniform;    // n_tiles
+    // n_tiles, derived from the masks above by launch_tile_meta: what the
+    // walk's L4 and chunk tests decide for every voxel of a tile, beside the
+    // tile LUT byte (layout in vx_walk.cuh at kMetaChunkOnly).  nullptr for caller-owned worlds: the
+    // walk then evaluates the tests from the masks.
+    uint16_t *tile_meta;
 };
 
 // Per-frame constants of the traversal kernels (passed by value).
@@ -132,6 +137,8 @@ cudaError_t launch_gen_slots(const DevWorld &w, uint64_t seed, const GenPlan &p,
 cudaError_t launch_generate(const DevWorld &w, const VxTerrainParams &t, int16_t *heights,
                             cudaStream_t s);
 cudaError_t launch_rebuild_pyramid(const DevWorld &w, cudaStream_t s);
+// tile_meta of every tile from the masks and the tile LUT
+cudaError_t launch_tile_meta(const DevWorld &w, cudaStream_t s);
 // Persistent edits: ed[i] = {brick, voxel | material << 8}, distinct voxels;
 // idx the distinct bricks they touch (uniform bytes and masks refreshed).
 cudaError_t launch_edits(const DevWorld &w, const uint2 *ed, size_t n_edits, const uint32_t *idx,

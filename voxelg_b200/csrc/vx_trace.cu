@@ -790,9 +790,38 @@ __global__ void __launch_bounds__(128) k_ao(DevWorld w, VxCamera c,
     ao[idx] = r;
 }
 
+// DevWorld::tile_meta of tile ti (layout at kMetaChunkOnly): the L4 and
+// chunk tests (raymarch.wgsl:4648-4668) as trace evaluates them at any voxel
+// of the tile, beside the tile LUT byte.
+__global__ void k_tile_meta(DevWorld w) {
+    const int64_t ti = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const Dims &d = w.d;
+    if (ti >= d.n_tiles) return;
+    const int32_t tx = (int32_t)(ti % d.tx);
+    const int32_t ty = (int32_t)((ti / d.tx) % d.ty);
+    const int32_t tz = (int32_t)(ti / ((int64_t)d.tx * d.ty));
+    const int32_t cx = tx >> 2, cy = ty >> 2, cz = tz >> 2;
+    const uint64_t lw =
+        w.l4_mask[(cx >> 2) + (int64_t)(cy >> 2) * d.lx + (int64_t)(cz >> 2) * d.lx * d.ly];
+    const uint64_t cw = w.chunk_mask[cx + (int64_t)cy * d.cx + (int64_t)cz * d.cx * d.cy];
+    const bool tile_clear = !bit64(cw, child_bit(tx & 3, ty & 3, tz & 3));
+    uint32_t code = 0u;
+    if (lw == 0ull) code = 3u;
+    else if (!bit64(lw, child_bit(cx & 3, cy & 3, cz & 3))) code = 2u;
+    else if (tile_clear) code = 1u;
+    w.tile_meta[ti] =
+        (uint16_t)((uint32_t)w.tile_uniform[ti] | (code << 8) | (tile_clear ? kMetaChunkOnly : 0u));
+}
+
 }  // namespace
 
 // ------------------------------------------------------------- launchers
+cudaError_t launch_tile_meta(const DevWorld &w, cudaStream_t s) {
+    if (!w.tile_meta) return cudaGetLastError();
+    k_tile_meta<<<(unsigned)((w.d.n_tiles + 255) / 256), 256, 0, s>>>(w);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_ao(const DevWorld &w, const VxCamera &cam, const VxHitRecord *rec, float *ao,
                       cudaStream_t s) {
     const uint32_t W = (uint32_t)cam.res_x, H = (uint32_t)cam.res_y;

@@ -325,6 +325,16 @@ __device__ __forceinline__ int child_of(uint32_t sx, uint32_t sy, uint32_t sz, i
     return (int)(((sx >> sh) & 3u) + ((sz >> sh) & 3u) * 4u + ((sy >> sh) & 3u) * 16u);
 }
 
+// ------------------------------------------------------------ tile meta
+// DevWorld::tile_meta word.  Every voxel of a tile shares the tile's chunk
+// and L4 cell, so trace's L4 and chunk tests (raymarch.wgsl:4648-4668) have
+// one outcome per tile:
+//   bits 0-7   the tile LUT byte
+//   bits 8-9   the cell the L4 and chunk tests skip: 0 none, 1 the 16-voxel
+//              tile, 2 the 64-voxel chunk, 3 the 256-voxel L4 cell
+//   bit 10     the chunk test alone skips the tile (walks without L4)
+constexpr uint32_t kMetaChunkOnly = 1u << 10;
+
 // ------------------------------------------------------------------ walk
 // One traversal = dda_init + repeated cascade iterations.  The three kinds
 // share the level cascade and differ only where the reference differs:
@@ -398,20 +408,34 @@ __device__ __forceinline__ int walk_step(const DevWorld &w, const Geo &g, const 
     const uint32_t sy = (uint32_t)s.vy;
     const uint32_t ti = tile_index(g, sx, sy, sz);
     // batch 1: every coarse word addressed by the slot coordinate
-    uint64_t lw = ~0ull;
-    if (use_l4) lw = ldg(w.l4_mask + l4_index(g, sx, sy, sz));
-    const uint64_t cw = ldg(w.chunk_mask + chunk_index(g, sx, sy, sz));
     const uint64_t tw = ldg(w.tile_mask + ti);
-    const uint32_t tum = f_lut ? (uint32_t)ldg(w.tile_uniform + ti) : 0u;
+    uint32_t tum;
     int32_t cell = 0;
-    if (use_l4) {
-        if (STATS) bytes += 8;
-        if (lw == 0ull) cell = 256;
-        else if (!bit64(lw, child_of(sx, sy, sz, 6))) cell = 64;
-    }
-    if (cell == 0) {
-        if (STATS) bytes += 8;
-        if (!bit64(cw, child_of(sx, sy, sz, 4))) cell = 16;
+    if (w.tile_meta != nullptr) {
+        const uint32_t meta = ldg(w.tile_meta + ti);
+        tum = f_lut ? (meta & 0xFFu) : 0u;
+        if (use_l4) {
+            const uint32_t code = (meta >> 8) & 3u;
+            if (STATS) bytes += code >= 2u ? 8 : 16;
+            if (code != 0u) cell = 4 << (2 * code);
+        } else {
+            if (STATS) bytes += 8;
+            if ((meta & kMetaChunkOnly) != 0u) cell = 16;
+        }
+    } else {
+        uint64_t lw = ~0ull;
+        if (use_l4) lw = ldg(w.l4_mask + l4_index(g, sx, sy, sz));
+        const uint64_t cw = ldg(w.chunk_mask + chunk_index(g, sx, sy, sz));
+        tum = f_lut ? (uint32_t)ldg(w.tile_uniform + ti) : 0u;
+        if (use_l4) {
+            if (STATS) bytes += 8;
+            if (lw == 0ull) cell = 256;
+            else if (!bit64(lw, child_of(sx, sy, sz, 6))) cell = 64;
+        }
+        if (cell == 0) {
+            if (STATS) bytes += 8;
+            if (!bit64(cw, child_of(sx, sy, sz, 4))) cell = 16;
+        }
     }
     if (cell == 0) {
         // tile-level LOD (raymarch.wgsl:4672-4689)

@@ -302,7 +302,7 @@ cudaError_t launch_edits(const DevWorld &w, const uint2 *ed, size_t n_edits, con
     k_dirty_tiles<<<b, 128, 0, s>>>(w, idx, n_bricks);
     k_dirty_chunks<<<b, 128, 0, s>>>(w, idx, n_bricks);
     k_dirty_l4<<<b, 128, 0, s>>>(w, idx, n_bricks);
-    return cudaGetLastError();
+    return launch_tile_meta(w, s);
 }
 
 cudaError_t launch_bricks_from_aos(const DevWorld &w, const VxBrick *aos, int64_t first,
@@ -323,8 +323,10 @@ cudaError_t launch_rebuild_pyramid(const DevWorld &w, cudaStream_t s) {
     k_build_tiles<<<blocks_for(w.d.n_tiles, 128), 128, 0, s>>>(w);
     k_build_chunks<<<blocks_for(w.d.n_chunks, 128), 128, 0, s>>>(w);
     k_build_l4<<<blocks_for(w.d.n_l4, 128), 128, 0, s>>>(w);
-    return cudaGetLastError();
+    return launch_tile_meta(w, s);
 }
+
+
 
 cudaError_t launch_generate(const DevWorld &w, const VxTerrainParams &t, int16_t *heights,
                             cudaStream_t s) {
@@ -350,7 +352,7 @@ cudaError_t launch_apply_dirty(const DevWorld &w, const uint32_t *idx, const VxB
     k_dirty_tiles<<<b, 128, 0, s>>>(w, idx, n);
     k_dirty_chunks<<<b, 128, 0, s>>>(w, idx, n);
     k_dirty_l4<<<b, 128, 0, s>>>(w, idx, n);
-    return cudaGetLastError();
+    return launch_tile_meta(w, s);
 }
 
 }  // namespace vx
