@@ -465,9 +465,22 @@ def test_world_checkpoint_round_trip(tmp_path):
         for k in po.World.NAMES:
             assert np.array_equal(np.ascontiguousarray(gx[k]).view(np.uint8),
                                   np.ascontiguousarray(gy[k]).view(np.uint8)), k
+    def same_frame(x, y, wo):
+        # the restored world traces like the original (its derived per-tile
+        # words included)
+        cam = vg.camera_from_pose((wo[0] + 256.0, 150.0, wo[2] + 256.0), 0.5, -0.4, 1.2, 128, 72,
+                                  world_origin=wo)
+        p = vg.default_params(po.OR_F_L4 | po.OR_F_LUT | po.OR_F_LOD | po.OR_F_BEAM | po.OR_F_SHADOW)
+        rx, sx = vg.render_primary(x, cam, p)
+        ry, sy = vg.render_primary(y, cam, p)
+        assert np.array_equal(vg.records(rx).view(np.uint8), vg.records(ry).view(np.uint8))
+        assert np.array_equal(vg.shadows(sx).view(np.uint8), vg.shadows(sy).view(np.uint8))
+        assert (vg.records(rx)["flags"] & 1).mean() > 0.3
     same(a, b)
+    same_frame(a, b, (64, 0, -32))
     assert a.shift_origin(8, 0) == b.shift_origin(8, 0) > 0
     same(a, b)
+    same_frame(a, b, (256, 0, 0))
     assert _material_at_world(b, (8, 0), 700, 95, 60) == MAT_GLASS
     small = vg.DeviceWorld(64, 64, 64)
     with pytest.raises(L.VxError) as e:
