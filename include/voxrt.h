@@ -269,7 +269,8 @@ int vx_render_primary(VxWorld *w, const VxCamera *cam, const VxTraceParams *p,
 int vx_render_ao(VxWorld *w, const VxCamera *cam, const VxHitRecord *rec_dev, float *ao_dev,
                  void *stream);
 /* Same frame through host buffers: the records are copied to rec_host /
- * shadow_host (pinned memory recommended) before the call returns. */
+ * shadow_host (pinned memory recommended) before the call returns.  The
+ * frame renders in four row bands, each copied while the next renders. */
 int vx_render_primary_host(VxWorld *w, const VxCamera *cam, const VxTraceParams *p,
                            VxHitRecord *rec_host, VxShadowRecord *shadow_host);
 /* The same, for frame pipelines: enqueues the frame and returns.  Its
@@ -277,7 +278,9 @@ int vx_render_primary_host(VxWorld *w, const VxCamera *cam, const VxTraceParams 
  * until then the caller must neither read nor free those buffers (pinned
  * memory, for the copies to overlap).  Frames alternate between two device
  * buffers, so frame N+1's traversal overlaps frame N's copies to the host,
- * and the copies of successive frames land in call order. */
+ * and the copies of successive frames land in call order.  Each frame is
+ * copied whole (one copy per buffer): in a pipeline, fewer copies are
+ * faster than bands. */
 int vx_render_primary_host_async(VxWorld *w, const VxCamera *cam, const VxTraceParams *p,
                                  VxHitRecord *rec_host, VxShadowRecord *shadow_host);
 /* Waits until every frame enqueued by vx_render_primary_host_async has
