@@ -585,7 +585,7 @@ def run_ours(args, cfg):
     for i in range(3):
         vg.render_primary_host_async(dw, cam, params, rec_np[i & 1], sh_np[i & 1])
     vg.render_host_wait(dw)
-    e2e_steps = max(10, min(args.steps, 100))
+    e2e_steps = max(40, min(args.steps, 200))   # PCIe-bound: a longer sample steadies it
     barrier(world)
     torch.cuda.synchronize(device)
     t1 = time.perf_counter()
