@@ -228,6 +228,17 @@ int vx_world_load(VxWorld *w, const char *path);
  * bricks are host arrays of n entries; duplicates allowed (last wins). */
 int vx_world_apply_dirty(VxWorld *w, const uint32_t *brick_idx, const VxBrick *bricks,
                          size_t n, void *stream);
+/* The checked library.  libvoxrt_checked.so is built from the same sources
+ * with every world-array load of the traversal compared with the array's
+ * length first (a stand-in for a memory checker).  A bad index is not read:
+ * the load returns 0 and the first such index is kept in a per-world word,
+ * array id << 56 | index (ids: 1 L4 mask, 2 chunk mask, 3 tile mask,
+ * 4 tile skip word, 5 tile LUT, 6 occupancy, 7 brick LUT, 8 materials).
+ * vx_checked_build returns 1 in the checked library and 0 in libvoxrt.so,
+ * whose word stays 0.  vx_world_oob waits for the device, reads the word
+ * (0 = no bad index) and clears it when `clear` is nonzero. */
+int vx_checked_build(void);
+int vx_world_oob(VxWorld *w, uint64_t *word, int32_t clear);
 /* Counts of each array: bricks, tiles, chunks, l4 cells. */
 int vx_world_counts(const VxWorld *w, uint64_t counts[4]);
 

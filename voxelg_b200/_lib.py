@@ -8,11 +8,15 @@ VX_ERR_CUDA when no GPU is usable.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from pathlib import Path
 
 import numpy as np
 
-LIB_PATH = Path(__file__).resolve().parent / "lib" / "libvoxrt.so"
+# VOXRT_CHECKED=1 loads the checked library (every world load bounds-checked,
+# see vx_world_oob) instead of libvoxrt.so.
+LIB_PATH = Path(__file__).resolve().parent / "lib" / (
+    "libvoxrt_checked.so" if os.environ.get("VOXRT_CHECKED") == "1" else "libvoxrt.so")
 
 VX_OK = 0
 VX_ERR_INVALID = -1
@@ -155,6 +159,8 @@ SIGNATURES = [
     ("vx_world_load", C.c_int, [_vp, C.c_char_p]),
     ("vx_world_apply_dirty", C.c_int, [_vp, _vp, _vp, C.c_size_t, _vp]),
     ("vx_world_counts", C.c_int, [_vp, _P(C.c_uint64)]),
+    ("vx_checked_build", C.c_int, []),
+    ("vx_world_oob", C.c_int, [_vp, _P(C.c_uint64), C.c_int32]),
     ("vx_world_set_tuning", C.c_int, [_vp, _P(VxTuning)]),
     ("vx_world_get_tuning", C.c_int, [_vp, _P(VxTuning)]),
     ("vx_raycast", C.c_int, [_vp, _P(C.c_float), _P(C.c_float), _P(C.c_int32), _P(VxPickHit)]),
@@ -234,7 +240,7 @@ def load() -> C.CDLL:
     if _lib is not None:
         return _lib
     if not LIB_PATH.exists():
-        raise ImportError(f"libvoxrt.so not built at {LIB_PATH}; run python -m voxelg_b200.build")
+        raise ImportError(f"{LIB_PATH.name} not built at {LIB_PATH}; run python -m voxelg_b200.build")
     lib = C.CDLL(str(LIB_PATH))
     for name, res, args in SIGNATURES:
         fn = getattr(lib, name)

@@ -1,12 +1,15 @@
 """Build libvoxrt.so in-tree with nvcc for sm_100a.
 
-Usage: python -m voxelg_b200.build [--force]
+Usage: python -m voxelg_b200.build [--force] [--no-checked]
 
 The traversal and world kernels are compiled with --fmad=false and IEEE
 divide/sqrt so that every float operation is a single IEEE binary32
 operation in the reference's order (hit records must be bit-exact against
 the CPU restatement).  Objects go to voxelg_b200/_build/, the library to
-voxelg_b200/lib/libvoxrt.so.
+voxelg_b200/lib/libvoxrt.so.  The checked library (VX_CHECKED: every
+world-array load of the traversal bounds-checked, vx_world_oob) is built
+beside it from the same sources, objects in voxelg_b200/_build/checked/.
+Translation units compile in parallel.
 """
 from __future__ import annotations
 
@@ -14,6 +17,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
@@ -21,6 +25,7 @@ ROOT = PKG.parent
 CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = PKG / "lib" / "libvoxrt.so"
+LIB_CHECKED = PKG / "lib" / "libvoxrt_checked.so"
 INCLUDE = ROOT / "include"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -61,35 +66,47 @@ def _newer(src: Path, dst: Path, deps: list[Path]) -> bool:
     return any(p.stat().st_mtime > t for p in [src, *deps])
 
 
-def build(force: bool = False, verbose: bool = False) -> Path:
-    BUILD.mkdir(exist_ok=True)
-    LIB.parent.mkdir(exist_ok=True)
+def _build_lib(build_dir: Path, lib: Path, defines: list[str], force: bool,
+               verbose: bool) -> Path:
+    build_dir.mkdir(parents=True, exist_ok=True)
+    lib.parent.mkdir(exist_ok=True)
     headers = list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + list(INCLUDE.glob("*.h"))
-    objs = []
-    changed = force
+    objs, cmds = [], []
     for name, extra in SOURCES:
         src = CSRC / name
-        obj = BUILD / (name + ".o")
+        obj = build_dir / (name + ".o")
         objs.append(obj)
         if force or _newer(src, obj, headers):
-            cmd = [nvcc(), *ARCH, *COMMON, *extra, "-c", str(src), "-o", str(obj)]
-            if name.endswith(".cpp"):
-                cmd = [nvcc(), "-x", "cu", *ARCH, *COMMON, *extra, "-c", str(src), "-o", str(obj)]
-            if verbose:
-                print(" ".join(cmd), flush=True)
-            subprocess.run(cmd, check=True)
-            changed = True
-    if changed or not LIB.exists():
-        tmp = LIB.with_suffix(".so.tmp")
-        cmd = [nvcc(), *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-lcudart_static",
-               "-Xlinker", "--no-undefined", "-lpthread", "-ldl", "-lrt"]
+            lang = ["-x", "cu"] if name.endswith(".cpp") else []
+            cmds.append([nvcc(), *lang, *ARCH, *COMMON, *defines, *extra, "-c", str(src),
+                         "-o", str(obj)])
+
+    def run(cmd):
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
-        os.replace(tmp, LIB)
+
+    if cmds:
+        with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+            list(ex.map(run, cmds))
+    if cmds or not lib.exists():
+        tmp = lib.with_suffix(".so.tmp")
+        run([nvcc(), *ARCH, "-shared", "-o", str(tmp), *map(str, objs), "-lcudart_static",
+             "-Xlinker", "--no-undefined", "-lpthread", "-ldl", "-lrt"])
+        os.replace(tmp, lib)
+    return lib
+
+
+def build(force: bool = False, verbose: bool = False, checked: bool = True) -> Path:
+    """libvoxrt.so, and the checked library beside it unless checked=False."""
+    jobs = [(BUILD, LIB, [])]
+    if checked:
+        jobs.append((BUILD / "checked", LIB_CHECKED, ["-DVX_CHECKED=1"]))
+    with ThreadPoolExecutor(max_workers=len(jobs)) as ex:
+        list(ex.map(lambda j: _build_lib(*j, force, verbose), jobs))
     return LIB
 
 
 if __name__ == "__main__":
-    build(force="--force" in sys.argv, verbose=True)
+    build(force="--force" in sys.argv, verbose=True, checked="--no-checked" not in sys.argv)
     print(LIB)

@@ -131,6 +131,7 @@ void free_world(VxWorld *w) {
     cudaFree(w->dw.brick_uniform);
     cudaFree(w->dw.tile_uniform);
     cudaFree(w->dw.tile_meta);
+    cudaFree(w->dw.oob);
     cudaFree(w->beam);
     cudaFree(w->d_idx);
     cudaFree(w->d_bricks);
@@ -328,6 +329,8 @@ int vx_world_create(const VxWorldDesc *desc, VxWorld **out) {
     VX_CKW(cudaMalloc(&w->dw.brick_uniform, d.n_bricks));
     VX_CKW(cudaMalloc(&w->dw.tile_uniform, d.n_tiles));
     VX_CKW(cudaMalloc(&w->dw.tile_meta, d.n_tiles * sizeof(uint16_t)));
+    VX_CKW(cudaMalloc(&w->dw.oob, sizeof(unsigned long long)));
+    VX_CKW(cudaMemsetAsync(w->dw.oob, 0, sizeof(unsigned long long), w->stream));
     VX_CKW(cudaMalloc(&w->d_stats, 4 * sizeof(unsigned long long)));
     VX_CKW(cudaMalloc(&w->d_work, 2 * sizeof(uint32_t)));
     VX_CKW(cudaMemsetAsync(w->d_work, 0, 2 * sizeof(uint32_t), w->stream));
@@ -765,6 +768,31 @@ int vx_world_shift_origin(VxWorld *w, int32_t origin_cx, int32_t origin_cz,
     w->gen_origin[0] = origin_cx;
     w->gen_origin[1] = origin_cz;
     if (n_regenerated) *n_regenerated = (uint32_t)(chunks.size() / 3);
+    return VX_OK;
+}
+
+int vx_checked_build(void) {
+#ifdef VX_CHECKED
+    return 1;
+#else
+    return 0;
+#endif
+}
+
+int vx_world_oob(VxWorld *w, uint64_t *word, int32_t clear) {
+    if (!w || !word) {
+        vx::set_error("vx_world_oob: null argument");
+        return VX_ERR_INVALID;
+    }
+    int rc = use_device(w);
+    if (rc != VX_OK) return rc;
+    std::lock_guard<std::mutex> lk(w->mu);
+    // kernels of this world may run on any stream of the device
+    VX_CK(cudaDeviceSynchronize());
+    unsigned long long v = 0;
+    VX_CK(cudaMemcpy(&v, w->dw.oob, sizeof(v), cudaMemcpyDeviceToHost));
+    if (clear) VX_CK(cudaMemset(w->dw.oob, 0, sizeof(v)));
+    *word = v;
     return VX_OK;
 }
 

@@ -64,6 +64,9 @@ struct DevWorld {
     // tile LUT byte (layout in vx_walk.cuh at kMetaChunkOnly).  nullptr for caller-owned worlds: the
     // walk then evaluates the tests from the masks.
     uint16_t *tile_meta;
+    // First out-of-range world index met by a load of the checked library
+    // (array id << 56 | index; 0 = none).  nullptr: not recorded.
+    unsigned long long *oob;
 };
 
 // Per-frame constants of the traversal kernels (passed by value).

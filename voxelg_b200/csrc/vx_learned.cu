@@ -69,10 +69,10 @@ __device__ __forceinline__ int cell_level(const DevWorld &w, const Geo &g, const
     if (sx >= w.d.vx) sx -= w.d.vx;
     if (sz >= w.d.vz) sz -= w.d.vz;
     const uint32_t ux = (uint32_t)sx, uy = (uint32_t)ly, uz = (uint32_t)sz;
-    const uint64_t cw = ldg(w.chunk_mask + chunk_index(g, ux, uy, uz));
+    const uint64_t cw = ld_chunk(w, chunk_index(g, ux, uy, uz));
     if (L4 && cw == 0ull) return 64;
     if (!bit64(cw, child_of(ux, uy, uz, 4))) return 16;
-    const uint64_t tw = ldg(w.tile_mask + tile_index(g, ux, uy, uz));
+    const uint64_t tw = ld_tile(w, tile_index(g, ux, uy, uz));
     if (!bit64(tw, child_of(ux, uy, uz, 2))) return 4;
     return 0;
 }
@@ -111,14 +111,14 @@ __device__ __forceinline__ uint64_t chunk_word_of(const DevWorld &w, const Geo &
     int32_t sx = (tx << 4) + sl.rox, sz = (tz << 4) + sl.roz;
     if (sx >= w.d.vx) sx -= w.d.vx;
     if (sz >= w.d.vz) sz -= w.d.vz;
-    return ldg(w.chunk_mask + chunk_index(g, (uint32_t)sx, (uint32_t)(ty << 4), (uint32_t)sz));
+    return ld_chunk(w, chunk_index(g, (uint32_t)sx, (uint32_t)(ty << 4), (uint32_t)sz));
 }
 __device__ __forceinline__ uint64_t tile_word_of(const DevWorld &w, const Geo &g, const Slots &sl,
                                                  int32_t tx, int32_t ty, int32_t tz) {
     int32_t sx = (tx << 4) + sl.rox, sz = (tz << 4) + sl.roz;
     if (sx >= w.d.vx) sx -= w.d.vx;
     if (sz >= w.d.vz) sz -= w.d.vz;
-    return ldg(w.tile_mask + tile_index(g, (uint32_t)sx, (uint32_t)(ty << 4), (uint32_t)sz));
+    return ld_tile(w, tile_index(g, (uint32_t)sx, (uint32_t)(ty << 4), (uint32_t)sz));
 }
 // child bit x + z*4 + y*16 of cell coordinates (any level)
 __device__ __forceinline__ int cbit(int32_t x, int32_t y, int32_t z) {

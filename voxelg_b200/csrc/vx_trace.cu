@@ -52,6 +52,12 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
     return ok != 0u;
 }
 
+// chunk word ci of the shared-memory copy of the chunk masks (checked like
+// ld_chunk in the checked library)
+__device__ __forceinline__ uint64_t s_chunk_at(const DevWorld &w, const uint64_t *s, uint32_t ci) {
+    return index_ok(w, ci, w.d.n_chunks, ARR_CHUNK) ? s[ci] : 0ull;
+}
+
 // cs_beam + trace_first_tile, beam.wgsl:30-113 (world, non-rebased coords).
 // SMEM: the whole chunk-mask array is brought into shared memory by one bulk
 // TMA copy (cp.async.bulk completing on an mbarrier) before the walk, so each
@@ -140,7 +146,8 @@ __global__ void __launch_bounds__(128) k_beam(FrameArgs fa, float *beam_out) {
                                     (stz >> 2) * (uint32_t)(d.cx * d.cy);
                 const int lin = (int)((stx & 3u) + (stz & 3u) * 4u + (sty & 3u) * 16u);
                 if (STATS) bytes += 8;
-                const uint64_t cw = (SMEM && staged) ? s_chunk[ci] : ldg(fa.ta.w.chunk_mask + ci);
+                const uint64_t cw = (SMEM && staged) ? s_chunk_at(fa.ta.w, s_chunk, ci)
+                                                     : ld_chunk(fa.ta.w, ci);
                 if (bit64(cw, lin)) {
                     result = t_cur;
                     break;
@@ -420,11 +427,11 @@ __device__ __forceinline__ bool o1_in_solid(const DevWorld &w, const int32_t v[3
     const int32_t sx = pos_mod(v[0], d.vx), sy = v[1], sz = pos_mod(v[2], d.vz);
     const int64_t bi = (int64_t)(sx >> 2) + (int64_t)(sy >> 2) * d.bx +
                        (int64_t)(sz >> 2) * d.bx * d.by;
-    const uint64_t occ = ldg(w.occ + bi);
+    const uint64_t occ = ld_occ(w, (uint64_t)bi);
     if (occ == 0ull) return false;
     const int vi = child_bit(sx & 3, sy & 3, sz & 3);
     if (!bit64(occ, vi)) return false;
-    return ldg(w.mat + bi * 64 + vi) != 33u;
+    return ld_mat(w, (uint64_t)bi, (uint32_t)vi) != 33u;
 }
 
 // The walk of raycast(): direction normalised as glam 0.29.3's
@@ -722,14 +729,14 @@ __device__ __forceinline__ bool ao_occluder(const DevWorld &w, const Geo &g, Ro 
         return false;
     const uint32_t sx = (uint32_t)pos_mod(x, d.vx), sy = (uint32_t)y,
                    sz = (uint32_t)pos_mod(z, d.vz);
-    if (!bit64(ldg(w.chunk_mask + chunk_index(g, sx, sy, sz)), child_of(sx, sy, sz, 4)))
+    if (!bit64(ld_chunk(w, chunk_index(g, sx, sy, sz)), child_of(sx, sy, sz, 4)))
         return false;
-    if (!bit64(ldg(w.tile_mask + tile_index(g, sx, sy, sz)), child_of(sx, sy, sz, 2)))
+    if (!bit64(ld_tile(w, tile_index(g, sx, sy, sz)), child_of(sx, sy, sz, 2)))
         return false;
     const uint32_t bi = brick_index(g, sx >> 2, sy >> 2, sz >> 2);
     const int vi = child_of(sx, sy, sz, 0);
-    if (!bit64(ldg(w.occ + bi), vi)) return false;
-    return !is_decoration((uint32_t)ldg(w.mat + (size_t)bi * 64u + vi));
+    if (!bit64(ld_occ(w, bi), vi)) return false;
+    return !is_decoration(ld_mat(w, bi, (uint32_t)vi));
 }
 
 // ao_corner: the two side voxels and the diagonal of one face corner

@@ -73,6 +73,60 @@ __device__ __forceinline__ bool bit64(uint64_t w, int b) { return (w >> b) & 1ul
 template <typename T>
 __device__ __forceinline__ T ldg(const T *p) { return __ldg(p); }
 
+// ------------------------------------------------------------ world loads
+// Every load of a world array by the traversal goes through these.  The
+// checked library (libvoxrt_checked.so, built with VX_CHECKED) first compares
+// the index with the array's length.  A bad index is recorded in w.oob (array
+// id << 56 | index, the first one wins) and the load returns 0 without
+// reading; nothing traps, and the host reads the word (vx_world_oob).
+enum : uint32_t {
+    ARR_L4 = 1, ARR_CHUNK = 2, ARR_TILE = 3, ARR_TILE_META = 4, ARR_TILE_UNIFORM = 5,
+    ARR_OCC = 6, ARR_BRICK_UNIFORM = 7, ARR_MAT = 8
+};
+// checked library: is i inside an array of n entries?  If not, record it.
+__device__ __forceinline__ bool index_ok(const DevWorld &w, uint64_t i, int64_t n, uint32_t arr) {
+#ifdef VX_CHECKED
+    if (i < (uint64_t)n) return true;
+    if (w.oob)
+        atomicCAS(w.oob, 0ull, ((unsigned long long)arr << 56) | (i & ((1ull << 56) - 1ull)));
+    return false;
+#else
+    (void)w; (void)i; (void)n; (void)arr;
+    return true;
+#endif
+}
+template <typename T>
+__device__ __forceinline__ T wload(const DevWorld &w, const T *base, uint64_t i, int64_t n,
+                                   uint32_t arr) {
+    if (!index_ok(w, i, n, arr)) return T(0);
+    return __ldg(base + i);
+}
+__device__ __forceinline__ uint64_t ld_l4(const DevWorld &w, uint64_t i) {
+    return wload(w, w.l4_mask, i, w.d.n_l4, ARR_L4);
+}
+__device__ __forceinline__ uint64_t ld_chunk(const DevWorld &w, uint64_t i) {
+    return wload(w, w.chunk_mask, i, w.d.n_chunks, ARR_CHUNK);
+}
+__device__ __forceinline__ uint64_t ld_tile(const DevWorld &w, uint64_t i) {
+    return wload(w, w.tile_mask, i, w.d.n_tiles, ARR_TILE);
+}
+__device__ __forceinline__ uint32_t ld_tile_meta(const DevWorld &w, uint64_t i) {
+    return wload(w, w.tile_meta, i, w.d.n_tiles, ARR_TILE_META);
+}
+__device__ __forceinline__ uint32_t ld_tile_uniform(const DevWorld &w, uint64_t i) {
+    return wload(w, w.tile_uniform, i, w.d.n_tiles, ARR_TILE_UNIFORM);
+}
+__device__ __forceinline__ uint64_t ld_occ(const DevWorld &w, uint64_t bi) {
+    return wload(w, w.occ, bi, w.d.n_bricks, ARR_OCC);
+}
+__device__ __forceinline__ uint32_t ld_brick_uniform(const DevWorld &w, uint64_t bi) {
+    return wload(w, w.brick_uniform, bi, w.d.n_bricks, ARR_BRICK_UNIFORM);
+}
+// material byte vi (0..63) of brick bi
+__device__ __forceinline__ uint32_t ld_mat(const DevWorld &w, uint64_t bi, uint32_t vi) {
+    return wload(w, w.mat, bi * 64u + vi, w.d.n_bricks * 64, ARR_MAT);
+}
+
 #ifndef VX_MIN_BLOCKS
 #define VX_MIN_BLOCKS 0
 #endif
@@ -265,7 +319,7 @@ __device__ __forceinline__ void set_hit(const Dims &d, const Dda &s, int la, uin
 
 // brick_topmost_material, raymarch.wgsl:253-295
 template <bool STATS>
-__device__ __forceinline__ uint32_t brick_topmost(const uint8_t *__restrict__ mrow, uint64_t occ,
+__device__ __forceinline__ uint32_t brick_topmost(const DevWorld &w, uint64_t bi, uint64_t occ,
                                                   uint64_t &bytes) {
     const uint32_t lo = (uint32_t)occ, hi = (uint32_t)(occ >> 32);
     const uint32_t layer[4] = {(hi >> 16) & 0xFFFFu, hi & 0xFFFFu, (lo >> 16) & 0xFFFFu,
@@ -274,7 +328,7 @@ __device__ __forceinline__ uint32_t brick_topmost(const uint8_t *__restrict__ mr
     for (int i = 0; i < 4; ++i) {
         if (layer[i] != 0u) {
             const int bit = __ffs(layer[i]) - 1;
-            const uint32_t m = ldg(mrow + (48 - 16 * i) + bit);
+            const uint32_t m = ld_mat(w, bi, (uint32_t)((48 - 16 * i) + bit));
             if (STATS) bytes += 1;
             if (m != 35u) return m;
         }
@@ -408,11 +462,11 @@ __device__ __forceinline__ int walk_step(const DevWorld &w, const Geo &g, const 
     const uint32_t sy = (uint32_t)s.vy;
     const uint32_t ti = tile_index(g, sx, sy, sz);
     // batch 1: every coarse word addressed by the slot coordinate
-    const uint64_t tw = ldg(w.tile_mask + ti);
+    const uint64_t tw = ld_tile(w, ti);
     uint32_t tum;
     int32_t cell = 0;
     if (w.tile_meta != nullptr) {
-        const uint32_t meta = ldg(w.tile_meta + ti);
+        const uint32_t meta = ld_tile_meta(w, ti);
         tum = f_lut ? (meta & 0xFFu) : 0u;
         if (use_l4) {
             const uint32_t code = (meta >> 8) & 3u;
@@ -424,9 +478,9 @@ __device__ __forceinline__ int walk_step(const DevWorld &w, const Geo &g, const 
         }
     } else {
         uint64_t lw = ~0ull;
-        if (use_l4) lw = ldg(w.l4_mask + l4_index(g, sx, sy, sz));
-        const uint64_t cw = ldg(w.chunk_mask + chunk_index(g, sx, sy, sz));
-        tum = f_lut ? (uint32_t)ldg(w.tile_uniform + ti) : 0u;
+        if (use_l4) lw = ld_l4(w, l4_index(g, sx, sy, sz));
+        const uint64_t cw = ld_chunk(w, chunk_index(g, sx, sy, sz));
+        tum = f_lut ? ld_tile_uniform(w, ti) : 0u;
         if (use_l4) {
             if (STATS) bytes += 8;
             if (lw == 0ull) cell = 256;
@@ -448,7 +502,7 @@ __device__ __forceinline__ int walk_step(const DevWorld &w, const Geo &g, const 
                                                  (sy >> 4) * 4u + (uint32_t)((lin >> 4) & 3),
                                                  (sz >> 4) * 4u + (uint32_t)((lin >> 2) & 3));
                 if (STATS) bytes += 8;
-                lm = brick_topmost<STATS>(w.mat + (size_t)rbi * 64u, ldg(w.occ + rbi), bytes);
+                lm = brick_topmost<STATS>(w, rbi, ld_occ(w, rbi), bytes);
             }
             if (lm != 0u && is_uniform_optimisable(lm)) {
                 set_hit(d, s, k.la, lm, true, h);
@@ -468,8 +522,8 @@ __device__ __forceinline__ int walk_step(const DevWorld &w, const Geo &g, const 
         } else {
             const uint32_t bi = brick_index(g, sx >> 2, sy >> 2, sz >> 2);
             // batch 2: brick occupancy + brick LUT byte
-            const uint64_t occ = ldg(w.occ + bi);
-            const uint32_t bum = f_lut ? (uint32_t)ldg(w.brick_uniform + bi) : 0u;
+            const uint64_t occ = ld_occ(w, bi);
+            const uint32_t bum = f_lut ? ld_brick_uniform(w, bi) : 0u;
             if (f_lut) {
                 if (STATS) bytes += 1;
                 if (bum != 0u && is_uniform_optimisable(bum)) {
@@ -477,7 +531,6 @@ __device__ __forceinline__ int walk_step(const DevWorld &w, const Geo &g, const 
                     return WALK_HIT;
                 }
             }
-            const uint8_t *mrow = w.mat + (size_t)bi * 64u;
             bool lod_done = false;
             if (f_lod && k.t_cur > p.lod_brick_t) {
                 if (STATS) bytes += 8;
@@ -485,7 +538,7 @@ __device__ __forceinline__ int walk_step(const DevWorld &w, const Geo &g, const 
                     cell = 4;
                     lod_done = true;
                 } else {
-                    const uint32_t m = brick_topmost<STATS>(mrow, occ, bytes);
+                    const uint32_t m = brick_topmost<STATS>(w, bi, occ, bytes);
                     if (!is_foliage(m)) {
                         set_hit(d, s, k.la, m, true, h);
                         return WALK_HIT;
@@ -497,7 +550,7 @@ __device__ __forceinline__ int walk_step(const DevWorld &w, const Geo &g, const 
                 if (STATS) bytes += 8;
                 if (bit64(occ, vi)) {
                     // batch 3: the material byte of a solid voxel
-                    const uint32_t m = ldg(mrow + vi);
+                    const uint32_t m = ld_mat(w, bi, (uint32_t)vi);
                     if (STATS) bytes += 1;
                     const bool stop = kind == KIND_TRACE ? resolves_cube(m)
                                       : (kind == KIND_ANY ? shadow_occludes(m) : !is_transparent(m));

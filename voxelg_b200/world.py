@@ -131,6 +131,13 @@ class DeviceWorld:
         L.check(self._lib.vx_world_shift_origin(self.handle, origin_cx, origin_cz, C.byref(n)))
         return n.value
 
+    def oob(self, clear: bool = True) -> int:
+        """First out-of-range world index the checked library met (array id
+        << 56 | index), 0 if none; always 0 in libvoxrt.so."""
+        v = C.c_uint64(0)
+        L.check(self._lib.vx_world_oob(self.handle, C.byref(v), 1 if clear else 0))
+        return int(v.value)
+
     def apply_edit(self, wx: int, wy: int, wz: int, mat: int):
         """A persistent edit at a world voxel (apply_edit): written now when
         inside the window, and replayed into every chunk generated later."""
