@@ -492,3 +492,40 @@ def test_world_checkpoint_round_trip(tmp_path):
         b.load(cut)
     for w in (a, b, small):
         w.close()
+
+
+@pytest.mark.gpu
+def test_frame_far_from_origin():
+    """renderer.rs:7612-7630 (renders_far_from_origin): the window streamed
+    100,000 chunks from spawn, 3.2M voxels, where an f32 ulp is 0.25 voxel.
+    With the origin rebased, the frame and the picks traced there equal the
+    oracle's bit for bit and, like the spawn frame, show terrain and sky."""
+    _gpu()
+    import voxelg_b200 as vg
+    flags = po.OR_F_L4 | po.OR_F_LUT | po.OR_F_LOD | po.OR_F_BEAM | po.OR_F_SHADOW
+    p = vg.default_params(flags)
+    dw = vg.DeviceWorld(*DEMO)
+    fractions = []
+    for oc in [(0, 0), (100_000, 100_000), (-100_000, 37)]:
+        dw.fill_window(SEED, *oc)
+        ow = _oracle_window(DEMO, SEED, *oc)
+        wo = (oc[0] * 32, 0, oc[1] * 32)
+        cam = vg.camera_from_pose((wo[0] + 256.0, 150.0, wo[2] + 256.0), 0.7, -0.3, 1.2, 320, 180,
+                                  world_origin=wo)
+        rec, sh = vg.render_primary(dw, cam, p)
+        want, wsh, _, _, _ = po.render_frame(ow, cam, p)
+        got = vg.records(rec)
+        assert np.array_equal(got.view(np.uint8), want.view(np.uint8)), oc
+        assert np.array_equal(vg.shadows(sh).view(np.uint8), wsh.view(np.uint8)), oc
+        fractions.append(float((got["flags"] & 1).mean()))
+        rng = np.random.default_rng(oc[0] & 0xFFFF)
+        cams = (np.array(wo, np.float64) + rng.uniform([0, 100, 0], [512, 200, 512], (500, 3)))
+        cams = cams.astype(np.float32)
+        dirs = rng.normal(size=(500, 3)).astype(np.float32)
+        picks, hits = vg.raycast_batch(dw, cams, dirs, origin=wo)
+        wpicks, whits, _ = po.raycast_batch(ow, cams, dirs, origin=wo)
+        assert np.array_equal(hits, whits) and np.array_equal(picks.view(np.uint8),
+                                                              wpicks.view(np.uint8)), oc
+    # terrain and sky in every frame, far frames like the spawn frame
+    assert all(0.2 < f < 0.95 for f in fractions), fractions
+    dw.close()
