@@ -674,3 +674,45 @@ def test_rebuild_in_place_grow_shrink_stream(vg):
     got = vg.render_primary(dw, cam, p)[0]
     assert_same_records(vg.records(got), po.render_frame(sw, cam, p)[0], "streamed")
     dw.close()
+
+
+def test_empty_and_single_item_batches(vg, dev_c1, c1_oracle_world):
+    """Zero and one item through every batched entry point, and the smallest
+    frames: nothing is launched for an empty batch, a single item equals the
+    oracle, 1x1 and 1x2 frames trace like any pixel."""
+    import torch
+    from voxelg_b200 import queue as q
+    ow = c1_oracle_world
+    p = vg.default_params(METHOD)
+    one = np.zeros(1, po.RAY)
+    one["org"] = (100.5, 150.25, 300.75)
+    one["dir"] = (0.3, -0.8, 0.52)
+    one["dir"] /= np.float32(math.sqrt(float((one["dir"][0] ** 2).sum())))
+    one["tmax"] = 700.0
+    for kind in (0, 1, 2):
+        one["kind"] = kind
+        assert len(vg.records(vg.trace(dev_c1, np.zeros(0, po.RAY), p))) == 0
+        assert_same_records(vg.records(vg.trace(dev_c1, one, p)), po.trace_batch(ow, one, p)[0],
+                            f"one ray kind {kind}")
+    picks, hits = vg.raycast_batch(dev_c1, np.zeros((0, 3), np.float32), np.zeros((0, 3), np.float32))
+    assert len(picks) == 0 and len(hits) == 0
+    picks, hits = vg.raycast_batch(dev_c1, one["org"], one["dir"])
+    wp, wh, _ = po.raycast_batch(ow, one["org"], one["dir"])
+    assert np.array_equal(hits, wh) and np.array_equal(picks.view(np.uint8), wp.view(np.uint8))
+    p_sh = vg.default_params(po.OR_F_L4 | po.OR_F_LUT | po.OR_F_LOD | po.OR_F_SHADOW)
+    one["kind"] = 0
+    for rays in (np.zeros(0, po.RAY), one):
+        for so in (0, 1):
+            t = q.default_tuning()
+            t.sort = so
+            _, out, sh = q.run(dev_c1, rays, p_sh, tuning=t)
+            torch.cuda.synchronize()
+            want, wsh, _, _ = po.trace_batch(ow, rays, p_sh, shadows=True)
+            assert np.array_equal(out.cpu().numpy(), want.view(np.uint8)), (len(rays), so)
+            assert np.array_equal(sh.cpu().numpy(), wsh.view(np.uint8)), (len(rays), so)
+    dev_c1.apply_dirty(np.zeros(0, np.uint32), np.zeros(0, po.BRICK))
+    for w, h in ((1, 1), (1, 2), (2, 1), (9, 7)):
+        cam = vg.camera_from_pose((256.0, 140.0, 256.0), 0.4, -0.3, 1.2, w, h)
+        rec, sh, (wrec, wsh, _, _, _) = frame_pair(vg, dev_c1, ow, cam, METHOD | po.OR_F_SHADOW)
+        assert_same_records(rec, wrec, f"{w}x{h} frame")
+        assert np.array_equal(sh.view(np.uint8), wsh.view(np.uint8))
