@@ -139,10 +139,18 @@ class ClockSampler:
 
 
 def measured_peaks() -> dict:
+    """HBM copy bandwidth of this pool's B200s: MEASURED_PEAKS.json's hbm_gbs
+    (a number, or an object holding one) when the file is there and readable,
+    else the earlier measurement of 6.65 TB/s."""
     p = ROOT / "MEASURED_PEAKS.json"
-    if p.exists():
-        d = json.loads(p.read_text())
-        return {"hbm_gbs": d["hbm_gbs"], "source": "measured"}
+    try:
+        v = json.loads(p.read_text()).get("hbm_gbs")
+        if isinstance(v, dict):
+            v = next((v[k] for k in ("value", "burst", "gbs", "measured") if k in v), None)
+        if isinstance(v, (int, float)) and v > 0:
+            return {"hbm_gbs": float(v), "source": "measured"}
+    except (OSError, ValueError, AttributeError):
+        pass
     return {"hbm_gbs": 6650.0, "source": "fallback"}
 
 

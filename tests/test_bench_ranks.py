@@ -61,3 +61,19 @@ def test_reference_arm_other_ranks_exit_without_work(monkeypatch, capsys):
     monkeypatch.setenv("RANK", "1")
     assert bench.run_reference(None, configs.CONFIGS[bench.CONFIG_NAME]) is None
     assert capsys.readouterr().out == ""
+
+
+@pytest.mark.parametrize("content,want", [('{"hbm_gbs": 7100.5}', (7100.5, "measured")),
+                                          ('{"hbm_gbs": {"burst": 7000}}', (7000.0, "measured")),
+                                          ("not json", (6650.0, "fallback")),
+                                          ('{"bf16_tflops": 1590}', (6650.0, "fallback")),
+                                          (None, (6650.0, "fallback"))])
+def test_measured_peaks_file_shapes(monkeypatch, tmp_path, content, want):
+    """The roofline denominator: the driver-written HBM figure when readable,
+    else the fallback, never an exception."""
+    import bench
+    if content is not None:
+        (tmp_path / "MEASURED_PEAKS.json").write_text(content)
+    monkeypatch.setattr(bench, "ROOT", tmp_path)
+    got = bench.measured_peaks()
+    assert (got["hbm_gbs"], got["source"]) == want
