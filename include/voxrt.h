@@ -279,6 +279,16 @@ int vx_render_primary(VxWorld *w, const VxCamera *cam, const VxTraceParams *p,
  * leaf fringe).  ao_dev[i] = 1 for misses and skipped hits. */
 int vx_render_ao(VxWorld *w, const VxCamera *cam, const VxHitRecord *rec_dev, float *ao_dev,
                  void *stream);
+/* Rows [y0, y1) of the frame of vx_render_primary (beam over the whole
+ * frame): their records and shadow records are written at their frame
+ * positions, rec_dev[y * res_x + x], and every other entry is left as it
+ * was, so rec_dev must hold y1 * res_x records.  Ranks that split a frame by
+ * rows each render their range into a frame-sized buffer and gather the
+ * ranges (voxelg_b200/replicas.py render_split).  Records equal the whole
+ * frame's.  Asynchronous on `stream`. */
+int vx_render_primary_rows(VxWorld *w, const VxCamera *cam, const VxTraceParams *p, uint32_t y0,
+                           uint32_t y1, VxHitRecord *rec_dev, VxShadowRecord *shadow_dev,
+                           void *stream);
 /* Same frame through host buffers: the records are copied to rec_host /
  * shadow_host (pinned memory recommended) before the call returns.  The
  * frame renders in four row bands, each copied while the next renders. */

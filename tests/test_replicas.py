@@ -149,3 +149,119 @@ def test_nccl_replica_matches_oracle():
         dw.close()
     finally:
         dist.destroy_process_group()
+
+
+# ------------------------------------------------------ one frame split by rows
+def test_split_rows_cover_every_row_once():
+    from voxelg_b200.replicas import split_rows
+    for h in (1, 2, 7, 90, 1080):
+        for n in (1, 2, 3, 7, 8):
+            rows = [r for k in range(n) for r in range(*split_rows(h, n, k)[:2])]
+            assert rows == list(range(h)), (h, n)
+            assert len({split_rows(h, n, k)[2] for k in range(n)}) == 1
+
+
+def _gather_rank(rank, world_size, port, q, W, H):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank),
+                      WORLD_SIZE=str(world_size))
+    import torch
+    import torch.distributed as dist
+
+    from voxelg_b200.replicas import gather_rows, split_rows
+    dist.init_process_group("gloo", rank=rank, world_size=world_size,
+                            timeout=timedelta(seconds=60))
+    try:
+        y0, y1, per = split_rows(H, world_size, rank)
+        rec = torch.zeros(world_size * per * W * 24, dtype=torch.uint8)
+        sh = torch.zeros(world_size * per * W * 8, dtype=torch.uint8)
+        for y in range(y0, y1):          # this rank's rows, as the row renderer writes them
+            rec[y * W * 24:(y + 1) * W * 24] = (y * 7 + 1) % 251
+            sh[y * W * 8:(y + 1) * W * 8] = (y * 3 + 2) % 253
+        got_rec, got_sh = gather_rows(rec, sh, W, H)
+        q.put((rank, got_rec.numpy().tobytes(), got_sh.numpy().tobytes()))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_ranks_gather_a_frame_split_by_rows():
+    import torch.multiprocessing as mp
+    W, H = 5, 7                          # odd: the last rank's slice has a padding row
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_gather_rank, args=(r, 2, port, q, W, H)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=120)
+    assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
+    got = sorted(q.get(timeout=10) for _ in range(2))
+    want_rec = b"".join(bytes([(y * 7 + 1) % 251]) * (W * 24) for y in range(H))
+    want_sh = b"".join(bytes([(y * 3 + 2) % 253]) * (W * 8) for y in range(H))
+    for _, rec, sh in got:
+        assert rec == want_rec and sh == want_sh
+
+
+@pytest.mark.gpu
+def test_row_ranges_compose_the_frame():
+    """vx_render_primary_rows: uneven row ranges rendered into one buffer give
+    the whole frame's records; rows outside a range stay untouched; a range
+    past the frame is rejected."""
+    import torch
+
+    import voxelg_b200 as vg
+    from voxelg_b200 import _lib as L
+    cfg = vg.CONFIGS["c1"]
+    dw = vg.DeviceWorld(*cfg.bricks)
+    dw.generate(cfg.terrain)
+    cam = vg.default_camera(dw, 160, 90)
+    p = vg.default_params(po.OR_F_L4 | po.OR_F_LUT | po.OR_F_LOD | po.OR_F_BEAM | po.OR_F_SHADOW)
+    whole, whole_sh = vg.render_primary(dw, cam, p)
+    rec = torch.full_like(whole, 0xAB)
+    sh = torch.full_like(whole_sh, 0xCD)
+    vg.render_primary_rows(dw, cam, p, 37, 38, rec, sh)
+    torch.cuda.synchronize()
+    r, s = rec.cpu().numpy(), sh.cpu().numpy()
+    assert np.array_equal(r[37 * 160 * 24:38 * 160 * 24], whole.cpu().numpy()[37 * 160 * 24:38 * 160 * 24])
+    assert (r[:37 * 160 * 24] == 0xAB).all() and (r[38 * 160 * 24:] == 0xAB).all()
+    assert (s[:37 * 160 * 8] == 0xCD).all() and (s[38 * 160 * 8:] == 0xCD).all()
+    for y0, y1 in ((0, 37), (38, 90), (90, 90)):
+        vg.render_primary_rows(dw, cam, p, y0, y1, rec, sh)
+    torch.cuda.synchronize()
+    assert np.array_equal(rec.cpu().numpy(), whole.cpu().numpy())
+    assert np.array_equal(sh.cpu().numpy(), whole_sh.cpu().numpy())
+    big = torch.empty(91 * 160 * 24, dtype=torch.uint8, device=rec.device)
+    with pytest.raises(L.VxError):                  # the library rejects rows past the frame
+        vg.render_primary_rows(dw, cam, p, 10, 91, big, None)
+    with pytest.raises(ValueError):                 # the binding rejects short buffers
+        vg.render_primary_rows(dw, cam, p, 0, 90, rec[:100], sh)
+    dw.close()
+
+
+@pytest.mark.gpu
+def test_nccl_split_frame_equals_the_frame():
+    """render_split over one NCCL rank: the row slices travel through the
+    all-gather and assemble the frame of vx_render_primary."""
+    import torch
+    import torch.distributed as dist
+
+    import voxelg_b200 as vg
+    from voxelg_b200.replicas import render_split
+    torch.cuda.set_device(0)
+    port = _free_port()
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0,
+                            world_size=1, timeout=timedelta(seconds=60))
+    try:
+        cfg = vg.CONFIGS["c1"]
+        dw = vg.DeviceWorld(*cfg.bricks)
+        dw.generate(cfg.terrain)
+        cam = vg.default_camera(dw, 200, 113)
+        p = vg.default_params(po.OR_F_L4 | po.OR_F_LUT | po.OR_F_LOD | po.OR_F_BEAM | po.OR_F_SHADOW)
+        rec, sh = render_split(dw, cam, p)
+        whole, whole_sh = vg.render_primary(dw, cam, p)
+        torch.cuda.synchronize()
+        assert np.array_equal(rec.cpu().numpy(), whole.cpu().numpy())
+        assert np.array_equal(sh.cpu().numpy(), whole_sh.cpu().numpy())
+        dw.close()
+    finally:
+        dist.destroy_process_group()

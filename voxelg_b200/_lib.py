@@ -160,6 +160,7 @@ SIGNATURES = [
     ("vx_world_apply_dirty", C.c_int, [_vp, _vp, _vp, C.c_size_t, _vp]),
     ("vx_world_counts", C.c_int, [_vp, _P(C.c_uint64)]),
     ("vx_checked_build", C.c_int, []),
+    ("vx_render_primary_rows", C.c_int, [_vp, _vp, _vp, C.c_uint32, C.c_uint32, _vp, _vp, _vp]),
     ("vx_world_oob", C.c_int, [_vp, _P(C.c_uint64), C.c_int32]),
     ("vx_world_set_tuning", C.c_int, [_vp, _P(VxTuning)]),
     ("vx_world_get_tuning", C.c_int, [_vp, _P(VxTuning)]),

@@ -1085,6 +1085,37 @@ int vx_render_primary(VxWorld *w, const VxCamera *cam, const VxTraceParams *p,
     return run_frame(w, fa, as_stream(stream));
 }
 
+int vx_render_primary_rows(VxWorld *w, const VxCamera *cam, const VxTraceParams *p, uint32_t y0,
+                           uint32_t y1, VxHitRecord *rec_dev, VxShadowRecord *shadow_dev,
+                           void *stream) {
+    vx::Range nvtx_range("vx_render_primary_rows");
+    if (!w || !rec_dev) {
+        vx::set_error("vx_render_primary_rows: null argument");
+        return VX_ERR_INVALID;
+    }
+    int rc = check_frame(cam);
+    if (rc == VX_OK) rc = check_params(p);
+    if (rc != VX_OK) return rc;
+    if (y0 > y1 || y1 > (uint32_t)cam->res_y) {
+        vx::set_error("vx_render_primary_rows: need y0 <= y1 <= res_y");
+        return VX_ERR_INVALID;
+    }
+    if ((reinterpret_cast<uintptr_t>(rec_dev) & 7u) || (reinterpret_cast<uintptr_t>(shadow_dev) & 7u)) {
+        vx::set_error("vx_render_primary_rows: records must be 8-byte aligned");
+        return VX_ERR_INVALID;
+    }
+    rc = use_device(w);
+    if (rc != VX_OK) return rc;
+    std::lock_guard<std::mutex> lk(w->mu);
+    vx::FrameArgs fa = make_frame(w, cam, p);
+    fa.work = nullptr;  // the grid form renders a row range; the persistent one whole frames
+    fa.y0 = y0;
+    fa.y1 = y1;
+    fa.rec = rec_dev;
+    fa.shadow = shadow_dev;
+    return run_frame(w, fa, as_stream(stream));
+}
+
 int vx_queue_default_tuning(VxQueueTuning *t) {
     if (!t) return VX_ERR_INVALID;
     std::memset(t, 0, sizeof(*t));

@@ -93,6 +93,21 @@ def render_primary(world: DeviceWorld, cam: L.VxCamera, params: L.VxTraceParams,
     return rec, shadow
 
 
+def render_primary_rows(world: DeviceWorld, cam: L.VxCamera, params: L.VxTraceParams, y0: int,
+                        y1: int, rec, shadow=None, stream: int = 0):
+    """Rows [y0, y1) of the frame into rec / shadow (uint8 CUDA tensors of at
+    least y1 * res_x records), at their frame positions; other rows are left
+    as they were."""
+    n = int(y1) * int(cam.res_x)
+    if rec.numel() < n * 24 or (shadow is not None and shadow.numel() < n * 8):
+        raise ValueError("render_primary_rows: buffers hold fewer than y1 * res_x records")
+    L.check(L.load().vx_render_primary_rows(world.handle, C.byref(cam), C.byref(params),
+                                            int(y0), int(y1), C.c_void_p(rec.data_ptr()),
+                                            C.c_void_p(shadow.data_ptr() if shadow is not None else 0),
+                                            C.c_void_p(stream)))
+    return rec, shadow
+
+
 def tile_mask_words(width: int, height: int) -> int:
     """u32 words of an 8x8-tile dirty mask (src/app.rs:643-648)."""
     return ((width + 7) // 8 * ((height + 7) // 8) + 31) // 32
