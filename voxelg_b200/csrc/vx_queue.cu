@@ -248,45 +248,96 @@ __global__ void __launch_bounds__(256) k_radix_rowscan(uint32_t *counts, uint32_
     }
 }
 
-// Stable scatter: each warp stages its tile's (key, ray) pairs in shared
-// memory (coalesced 16-byte loads), then walks the tile in index order, 32
-// items a round; lanes sharing a digit take consecutive slots in lane order.
-// A pair is stored as one 8-byte word, so each item dirties one sector.
-constexpr uint32_t kScatterWarps = 2;
+// Stable scatter, one 2048-item tile per CTA of eight warps; warp w owns
+// items [256 w, 256 w + 256) of the tile.
+//   1. each warp reads its slice (8 items a lane, kept in registers) and
+//      ranks every item among the slice's items of the same digit (lanes
+//      sharing a digit in a round rank in lane order);
+//   2. per digit, the counts of the warps give each warp's first rank and the
+//      digit's total; a scan over the 256 digits gives each digit's first
+//      slot in the tile;
+//   3. every item moves to its slot of the tile sorted by (digit, index), in
+//      shared memory;
+//   4. the sorted tile is written out in slot order: slot j of digit d goes
+//      to the digit's first position for this tile (the scanned counts) plus
+//      j minus the digit's first slot.  Items of one digit leave as one run,
+//      so stores coalesce instead of touching one sector per item.
+// The order is the stable one: by tile, then by index within the tile.
+constexpr uint32_t kScatterWarps = 8;
+constexpr uint32_t kSliceItems = kTileItems / kScatterWarps;   // 256 = 8 rounds of 32
 __global__ void __launch_bounds__(32 * kScatterWarps) k_radix_scatter(
     const uint2 *in, uint32_t n, uint32_t shift, uint32_t tiles, const uint32_t *counts,
     uint2 *out) {
-    __shared__ __align__(16) uint2 st[kScatterWarps][kTileItems];
-    __shared__ uint32_t off[kScatterWarps][256];
-    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
-    const uint32_t tile = blockIdx.x * kScatterWarps + warp;
-    if (tile >= tiles) return;
-    for (uint32_t d = lane; d < 256u; d += 32u) off[warp][d] = counts[d * tiles + tile];
+    __shared__ __align__(16) uint2 st[kTileItems];
+    __shared__ uint32_t wrank[kScatterWarps][256];   // per warp and digit: count, then first rank
+    __shared__ uint32_t dfirst[256];                 // first slot of each digit in the tile
+    __shared__ uint32_t gbase[256];                  // first output position of each digit
+    __shared__ uint32_t wtot[kScatterWarps];
+    const uint32_t tid = threadIdx.x, warp = tid >> 5, lane = tid & 31u;
+    const uint32_t tile = blockIdx.x;
     const uint32_t begin = tile * kTileItems, end = min(n, begin + kTileItems);
     const uint32_t cnt = end - begin;
-    if (cnt == kTileItems) {
-        // begin is a multiple of 2048 pairs: 16-byte aligned
-        const uint4 *src = reinterpret_cast<const uint4 *>(in + begin);
-        uint4 *dst = reinterpret_cast<uint4 *>(st[warp]);
-#pragma unroll 4
-        for (uint32_t q = lane; q < kTileItems / 2u; q += 32u) dst[q] = src[q];
-    } else {
-        for (uint32_t q = lane; q < cnt; q += 32u) st[warp][q] = in[begin + q];
-    }
-    __syncwarp();
-    for (uint32_t r = 0; r < cnt; r += 32u) {
-        const uint32_t i = r + lane;
+    for (uint32_t i = tid; i < kScatterWarps * 256u; i += blockDim.x) (&wrank[0][0])[i] = 0u;
+    __syncthreads();
+    // 1. rank within the warp's slice
+    const uint32_t s0 = warp * kSliceItems;
+    uint2 v[8];
+    uint32_t rk[8];
+#pragma unroll
+    for (uint32_t k = 0; k < 8u; ++k) {
+        const uint32_t i = s0 + k * 32u + lane;
         const unsigned valid = __ballot_sync(0xFFFFFFFFu, i < cnt);
+        v[k] = make_uint2(0u, 0u);
+        rk[k] = 0u;
         if (i < cnt) {
-            const uint2 item = st[warp][i];
-            const uint32_t dg = (item.x >> shift) & 255u;
+            v[k] = in[begin + i];
+            const uint32_t dg = (v[k].x >> shift) & 255u;
             const unsigned peers = __match_any_sync(valid, dg);
-            const uint32_t base = off[warp][dg];
-            out[base + (uint32_t)__popc(peers & ((1u << lane) - 1u))] = item;
+            rk[k] = wrank[warp][dg] + (uint32_t)__popc(peers & ((1u << lane) - 1u));
             __syncwarp(valid);
-            if ((uint32_t)(__ffs(peers) - 1) == lane) off[warp][dg] = base + (uint32_t)__popc(peers);
+            if ((uint32_t)(__ffs(peers) - 1) == lane) wrank[warp][dg] += (uint32_t)__popc(peers);
         }
         __syncwarp();
+    }
+    __syncthreads();
+    // 2. per digit (one thread each): warps' first ranks, the digit's total,
+    //    then an exclusive scan of the totals over the digits
+    const uint32_t d = tid;                          // blockDim.x == 256
+    uint32_t tot = 0;
+#pragma unroll
+    for (uint32_t w = 0; w < kScatterWarps; ++w) {
+        const uint32_t c = wrank[w][d];
+        wrank[w][d] = tot;
+        tot += c;
+    }
+    gbase[d] = counts[d * tiles + tile];
+    uint32_t inc = tot;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, inc, o);
+        if ((int)lane >= o) inc += t;
+    }
+    if (lane == 31u) wtot[warp] = inc;
+    __syncthreads();
+    uint32_t before = 0;
+    for (uint32_t w = 0; w < warp; ++w) before += wtot[w];
+    dfirst[d] = before + inc - tot;
+    __syncthreads();
+    // 3. each item to its slot of the sorted tile
+#pragma unroll
+    for (uint32_t k = 0; k < 8u; ++k) {
+        const uint32_t i = s0 + k * 32u + lane;
+        if (i < cnt) {
+            const uint32_t dg = (v[k].x >> shift) & 255u;
+            st[dfirst[dg] + wrank[warp][dg] + rk[k]] = v[k];
+        }
+    }
+    __syncthreads();
+    // 4. slot order out: runs of one digit go to consecutive positions
+    for (uint32_t j = tid; j < cnt; j += blockDim.x) {
+        const uint2 item = st[j];
+        const uint32_t dg = (item.x >> shift) & 255u;
+        out[gbase[dg] + (j - dfirst[dg])] = item;
     }
 }
 
@@ -362,8 +413,8 @@ cudaError_t launch_queue(const TraceArgs &ta, const VxRay *rays, size_t n, VxHit
             k_radix_hist<<<tb, 128, 0, s>>>(in, nn, shift, tiles, sc.hist);
             k_radix_rowsum<<<32, 256, 0, s>>>(sc.hist, tiles, sc.hist + (size_t)tiles * 256u);
             k_radix_rowscan<<<32, 256, 0, s>>>(sc.hist, tiles, sc.hist + (size_t)tiles * 256u);
-            k_radix_scatter<<<(tiles + kScatterWarps - 1) / kScatterWarps, 32 * kScatterWarps, 0,
-                              s>>>(in, nn, shift, tiles, sc.hist, out);
+            k_radix_scatter<<<tiles, 32 * kScatterWarps, 0, s>>>(in, nn, shift, tiles, sc.hist,
+                                                                 out);
             std::swap(in, out);
         }
         order = in;
