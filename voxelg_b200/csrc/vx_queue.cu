@@ -212,9 +212,24 @@ __global__ void __launch_bounds__(128) k_radix_hist(const uint2 *kv, uint32_t n,
     }
 }
 
-// Exclusive scan of the digit-major counts, one warp per digit row: first
-// the row totals, then each row scanned from its digit's base (the totals
-// of the smaller digits), 32 entries at a time.
+// Exclusive scan of the digit-major counts: first the row totals, then each
+// row scanned by one 256-thread CTA from its digit's base (the totals of the
+// smaller digits), 1024 entries a round, four per thread.
+__device__ __forceinline__ uint32_t block_sum256(uint32_t v, uint32_t *wsum) {
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+    __syncthreads();                       // wsum may still be read by a previous call
+    if (lane == 0) wsum[warp] = v;
+    __syncthreads();
+    uint32_t t = 0;
+#pragma unroll
+    for (uint32_t w = 0; w < 8u; ++w) t += wsum[w];
+    return t;
+}
+
+// row totals: one warp per digit row (its loads are independent, so one warp
+// keeps many in flight; a CTA per row measured slower)
 __global__ void __launch_bounds__(256) k_radix_rowsum(const uint32_t *counts, uint32_t tiles,
                                                       uint32_t *rowsum) {
     const uint32_t d = blockIdx.x * 8u + (threadIdx.x >> 5), lane = threadIdx.x & 31u;
@@ -228,23 +243,43 @@ __global__ void __launch_bounds__(256) k_radix_rowsum(const uint32_t *counts, ui
 
 __global__ void __launch_bounds__(256) k_radix_rowscan(uint32_t *counts, uint32_t tiles,
                                                        const uint32_t *rowsum) {
-    const uint32_t d = blockIdx.x * 8u + (threadIdx.x >> 5), lane = threadIdx.x & 31u;
+    __shared__ uint32_t wsum[8];
+    const uint32_t d = blockIdx.x, tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
     uint32_t base = 0;
-    for (uint32_t k = lane; k < d; k += 32u) base += rowsum[k];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) base += __shfl_xor_sync(0xFFFFFFFFu, base, o);
+    for (uint32_t k = tid; k < d; k += blockDim.x) base += rowsum[k];
+    base = block_sum256(base, wsum);
     uint32_t *row = counts + (size_t)d * tiles;
-    for (uint32_t t0 = 0; t0 < tiles; t0 += 32u) {
-        const uint32_t t = t0 + lane;
-        const uint32_t c = t < tiles ? row[t] : 0u;
-        uint32_t inc = c;
+    for (uint32_t c0 = 0; c0 < tiles; c0 += 1024u) {
+        const uint32_t t0 = c0 + tid * 4u;
+        uint32_t x[4], run = 0;
+#pragma unroll
+        for (uint32_t i = 0; i < 4u; ++i) {
+            x[i] = t0 + i < tiles ? row[t0 + i] : 0u;
+            const uint32_t c = x[i];
+            x[i] = run;                    // exclusive within the thread
+            run += c;
+        }
+        uint32_t inc = run;                // inclusive scan of thread totals in the warp
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const uint32_t v = __shfl_up_sync(0xFFFFFFFFu, inc, o);
             if ((int)lane >= o) inc += v;
         }
-        if (t < tiles) row[t] = base + inc - c;
-        base += __shfl_sync(0xFFFFFFFFu, inc, 31);
+        __syncthreads();                   // wsum of the previous round is consumed
+        if (lane == 31u) wsum[warp] = inc;
+        __syncthreads();
+        uint32_t before = 0, total = 0;
+#pragma unroll
+        for (uint32_t w = 0; w < 8u; ++w) {
+            const uint32_t s = wsum[w];
+            before += w < warp ? s : 0u;
+            total += s;
+        }
+        const uint32_t first = base + before + inc - run;
+#pragma unroll
+        for (uint32_t i = 0; i < 4u; ++i)
+            if (t0 + i < tiles) row[t0 + i] = first + x[i];
+        base += total;
     }
 }
 
@@ -412,7 +447,7 @@ cudaError_t launch_queue(const TraceArgs &ta, const VxRay *rays, size_t n, VxHit
         for (uint32_t shift = 0; shift < 32u; shift += 8u) {
             k_radix_hist<<<tb, 128, 0, s>>>(in, nn, shift, tiles, sc.hist);
             k_radix_rowsum<<<32, 256, 0, s>>>(sc.hist, tiles, sc.hist + (size_t)tiles * 256u);
-            k_radix_rowscan<<<32, 256, 0, s>>>(sc.hist, tiles, sc.hist + (size_t)tiles * 256u);
+            k_radix_rowscan<<<256, 256, 0, s>>>(sc.hist, tiles, sc.hist + (size_t)tiles * 256u);
             k_radix_scatter<<<tiles, 32 * kScatterWarps, 0, s>>>(in, nn, shift, tiles, sc.hist,
                                                                  out);
             std::swap(in, out);
