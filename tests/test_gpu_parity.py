@@ -716,3 +716,64 @@ def test_empty_and_single_item_batches(vg, dev_c1, c1_oracle_world):
         rec, sh, (wrec, wsh, _, _, _) = frame_pair(vg, dev_c1, ow, cam, METHOD | po.OR_F_SHADOW)
         assert_same_records(rec, wrec, f"{w}x{h} frame")
         assert np.array_equal(sh.view(np.uint8), wsh.view(np.uint8))
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_random_worlds_bit_exact(vg, seed):
+    """Seeded random worlds (boxes and scattered voxels of every material
+    class, water, glass, foliage, decoration and leaf fringe included), a
+    random window origin, flag set and camera: the frame, rays of the three
+    kinds (degenerate ones among them) and picks equal the oracle's."""
+    rng = np.random.default_rng(1000 + seed)
+    bx, by, bz = 64, 16, 64
+    VX, VY, VZ = bx * 4, by * 4, bz * 4
+    classes = np.array([1, 2, 3, 4, 5, 8, 12, 14, 18, 25, 30, 31, 33, 34, 35, 36, 37], np.uint8)
+    m = np.zeros((VX, VY, VZ), np.uint8)
+    for _ in range(int(rng.integers(5, 40))):
+        lo = rng.integers([0, 0, 0], [VX, VY, VZ])
+        size = rng.integers(1, [64, 24, 64])
+        hi = np.minimum(lo + size, [VX, VY, VZ])
+        m[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]] = rng.choice(classes)
+    sparse = rng.random(m.shape) < rng.uniform(0.0, 0.03)
+    m[sparse] = rng.choice(classes, int(sparse.sum()))
+    ow = po.World(bx, by, bz)
+    x, y, z = np.meshgrid(np.arange(VX), np.arange(VY), np.arange(VZ), indexing="ij")
+    vi = (x & 3) + (z & 3) * 4 + (y & 3) * 16
+    bi = (x >> 2) + (y >> 2) * bx + (z >> 2) * bx * by
+    mats = ow.a["bricks"]["materials"]
+    mats[bi.ravel(), vi.ravel()] = m.ravel()
+    occ = (mats != 0).astype(np.uint64) << np.arange(64, dtype=np.uint64)
+    ow.a["bricks"]["occupancy"] = np.bitwise_or.reduce(occ, axis=1)
+    ow.rebuild()
+    dw = upload_oracle(vg, ow)
+    wo = (int(rng.integers(-3, 4)) * 32 + int(rng.integers(0, 32)), 0,
+          int(rng.integers(-3, 4)) * 32 + int(rng.integers(0, 32)))
+    flags = int(rng.choice([METHOD, METHOD | po.OR_F_SHADOW, po.OR_F_L4 | po.OR_F_LUT,
+                            po.OR_F_LOD | po.OR_F_SHADOW, 0]))
+    p = vg.default_params(flags)
+    pos = (wo[0] + float(rng.uniform(-20, VX + 20)), float(rng.uniform(5, 120)),
+           wo[2] + float(rng.uniform(-20, VZ + 20)))
+    cam = vg.camera_from_pose(pos, float(rng.uniform(0, 6.28)), float(rng.uniform(-1.2, 0.6)),
+                              1.2, 80, 45, world_origin=wo)
+    rec, sh, (wrec, wsh, _, _, _) = frame_pair(vg, dw, ow, cam, flags)
+    assert_same_records(rec, wrec, f"seed {seed} frame")
+    if sh is not None:
+        assert np.array_equal(sh.view(np.uint8), wsh.view(np.uint8))
+    n = 3000
+    rays = np.zeros(n, po.RAY)
+    rays["org"] = (np.array(wo, np.float64) + rng.uniform([-40, -20, -40], [VX + 40, VY + 60, VZ + 40],
+                                                         (n, 3))).astype(np.float32)
+    d = rng.normal(size=(n, 3)).astype(np.float32)
+    d[::29] = 0.0
+    d[1::31, 1] = 0.0
+    d[2::37] *= np.float32(1e-9)
+    rays["dir"] = d
+    rays["tmax"] = rng.uniform(0.5, 900, n).astype(np.float32)
+    for kind in (0, 1, 2):
+        rays["kind"] = kind
+        got = vg.records(vg.trace(dw, rays, p, origin=wo))
+        assert_same_records(got, po.trace_batch(ow, rays, p, origin=wo)[0], f"seed {seed} kind {kind}")
+    picks, hits = vg.raycast_batch(dw, rays["org"], d, origin=wo)
+    wp, wh, _ = po.raycast_batch(ow, rays["org"], d, origin=wo)
+    assert np.array_equal(hits, wh) and np.array_equal(picks.view(np.uint8), wp.view(np.uint8))
+    dw.close()
