@@ -776,4 +776,21 @@ def test_random_worlds_bit_exact(vg, seed):
     picks, hits = vg.raycast_batch(dw, rays["org"], d, origin=wo)
     wp, wh, _ = po.raycast_batch(ow, rays["org"], d, origin=wo)
     assert np.array_equal(hits, wh) and np.array_equal(picks.view(np.uint8), wp.view(np.uint8))
+    # the same rays as one mixed queue: kinds shuffled, some kind-0 rays spawning
+    # a shadow ray at their hit, sorted and unsorted
+    import torch
+    from voxelg_b200 import _lib as L
+    from voxelg_b200 import queue as q
+    kinds = rng.integers(0, 3, n).astype(np.uint32)
+    kinds[(kinds == 0) & (rng.random(n) < 0.5)] |= np.uint32(L.VX_RAY_SPAWN_SHADOW)
+    rays["kind"] = kinds
+    pq = vg.default_params(flags | po.OR_F_SHADOW)
+    want, wsh, _, _ = po.trace_batch(ow, rays, pq, origin=wo, shadows=True)
+    for so in (0, 1):
+        t = q.default_tuning()
+        t.sort = so
+        _, out, qsh = q.run(dw, rays, pq, tuning=t, origin=wo)
+        torch.cuda.synchronize()
+        assert np.array_equal(out.cpu().numpy(), want.view(np.uint8)), f"seed {seed} queue sort={so}"
+        assert np.array_equal(qsh.cpu().numpy(), wsh.view(np.uint8)), f"seed {seed} shadows sort={so}"
     dw.close()
