@@ -718,14 +718,9 @@ def test_empty_and_single_item_batches(vg, dev_c1, c1_oracle_world):
         assert np.array_equal(sh.view(np.uint8), wsh.view(np.uint8))
 
 
-@pytest.mark.parametrize("seed", range(12))
-def test_random_worlds_bit_exact(vg, seed):
-    """Seeded random worlds (boxes and scattered voxels of every material
-    class, water, glass, foliage, decoration and leaf fringe included), a
-    random window origin, flag set and camera: the frame, rays of the three
-    kinds (degenerate ones among them) and picks equal the oracle's."""
-    rng = np.random.default_rng(1000 + seed)
-    bx, by, bz = 64, 16, 64
+def _random_world(rng, bx=64, by=16, bz=64):
+    """Boxes and scattered voxels of every material class (water, glass,
+    foliage, decoration and leaf fringe included) in a bx*by*bz-brick world."""
     VX, VY, VZ = bx * 4, by * 4, bz * 4
     classes = np.array([1, 2, 3, 4, 5, 8, 12, 14, 18, 25, 30, 31, 33, 34, 35, 36, 37], np.uint8)
     m = np.zeros((VX, VY, VZ), np.uint8)
@@ -745,6 +740,18 @@ def test_random_worlds_bit_exact(vg, seed):
     occ = (mats != 0).astype(np.uint64) << np.arange(64, dtype=np.uint64)
     ow.a["bricks"]["occupancy"] = np.bitwise_or.reduce(occ, axis=1)
     ow.rebuild()
+    return ow
+
+
+@pytest.mark.parametrize("seed", range(12))
+def test_random_worlds_bit_exact(vg, seed):
+    """Seeded random worlds (boxes and scattered voxels of every material
+    class, water, glass, foliage, decoration and leaf fringe included), a
+    random window origin, flag set and camera: the frame, rays of the three
+    kinds (degenerate ones among them) and picks equal the oracle's."""
+    rng = np.random.default_rng(1000 + seed)
+    ow = _random_world(rng)
+    VX, VY, VZ = ow.voxels
     dw = upload_oracle(vg, ow)
     wo = (int(rng.integers(-3, 4)) * 32 + int(rng.integers(0, 32)), 0,
           int(rng.integers(-3, 4)) * 32 + int(rng.integers(0, 32)))
@@ -793,4 +800,40 @@ def test_random_worlds_bit_exact(vg, seed):
         torch.cuda.synchronize()
         assert np.array_equal(out.cpu().numpy(), want.view(np.uint8)), f"seed {seed} queue sort={so}"
         assert np.array_equal(qsh.cpu().numpy(), wsh.view(np.uint8)), f"seed {seed} shadows sort={so}"
+    dw.close()
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_random_worlds_ao_and_learned(vg, seed):
+    """On seeded random worlds with a chunk-aligned window: contact AO of the
+    frame's hits equals the oracle's, and the learned form's verification
+    walk and restart (no network) give the plain frame's records but for
+    steps."""
+    import torch
+    from voxelg_b200 import learned as vl
+    rng = np.random.default_rng(5000 + seed)
+    ow = _random_world(rng)
+    VX, VY, VZ = ow.voxels
+    dw = upload_oracle(vg, ow)
+    wo = (int(rng.integers(-2, 3)) * 64, 0, int(rng.integers(-2, 3)) * 64)
+    pos = (wo[0] + float(rng.uniform(0, VX)), float(rng.uniform(20, 120)), wo[2] + float(rng.uniform(0, VZ)))
+    cam = vg.camera_from_pose(pos, float(rng.uniform(0, 6.28)), float(rng.uniform(-1.2, 0.3)),
+                              1.2, 96, 54, world_origin=wo)
+    flags = METHOD | po.OR_F_SHADOW
+    rec, sh, (wrec, _, _, _, _) = frame_pair(vg, dw, ow, cam, flags)
+    assert_same_records(rec, wrec, f"seed {seed} frame")
+    p = vg.default_params(flags)
+    rt, _ = vg.render_primary(dw, cam, p)
+    ao = vg.render_ao(dw, cam, rt).cpu().numpy()
+    assert np.array_equal(ao.view(np.uint32), po.render_ao(ow, cam, wrec).view(np.uint32))
+    for fl in (po.OR_F_L4 | po.OR_F_LUT | po.OR_F_LOD, 0):
+        pl = vg.default_params(fl)
+        plain, _ = vg.render_primary(dw, cam, pl)
+        out = torch.empty_like(plain)
+        st = vl.render_learned(dw, None, cam, pl, out)
+        a, b = vg.records(plain).copy(), vg.records(out).copy()
+        a["steps"] = 0
+        b["steps"] = 0
+        assert np.array_equal(a.view(np.uint8), b.view(np.uint8)), (seed, fl)
+        assert st.rays == 96 * 54
     dw.close()
