@@ -40,9 +40,9 @@ struct VxWorld {
     VxShadowRecord *sh = nullptr;
     size_t sh_cap = 0;
     // single-ray picking: pinned, device-mapped host block that the kernel
-    // reads its ray from and writes its result to (no copies, one sync)
+    // writes its result to (the ray travels in the launch parameters; no
+    // copies, one sync)
     struct PickBox {
-        float in[8];
         VxPickHit out;
         int32_t hit;
     };
@@ -1009,14 +1009,10 @@ int vx_raycast(VxWorld *w, const float cam[3], const float dir[3], const int32_t
     int rc = use_device(w);
     if (rc != VX_OK) return rc;
     std::lock_guard<std::mutex> lk(w->mu);
-    // the ray goes in and the result comes back through the mapped block:
-    // one launch and one synchronization, no copies
-    for (int k = 0; k < 3; ++k) {
-        w->pick->in[k] = cam[k];
-        w->pick->in[3 + k] = dir[k];
-    }
-    VX_CK(vx::launch_raycast(w->dw, origin, w->pick_dev->in, w->pick_dev->in + 3, 1,
-                             &w->pick_dev->out, &w->pick_dev->hit, w->stream));
+    // the ray goes in with the launch's parameters and the result comes back
+    // through the mapped block: one launch and one synchronization, no copies
+    VX_CK(vx::launch_raycast_one(w->dw, origin, cam, dir, &w->pick_dev->out, &w->pick_dev->hit,
+                                 w->stream));
     VX_CK(cudaStreamSynchronize(w->stream));
     *out = w->pick->out;
     return w->pick->hit ? 1 : 0;

@@ -94,6 +94,9 @@ cudaError_t launch_beam(const FrameArgs &fa, float *beam_out, cudaStream_t s);
 cudaError_t launch_primary(const FrameArgs &fa, cudaStream_t s);
 cudaError_t launch_trace_rays(const TraceArgs &ta, const VxRay *rays, size_t n, VxHitRecord *out,
                               cudaStream_t s);
+// one pick ray whose camera and direction travel in the launch parameters
+cudaError_t launch_raycast_one(const DevWorld &w, const int32_t origin[3], const float cam[3],
+                               const float dir[3], VxPickHit *out, int32_t *hit, cudaStream_t s);
 cudaError_t launch_raycast(const DevWorld &w, const int32_t origin[3], const float *cams,
                            const float *dirs, size_t n, VxPickHit *out, int32_t *hit,
                            cudaStream_t s);

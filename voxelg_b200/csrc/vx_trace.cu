@@ -412,6 +412,7 @@ __global__ void __launch_bounds__(128) k_trace_rays(TraceArgs ta, const VxRay *_
 struct PickArgs {
     DevWorld w;
     int32_t origin[3];
+    float ray[6];   // single calls: camera and direction, when cams is null
 };
 
 __device__ __forceinline__ bool o1_in_window(const Dims &d, const int32_t v[3],
@@ -563,8 +564,11 @@ __global__ void __launch_bounds__(32) k_raycast_warp(PickArgs pa, const float *_
     const uint32_t lane = threadIdx.x;
     const Dims &d = pa.w.d;
     const int32_t *o = pa.origin;
-    const float cam[3] = {cams[0], cams[1], cams[2]};
-    const float din[3] = {dirs[0], dirs[1], dirs[2]};
+    // a single call passes its ray in the launch parameters: no read of
+    // host-mapped memory before the walk can start
+    const float *rc = cams ? cams : pa.ray, *rd = cams ? dirs : pa.ray + 3;
+    const float cam[3] = {rc[0], rc[1], rc[2]};
+    const float din[3] = {rd[0], rd[1], rd[2]};
     VxPickHit res;
     res.voxel[0] = res.voxel[1] = res.voxel[2] = 0;
     res.normal[0] = res.normal[1] = res.normal[2] = 0;
@@ -920,6 +924,19 @@ cudaError_t launch_trace_rays(const TraceArgs &ta, const VxRay *rays, size_t n, 
     VxHitRecord *o = out;
     void *args[] = {&a, &r, &nn, &o};
     return cudaLaunchKernel(fn, dim3(blocks), dim3(128), args, 0, s);
+}
+
+cudaError_t launch_raycast_one(const DevWorld &w, const int32_t origin[3], const float cam[3],
+                               const float dir[3], VxPickHit *out, int32_t *hit, cudaStream_t s) {
+    PickArgs pa;
+    pa.w = w;
+    for (int k = 0; k < 3; ++k) {
+        pa.origin[k] = origin[k];
+        pa.ray[k] = cam[k];
+        pa.ray[3 + k] = dir[k];
+    }
+    k_raycast_warp<<<1, 32, 0, s>>>(pa, nullptr, nullptr, out, hit);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_raycast(const DevWorld &w, const int32_t origin[3], const float *cams,
