@@ -837,3 +837,42 @@ def test_random_worlds_ao_and_learned(vg, seed):
         assert np.array_equal(a.view(np.uint8), b.view(np.uint8)), (seed, fl)
         assert st.rays == 96 * 54
     dw.close()
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_random_worlds_edits_keep_the_walk_exact(vg, seed):
+    """Rounds of edits on seeded random worlds: random voxels through
+    vx_world_apply_edit, then a slab of whole bricks emptied through
+    vx_world_apply_dirty so that tile, chunk and L4 bits flip.  After every
+    round the device arrays equal the oracle's after the same changes, and so
+    does a frame (the per-tile skip words follow the masks)."""
+    rng = np.random.default_rng(9000 + seed)
+    ow = _random_world(rng)
+    VX, VY, VZ = ow.voxels
+    bx, by, bz = ow.dims
+    dw = upload_oracle(vg, ow)
+    classes = np.array([0, 0, 0, 2, 4, 12, 14, 18, 33, 35], np.uint8)
+    cam = vg.camera_from_pose((VX / 2 + 0.3, 90.0, VZ / 2 + 0.7), float(rng.uniform(0, 6.28)),
+                              -0.5, 1.2, 96, 54)
+    for rnd in range(4):
+        for _ in range(300):
+            x, y, z = int(rng.integers(VX)), int(rng.integers(VY)), int(rng.integers(VZ))
+            m = int(rng.choice(classes))
+            dw.apply_edit(x, y, z, m)
+            ow.set_voxel(x, y, z, m)
+        # a slab of empty bricks, 16 bricks (one chunk) wide in x and z, all heights
+        b0x, b0z = int(rng.integers(0, bx - 16)), int(rng.integers(0, bz - 16))
+        gx, gy, gz = np.meshgrid(np.arange(b0x, b0x + 16), np.arange(by), np.arange(b0z, b0z + 16),
+                                 indexing="ij")
+        idx = (gx + gy * bx + gz * bx * by).astype(np.uint32).ravel()
+        dw.apply_dirty(idx, np.zeros(len(idx), po.BRICK))
+        ow.a["bricks"][idx] = np.zeros(len(idx), po.BRICK)
+        ow.rebuild()
+        got = dw.download()
+        for k in po.World.NAMES:
+            assert np.array_equal(np.ascontiguousarray(got[k]).view(np.uint8),
+                                  np.ascontiguousarray(ow.a[k]).view(np.uint8)), (seed, rnd, k)
+        rec, sh, (wrec, wsh, _, _, _) = frame_pair(vg, dw, ow, cam, METHOD | po.OR_F_SHADOW)
+        assert_same_records(rec, wrec, f"seed {seed} round {rnd}")
+        assert np.array_equal(sh.view(np.uint8), wsh.view(np.uint8))
+    dw.close()
