@@ -67,7 +67,7 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--cpu-sample-seconds", type=float, default=10.0)
+    ap.add_argument("--cpu-sample-seconds", type=float, default=4.0)
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the mixed-queue, learned and serving workloads")
     ap.add_argument("--profile", action="store_true",
@@ -211,25 +211,20 @@ def frame_setup(vg, cfg, device: int):
 
 
 # -------------------------------------------------------------- cpu sample
-def cpu_sample(ow, cam, params, seconds: float, threads: int, offset0: int = 0):
-    """Time the oracle on rows offset, offset+s, ... of the frame, growing
-    the sample until it takes about `seconds` of wall time."""
+def cpu_sample(ow, cam, params, seconds: float, threads: int):
+    """Time the oracle on whole frames (beam pre-pass, every primary ray and
+    its shadow ray; rows handed out to the threads one at a time), repeated
+    until about `seconds` of wall time.  Returns (Mrays/s, frames, seconds)."""
     from oracle import pyoracle as po
-    beam, _ = po.beam_pass(ow, cam)
-    H = int(cam.res_y)
-    stride = 64
-    total_rays, total_s, rows = 0, 0.0, 0
-    offset = offset0
+    total_rays, total_s, frames = 0, 0.0, 0
     while True:
-        rec, sh, secs, _ = po.render_row_set(ow, cam, params, beam, stride, offset % stride,
-                                             threads)
+        rec, sh, _, secs, _ = po.render_frame(ow, cam, params, threads=threads)
         total_rays += len(rec) + int(sh["traced"].sum())
         total_s += secs
-        rows += len(rec) // int(cam.res_x)
-        offset += 1
-        if total_s >= seconds or rows >= H:
+        frames += 1
+        if total_s >= seconds:
             break
-    return total_rays / total_s / 1e6, rows, total_s
+    return total_rays / total_s / 1e6, frames, total_s
 
 
 def run_reference(args, cfg):
@@ -249,12 +244,13 @@ def run_reference(args, cfg):
     cam = po.camera_from_pose((cx, 140.0, cz), 0.0, math.radians(-15.0), math.radians(70.0),
                               cfg.width, cfg.height)
     params = po.default_params(cfg.flags, frame=7.0)
-    beam, _ = po.beam_pass(ow, cam)
-    stride = 16
+    # one step = the whole frame, as the device arm renders it: beam
+    # pre-pass, every primary ray and its shadow ray, rows handed out to all
+    # host threads one at a time
     per_step = []
     rays_step = []
     for s in range(args.warmup + args.steps):
-        rec, sh, secs, _ = po.render_row_set(ow, cam, params, beam, stride, s % stride, threads)
+        rec, sh, _, secs, _ = po.render_frame(ow, cam, params, threads=threads)
         if s >= args.warmup:
             per_step.append(secs)
             rays_step.append(len(rec) + int(sh["traced"].sum()))
@@ -265,12 +261,13 @@ def run_reference(args, cfg):
         "ms_per_step": round(1e3 * statistics.mean(per_step), 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": f"{CONFIG_NAME}: 2048x256x2048 world, 1920x1080 primary + shadow "
-                               "rays, beam/LUT/LOD on", "sample": f"every {stride}th row per step"},
+                               "rays, beam/LUT/LOD on", "sample": "the whole frame every step"},
         "cpu_baseline": {"value": round(value, 3), "unit": UNIT, "cores": threads,
                          "kind": "port",
-                         "sample": f"rows offset+{stride}k of the 1920x1080 frame per step "
-                                   f"(~{int(sum(rays_step) / len(rays_step))} rays), "
-                                   "oracle restatement of raycast/raymarch traversal"},
+                         "sample": f"the whole 1920x1080 frame per step (beam pre-pass, "
+                                   f"{int(sum(rays_step) / len(rays_step))} primary + shadow "
+                                   "rays), C restatement of the reference traversal (the Rust "
+                                   "reference cannot be built here)"},
         "e2e": {"value": round(value, 3), "unit": UNIT, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -624,13 +621,12 @@ def run_ours(args, cfg):
         arrays = dw.download()
         ow = po.World(*cfg.bricks, arrays=arrays)
         threads = os.cpu_count() or 1
-        cval, rows, secs = cpu_sample(ow, cam, params, args.cpu_sample_seconds, threads)
-        what = ("the full frame" if rows >= H else
-                f"{rows} of {H} rows (every 64th row, rotating offsets)")
+        cval, frames, secs = cpu_sample(ow, cam, params, args.cpu_sample_seconds, threads)
         cpu = {"value": round(cval, 3), "unit": UNIT, "cores": threads, "kind": "port",
-               "sample": f"{what} of the same frame incl. beam pre-pass and shadow rays, "
-                         f"{secs:.1f} s wall on {threads} threads; C restatement of the "
-                         "reference traversal (the Rust reference cannot be built here)"}
+               "sample": f"{frames} whole frames of the same workload (beam pre-pass, primary "
+                         f"and shadow rays), {secs:.1f} s wall on {threads} threads; C "
+                         "restatement of the reference traversal (the Rust reference cannot "
+                         "be built here)"}
         del ow, arrays
 
     extras = {}

@@ -305,7 +305,14 @@ int vx_render_primary_host(VxWorld *w, const VxCamera *cam, const VxTraceParams 
 int vx_render_primary_host_async(VxWorld *w, const VxCamera *cam, const VxTraceParams *p,
                                  VxHitRecord *rec_host, VxShadowRecord *shadow_host);
 /* Waits until every frame enqueued by vx_render_primary_host_async has
- * landed in its host buffers. */
+ * landed in its host buffers.
+ * Lost staging copies: the beam pre-pass stages the chunk masks in shared
+ * memory with one bulk copy and waits for it a bounded time.  A block that
+ * gives up reads global memory instead (its beam cells stay exact) and, if
+ * the copy has still not landed when it exits, records that in the world.
+ * The next synchronising call on the world -- vx_render_primary_host,
+ * vx_render_host_wait, vx_render_primary_stats, vx_render_primary_timed or
+ * vx_world_oob -- then returns VX_ERR_DEVICE once with a message. */
 int vx_render_host_wait(VxWorld *w);
 /* The frame of vx_render_primary, run once more with algorithmic load
  * counters on: bytes the method reads (8 per mask word / occupancy, 1 per
@@ -470,12 +477,18 @@ typedef struct {
 
 /* vx_render_primary over a caller-owned world, allocating nothing: the beam
  * scratch is a static device array of 480x270 cells built into the library
- * (each GPU that loads it holds 512 KiB until exit), so frames whose beam
- * grid exceeds 129600 cells (beyond 3840x2160) are rejected with
- * VX_ERR_INVALID.  Runs on the calling thread's current device.  The first
- * call on a device looks up the array's address there (make it before any
- * stream capture).  All calls share the array: calls that overlap on the GPU
- * race.  Asynchronous on `stream`. */
+ * (each GPU that loads it holds 512 KiB until exit).  With VX_F_BEAM set, a
+ * frame whose beam grid (ceil(w/8) x ceil(h/8) cells) exceeds 129600 cells
+ * is rejected with VX_ERR_INVALID; without the beam any resolution up to
+ * 32768 passes.  occupancy, the three mask arrays, rec_dev and shadow_dev
+ * must be 8-byte aligned (else VX_ERR_INVALID, nothing launched).  Runs on
+ * the calling thread's current device and context.  The first call in a
+ * context looks up the array's address there (make it before any stream
+ * capture); the address is cached with the context's id, so calls after a
+ * cudaDeviceReset look it up again.  All calls on a device share the array:
+ * calls that overlap on the GPU race on it.  The beam pre-pass reads the
+ * chunk masks with plain loads here (no shared-memory staging).
+ * Asynchronous on `stream`. */
 int vx_render_primary_noalloc(const VxWorldView *world, const VxCamera *cam,
                               const VxTraceParams *p, VxHitRecord *rec_dev,
                               VxShadowRecord *shadow_dev, void *stream);

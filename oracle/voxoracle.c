@@ -23,6 +23,7 @@
 
 #include <math.h>
 #include <pthread.h>
+#include <stdatomic.h>
 #include <stdlib.h>
 #include <string.h>
 #include <time.h>
@@ -1465,15 +1466,23 @@ typedef struct {
     const OrCamera *c;
     const OrParams *p;
     const float *beam;
-    uint32_t y0, y1;
+    uint32_t H;
+    _Atomic uint32_t *next_row;   /* rows are handed out one at a time */
     OrRecord *rec;
     OrShadow *sh;
     OrStats st;
 } RowJob;
 
+/* Rows cost very different amounts (sky rows end at once, terrain rows
+ * step through surfaces), so every thread takes the next untraced row until
+ * none is left. */
 static void *row_thread(void *arg) {
     RowJob *j = (RowJob *)arg;
-    or_render_rows(j->w, j->c, j->p, j->beam, j->y0, j->y1, j->rec, j->sh, &j->st);
+    for (;;) {
+        uint32_t y = atomic_fetch_add(j->next_row, 1u);
+        if (y >= j->H) break;
+        or_render_rows(j->w, j->c, j->p, j->beam, y, y + 1, j->rec, j->sh, &j->st);
+    }
     return NULL;
 }
 
@@ -1486,13 +1495,11 @@ double or_render_frame(const OrWorld *w, const OrCamera *c, const OrParams *p, O
     uint32_t H = (uint32_t)c->res_y;
     pthread_t th[256];
     RowJob jobs[256];
+    _Atomic uint32_t next_row = 0;
     int used = 0;
-    for (int i = 0; i < nthreads; ++i) {
-        uint32_t a = (uint32_t)((uint64_t)H * i / nthreads);
-        uint32_t b = (uint32_t)((uint64_t)H * (i + 1) / nthreads);
-        if (b <= a) continue;
+    for (int i = 0; i < nthreads && (uint32_t)i < H; ++i) {
         RowJob *j = &jobs[used++];
-        j->w = w; j->c = c; j->p = p; j->beam = beam; j->y0 = a; j->y1 = b;
+        j->w = w; j->c = c; j->p = p; j->beam = beam; j->H = H; j->next_row = &next_row;
         j->rec = rec; j->sh = sh;
         j->st.bytes = 0; j->st.iters = 0;
     }

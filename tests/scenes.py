@@ -147,3 +147,53 @@ def stone_blocks() -> po.World:
                     b["materials"][vi] = m
     w.rebuild()
     return w
+
+
+def pattern_world(kind, seed=0):
+    """Smallest legal window (64x16x64 bricks = 256x64x256 voxels) filled
+    with a pattern: 'full' stone, a 3D 'checker' of alternating voxels, or
+    'sparse' random voxels (5 %) of every material class."""
+    bx, by, bz = 64, 16, 64
+    x, y, z = np.meshgrid(np.arange(bx * 4), np.arange(by * 4), np.arange(bz * 4), indexing="ij")
+    if kind == "full":
+        m = np.full(x.shape, 4, np.uint8)
+    elif kind == "checker":
+        m = np.where((x + y + z) % 2 == 0, 2, 0).astype(np.uint8)
+    else:
+        rng = np.random.default_rng(seed)
+        classes = np.array([1, 2, 3, 4, 12, 14, 18, 25, 30, 31, 33, 35, 36], np.uint8)
+        m = np.where(rng.random(x.shape) < 0.05, rng.choice(classes, x.shape), 0).astype(np.uint8)
+    w = po.World(bx, by, bz)
+    vi = (x & 3) + (z & 3) * 4 + (y & 3) * 16
+    bi = (x >> 2) + (y >> 2) * bx + (z >> 2) * bx * by
+    mats = w.a["bricks"]["materials"]
+    mats[bi.ravel(), vi.ravel()] = m.ravel()
+    occ = (mats != 0).astype(np.uint64) << np.arange(64, dtype=np.uint64)
+    w.a["bricks"]["occupancy"] = np.bitwise_or.reduce(occ, axis=1)
+    w.rebuild()
+    return w
+
+
+def random_world(rng, bx=64, by=16, bz=64):
+    """Boxes and scattered voxels of every material class (water, glass,
+    foliage, decoration and leaf fringe included) in a bx*by*bz-brick world."""
+    VX, VY, VZ = bx * 4, by * 4, bz * 4
+    classes = np.array([1, 2, 3, 4, 5, 8, 12, 14, 18, 25, 30, 31, 33, 34, 35, 36, 37], np.uint8)
+    m = np.zeros((VX, VY, VZ), np.uint8)
+    for _ in range(int(rng.integers(5, 40))):
+        lo = rng.integers([0, 0, 0], [VX, VY, VZ])
+        size = rng.integers(1, [64, 24, 64])
+        hi = np.minimum(lo + size, [VX, VY, VZ])
+        m[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]] = rng.choice(classes)
+    sparse = rng.random(m.shape) < rng.uniform(0.0, 0.03)
+    m[sparse] = rng.choice(classes, int(sparse.sum()))
+    ow = po.World(bx, by, bz)
+    x, y, z = np.meshgrid(np.arange(VX), np.arange(VY), np.arange(VZ), indexing="ij")
+    vi = (x & 3) + (z & 3) * 4 + (y & 3) * 16
+    bi = (x >> 2) + (y >> 2) * bx + (z >> 2) * bx * by
+    mats = ow.a["bricks"]["materials"]
+    mats[bi.ravel(), vi.ravel()] = m.ravel()
+    occ = (mats != 0).astype(np.uint64) << np.arange(64, dtype=np.uint64)
+    ow.a["bricks"]["occupancy"] = np.bitwise_or.reduce(occ, axis=1)
+    ow.rebuild()
+    return ow

@@ -131,3 +131,33 @@ def test_header_compiles_as_c99_and_links(tmp_path):
     out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120)
     assert out.returncode == 0, out.stderr
     assert "c abi ok" in out.stdout
+
+
+def test_noalloc_refuses_misaligned_arrays_without_gpu():
+    """vx_render_primary_noalloc reads occupancy and mask words and writes
+    records as 8-byte words; a caller array that is not 8-byte aligned would
+    fault the device, so it is refused with VX_ERR_INVALID before any CUDA
+    call (this runs on a machine without a GPU)."""
+    import voxelg_b200 as vg
+    from voxelg_b200 import _lib as L
+    lib = L.load()
+    cam = vg.camera_from_pose((256.0, 140.0, 256.0), 0.0, -0.26, 1.22, 64, 36)
+    p = vg.default_params()
+    # every call below is refused before it reaches a device: the pointers
+    # are never dereferenced (byte arrays have no alignment rule, so no
+    # call here offsets one of them)
+    good = [256] * 7
+    word_arrays = {"occupancy": 0, "tile_mask": 2, "chunk_mask": 3, "l4_mask": 4}
+    for name, i in word_arrays.items():
+        ptrs = list(good)
+        ptrs[i] = 256 + 4
+        view = L.VxWorldView(128, 64, 128, *ptrs)
+        rc = lib.vx_render_primary_noalloc(C.byref(view), C.byref(cam), C.byref(p),
+                                           C.c_void_p(256), C.c_void_p(512), None)
+        assert rc == L.VX_ERR_INVALID, name
+        assert b"8-byte aligned" in lib.vx_last_error(), name
+    view = L.VxWorldView(128, 64, 128, *good)
+    for rec, sh in ((260, 512), (256, 516)):
+        rc = lib.vx_render_primary_noalloc(C.byref(view), C.byref(cam), C.byref(p),
+                                           C.c_void_p(rec), C.c_void_p(sh), None)
+        assert rc == L.VX_ERR_INVALID and b"8-byte aligned" in lib.vx_last_error()

@@ -7,6 +7,7 @@ import numpy as np
 import pytest
 
 from oracle import pyoracle as po
+from scenes import pattern_world, random_world
 
 pytestmark = pytest.mark.gpu
 
@@ -518,38 +519,13 @@ def test_host_frame_pipeline_bit_exact(vg, dev_c1, c1_oracle_world):
         assert np.array_equal(s.numpy(), wsh.view(np.uint8))
 
 
-def _pattern_world(kind, seed=0):
-    """Smallest legal window (64x16x64 bricks = 256x64x256 voxels) filled
-    with a pattern: 'full' stone, a 3D 'checker' of alternating voxels, or
-    'sparse' random voxels (5 %) of every material class."""
-    bx, by, bz = 64, 16, 64
-    x, y, z = np.meshgrid(np.arange(bx * 4), np.arange(by * 4), np.arange(bz * 4), indexing="ij")
-    if kind == "full":
-        m = np.full(x.shape, 4, np.uint8)
-    elif kind == "checker":
-        m = np.where((x + y + z) % 2 == 0, 2, 0).astype(np.uint8)
-    else:
-        rng = np.random.default_rng(seed)
-        classes = np.array([1, 2, 3, 4, 12, 14, 18, 25, 30, 31, 33, 35, 36], np.uint8)
-        m = np.where(rng.random(x.shape) < 0.05, rng.choice(classes, x.shape), 0).astype(np.uint8)
-    w = po.World(bx, by, bz)
-    vi = (x & 3) + (z & 3) * 4 + (y & 3) * 16
-    bi = (x >> 2) + (y >> 2) * bx + (z >> 2) * bx * by
-    mats = w.a["bricks"]["materials"]
-    mats[bi.ravel(), vi.ravel()] = m.ravel()
-    occ = (mats != 0).astype(np.uint64) << np.arange(64, dtype=np.uint64)
-    w.a["bricks"]["occupancy"] = np.bitwise_or.reduce(occ, axis=1)
-    w.rebuild()
-    return w
-
-
 @pytest.mark.parametrize("kind", ["full", "checker", "sparse"])
 def test_pattern_worlds_bit_exact(vg, kind):
     """Extreme worlds: every level uniform (full), the densest voxel-level
     stepping (checker), and every material class scattered (sparse), with
     the camera inside the world; frames under two flag sets and 4k random
     rays of each kind against the oracle."""
-    ow = _pattern_world(kind)
+    ow = pattern_world(kind)
     dw = upload_oracle(vg, ow)
     for pose in [((128.5, 30.2, 128.5), 0.4, -0.3), ((3.0, 63.0, 250.0), 2.2, -0.9)]:
         cam = vg.camera_from_pose(pose[0], pose[1], pose[2], 1.2, 96, 54)
@@ -718,31 +694,6 @@ def test_empty_and_single_item_batches(vg, dev_c1, c1_oracle_world):
         assert np.array_equal(sh.view(np.uint8), wsh.view(np.uint8))
 
 
-def _random_world(rng, bx=64, by=16, bz=64):
-    """Boxes and scattered voxels of every material class (water, glass,
-    foliage, decoration and leaf fringe included) in a bx*by*bz-brick world."""
-    VX, VY, VZ = bx * 4, by * 4, bz * 4
-    classes = np.array([1, 2, 3, 4, 5, 8, 12, 14, 18, 25, 30, 31, 33, 34, 35, 36, 37], np.uint8)
-    m = np.zeros((VX, VY, VZ), np.uint8)
-    for _ in range(int(rng.integers(5, 40))):
-        lo = rng.integers([0, 0, 0], [VX, VY, VZ])
-        size = rng.integers(1, [64, 24, 64])
-        hi = np.minimum(lo + size, [VX, VY, VZ])
-        m[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]] = rng.choice(classes)
-    sparse = rng.random(m.shape) < rng.uniform(0.0, 0.03)
-    m[sparse] = rng.choice(classes, int(sparse.sum()))
-    ow = po.World(bx, by, bz)
-    x, y, z = np.meshgrid(np.arange(VX), np.arange(VY), np.arange(VZ), indexing="ij")
-    vi = (x & 3) + (z & 3) * 4 + (y & 3) * 16
-    bi = (x >> 2) + (y >> 2) * bx + (z >> 2) * bx * by
-    mats = ow.a["bricks"]["materials"]
-    mats[bi.ravel(), vi.ravel()] = m.ravel()
-    occ = (mats != 0).astype(np.uint64) << np.arange(64, dtype=np.uint64)
-    ow.a["bricks"]["occupancy"] = np.bitwise_or.reduce(occ, axis=1)
-    ow.rebuild()
-    return ow
-
-
 @pytest.mark.parametrize("seed", range(12))
 def test_random_worlds_bit_exact(vg, seed):
     """Seeded random worlds (boxes and scattered voxels of every material
@@ -750,7 +701,7 @@ def test_random_worlds_bit_exact(vg, seed):
     random window origin, flag set and camera: the frame, rays of the three
     kinds (degenerate ones among them) and picks equal the oracle's."""
     rng = np.random.default_rng(1000 + seed)
-    ow = _random_world(rng)
+    ow = random_world(rng)
     VX, VY, VZ = ow.voxels
     dw = upload_oracle(vg, ow)
     wo = (int(rng.integers(-3, 4)) * 32 + int(rng.integers(0, 32)), 0,
@@ -812,7 +763,7 @@ def test_random_worlds_ao_and_learned(vg, seed):
     import torch
     from voxelg_b200 import learned as vl
     rng = np.random.default_rng(5000 + seed)
-    ow = _random_world(rng)
+    ow = random_world(rng)
     VX, VY, VZ = ow.voxels
     dw = upload_oracle(vg, ow)
     wo = (int(rng.integers(-2, 3)) * 64, 0, int(rng.integers(-2, 3)) * 64)
@@ -847,7 +798,7 @@ def test_random_worlds_edits_keep_the_walk_exact(vg, seed):
     round the device arrays equal the oracle's after the same changes, and so
     does a frame (the per-tile skip words follow the masks)."""
     rng = np.random.default_rng(9000 + seed)
-    ow = _random_world(rng)
+    ow = random_world(rng)
     VX, VY, VZ = ow.voxels
     bx, by, bz = ow.dims
     dw = upload_oracle(vg, ow)

@@ -45,6 +45,7 @@ struct VxWorld {
     struct PickBox {
         VxPickHit out;
         int32_t hit;
+        uint32_t fault;               // DevWorld::fault (kFaultBeamCopyLost)
     };
     PickBox *pick = nullptr;          // host address
     PickBox *pick_dev = nullptr;      // device address of the same block
@@ -207,6 +208,20 @@ int run_frame(VxWorld *w, vx::FrameArgs &fa, cudaStream_t s) {
     return VX_OK;
 }
 
+// After a synchronisation: a fault the kernels of this world recorded in its
+// mapped fault word (a beam CTA that left before its bulk copy landed) turns
+// the call's result into VX_ERR_DEVICE, once.
+int take_fault(VxWorld *w, const char *fn) {
+    volatile uint32_t *f = &w->pick->fault;
+    const uint32_t v = *f;
+    if (v == 0u) return VX_OK;
+    *f = 0u;
+    vx::set_error(std::string(fn) + ": a beam pre-pass block exited before its bulk copy of the "
+                  "chunk masks completed (bounded wait ran out); records of the frame are "
+                  "valid, shared memory of a later block may have been overwritten");
+    return VX_ERR_DEVICE;
+}
+
 int check_params(const VxTraceParams *p) {
     if (!p || p->max_iters < 0 || p->any_max_iters < 0 || p->max_iters > (1 << 20) ||
         p->any_max_iters > (1 << 20)) {
@@ -337,6 +352,8 @@ int vx_world_create(const VxWorldDesc *desc, VxWorld **out) {
     VX_CKW(cudaHostAlloc(reinterpret_cast<void **>(&w->pick), sizeof(VxWorld::PickBox),
                          cudaHostAllocMapped));
     VX_CKW(cudaHostGetDevicePointer(reinterpret_cast<void **>(&w->pick_dev), w->pick, 0));
+    w->pick->fault = 0u;
+    w->dw.fault = &w->pick_dev->fault;
     VX_CKW(cudaMemsetAsync(w->dw.occ, 0, d.n_bricks * sizeof(uint64_t), w->stream));
     VX_CKW(cudaMemsetAsync(w->dw.mat, 0, d.n_bricks * 64, w->stream));
     VX_CKW(cudaMemsetAsync(w->dw.tile_mask, 0, d.n_tiles * sizeof(uint64_t), w->stream));
@@ -793,7 +810,7 @@ int vx_world_oob(VxWorld *w, uint64_t *word, int32_t clear) {
     VX_CK(cudaMemcpy(&v, w->dw.oob, sizeof(v), cudaMemcpyDeviceToHost));
     if (clear) VX_CK(cudaMemset(w->dw.oob, 0, sizeof(v)));
     *word = v;
-    return VX_OK;
+    return take_fault(w, "vx_world_oob");
 }
 
 int vx_world_apply_edit(VxWorld *w, int32_t wx, int32_t wy, int32_t wz, uint8_t mat) {
@@ -1401,7 +1418,7 @@ int vx_render_primary_host(VxWorld *w, const VxCamera *cam, const VxTraceParams 
     if (rc != VX_OK) return rc;
     VX_CK(cudaStreamSynchronize(w->copy_stream));
     VX_CK(cudaStreamSynchronize(w->stream));
-    return VX_OK;
+    return take_fault(w, "vx_render_primary_host");
 }
 
 int vx_render_primary_host_async(VxWorld *w, const VxCamera *cam, const VxTraceParams *p,
@@ -1423,7 +1440,7 @@ int vx_render_host_wait(VxWorld *w) {
     std::lock_guard<std::mutex> lk(w->mu);
     if (w->copy_stream) VX_CK(cudaStreamSynchronize(w->copy_stream));
     VX_CK(cudaStreamSynchronize(w->stream));
-    return VX_OK;
+    return take_fault(w, "vx_render_host_wait");
 }
 
 int vx_render_primary_stats(VxWorld *w, const VxCamera *cam, const VxTraceParams *p,
@@ -1458,7 +1475,7 @@ int vx_render_primary_stats(VxWorld *w, const VxCamera *cam, const VxTraceParams
     VX_CK(cudaMemcpyAsync(h, w->d_stats, sizeof(h), cudaMemcpyDeviceToHost, w->stream));
     VX_CK(cudaStreamSynchronize(w->stream));
     for (int k = 0; k < 4; ++k) stats[k] = h[k];
-    return VX_OK;
+    return take_fault(w, "vx_render_primary_stats");
 }
 
 int vx_render_primary_timed(VxWorld *w, const VxCamera *cam, const VxTraceParams *p,
@@ -1493,7 +1510,7 @@ int vx_render_primary_timed(VxWorld *w, const VxCamera *cam, const VxTraceParams
     VX_CK(cudaEventSynchronize(w->ev[2]));
     VX_CK(cudaEventElapsedTime(&ms[0], w->ev[0], w->ev[1]));
     VX_CK(cudaEventElapsedTime(&ms[1], w->ev[1], w->ev[2]));
-    return VX_OK;
+    return take_fault(w, "vx_render_primary_timed");
 }
 
 struct VxQueueGraph {

@@ -67,7 +67,14 @@ struct DevWorld {
     // First out-of-range world index met by a load of the checked library
     // (array id << 56 | index; 0 = none).  nullptr: not recorded.
     unsigned long long *oob;
+    // Device-visible word (host-mapped) for faults the kernels survive but
+    // must report: bit 0 = a beam CTA exited before its bulk copy of the
+    // chunk masks into shared memory had completed (both bounded waits ran
+    // out).  nullptr: the world has no place to report one, and the beam
+    // pre-pass then reads the masks with plain loads instead of staging them.
+    uint32_t *fault;
 };
+constexpr uint32_t kFaultBeamCopyLost = 1u;
 
 // Per-frame constants of the traversal kernels (passed by value).
 struct TraceArgs {

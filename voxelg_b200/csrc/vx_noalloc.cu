@@ -10,16 +10,24 @@
 // file-scope device array that exists for as long as the library is loaded
 // (every GPU that loads the module holds its 512 KiB until process exit).
 //
-// Set-up: the device address of the array is looked up once per device, by
-// the first call made with that device current (cudaGetSymbolAddress); make
-// that first call before any stream capture.  Host code must never pass the
-// array's name to a kernel -- on the host it is only a stand-in, not a device
-// address.
+// Set-up: the device address of the array is looked up once per CUDA
+// context, by the first call made with that context current
+// (cudaGetSymbolAddress); make that first call before any stream capture.
+// The address is cached together with the context's unique id, so a call
+// after cudaDeviceReset (which destroys the primary context and, with it,
+// the module that holds the array) looks the address up again instead of
+// using a stale one.  Host code must never pass the array's name to a kernel
+// -- on the host it is only a stand-in, not a device address.
 //
 // Sharing: every call on a device uses the same array.  The beam kernel
 // rewrites every cell a frame reads before the primary kernel reads it, so
 // nothing needs clearing between calls, but calls that overlap on the GPU
 // (two streams, or two threads without ordering) race on it.
+//
+// The beam pre-pass here reads the chunk masks with plain loads: a
+// caller-owned world has no fault word through which a shared-memory staging
+// copy that never landed could be reported.
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -36,12 +44,57 @@ static __device__ __align__(256) float g_beam_scratch[kMaxBeamCells];
 
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
-float *g_scratch_addr[kMaxDevices] = {};
+struct Cached {
+    unsigned long long ctx_id;   // cuCtxGetId of the context the address belongs to
+    float *addr;
+};
+Cached g_scratch[kMaxDevices] = {};
 
-// Device address of g_beam_scratch on `dev` (which must be current).
+// cuCtxGetCurrent / cuCtxGetId through the runtime's driver entry points
+// (the library links the static runtime, not libcuda).  Caller holds g_mu.
+using CtxGetCurrentFn = CUresult (*)(CUcontext *);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long *);
+CtxGetCurrentFn g_get_cur = nullptr;
+CtxGetIdFn g_get_id = nullptr;
+
+// Unique id of the calling thread's current context, 0 when none is current.
+int current_ctx_id(unsigned long long *id) {
+    *id = 0;
+    if (!g_get_cur || !g_get_id) {
+        void *a = nullptr, *b = nullptr;
+        cudaDriverEntryPointQueryResult qa{}, qb{};
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &a, cudaEnableDefault, &qa) != cudaSuccess ||
+            cudaGetDriverEntryPoint("cuCtxGetId", &b, cudaEnableDefault, &qb) != cudaSuccess ||
+            qa != cudaDriverEntryPointSuccess || qb != cudaDriverEntryPointSuccess || !a || !b) {
+            vx::set_error("vx_render_primary_noalloc: cuCtxGetCurrent/cuCtxGetId unavailable");
+            return VX_ERR_CUDA;
+        }
+        g_get_cur = reinterpret_cast<CtxGetCurrentFn>(a);
+        g_get_id = reinterpret_cast<CtxGetIdFn>(b);
+    }
+    CUcontext ctx = nullptr;
+    if (g_get_cur(&ctx) != CUDA_SUCCESS) {
+        vx::set_error("vx_render_primary_noalloc: cuCtxGetCurrent failed");
+        return VX_ERR_CUDA;
+    }
+    if (ctx && g_get_id(ctx, id) != CUDA_SUCCESS) {
+        vx::set_error("vx_render_primary_noalloc: cuCtxGetId failed");
+        return VX_ERR_CUDA;
+    }
+    return VX_OK;
+}
+
+// Device address of g_beam_scratch in the current context of `dev`, looked
+// up again whenever that context is not the one the cached address came
+// from (cudaGetSymbolAddress also creates the device's primary context when
+// no context is current yet).
 int scratch_for(int dev, float **out) {
     std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_scratch_addr[dev]) {
+    unsigned long long id = 0;
+    int rc = current_ctx_id(&id);
+    if (rc != VX_OK) return rc;
+    Cached &c = g_scratch[dev];
+    if (!c.addr || id == 0 || c.ctx_id != id) {
         void *p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_beam_scratch);
         if (e != cudaSuccess || !p) {
@@ -49,9 +102,16 @@ int scratch_for(int dev, float **out) {
                           cudaGetErrorString(e));
             return VX_ERR_CUDA;
         }
-        g_scratch_addr[dev] = static_cast<float *>(p);
+        rc = current_ctx_id(&id);
+        if (rc != VX_OK) return rc;
+        if (id == 0) {
+            vx::set_error("vx_render_primary_noalloc: no current CUDA context");
+            return VX_ERR_CUDA;
+        }
+        c.addr = static_cast<float *>(p);
+        c.ctx_id = id;
     }
-    *out = g_scratch_addr[dev];
+    *out = c.addr;
     return VX_OK;
 }
 
@@ -88,8 +148,17 @@ extern "C" int vx_render_primary_noalloc(const VxWorldView *view, const VxCamera
         vx::set_error("vx_render_primary_noalloc: iteration caps outside [0, 2^20]");
         return VX_ERR_INVALID;
     }
-    if (reinterpret_cast<uintptr_t>(rec_dev) & 7u) {
-        vx::set_error("vx_render_primary_noalloc: records must be 8-byte aligned");
+    // 8-byte loads and stores: a misaligned one faults the device, so refuse
+    // it here, before anything is launched
+    const uintptr_t mis = (reinterpret_cast<uintptr_t>(rec_dev) |
+                           reinterpret_cast<uintptr_t>(shadow_dev) |
+                           reinterpret_cast<uintptr_t>(view->occupancy) |
+                           reinterpret_cast<uintptr_t>(view->tile_mask) |
+                           reinterpret_cast<uintptr_t>(view->chunk_mask) |
+                           reinterpret_cast<uintptr_t>(view->l4_mask)) & 7u;
+    if (mis) {
+        vx::set_error("vx_render_primary_noalloc: records, shadow records, occupancy and the "
+                      "three mask arrays must be 8-byte aligned");
         return VX_ERR_INVALID;
     }
     vx::FrameArgs fa{};

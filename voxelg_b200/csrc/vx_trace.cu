@@ -168,6 +168,10 @@ __global__ void __launch_bounds__(128) k_beam(FrameArgs fa, float *beam_out) {
         // the copy still targets this CTA's shared memory: let it land (bounded)
         bool done = false;
         for (uint32_t it = 0; it < kWaitLimit && !done; ++it) done = mbar_try_wait(bar, 0u);
+        // still in flight: the CTA exits anyway (no unbounded wait), and the
+        // host learns of it through the world's fault word (VX_ERR_DEVICE at
+        // the next synchronising call); SMEM launches always have one
+        if (!done) *reinterpret_cast<volatile uint32_t *>(fa.ta.w.fault) = kFaultBeamCopyLost;
     }
 }
 
@@ -858,7 +862,9 @@ cudaError_t launch_refresh_tiles(uint32_t tiles_w, uint32_t tiles_h, uint32_t sp
 cudaError_t launch_beam(const FrameArgs &fa, float *beam_out, cudaStream_t s) {
     dim3 block(128), grid((fa.bw + 127) / 128, fa.bh);
     const uint64_t bytes = (uint64_t)fa.ta.w.d.n_chunks * 8u;
-    const bool smem = bytes <= kBeamSmemBytes && (bytes % 16u) == 0u &&
+    // staging needs a place to report a copy that never lands (w.fault)
+    const bool smem = fa.ta.w.fault != nullptr && bytes <= kBeamSmemBytes &&
+                      (bytes % 16u) == 0u &&
                       (reinterpret_cast<uintptr_t>(fa.ta.w.chunk_mask) & 15u) == 0u;
     if (smem) {
         if (fa.stats) k_beam<true, true><<<grid, block, (size_t)bytes, s>>>(fa, beam_out);
