@@ -42,6 +42,7 @@ SOURCES = [
     ("vx_noalloc.cu", EXACT),
     ("vx_queue.cu", EXACT),
     ("vx_learned.cu", EXACT),
+    ("vx_distfield.cu", []),
     # the proposal network: its values only steer the verified restart
     ("vx_mlp.cu", []),
     ("vx_proposal.cpp", []),

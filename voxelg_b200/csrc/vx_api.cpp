@@ -2,6 +2,8 @@
 // lifetime, uploads, the traversal entry points and error reporting.
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 #include <algorithm>
 #include <array>
 #include <cmath>
@@ -78,11 +80,65 @@ struct VxWorld {
     size_t gen_cap = 0;              // bytes
     void *h_gen = nullptr;           // pinned staging of the generator's plan
     size_t h_gen_cap = 0;            // bytes
+    // empty-space distance fields of the learned form, rebuilt on demand when
+    // the masks changed (mask_gen) since they were built (df_gen)
+    uint8_t *bdf = nullptr, *tdf = nullptr, *df_tmp = nullptr;
+    std::atomic<uint64_t> mask_gen{1};
+    uint64_t df_gen = 0;
+    float *lrn_depth = nullptr;      // per-tile proven depths of learned frames without a proposal
+    size_t lrn_depth_cap = 0;
 };
 
 namespace vx {
 DevWorld world_dev(const VxWorld *w) { return w->dw; }
 int world_device(const VxWorld *w) { return w->device; }
+void world_masks_changed(VxWorld *w) { w->mask_gen.fetch_add(1, std::memory_order_relaxed); }
+
+int world_dist_fields(VxWorld *w, cudaStream_t s, DevWorld *out) {
+    std::lock_guard<std::mutex> lk(w->mu);
+    cudaError_t e = cudaSuccess;
+    if (!w->bdf) {
+        e = cudaMalloc(&w->bdf, (size_t)w->dw.d.n_bricks);
+        if (e == cudaSuccess) e = cudaMalloc(&w->tdf, (size_t)w->dw.d.n_tiles);
+        if (e == cudaSuccess) e = cudaMalloc(&w->df_tmp, (size_t)w->dw.d.n_bricks);
+        if (e != cudaSuccess) {
+            cudaFree(w->bdf);
+            cudaFree(w->tdf);
+            cudaFree(w->df_tmp);
+            w->bdf = w->tdf = w->df_tmp = nullptr;
+        }
+    }
+    const uint64_t gen = w->mask_gen.load(std::memory_order_relaxed);
+    if (e == cudaSuccess && w->df_gen != gen) {
+        e = launch_dist_fields(w->dw, w->bdf, w->tdf, w->df_tmp, s);
+        if (e == cudaSuccess) w->df_gen = gen;
+    }
+    if (e != cudaSuccess) {
+        set_error(std::string("distance fields: ") + cudaGetErrorString(e));
+        return e == cudaErrorMemoryAllocation ? VX_ERR_OOM : VX_ERR_CUDA;
+    }
+    *out = w->dw;
+    out->bdf = w->bdf;
+    out->tdf = w->tdf;
+    return VX_OK;
+}
+
+int world_learned_depth(VxWorld *w, size_t n, float **out) {
+    std::lock_guard<std::mutex> lk(w->mu);
+    if (w->lrn_depth_cap < n) {
+        cudaFree(w->lrn_depth);
+        w->lrn_depth = nullptr;
+        w->lrn_depth_cap = 0;
+        const cudaError_t e = cudaMalloc(&w->lrn_depth, std::max<size_t>(n, 1) * sizeof(float));
+        if (e != cudaSuccess) {
+            set_error(std::string("learned frame scratch: ") + cudaGetErrorString(e));
+            return e == cudaErrorMemoryAllocation ? VX_ERR_OOM : VX_ERR_CUDA;
+        }
+        w->lrn_depth_cap = n;
+    }
+    *out = w->lrn_depth;
+    return VX_OK;
+}
 }  // namespace vx
 
 namespace {
@@ -144,6 +200,10 @@ void free_world(VxWorld *w) {
     cudaFree(w->d_gate_idx);
     cudaFree(w->d_gen);
     cudaFree(w->d_edits);
+    cudaFree(w->bdf);
+    cudaFree(w->tdf);
+    cudaFree(w->df_tmp);
+    cudaFree(w->lrn_depth);
     if (w->h_gen) cudaFreeHost(w->h_gen);
     if (w->copy_stream) cudaStreamSynchronize(w->copy_stream);
     for (int i = 0; i < 2; ++i) {
@@ -429,6 +489,7 @@ int vx_world_upload(VxWorld *w, const VxBrick *bricks, const uint64_t *tile_mask
     VX_CK(cudaMemcpyAsync(w->dw.l4_mask, l4_mask, d.n_l4 * 8, cudaMemcpyHostToDevice, w->stream));
     VX_CK(cudaMemcpyAsync(w->dw.brick_uniform, brick_uniform, d.n_bricks, cudaMemcpyHostToDevice, w->stream));
     VX_CK(cudaMemcpyAsync(w->dw.tile_uniform, tile_uniform, d.n_tiles, cudaMemcpyHostToDevice, w->stream));
+    vx::world_masks_changed(w);
     VX_CK(vx::launch_tile_meta(w->dw, w->stream));
     VX_CK(cudaStreamSynchronize(w->stream));
     return VX_OK;
@@ -476,6 +537,7 @@ int vx_world_generate(VxWorld *w, const VxTerrainParams *t) {
     const vx::Dims &d = w->dw.d;
     int16_t *heights = nullptr;
     VX_CK(cudaMallocAsync(&heights, (size_t)d.vx * d.vz * sizeof(int16_t), w->stream));
+    vx::world_masks_changed(w);
     cudaError_t e = vx::launch_generate(w->dw, *t, heights, w->stream);
     cudaFreeAsync(heights, w->stream);
     VX_CK(e);
@@ -518,6 +580,7 @@ int write_edits_locked(VxWorld *w, const std::vector<std::array<int32_t, 4>> &li
                           w->stream));
     VX_CK(cudaMemcpyAsync(w->d_idx, bricks.data(), bricks.size() * sizeof(uint32_t),
                           cudaMemcpyHostToDevice, w->stream));
+    vx::world_masks_changed(w);
     VX_CK(vx::launch_edits(w->dw, w->d_edits, ed.size(), w->d_idx, bricks.size(), w->stream));
     VX_CK(cudaStreamSynchronize(w->stream));
     return VX_OK;
@@ -566,6 +629,7 @@ int run_gen_plan(VxWorld *w, uint64_t seed, vx::GenPlan &plan, const std::vector
     plan.colw = reinterpret_cast<uint32_t *>(base + off_colw);
     plan.hdr = reinterpret_cast<int32_t *>(base + off_hdr);
     plan.prims = base + off_prim;
+    vx::world_masks_changed(w);
     VX_CK(vx::launch_gen_slots(w->dw, seed, plan, w->stream));
     VX_CK(cudaStreamSynchronize(w->stream));
     return VX_OK;
@@ -1010,6 +1074,7 @@ int vx_world_apply_dirty(VxWorld *w, const uint32_t *brick_idx, const VxBrick *b
                           cudaMemcpyHostToDevice, s));
     VX_CK(cudaMemcpyAsync(w->d_bricks, pay.data(), pay.size() * sizeof(VxBrick),
                           cudaMemcpyHostToDevice, s));
+    vx::world_masks_changed(w);
     VX_CK(vx::launch_apply_dirty(w->dw, w->d_idx, w->d_bricks, idx.size(), s));
     // the staging vectors die with this call: finish the copies first
     VX_CK(cudaStreamSynchronize(s));

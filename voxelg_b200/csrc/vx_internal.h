@@ -73,8 +73,16 @@ struct DevWorld {
     // out).  nullptr: the world has no place to report one, and the beam
     // pre-pass then reads the masks with plain loads instead of staging them.
     uint32_t *fault;
+    // Empty-space distance fields (vx_distfield.cu), built on demand for the
+    // learned form: per brick / per tile the Chebyshev distance, in cells of
+    // that level, to the nearest non-empty cell (0 = non-empty, cap + 1 =
+    // nothing within the cap).  nullptr when not built.
+    const uint8_t *bdf;
+    const uint8_t *tdf;
 };
 constexpr uint32_t kFaultBeamCopyLost = 1u;
+constexpr int32_t kBrickFieldCap = 16;  // bricks (64 voxels)
+constexpr int32_t kTileFieldCap = 12;   // tiles (192 voxels)
 
 // Per-frame constants of the traversal kernels (passed by value).
 struct TraceArgs {
@@ -150,6 +158,9 @@ cudaError_t launch_gen_slots(const DevWorld &w, uint64_t seed, const GenPlan &p,
 cudaError_t launch_generate(const DevWorld &w, const VxTerrainParams &t, int16_t *heights,
                             cudaStream_t s);
 cudaError_t launch_rebuild_pyramid(const DevWorld &w, cudaStream_t s);
+// the brick and tile distance fields of w (tmp: n_bricks bytes of scratch)
+cudaError_t launch_dist_fields(const DevWorld &w, uint8_t *bdf, uint8_t *tdf, uint8_t *tmp,
+                               cudaStream_t s);
 // tile_meta of every tile from the masks and the tile LUT
 cudaError_t launch_tile_meta(const DevWorld &w, cudaStream_t s);
 // Persistent edits: ed[i] = {brick, voxel | material << 8}, distinct voxels;
@@ -204,8 +215,11 @@ cudaError_t mlp_grad(Mlp &m, const float *X, const float *target, int B, cudaStr
 cudaError_t mlp_adam(Mlp &m, float lr, cudaStream_t s);
 cudaError_t mlp_infer_features(const Mlp &m, const float *feats, size_t n, float *out,
                                cudaStream_t s);
+// proposals of a camera frame, one per bw x bh pixel block (the ray through
+// the block's centre), row-major with ceil(W / bw) blocks per row
 cudaError_t mlp_infer_frame(const Mlp &m, const DevWorld &w, const VxCamera &cam,
-                            const int32_t ro[3], float *out, cudaStream_t s);
+                            const int32_t ro[3], uint32_t bw, uint32_t bh, float *out,
+                            cudaStream_t s);
 // features of rays idx(j) = ((base + j) % n) * mult % n, j < count (mult = 1: in order)
 cudaError_t mlp_features(const DevWorld &w, const int32_t ro[3], const VxRay *rays, size_t n,
                          uint64_t base, uint64_t mult, size_t count, float *feats,
@@ -214,13 +228,39 @@ cudaError_t mlp_targets(const VxHitRecord *rec, size_t n, float max_dist, float 
                         cudaStream_t s);
 cudaError_t mlp_pose_rays(const VxCamera &c, uint64_t seed, size_t n, VxRay *rays,
                           float max_dist, cudaStream_t s);
-cudaError_t launch_learned(const TraceArgs &ta, const VxCamera &cam, const float *proposal,
-                           float scale, VxHitRecord *rec, unsigned long long *stats,
-                           cudaStream_t s);
+// learned frame: a frustum pre-pass proves, per 8 x 4 pixel tile, the rays'
+// common segment from the camera empty as far as it can into depth (one
+// float per tile, ceil(W / 8) per row); every pixel then restarts the plain
+// DDA inside its proven segment, at exp(proposal) * scale where the proof
+// covers that (proposal: log t per 16 x 8 pixel block, ceil(W / 16) per row,
+// or nullptr)
+constexpr uint32_t kLearnedTileW = 8, kLearnedTileH = 4;
+constexpr uint32_t kLearnedPropW = 16, kLearnedPropH = 8;
+// does the window suit the proof (fields built, corner a multiple of 16 in
+// x and z)?
+bool learned_proof_ok(const TraceArgs &ta);
+// the pre-pass: the proofs into depth and, when mlp and pred are given, the
+// proposals into pred, in one launch
+cudaError_t launch_learned_prepass(const TraceArgs &ta, const VxCamera &cam, float *depth,
+                                   const Mlp *mlp, float *pred, unsigned long long *stats,
+                                   cudaStream_t s);
+// depth: the proof's output, or nullptr = the plain DDA for every ray
+cudaError_t launch_learned(const TraceArgs &ta, const VxCamera &cam, const float *depth,
+                           const float *proposal, float scale, VxHitRecord *rec,
+                           unsigned long long *stats, cudaStream_t s);
 
 // accessors for library parts outside vx_api.cpp
 DevWorld world_dev(const VxWorld *w);
 int world_device(const VxWorld *w);
+// The world's masks changed (every path that rewrites them calls this): the
+// distance fields are stale until the next world_dist_fields.
+void world_masks_changed(VxWorld *w);
+// DevWorld of w with its distance fields, (re)built on `s` first when the
+// masks changed since they were last built; VX_OK or an error code.
+int world_dist_fields(VxWorld *w, cudaStream_t s, DevWorld *out);
+// n floats of per-tile depth scratch owned by w, for learned frames without
+// a proposal (grown on demand; learned frames on one world must not overlap)
+int world_learned_depth(VxWorld *w, size_t n, float **out);
 
 // thread-local error text
 void set_error(const std::string &msg);

@@ -2,11 +2,8 @@
 // with GELU (tanh form) that predicts log(first-hit t) of a ray from 6 ray
 // values and the 64 tile bits of the chunk holding the ray origin.
 //
-//   inference  BF16 tensor cores (mma.sync m16n8k16, FP32 accumulation); one
-//              warp per 16 rays, the three hidden layers chained in registers
-//              (the accumulators of two n8 tiles, packed to bf16x2, are the
-//              A operand of one k16 tile); GELU in bf16x2; weights staged in
-//              shared memory with padded rows (conflict-free B fragments);
+//   inference  BF16 tensor cores (mma.sync, FP32 accumulation), in
+//              vx_mlp_infer.cuh;
 //   training   FP32 kernels: tiled GEMM (split-K with atomics for the weight
 //              gradients), bias + GELU forward/backward, MSE loss, Adam.
 //
@@ -23,212 +20,15 @@
 #include <cmath>
 
 #include "vx_internal.h"
+#include "vx_mlp_infer.cuh"
 
 namespace vx {
 
 namespace {
 
-constexpr int kIn = kMlpIn, kH = kMlpHidden;
-constexpr int kW1 = 0, kB1 = kW1 + kH * kIn, kW2 = kB1 + kH, kB2 = kW2 + kH * kH,
-              kW3 = kB2 + kH, kB3 = kW3 + kH * kH, kWo = kB3 + kH, kBo = kWo + kH;
-static_assert(kBo + 1 == kMlpFloats, "parameter layout");
-// padded bf16 rows of the inference copy (stride in elements)
-constexpr int kS1 = kIn + 8, kS2 = kH + 8;
-constexpr int kW16 = kH * kS1 + 2 * kH * kS2;
-
-__device__ __forceinline__ float feature(const float o[3], const float d[3], uint64_t mask,
-                                         int col) {
-    if (col < 3) return (o[col] - 64.0f * floorf(o[col] * (1.0f / 64.0f))) * (1.0f / 64.0f);
-    if (col < 6) return d[col - 3];
-    if (col < 70) return (float)((mask >> (col - 6)) & 1ull);
-    return 0.0f;
-}
-
-// tile bits of the chunk holding the origin (slot coordinates; 0 outside the window)
-__device__ __forceinline__ uint64_t origin_chunk_word(const DevWorld &w, const int32_t ro[3],
-                                                      const float o[3]) {
-    const Dims &d = w.d;
-    const float fx = floorf(o[0]), fy = floorf(o[1]), fz = floorf(o[2]);
-    if (!(fx >= -1.0e9f && fx <= 1.0e9f && fy >= -1.0e9f && fy <= 1.0e9f && fz >= -1.0e9f &&
-          fz <= 1.0e9f))
-        return 0ull;
-    const int32_t vx = (int32_t)fx, vy = (int32_t)fy, vz = (int32_t)fz;
-    if ((uint32_t)(vx - ro[0]) >= (uint32_t)d.vx || (uint32_t)(vy - ro[1]) >= (uint32_t)d.vy ||
-        (uint32_t)(vz - ro[2]) >= (uint32_t)d.vz)
-        return 0ull;
-    const int32_t sx = ((vx % d.vx) + d.vx) % d.vx, sz = ((vz % d.vz) + d.vz) % d.vz;
-    if (vy < 0 || vy >= d.vy) return 0ull;
-    const int64_t ci = (sx >> 6) + (int64_t)(vy >> 6) * d.cx + (int64_t)(sz >> 6) * d.cx * d.cy;
-    return __ldg(w.chunk_mask + ci);
-}
-
-__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
-    const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
-    return *reinterpret_cast<const uint32_t *>(&v);
-}
-
-// GELU (tanh form) in f32 with the approximate tanh: 0.5x + 0.5x tanh(u),
-// u = x (k0 + k1 x^2).  (bf16 arithmetic here loses the negative tail to
-// cancellation in 1 + tanh(u).)
-__device__ __forceinline__ float gelu_fast(float x) {
-    const float u = x * fmaf(0.0356774081f, x * x, 0.7978845608f);
-    float t;
-    asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(u));
-    const float hx = 0.5f * x;
-    return fmaf(hx, t, hx);
-}
-__device__ __forceinline__ uint32_t gelu2(float lo, float hi) {
-    return pack_bf16(gelu_fast(lo), gelu_fast(hi));
-}
-
-__device__ __forceinline__ void mma_bf16(float c[4], const uint32_t a[4], uint32_t b0, uint32_t b1) {
-    asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 "
-        "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
-        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
-}
-
-struct InferArgs {
-    const __nv_bfloat16 *w;  // padded bf16 W1 | W2 | W3
-    const float *f32;        // f32 parameters (biases, output layer)
-    const float *feats;      // n x 80 features, or nullptr = camera rays
-    VxCamera cam;
-    uint32_t W, n;
-    DevWorld world;
-    int32_t ro[3];
-    float *out;              // n: predicted log t
-};
-
-// camera ray of pixel r (approximate normalization: features only)
-__device__ __forceinline__ void camera_ray(const InferArgs &a, uint32_t r, float o[3], float d[3]) {
-    const VxCamera &c = a.cam;
-    const uint32_t px = r % a.W, py = r / a.W;
-    const float u = (((float)px + 0.5f) + c.jitter_x) / c.res_x;
-    const float v = (((float)py + 0.5f) + c.jitter_y) / c.res_y;
-    const float ax = (u * 2.0f - 1.0f) * c.tan_half_fov * (c.res_x / c.res_y);
-    const float by = (1.0f - v * 2.0f) * c.tan_half_fov;
-    const float x = (c.forward[0] + c.right[0] * ax) + c.up[0] * by;
-    const float y = (c.forward[1] + c.right[1] * ax) + c.up[1] * by;
-    const float z = (c.forward[2] + c.right[2] * ax) + c.up[2] * by;
-    const float inv = rsqrtf(x * x + y * y + z * z);
-    o[0] = c.origin[0]; o[1] = c.origin[1]; o[2] = c.origin[2];
-    d[0] = x * inv; d[1] = y * inv; d[2] = z * inv;
-}
-
-// One warp = 16 rays per pass: lane g = lane/4 owns rays g and g+8 of the
-// pass, t = lane%4 the fragment columns 2t, 2t+1, 2t+8, 2t+9 of a k16 tile.
-// FRAME: camera rays of one frame.  Their origin features are the same for
-// every ray, so layer 1 is folded to z1 = c1 + W1[:, 3:6] . dir with
-// c1 = b1 + W1[:, 0:3] . origin features + W1[:, 6:70] . tile bits, computed
-// once per CTA in f32.
 template <bool FRAME>
 __global__ void __launch_bounds__(128) k_mlp_infer(InferArgs a) {
-    __shared__ __align__(16) __nv_bfloat16 sw[kW16];
-    __shared__ float4 l1[kH];   // FRAME: (W1[j][3], W1[j][4], W1[j][5], c1[j])
-    for (int i = threadIdx.x; i < kW16 / 2; i += blockDim.x)
-        reinterpret_cast<uint32_t *>(sw)[i] = reinterpret_cast<const uint32_t *>(a.w)[i];
-    if (FRAME && threadIdx.x < kH) {
-        const int j = threadIdx.x;
-        const float o[3] = {a.cam.origin[0], a.cam.origin[1], a.cam.origin[2]};
-        const float zd[3] = {0.f, 0.f, 0.f};
-        const uint64_t m = origin_chunk_word(a.world, a.ro, o);
-        const float *w1r = a.f32 + kW1 + j * kIn;
-        float c = a.f32[kB1 + j];
-        for (int k = 0; k < 3; ++k) c += w1r[k] * feature(o, zd, m, k);
-        for (int k = 6; k < 70; ++k) c += w1r[k] * feature(o, zd, m, k);
-        l1[j] = make_float4(w1r[3], w1r[4], w1r[5], c);
-    }
-    __syncthreads();
-    const __nv_bfloat16 *w1 = sw, *w2 = sw + kH * kS1, *w3 = w2 + kH * kS2;
-    const uint32_t lane = threadIdx.x & 31u, g = lane >> 2, t = lane & 3u;
-    const uint32_t warps = gridDim.x * (blockDim.x >> 5);
-    const uint32_t passes = (a.n + 15u) / 16u;
-    for (uint32_t pass = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); pass < passes;
-         pass += warps) {
-        const uint32_t r0 = pass * 16u + g, r1 = r0 + 8u;
-        const bool v0 = r0 < a.n, v1 = r1 < a.n;
-        float C[8][4];
-        if (FRAME) {
-            float o[3], d0[3] = {0, 0, 0}, d1[3] = {0, 0, 0};
-            if (v0) camera_ray(a, r0, o, d0);
-            if (v1) camera_ray(a, r1, o, d1);
-#pragma unroll
-            for (int nt = 0; nt < 8; ++nt) {
-                const float4 q0 = l1[nt * 8 + 2 * t], q1 = l1[nt * 8 + 2 * t + 1];
-                C[nt][0] = q0.w + q0.x * d0[0] + q0.y * d0[1] + q0.z * d0[2];
-                C[nt][1] = q1.w + q1.x * d0[0] + q1.y * d0[1] + q1.z * d0[2];
-                C[nt][2] = q0.w + q0.x * d1[0] + q0.y * d1[1] + q0.z * d1[2];
-                C[nt][3] = q1.w + q1.x * d1[0] + q1.y * d1[1] + q1.z * d1[2];
-            }
-        } else {
-            uint32_t A[5][4];
-            const float *p0 = a.feats + (size_t)(v0 ? r0 : 0) * kIn;
-            const float *p1 = a.feats + (size_t)(v1 ? r1 : 0) * kIn;
-#pragma unroll
-            for (int kt = 0; kt < 5; ++kt) {
-                const int c0 = kt * 16 + 2 * (int)t, c1 = c0 + 8;
-                const float2 z2 = make_float2(0.f, 0.f);
-                const float2 f00 = v0 ? *reinterpret_cast<const float2 *>(p0 + c0) : z2;
-                const float2 f10 = v1 ? *reinterpret_cast<const float2 *>(p1 + c0) : z2;
-                const float2 f01 = v0 ? *reinterpret_cast<const float2 *>(p0 + c1) : z2;
-                const float2 f11 = v1 ? *reinterpret_cast<const float2 *>(p1 + c1) : z2;
-                A[kt][0] = pack_bf16(f00.x, f00.y);
-                A[kt][1] = pack_bf16(f10.x, f10.y);
-                A[kt][2] = pack_bf16(f01.x, f01.y);
-                A[kt][3] = pack_bf16(f11.x, f11.y);
-            }
-#pragma unroll
-            for (int nt = 0; nt < 8; ++nt) {
-                const float b0 = a.f32[kB1 + nt * 8 + 2 * t], b1 = a.f32[kB1 + nt * 8 + 2 * t + 1];
-                C[nt][0] = b0; C[nt][1] = b1; C[nt][2] = b0; C[nt][3] = b1;
-                const __nv_bfloat16 *wr = w1 + (nt * 8 + g) * kS1 + 2 * t;
-#pragma unroll
-                for (int kt = 0; kt < 5; ++kt)
-                    mma_bf16(C[nt], A[kt], *reinterpret_cast<const uint32_t *>(wr + kt * 16),
-                             *reinterpret_cast<const uint32_t *>(wr + kt * 16 + 8));
-            }
-        }
-#pragma unroll
-        for (int layer = 0; layer < 2; ++layer) {
-            const __nv_bfloat16 *wl = layer == 0 ? w2 : w3;
-            const int boff = layer == 0 ? kB2 : kB3;
-            uint32_t Hf[4][4];
-#pragma unroll
-            for (int kt = 0; kt < 4; ++kt) {
-                Hf[kt][0] = gelu2(C[2 * kt][0], C[2 * kt][1]);
-                Hf[kt][1] = gelu2(C[2 * kt][2], C[2 * kt][3]);
-                Hf[kt][2] = gelu2(C[2 * kt + 1][0], C[2 * kt + 1][1]);
-                Hf[kt][3] = gelu2(C[2 * kt + 1][2], C[2 * kt + 1][3]);
-            }
-#pragma unroll
-            for (int nt = 0; nt < 8; ++nt) {
-                const float b0 = a.f32[boff + nt * 8 + 2 * t], b1 = a.f32[boff + nt * 8 + 2 * t + 1];
-                C[nt][0] = b0; C[nt][1] = b1; C[nt][2] = b0; C[nt][3] = b1;
-                const __nv_bfloat16 *wr = wl + (nt * 8 + g) * kS2 + 2 * t;
-#pragma unroll
-                for (int kt = 0; kt < 4; ++kt)
-                    mma_bf16(C[nt], Hf[kt], *reinterpret_cast<const uint32_t *>(wr + kt * 16),
-                             *reinterpret_cast<const uint32_t *>(wr + kt * 16 + 8));
-            }
-        }
-        // output: GELU(h3) . wo + bo, reduced over the four lanes of a quad
-        float y0 = 0.f, y1 = 0.f;
-#pragma unroll
-        for (int nt = 0; nt < 8; ++nt) {
-            const float wa = a.f32[kWo + nt * 8 + 2 * t], wb = a.f32[kWo + nt * 8 + 2 * t + 1];
-            y0 += gelu_fast(C[nt][0]) * wa + gelu_fast(C[nt][1]) * wb;
-            y1 += gelu_fast(C[nt][2]) * wa + gelu_fast(C[nt][3]) * wb;
-        }
-        y0 += __shfl_xor_sync(0xFFFFFFFFu, y0, 1);
-        y0 += __shfl_xor_sync(0xFFFFFFFFu, y0, 2);
-        y1 += __shfl_xor_sync(0xFFFFFFFFu, y1, 1);
-        y1 += __shfl_xor_sync(0xFFFFFFFFu, y1, 2);
-        if (t == 0) {
-            if (v0) a.out[r0] = y0 + a.f32[kBo];
-            if (v1) a.out[r1] = y1 + a.f32[kBo];
-        }
-    }
+    mlp_infer_body<FRAME>(a, blockIdx.x, gridDim.x);
 }
 
 // ------------------------------------------------------------- training
@@ -524,6 +324,8 @@ cudaError_t mlp_adam(Mlp &m, float lr, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+// Grid of the inference kernel: one 16-ray pass per warp (4 per CTA), at
+// most eight CTAs per SM; larger batches loop.
 static unsigned infer_blocks(size_t n) {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
@@ -533,13 +335,17 @@ static unsigned infer_blocks(size_t n) {
 }
 
 cudaError_t mlp_infer_frame(const Mlp &m, const DevWorld &w, const VxCamera &cam,
-                            const int32_t ro[3], float *out, cudaStream_t s) {
+                            const int32_t ro[3], uint32_t bw, uint32_t bh, float *out,
+                            cudaStream_t s) {
     InferArgs a{};
     a.w = reinterpret_cast<const __nv_bfloat16 *>(m.w16);
     a.f32 = m.p;
     a.cam = cam;
     a.W = (uint32_t)cam.res_x;
-    a.n = (uint32_t)cam.res_x * (uint32_t)cam.res_y;
+    a.blk_w = bw ? bw : 1u;
+    a.blk_h = bh ? bh : 1u;
+    a.bw = (a.W + a.blk_w - 1u) / a.blk_w;
+    a.n = a.bw * (((uint32_t)cam.res_y + a.blk_h - 1u) / a.blk_h);
     a.world = w;
     a.ro[0] = ro[0]; a.ro[1] = ro[1]; a.ro[2] = ro[2];
     a.out = out;

@@ -21,10 +21,14 @@ struct VxProposal {
     vx::Mlp m;
     cudaStream_t stream = nullptr;
     std::mutex mu;
-    float *pred = nullptr;             // per-pixel proposal of the last frame
-    size_t pred_cap = 0;
+    float *pred = nullptr;             // per-block proposals of the last frame
+    float *depth = nullptr;            // per-tile proven depths of the last frame
+    size_t pred_cap = 0, depth_cap = 0;
     unsigned long long *stats = nullptr;
-    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+    // frame timing (frame start / inference start / inference end / frame end)
+    // and the fork / join of the inference on `stream` beside the frame
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t fork = nullptr, join = nullptr;
 };
 
 namespace {
@@ -213,9 +217,12 @@ int vx_proposal_destroy(VxProposal *p) {
     if (p->stream) cudaStreamSynchronize(p->stream);
     vx::mlp_free(p->m);
     if (p->pred) cudaFree(p->pred);
+    if (p->depth) cudaFree(p->depth);
     if (p->stats) cudaFree(p->stats);
     for (auto &e : p->ev)
         if (e) cudaEventDestroy(e);
+    if (p->fork) cudaEventDestroy(p->fork);
+    if (p->join) cudaEventDestroy(p->join);
     if (p->stream) cudaStreamDestroy(p->stream);
     delete p;
     return VX_OK;
@@ -411,36 +418,57 @@ int vx_render_learned(VxWorld *w, VxProposal *prop, const VxCamera *cam, const V
     VX_CK(cudaSetDevice(device));
     cudaStream_t s = as_stream(stream);
     vx::TraceArgs ta{};
-    ta.w = vx::world_dev(w);
+    // the world with its empty-space distance fields, rebuilt on s when its
+    // masks changed since the last learned frame
+    int rc = vx::world_dist_fields(w, s, &ta.w);
+    if (rc != VX_OK) return rc;
     ta.p = *p;
     for (int k = 0; k < 3; ++k) ta.ro[k] = cam->world_origin[k];
-    const size_t npx = (size_t)cam->res_x * (size_t)cam->res_y;
-    // scratch: the proposal's, or a temporary one for a statistics call without it
+    // one proven depth per 8 x 4 pixel tile (the ray bundle of the frustum
+    // pre-pass) and one proposal per 16 x 8 pixels
+    const uint32_t W = (uint32_t)cam->res_x, H = (uint32_t)cam->res_y;
+    const size_t n_tiles = (size_t)((W + vx::kLearnedTileW - 1u) / vx::kLearnedTileW) *
+                           ((H + vx::kLearnedTileH - 1u) / vx::kLearnedTileH);
+    const size_t n_props = (size_t)((W + vx::kLearnedPropW - 1u) / vx::kLearnedPropW) *
+                           ((H + vx::kLearnedPropH - 1u) / vx::kLearnedPropH);
+    // scratch: the proposal's, or the world's (and temporary statistics
+    // scratch) for a call without it
     std::unique_lock<std::mutex> lk;
     unsigned long long *d_stats = nullptr;
-    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     if (prop) {
         lk = std::unique_lock<std::mutex>(prop->mu);
-        if (prop->pred_cap < npx) {
+        if (prop->pred_cap < n_props) {
             if (prop->pred) cudaFree(prop->pred);
             prop->pred = nullptr;
             prop->pred_cap = 0;
-            VX_CK(cudaMalloc(&prop->pred, npx * sizeof(float)));
-            prop->pred_cap = npx;
+            VX_CK(cudaMalloc(&prop->pred, n_props * sizeof(float)));
+            prop->pred_cap = n_props;
+        }
+        if (prop->depth_cap < n_tiles) {
+            if (prop->depth) cudaFree(prop->depth);
+            prop->depth = nullptr;
+            prop->depth_cap = 0;
+            VX_CK(cudaMalloc(&prop->depth, n_tiles * sizeof(float)));
+            prop->depth_cap = n_tiles;
+        }
+        if (!prop->fork) {
+            VX_CK(cudaEventCreateWithFlags(&prop->fork, cudaEventDisableTiming));
+            VX_CK(cudaEventCreateWithFlags(&prop->join, cudaEventDisableTiming));
         }
         if (stats) {
             if (!prop->stats) VX_CK(cudaMalloc(&prop->stats, 8 * sizeof(unsigned long long)));
             if (!prop->ev[0])
                 for (auto &e : prop->ev) VX_CK(cudaEventCreate(&e));
             d_stats = prop->stats;
-            for (int k = 0; k < 3; ++k) ev[k] = prop->ev[k];
+            for (int k = 0; k < 4; ++k) ev[k] = prop->ev[k];
         }
     }
     // a statistics call without a proposal uses temporary scratch, released
     // on every path out of this function
     struct Temp {
         unsigned long long *stats = nullptr;
-        cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+        cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
         ~Temp() {
             if (stats) cudaFree(stats);
             for (auto &x : ev)
@@ -451,17 +479,26 @@ int vx_render_learned(VxWorld *w, VxProposal *prop, const VxCamera *cam, const V
         VX_CK(cudaMalloc(&temp.stats, 8 * sizeof(unsigned long long)));
         for (auto &x : temp.ev) VX_CK(cudaEventCreate(&x));
         d_stats = temp.stats;
-        for (int k = 0; k < 3; ++k) ev[k] = temp.ev[k];
+        for (int k = 0; k < 4; ++k) ev[k] = temp.ev[k];
     }
+    float *depth = prop ? prop->depth : nullptr;
+    if (!prop) {
+        rc = vx::world_learned_depth(w, n_tiles, &depth);
+        if (rc != VX_OK) return rc;
+    }
+    // s: [ev0] pre-pass (proofs + proposals) -> frame [ev3]
     cudaError_t e = cudaSuccess;
     if (stats) e = cudaMemsetAsync(d_stats, 0, 8 * sizeof(unsigned long long), s);
     if (e == cudaSuccess && stats) e = cudaEventRecord(ev[0], s);
-    if (e == cudaSuccess && prop) e = vx::mlp_infer_frame(prop->m, ta.w, *cam, ta.ro, prop->pred, s);
-    if (e == cudaSuccess && stats) e = cudaEventRecord(ev[1], s);
+    const bool proof = e == cudaSuccess && vx::learned_proof_ok(ta);
+    if (proof)
+        e = vx::launch_learned_prepass(ta, *cam, depth, prop ? &prop->m : nullptr,
+                                       prop ? prop->pred : nullptr, d_stats, s);
     if (e == cudaSuccess)
-        e = vx::launch_learned(ta, *cam, prop ? prop->pred : nullptr, scale, rec_dev, d_stats, s);
-    if (e == cudaSuccess && stats) e = cudaEventRecord(ev[2], s);
-    if (e == cudaSuccess && stats) e = cudaEventSynchronize(ev[2]);
+        e = vx::launch_learned(ta, *cam, proof ? depth : nullptr,
+                               proof && prop ? prop->pred : nullptr, scale, rec_dev, d_stats, s);
+    if (e == cudaSuccess && stats) e = cudaEventRecord(ev[3], s);
+    if (e == cudaSuccess && stats) e = cudaEventSynchronize(ev[3]);
     if (e == cudaSuccess && stats) {
         unsigned long long h[8];
         e = cudaMemcpy(h, d_stats, sizeof(h), cudaMemcpyDeviceToHost);
@@ -474,9 +511,8 @@ int vx_render_learned(VxWorld *w, VxProposal *prop, const VxCamera *cam, const V
             stats->iters = h[5];
             stats->fallback = h[6];
             stats->rays = h[7];
-            e = cudaEventElapsedTime(&stats->infer_ms, ev[0], ev[1]);
-            if (e == cudaSuccess) e = cudaEventElapsedTime(&stats->trace_ms, ev[1], ev[2]);
-            if (!prop) stats->infer_ms = 0.0f;
+            stats->infer_ms = 0.0f;  // inside the pre-pass, beside the proofs
+            e = cudaEventElapsedTime(&stats->trace_ms, ev[0], ev[3]);
         }
     }
     if (e != cudaSuccess) {

@@ -203,8 +203,10 @@ bool run_edit(VxServer *s, Edit *e) {
         if (err == cudaSuccess)
             err = cudaMemcpyAsync(b.d_bricks, b.h_bricks, n * sizeof(VxBrick),
                                   cudaMemcpyHostToDevice, s->edit_stream);
-        if (err == cudaSuccess)
+        if (err == cudaSuccess) {
+            vx::world_masks_changed(s->world);
             err = vx::launch_apply_dirty(s->ta.w, b.d_idx, b.d_bricks, n, s->edit_stream);
+        }
         if (err == cudaSuccess) err = cudaEventRecord(b.used, s->edit_stream);
         if (err == cudaSuccess) err = cudaEventRecord(s->edit_done, s->edit_stream);
         if (err == cudaSuccess) {
