@@ -359,6 +359,13 @@ def trace_any_one(world: World, origin_world, d, params, ro=(0, 0, 0), max_dist=
     return bool(occ), int(steps.value)
 
 
+def ray_dir_uv(cam, u: float, v: float):
+    """ray_dir_uv (raymarch.wgsl:430-438) of a camera at screen (u, v)."""
+    out = (C.c_float * 3)()
+    load().or_ray_dir_uv(C.byref(camera_from(cam)), u, v, out)
+    return tuple(out)
+
+
 def camera_from_pose(pos, yaw, pitch, fov_y, width, height, world_origin=(0, 0, 0)) -> OrCamera:
     """src/camera.rs:25-42 (basis) and :140-166 (uniform) in f32 numpy."""
     import math

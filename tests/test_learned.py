@@ -232,11 +232,29 @@ def test_learned_unaligned_window_and_oracle(env, trained, c1_oracle_world):
     assert np.array_equal(a.view(np.uint8), want.view(np.uint8))
 
 
+def _batch_ms(frame, reps=20):
+    """Mean ms per frame of `reps` frames enqueued back to back on the
+    current stream between two CUDA events."""
+    import torch
+    st = torch.cuda.current_stream()
+    for _ in range(3):
+        frame()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(reps):
+        frame()
+    e1.record(st)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
 @pytest.mark.gpu
 def test_learned_gain_over_plain(env, trained):
-    """What the trained network buys on the 1920x1080 frame: fewer DDA
-    iterations per ray than the plain DDA, with identical records, and some
-    proposals accepted.  Prints rays/s of both forms."""
+    """What the learned form buys on the 1920x1080 frame: fewer DDA
+    iterations per ray than the plain DDA with identical records, and more
+    rays per second (frames enqueued back to back, the same way for both
+    forms)."""
     import torch
     from voxelg_b200 import learned as vl
     vg, dw, _ = env
@@ -245,16 +263,96 @@ def test_learned_gain_over_plain(env, trained):
     a, b, st = _plain_and_learned(vg, dw, cam, F_METHOD, trained[0])
     plain_iters = int(a["steps"].astype(np.int64).sum())
     assert _same_but_steps(a, b)
-    assert st.iters < 0.8 * plain_iters, (st.iters, plain_iters)
-    assert st.accepted + st.miss > 0.2 * st.rays
+    assert st.iters < 0.7 * plain_iters, (st.iters, plain_iters)
+    assert st.miss > 0.2 * st.rays and st.none < 0.01 * st.rays
     rec = torch.empty(1920 * 1080 * 24, dtype=torch.uint8, device="cuda")
-    for _ in range(3):
-        vg.render_primary_timed(dw, cam, p, rec)
-        vl.render_learned(dw, trained[0], cam, p, rec)
-    plain_ms = min(vg.render_primary_timed(dw, cam, p, rec)[1] for _ in range(10))
-    learned = [vl.render_learned(dw, trained[0], cam, p, rec) for _ in range(10)]
-    learned_ms = min(s.infer_ms + s.trace_ms for s in learned)
-    print(f"\nplain {plain_iters / st.rays:.2f} it/ray {plain_ms:.3f} ms; learned "
-          f"{st.iters / st.rays:.2f} it/ray {learned_ms:.3f} ms "
-          f"(accepted {st.accepted / st.rays:.1%}, partial {st.partial / st.rays:.1%}, "
+    plain_ms = min(_batch_ms(lambda: vg.render_primary(dw, cam, p, rec)) for _ in range(3))
+    learned_ms = min(_batch_ms(lambda: vl.render_learned(dw, trained[0], cam, p, rec,
+                                                         stats=False)) for _ in range(3))
+    print(f"\nplain {plain_iters / st.rays:.2f} it/ray {plain_ms:.4f} ms; learned "
+          f"{st.iters / st.rays:.2f} it/ray {learned_ms:.4f} ms ({plain_ms / learned_ms:.3f}x; "
+          f"accepted {st.accepted / st.rays:.1%}, partial {st.partial / st.rays:.1%}, "
           f"miss {st.miss / st.rays:.1%})")
+    assert learned_ms < 0.95 * plain_ms, (plain_ms, learned_ms)
+
+
+@pytest.mark.gpu
+def test_trained_network_predicts_first_hits(env, trained):
+    """The network the learned form runs: on the benchmark frame, its
+    per-block estimate of log first-hit distance (a miss counts as log tmax,
+    the label it is trained on) has under 0.6x the mean squared error of an
+    untrained network's.  The fixture's short training (1200 steps) still
+    over-estimates near hits, so the error is measured over every block
+    centre, hits and misses, as the training loss is.  The records stay the
+    plain DDA's whatever the network predicts."""
+    import torch
+    from voxelg_b200 import learned as vl
+    vg, dw, _ = env
+    cam = vg.default_camera(dw, 1920, 1080)
+    p = vg.default_params(F_METHOD)
+    plain, _ = vg.render_primary(dw, cam, p)
+    torch.cuda.synchronize()
+    a = vg.records(plain)
+    W, H, tmax = 1920, 1080, 700.0
+    # block centre rays of the 16x8 proposal blocks, as features
+    bx, by = np.meshgrid(np.arange(W // 16), np.arange(H // 8))
+    px = (bx * 16 + 8).ravel()
+    py = (by * 8 + 4).ravel()
+    r = a.reshape(H, W)[py, px]
+    hit = (r["flags"] & 1) != 0
+    target = np.where(hit, np.log(np.maximum(r["t"], 1e-3)), np.log(tmax))
+    rays = np.zeros(len(px), po.RAY)
+    rays["org"] = np.array(list(cam.origin), np.float32)
+    rays["dir"] = np.stack([np.array(po.ray_dir_uv(cam, (x + 0.5) / W, (y + 0.5) / H),
+                                     np.float32) for x, y in zip(px, py)])
+    rays["tmax"] = tmax
+    untrained = vl.Proposal(dw, seed=11)
+    mse = {}
+    for name, prop in (("trained", trained[0]), ("untrained", untrained)):
+        y = prop.infer(prop.features(dw, rays)).cpu().numpy()
+        mse[name] = float(np.mean((y - target) ** 2))
+    untrained.close()
+    print(f"\nmean squared log t error over {len(px)} block centres "
+          f"({hit.mean():.0%} hits): {mse}")
+    assert mse["trained"] < 0.6 * mse["untrained"], mse
+
+
+@pytest.mark.gpu
+def test_learned_equals_plain_on_the_2048_world(env, trained):
+    """The 2048x256x2048 benchmark world, where rays reach the tile LOD
+    distance (520) inside the window: the learned form (proofs capped before
+    tile_lod_t in brick cubes) gives the plain DDA's records except steps,
+    for several poses and flag sets."""
+    vg, dw_c1, _ = env
+    cfg = vg.CONFIGS["c2"]
+    dw = vg.DeviceWorld(*cfg.bricks)
+    dw.generate(cfg.terrain)
+    try:
+        for pos, yaw, pitch in (((1024.0, 140.0, 1024.0), 0.0, -15.0),
+                                ((300.5, 180.25, 1900.75), 2.4, -6.0),
+                                ((1700.0, 230.0, 200.0), 4.1, -3.0)):
+            cam = vg.camera_from_pose(pos, yaw, math.radians(pitch), math.radians(70.0), 640, 360)
+            for flags in (F_METHOD, 1 | 4, 4):
+                a, b, st = _plain_and_learned(vg, dw, cam, flags, None)
+                assert _same_but_steps(a, b), (pos, flags)
+                assert st.none < 0.01 * st.rays
+    finally:
+        dw.close()
+
+
+@pytest.mark.gpu
+def test_learned_iteration_cap_falls_back(env, trained):
+    """With a small iteration cap the restarted walks' inflated counters
+    reach it and the plain DDA decides those rays: records still equal."""
+    vg, dw, _ = env
+    cam = vg.default_camera(dw, 480, 270)
+    for cap in (6, 12, 20):
+        p = vg.default_params(F_METHOD)
+        p.max_iters = cap
+        import torch
+        from voxelg_b200 import learned as vl
+        plain, _ = vg.render_primary(dw, cam, p)
+        rec = torch.empty_like(plain)
+        st = vl.render_learned(dw, trained[0], cam, p, rec)
+        assert _same_but_steps(vg.records(plain), vg.records(rec)), cap
+        assert st.fallback > 0, cap
