@@ -116,6 +116,26 @@ typedef struct {
     uint16_t pad;
 } VxShadowRecord;
 
+/* One pixel's VxHitRecord and VxShadowRecord, losslessly in 16 bytes (half
+ * the 32 the pair takes), for frames delivered to host memory.
+ *   voxel   a hit's voxel relative to the window corner (world_origin),
+ *           rx + wx * (ry + wy * rz) with (wx, wy, wz) the window's voxel
+ *           counts; 0 for a miss (whose record voxel is 0, 0, 0)
+ *   face, mat, flags, t   as VxHitRecord (pad is always 0)
+ *   shadow  bit0 occluded, bit1 traced
+ *   steps   primary steps in bits 0-15, shadow steps in bits 16-31
+ * Frames packed this way need wx * wy * wz <= 2^32 and max_iters,
+ * any_max_iters <= 65535.  vx_unpack_records restores both records. */
+typedef struct {
+    uint32_t voxel;
+    uint8_t face;
+    uint8_t mat;
+    uint8_t flags;
+    uint8_t shadow;
+    float t;
+    uint32_t steps;
+} VxPackedRecord;
+
 /* src/raycast.rs:13-17 */
 typedef struct {
     int32_t voxel[3];
@@ -314,6 +334,22 @@ int vx_render_primary_host_async(VxWorld *w, const VxCamera *cam, const VxTraceP
  * vx_render_host_wait, vx_render_primary_stats, vx_render_primary_timed or
  * vx_world_oob -- then returns VX_ERR_DEVICE once with a message. */
 int vx_render_host_wait(VxWorld *w);
+/* vx_render_primary_host / _async with packed records: out_host (res_x *
+ * res_y entries, pinned memory recommended) receives the frame as
+ * VxPackedRecord, half the bytes of records plus shadow records.  The
+ * async form shares the two-buffer pipeline and vx_render_host_wait of
+ * vx_render_primary_host_async.  VX_ERR_INVALID when the window has more
+ * than 2^32 voxels or max_iters / any_max_iters exceed 65535. */
+int vx_render_primary_host_packed(VxWorld *w, const VxCamera *cam, const VxTraceParams *p,
+                                  VxPackedRecord *out_host);
+int vx_render_primary_host_packed_async(VxWorld *w, const VxCamera *cam,
+                                        const VxTraceParams *p, VxPackedRecord *out_host);
+/* Host: n packed records back to VxHitRecord / VxShadowRecord, byte for
+ * byte what vx_render_primary_host writes.  world_origin is the frame
+ * camera's world_origin, window_voxels the world's voxel counts
+ * (4 * bricks per axis).  Either output pointer may be NULL. */
+int vx_unpack_records(const VxPackedRecord *packed, size_t n, const int32_t world_origin[3],
+                      const uint32_t window_voxels[3], VxHitRecord *rec, VxShadowRecord *shadow);
 /* The frame of vx_render_primary, run once more with algorithmic load
  * counters on: bytes the method reads (8 per mask word / occupancy, 1 per
  * LUT or material byte) and loop iterations, summed over all rays.

@@ -133,8 +133,11 @@ SHADOW_DTYPE = np.dtype([("steps", "<u4"), ("occluded", "u1"), ("traced", "u1"),
 RAY_DTYPE = np.dtype([("org", "<f4", (3,)), ("dir", "<f4", (3,)), ("tmax", "<f4"),
                       ("kind", "<u4")])
 PICK_DTYPE = np.dtype([("voxel", "<i4", (3,)), ("normal", "<i4", (3,))])
+PACKED_DTYPE = np.dtype([("voxel", "<u4"), ("face", "u1"), ("mat", "u1"), ("flags", "u1"),
+                         ("shadow", "u1"), ("t", "<f4"), ("steps", "<u4")])
 assert BRICK_DTYPE.itemsize == 72 and RECORD_DTYPE.itemsize == 24
 assert SHADOW_DTYPE.itemsize == 8 and RAY_DTYPE.itemsize == 32
+assert PACKED_DTYPE.itemsize == 16
 
 # every symbol include/voxrt.h declares: (name, restype, argtypes)
 _vp = C.c_void_p
@@ -171,6 +174,11 @@ SIGNATURES = [
     ("vx_render_primary_host", C.c_int, [_vp, _P(VxCamera), _P(VxTraceParams), _vp, _vp]),
     ("vx_render_primary_host_async", C.c_int, [_vp, _P(VxCamera), _P(VxTraceParams), _vp, _vp]),
     ("vx_render_host_wait", C.c_int, [_vp]),
+    ("vx_render_primary_host_packed", C.c_int, [_vp, _P(VxCamera), _P(VxTraceParams), _vp]),
+    ("vx_render_primary_host_packed_async", C.c_int,
+     [_vp, _P(VxCamera), _P(VxTraceParams), _vp]),
+    ("vx_unpack_records", C.c_int,
+     [_vp, C.c_size_t, _P(C.c_int32), _P(C.c_uint32), _vp, _vp]),
     ("vx_render_ao", C.c_int, [_vp, _P(VxCamera), _vp, _vp, _vp]),
     ("vx_render_primary_stats", C.c_int, [_vp, _P(VxCamera), _P(VxTraceParams),
                                           _P(C.c_uint64)]),

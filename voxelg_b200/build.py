@@ -43,6 +43,7 @@ SOURCES = [
     ("vx_queue.cu", EXACT),
     ("vx_learned.cu", EXACT),
     ("vx_distfield.cu", []),
+    ("vx_pack.cu", []),
     # the proposal network: its values only steer the verified restart
     ("vx_mlp.cu", []),
     ("vx_proposal.cpp", []),

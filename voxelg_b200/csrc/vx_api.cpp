@@ -11,6 +11,7 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <thread>
 #include <new>
 #include <string>
 #include <unordered_map>
@@ -73,7 +74,8 @@ struct VxWorld {
     // after its last copy to the host (frame N+1 renders while N copies)
     VxHitRecord *hrec[2] = {nullptr, nullptr};
     VxShadowRecord *hsh[2] = {nullptr, nullptr};
-    size_t hrec_cap[2] = {0, 0}, hsh_cap[2] = {0, 0};
+    VxPackedRecord *hpk[2] = {nullptr, nullptr};   // packed frames (vx_pack.cu)
+    size_t hrec_cap[2] = {0, 0}, hsh_cap[2] = {0, 0}, hpk_cap[2] = {0, 0};
     cudaEvent_t copy_done[2] = {nullptr, nullptr};
     uint64_t host_frames = 0;
     void *d_gen = nullptr;           // chunk generator scratch: plan, column words, trees
@@ -209,6 +211,7 @@ void free_world(VxWorld *w) {
     for (int i = 0; i < 2; ++i) {
         cudaFree(w->hrec[i]);
         cudaFree(w->hsh[i]);
+        cudaFree(w->hpk[i]);
         if (w->copy_done[i]) cudaEventDestroy(w->copy_done[i]);
     }
     w->qs.release();
@@ -1408,8 +1411,14 @@ namespace {
 // between two device buffers; a frame first waits, on the device, for the
 // copies of the frame two calls back that used its buffer.  Caller holds
 // w->mu.
+// One frame into host memory on the world's two streams: the traversal in
+// row bands on w->stream, each band copied on copy_stream once it is done.
+// rec_host / shadow_host receive the full records; or, with packed_host set,
+// each band is packed (16 bytes per pixel, shadows included) and only the
+// packed form crosses to the host.
 int enqueue_host_frame(VxWorld *w, const VxCamera *cam, const VxTraceParams *p,
-                       VxHitRecord *rec_host, VxShadowRecord *shadow_host, uint32_t bands) {
+                       VxHitRecord *rec_host, VxShadowRecord *shadow_host,
+                       VxPackedRecord *packed_host, uint32_t bands) {
     static_assert(kSyncBands <= sizeof(w->band_ev) / sizeof(w->band_ev[0]), "one event per band");
     static_assert(kAsyncBands <= kSyncBands, "one event per band");
     vx::FrameArgs fa = make_frame(w, cam, p);
@@ -1422,14 +1431,16 @@ int enqueue_host_frame(VxWorld *w, const VxCamera *cam, const VxTraceParams *p,
     if (!w->copy_done[0]) {
         for (auto &e : w->copy_done) VX_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     }
-    if (w->hrec_cap[buf] < n || w->hsh_cap[buf] < n) {
+    const bool packed = packed_host != nullptr;
+    if (w->hrec_cap[buf] < n || w->hsh_cap[buf] < n || (packed && w->hpk_cap[buf] < n)) {
         VX_CK(cudaStreamSynchronize(w->copy_stream));   // no copy may read a freed buffer
         int rc = ensure(&w->hrec[buf], &w->hrec_cap[buf], n);
         if (rc == VX_OK) rc = ensure(&w->hsh[buf], &w->hsh_cap[buf], n);
+        if (rc == VX_OK && packed) rc = ensure(&w->hpk[buf], &w->hpk_cap[buf], n);
         if (rc != VX_OK) return rc;
     }
     fa.rec = w->hrec[buf];
-    fa.shadow = shadow_host ? w->hsh[buf] : nullptr;
+    fa.shadow = (shadow_host || packed) ? w->hsh[buf] : nullptr;
     VX_CK(cudaStreamWaitEvent(w->stream, w->copy_done[buf], 0));
     // bands of rows (the grid form only; the persistent form renders in one go)
     const uint32_t nb = fa.work ? 1u : bands;
@@ -1446,9 +1457,19 @@ int enqueue_host_frame(VxWorld *w, const VxCamera *cam, const VxTraceParams *p,
         if (fa.work) fa.y0 = 0, fa.y1 = fa.H;
         if (fa.y1 <= fa.y0) break;
         VX_CK(vx::launch_primary(fa, w->stream));
+        const size_t r0 = (size_t)fa.y0 * fa.W, rn = (size_t)(fa.y1 - fa.y0) * fa.W;
+        if (packed) {
+            const uint32_t wx = (uint32_t)w->dw.d.vx, wy = (uint32_t)w->dw.d.vy;
+            VX_CK(vx::launch_pack(fa.rec, fa.shadow, r0, rn, fa.ta.ro, wx, wy, w->hpk[buf],
+                                  w->stream));
+        }
         VX_CK(cudaEventRecord(w->band_ev[b], w->stream));
         VX_CK(cudaStreamWaitEvent(w->copy_stream, w->band_ev[b], 0));
-        const size_t r0 = (size_t)fa.y0 * fa.W, rn = (size_t)(fa.y1 - fa.y0) * fa.W;
+        if (packed) {
+            VX_CK(cudaMemcpyAsync(packed_host + r0, w->hpk[buf] + r0, rn * sizeof(VxPackedRecord),
+                                  cudaMemcpyDeviceToHost, w->copy_stream));
+            continue;
+        }
         VX_CK(cudaMemcpyAsync(rec_host + r0, fa.rec + r0, rn * sizeof(VxHitRecord),
                               cudaMemcpyDeviceToHost, w->copy_stream));
         if (shadow_host)
@@ -1479,7 +1500,7 @@ int vx_render_primary_host(VxWorld *w, const VxCamera *cam, const VxTraceParams 
     int rc = host_frame_args(w, cam, p, rec_host, "vx_render_primary_host");
     if (rc != VX_OK) return rc;
     std::lock_guard<std::mutex> lk(w->mu);
-    rc = enqueue_host_frame(w, cam, p, rec_host, shadow_host, kSyncBands);
+    rc = enqueue_host_frame(w, cam, p, rec_host, shadow_host, nullptr, kSyncBands);
     if (rc != VX_OK) return rc;
     VX_CK(cudaStreamSynchronize(w->copy_stream));
     VX_CK(cudaStreamSynchronize(w->stream));
@@ -1492,7 +1513,7 @@ int vx_render_primary_host_async(VxWorld *w, const VxCamera *cam, const VxTraceP
     int rc = host_frame_args(w, cam, p, rec_host, "vx_render_primary_host_async");
     if (rc != VX_OK) return rc;
     std::lock_guard<std::mutex> lk(w->mu);
-    return enqueue_host_frame(w, cam, p, rec_host, shadow_host, kAsyncBands);
+    return enqueue_host_frame(w, cam, p, rec_host, shadow_host, nullptr, kAsyncBands);
 }
 
 int vx_render_host_wait(VxWorld *w) {
@@ -1506,6 +1527,132 @@ int vx_render_host_wait(VxWorld *w) {
     if (w->copy_stream) VX_CK(cudaStreamSynchronize(w->copy_stream));
     VX_CK(cudaStreamSynchronize(w->stream));
     return take_fault(w, "vx_render_host_wait");
+}
+
+namespace {
+// the packed form's limits: a 32-bit window voxel index, 16-bit step counts
+int packed_args(VxWorld *w, const VxTraceParams *p, const char *fn) {
+    const uint64_t nvox = (uint64_t)w->dw.d.vx * (uint64_t)w->dw.d.vy * (uint64_t)w->dw.d.vz;
+    if (nvox > (1ull << 32)) {
+        vx::set_error(std::string(fn) + ": the window has more than 2^32 voxels");
+        return VX_ERR_INVALID;
+    }
+    if (p->max_iters > 65535 || p->any_max_iters > 65535) {
+        vx::set_error(std::string(fn) + ": max_iters and any_max_iters must be <= 65535");
+        return VX_ERR_INVALID;
+    }
+    return VX_OK;
+}
+}  // namespace
+
+int vx_render_primary_host_packed(VxWorld *w, const VxCamera *cam, const VxTraceParams *p,
+                                  VxPackedRecord *out_host) {
+    vx::Range nvtx_range("vx_render_primary_host_packed");
+    VxHitRecord *probe = reinterpret_cast<VxHitRecord *>(out_host);
+    int rc = host_frame_args(w, cam, p, probe, "vx_render_primary_host_packed");
+    if (rc == VX_OK) rc = packed_args(w, p, "vx_render_primary_host_packed");
+    if (rc != VX_OK) return rc;
+    std::lock_guard<std::mutex> lk(w->mu);
+    rc = enqueue_host_frame(w, cam, p, nullptr, nullptr, out_host, kSyncBands);
+    if (rc != VX_OK) return rc;
+    VX_CK(cudaStreamSynchronize(w->copy_stream));
+    VX_CK(cudaStreamSynchronize(w->stream));
+    return take_fault(w, "vx_render_primary_host_packed");
+}
+
+int vx_render_primary_host_packed_async(VxWorld *w, const VxCamera *cam,
+                                        const VxTraceParams *p, VxPackedRecord *out_host) {
+    vx::Range nvtx_range("vx_render_primary_host_packed_async");
+    VxHitRecord *probe = reinterpret_cast<VxHitRecord *>(out_host);
+    int rc = host_frame_args(w, cam, p, probe, "vx_render_primary_host_packed_async");
+    if (rc == VX_OK) rc = packed_args(w, p, "vx_render_primary_host_packed_async");
+    if (rc != VX_OK) return rc;
+    std::lock_guard<std::mutex> lk(w->mu);
+    return enqueue_host_frame(w, cam, p, nullptr, nullptr, out_host, kAsyncBands);
+}
+
+namespace {
+// vx_unpack_records over [i0, i1)
+void unpack_range(const VxPackedRecord *packed, size_t i0, size_t i1, const int32_t ro[3],
+                  uint64_t wx, uint64_t wy, VxHitRecord *rec, VxShadowRecord *shadow) {
+    // window index -> (rx, ry, rz): shifts and masks when wx and wy are
+    // powers of two (every library world), else 32-bit divisions (an index
+    // and wx, wy fit 32 bits; wx * wy may not, so it splits in two steps)
+    const bool pow2 = (wx & (wx - 1)) == 0 && (wy & (wy - 1)) == 0;
+    const uint32_t sx = pow2 ? (uint32_t)__builtin_ctzll(wx) : 0u;
+    const uint32_t sy = pow2 ? (uint32_t)__builtin_ctzll(wy) : 0u;
+    const uint32_t wx32 = (uint32_t)wx, wy32 = (uint32_t)wy;
+    for (size_t i = i0; i < i1; ++i) {
+        const VxPackedRecord &q = packed[i];
+        if (rec) {
+            VxHitRecord r;
+            if (q.flags & 1u) {
+                uint32_t rx, ry, rz;
+                if (pow2) {
+                    rx = q.voxel & (wx32 - 1u);
+                    ry = (q.voxel >> sx) & (wy32 - 1u);
+                    rz = (uint32_t)((uint64_t)q.voxel >> (sx + sy));
+                } else {
+                    const uint32_t row = q.voxel / wx32;
+                    rx = q.voxel - row * wx32;
+                    rz = row / wy32;
+                    ry = row - rz * wy32;
+                }
+                r.voxel[0] = ro[0] + (int32_t)rx;
+                r.voxel[1] = ro[1] + (int32_t)ry;
+                r.voxel[2] = ro[2] + (int32_t)rz;
+            } else {
+                r.voxel[0] = r.voxel[1] = r.voxel[2] = 0;
+            }
+            r.face = q.face;
+            r.mat = q.mat;
+            r.flags = q.flags;
+            r.pad = 0;
+            r.t = q.t;
+            r.steps = q.steps & 0xFFFFu;
+            rec[i] = r;
+        }
+        if (shadow) {
+            VxShadowRecord s;
+            s.steps = q.steps >> 16;
+            s.occluded = (uint8_t)(q.shadow & 1u);
+            s.traced = (uint8_t)((q.shadow >> 1) & 1u);
+            s.pad = 0;
+            shadow[i] = s;
+        }
+    }
+}
+}  // namespace
+
+int vx_unpack_records(const VxPackedRecord *packed, size_t n, const int32_t world_origin[3],
+                      const uint32_t window_voxels[3], VxHitRecord *rec, VxShadowRecord *shadow) {
+    if ((!packed && n) || !world_origin || !window_voxels) {
+        vx::set_error("vx_unpack_records: null argument");
+        return VX_ERR_INVALID;
+    }
+    const uint64_t wx = window_voxels[0], wy = window_voxels[1];
+    if (wx == 0 || wy == 0 || window_voxels[2] == 0) {
+        vx::set_error("vx_unpack_records: empty window");
+        return VX_ERR_INVALID;
+    }
+    // host threads over chunks of at least 256k records (memory-bound copy)
+    const size_t per = (size_t)1 << 18;
+    const size_t hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    const size_t nt = std::min(hw, (n + per - 1) / per);
+    if (nt <= 1) {
+        unpack_range(packed, 0, n, world_origin, wx, wy, rec, shadow);
+        return VX_OK;
+    }
+    std::vector<std::thread> th;
+    th.reserve(nt - 1);
+    const size_t chunk = (n + nt - 1) / nt;
+    for (size_t t = 1; t < nt; ++t) {
+        const size_t i0 = std::min(n, t * chunk), i1 = std::min(n, (t + 1) * chunk);
+        th.emplace_back(unpack_range, packed, i0, i1, world_origin, wx, wy, rec, shadow);
+    }
+    unpack_range(packed, 0, std::min(n, chunk), world_origin, wx, wy, rec, shadow);
+    for (auto &t : th) t.join();
+    return VX_OK;
 }
 
 int vx_render_primary_stats(VxWorld *w, const VxCamera *cam, const VxTraceParams *p,

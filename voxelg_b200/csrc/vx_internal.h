@@ -159,6 +159,11 @@ cudaError_t launch_generate(const DevWorld &w, const VxTerrainParams &t, int16_t
                             cudaStream_t s);
 cudaError_t launch_rebuild_pyramid(const DevWorld &w, cudaStream_t s);
 // the brick and tile distance fields of w (tmp: n_bricks bytes of scratch)
+// a frame's records (and shadow records, or nullptr) [first, first + n) in
+// the 16-byte packed form (vx_pack.cu)
+cudaError_t launch_pack(const VxHitRecord *rec, const VxShadowRecord *sh, size_t first, size_t n,
+                        const int32_t ro[3], uint32_t wx, uint32_t wy, VxPackedRecord *out,
+                        cudaStream_t s);
 cudaError_t launch_dist_fields(const DevWorld &w, uint8_t *bdf, uint8_t *tdf, uint8_t *tmp,
                                cudaStream_t s);
 // tile_meta of every tile from the masks and the tile LUT

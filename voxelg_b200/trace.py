@@ -165,6 +165,38 @@ def render_primary_host_async(world: DeviceWorld, cam: L.VxCamera, params: L.VxT
         C.c_void_p(L.ptr(shadow_host) if shadow_host is not None else 0)))
 
 
+def render_primary_host_packed(world: DeviceWorld, cam: L.VxCamera, params: L.VxTraceParams,
+                               out: Optional[np.ndarray] = None) -> np.ndarray:
+    """Frame through a host buffer of 16-byte packed records (records and
+    shadow records, losslessly); returns the PACKED_DTYPE array."""
+    n = int(cam.res_x) * int(cam.res_y)
+    if out is None:
+        out = np.empty(n, L.PACKED_DTYPE)
+    L.check(L.load().vx_render_primary_host_packed(world.handle, C.byref(cam), C.byref(params),
+                                                   C.c_void_p(L.ptr(out))))
+    return out
+
+
+def render_primary_host_packed_async(world: DeviceWorld, cam: L.VxCamera,
+                                     params: L.VxTraceParams, out: np.ndarray):
+    """Enqueue a packed frame into a (pinned) host buffer; it is there after
+    render_host_wait(world)."""
+    L.check(L.load().vx_render_primary_host_packed_async(world.handle, C.byref(cam),
+                                                         C.byref(params), C.c_void_p(L.ptr(out))))
+
+
+def unpack_records(packed: np.ndarray, world_origin, window_voxels):
+    """Packed records back to (RECORD_DTYPE, SHADOW_DTYPE) arrays."""
+    packed = np.ascontiguousarray(packed).view(L.PACKED_DTYPE)
+    n = len(packed)
+    rec = np.empty(n, L.RECORD_DTYPE)
+    sh = np.empty(n, L.SHADOW_DTYPE)
+    wv = (C.c_uint32 * 3)(*[int(v) for v in window_voxels])
+    L.check(L.load().vx_unpack_records(C.c_void_p(L.ptr(packed)), n, L.i3(world_origin), wv,
+                                       C.c_void_p(L.ptr(rec)), C.c_void_p(L.ptr(sh))))
+    return rec, sh
+
+
 def render_host_wait(world: DeviceWorld):
     """Wait until every enqueued host-buffer frame has landed."""
     L.check(L.load().vx_render_host_wait(world.handle))
