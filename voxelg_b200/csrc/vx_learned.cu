@@ -435,10 +435,10 @@ __global__ void __launch_bounds__(128, 8) k_learned(LearnedArgs la) {
                 if (outcome == OUT_PARTIAL || outcome == OUT_ACCEPTED) {
                     // restart at floor(P): its first iteration skips the same
                     // cell the plain DDA skips there
-                    Dda &s = k.s;
-                    s.vx = (int32_t)floorf(s.ox + s.dx * rs.t) + ro.x;
-                    s.vy = (int32_t)floorf(s.oy + s.dy * rs.t) + ro.y;
-                    s.vz = (int32_t)floorf(s.oz + s.dz * rs.t) + ro.z;
+                    Dda &s = k.s;  // (voxel relative to the window corner)
+                    s.vx = (int32_t)floorf(s.ox + s.dx * rs.t);
+                    s.vy = (int32_t)floorf(s.oy + s.dy * rs.t);
+                    s.vz = (int32_t)floorf(s.oz + s.dz * rs.t);
                     k.t_cur = rs.t;
                     k.la = -1;
                     k.iters = rs.bound;

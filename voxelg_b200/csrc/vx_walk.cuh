@@ -161,13 +161,18 @@ __device__ __forceinline__ bool shadow_occludes(uint32_t m) {
 }
 
 // ------------------------------------------------------------- DDA state
+// The voxel is kept relative to the window corner ro (the reference keeps
+// it absolute and subtracts ro wherever it forms a float or a window test;
+// every float the walk computes takes the relative value, so results are
+// unchanged).  pm* = -1 where the step is positive, else 0.
 struct Dda {
     float ox, oy, oz;      // origin rebased to the window corner
     float dx, dy, dz;
     float ix, iy, iz;      // safe_inv(dir)
     float mx, my, mz;      // t_max
-    int32_t vx, vy, vz;    // voxel, absolute world coords
+    int32_t vx, vy, vz;    // voxel - ro
     int32_t stx, sty, stz; // step
+    int32_t pmx, pmy, pmz; // -(step > 0)
 };
 
 struct Ro {
@@ -200,11 +205,13 @@ __device__ __forceinline__ bool dda_init(const Dims &d, Ro ro, float o0, float o
     float py = clampf(s.oy + d1 * tb, 0.01f, fy - 0.01f);
     float pz = clampf(s.oz + d2 * tb, 0.01f, fz - 0.01f);
     s.stx = sgn(d0); s.sty = sgn(d1); s.stz = sgn(d2);
-    int32_t lx = f2i(floorf(px)), ly = f2i(floorf(py)), lz = f2i(floorf(pz));
-    s.vx = lx + ro.x; s.vy = ly + ro.y; s.vz = lz + ro.z;
-    s.mx = s.stx > 0 ? ((float)(lx + 1) - s.ox) * s.ix : ((float)lx - s.ox) * s.ix;
-    s.my = s.sty > 0 ? ((float)(ly + 1) - s.oy) * s.iy : ((float)ly - s.oy) * s.iy;
-    s.mz = s.stz > 0 ? ((float)(lz + 1) - s.oz) * s.iz : ((float)lz - s.oz) * s.iz;
+    s.pmx = s.stx > 0 ? -1 : 0; s.pmy = s.sty > 0 ? -1 : 0; s.pmz = s.stz > 0 ? -1 : 0;
+    // p is clamped into the window, so the floor converts without saturating
+    const int32_t lx = __float2int_rd(px), ly = __float2int_rd(py), lz = __float2int_rd(pz);
+    s.vx = lx; s.vy = ly; s.vz = lz;
+    s.mx = ((float)(lx - s.pmx) - s.ox) * s.ix;
+    s.my = ((float)(ly - s.pmy) - s.oy) * s.iy;
+    s.mz = ((float)(lz - s.pmz) - s.oz) * s.iz;
     return true;
 }
 
@@ -222,39 +229,44 @@ __device__ __forceinline__ void first_cell_entry(const Dims &d, const Dda &s, in
     else *ax = 2;
 }
 
-// dda_step, raymarch.wgsl:3416-3448
-__device__ __forceinline__ void dda_step(const Dims &d, Dda &s, float &t_cur, int &la) {
-    if (s.mx < s.my && s.mx < s.mz) {
-        t_cur = s.mx;
-        s.vx += s.stx;
-        s.mx = s.mx + fabsf(s.ix);
-        la = 0;
-    } else if (s.my < s.mz) {
-        t_cur = s.my;
-        s.vy += s.sty;
-        s.my = s.my + fabsf(s.iy);
-        la = 1;
-    } else {
-        t_cur = s.mz;
-        s.vz += s.stz;
-        s.mz = s.mz + fabsf(s.iz);
-        la = 2;
-    }
+// dda_step, raymarch.wgsl:3416-3448: the axis of the smallest t_max (x
+// before y before z on ties, as the reference's strict compares order them),
+// written with selects so that lanes stepping different axes do not diverge
+__device__ __forceinline__ void dda_step(Dda &s, float &t_cur, int &la) {
+    const bool ax = s.mx < s.my && s.mx < s.mz;
+    const bool ay = !ax && s.my < s.mz;
+    const bool az = !ax && !ay;
+    t_cur = ax ? s.mx : (ay ? s.my : s.mz);
+    s.vx += ax ? s.stx : 0;
+    s.vy += ay ? s.sty : 0;
+    s.vz += az ? s.stz : 0;
+    s.mx = ax ? s.mx + fabsf(s.ix) : s.mx;
+    s.my = ay ? s.my + fabsf(s.iy) : s.my;
+    s.mz = az ? s.mz + fabsf(s.iz) : s.mz;
+    la = ax ? 0 : (ay ? 1 : 2);
 }
 
-// skip_to_cell, raymarch.wgsl:4807-4864.  cell is a power of two, so
-// v - pos_mod(v, cell) == v & ~(cell - 1) for every int v.
-__device__ __forceinline__ void skip_to_cell(const Dims &d, Ro ro, int32_t cell, Dda &s,
-                                             int &la) {
-    const int32_t hi = ~(cell - 1);
-    const int32_t cox = s.vx & hi, coy = s.vy & hi, coz = s.vz & hi;
-    // exit-face boundary per axis and the voxel just across it
-    const int32_t bx = s.stx > 0 ? cox + cell : cox, nbx = s.stx > 0 ? bx : cox - 1;
-    const int32_t by = s.sty > 0 ? coy + cell : coy, nby = s.sty > 0 ? by : coy - 1;
-    const int32_t bz = s.stz > 0 ? coz + cell : coz, nbz = s.stz > 0 ? bz : coz - 1;
-    const float tfx = ((float)(bx - ro.x) - s.ox) * s.ix;
-    const float tfy = ((float)(by - ro.y) - s.oy) * s.iy;
-    const float tfz = ((float)(bz - ro.z) - s.oz) * s.iz;
+// skip_to_cell, raymarch.wgsl:4807-4864, for the cell of edge `cell` (a
+// power of two dividing the window's dims) that holds the slot voxel
+// (sx, sy, sz).  The reference aligns the cell in absolute coordinates,
+// v - pos_mod(v, cell); the slot has the same residue mod cell, so the cell
+// corner relative to the window is v_rel - (slot & (cell - 1)), and the
+// exit-face boundary b - ro is that plus cell on positive-step axes: the same
+// integers the reference converts, so the same floats follow.
+// The landing floor(o + d * (t_min + 1e-3)) converts with saturation and no
+// further clamp: a landing outside the int range is outside the window, so
+// the next iteration ends the walk exactly as the reference's does, and the
+// snapped axis and t of the crossed face are exact either way.
+__device__ __forceinline__ void skip_to_cell(Dda &s, uint32_t sx, uint32_t sy, uint32_t sz,
+                                             int32_t cell, int &la) {
+    const uint32_t m = (uint32_t)cell - 1u;
+    // boundary of the exit face, relative to the window corner
+    const int32_t bx = s.vx - (int32_t)(sx & m) + (cell & s.pmx);
+    const int32_t by = s.vy - (int32_t)(sy & m) + (cell & s.pmy);
+    const int32_t bz = s.vz - (int32_t)(sz & m) + (cell & s.pmz);
+    const float tfx = ((float)bx - s.ox) * s.ix;
+    const float tfy = ((float)by - s.oy) * s.iy;
+    const float tfz = ((float)bz - s.oz) * s.iz;
     const float eps = 1e-6f;
     float t_min = 1e30f;
     int ax = 0;
@@ -262,17 +274,17 @@ __device__ __forceinline__ void skip_to_cell(const Dims &d, Ro ro, int32_t cell,
     if (s.sty != 0 && tfy > eps && tfy < t_min) { t_min = tfy; ax = 1; }
     if (s.stz != 0 && tfz > eps && tfz < t_min) { t_min = tfz; ax = 2; }
     const float tb = t_min + 1e-3f;
-    int32_t nx = f2i(floorf(s.ox + s.dx * tb)) + ro.x;
-    int32_t ny = f2i(floorf(s.oy + s.dy * tb)) + ro.y;
-    int32_t nz = f2i(floorf(s.oz + s.dz * tb)) + ro.z;
-    nx = ax == 0 ? nbx : nx;
-    ny = ax == 1 ? nby : ny;
-    nz = ax == 2 ? nbz : nz;
+    // the voxel across the crossed face: b on positive steps, b - 1 on
+    // negative ones (b is then the cell corner)
+    const int32_t nx = ax == 0 ? bx + ~s.pmx : __float2int_rd(s.ox + s.dx * tb);
+    const int32_t ny = ax == 1 ? by + ~s.pmy : __float2int_rd(s.oy + s.dy * tb);
+    const int32_t nz = ax == 2 ? bz + ~s.pmz : __float2int_rd(s.oz + s.dz * tb);
     s.vx = nx; s.vy = ny; s.vz = nz;
-    const int32_t lx = nx - ro.x, ly = ny - ro.y, lz = nz - ro.z;
-    s.mx = ((float)(s.stx > 0 ? lx + 1 : lx) - s.ox) * s.ix;
-    s.my = ((float)(s.sty > 0 ? ly + 1 : ly) - s.oy) * s.iy;
-    s.mz = ((float)(s.stz > 0 ? lz + 1 : lz) - s.oz) * s.iz;
+    // t_max of the new voxel (a saturated landing wraps here; that walk ends
+    // at its next window test)
+    s.mx = ((float)(int32_t)((uint32_t)nx - (uint32_t)s.pmx) - s.ox) * s.ix;
+    s.my = ((float)(int32_t)((uint32_t)ny - (uint32_t)s.pmy) - s.oy) * s.iy;
+    s.mz = ((float)(int32_t)((uint32_t)nz - (uint32_t)s.pmz) - s.oz) * s.iz;
     la = ax;
 }
 
@@ -299,7 +311,7 @@ __device__ __forceinline__ void set_miss(Hit &h) {
 }
 
 // entry_normal_and_t + last_axis_after_entry (raymarch.wgsl:3321-3342, :4800)
-__device__ __forceinline__ void set_hit(const Dims &d, const Dda &s, int la, uint32_t m,
+__device__ __forceinline__ void set_hit(const Dims &d, const Dda &s, Ro ro, int la, uint32_t m,
                                         bool early, Hit &h) {
     int ax;
     float t;
@@ -310,7 +322,7 @@ __device__ __forceinline__ void set_hit(const Dims &d, const Dda &s, int la, uin
         first_cell_entry(d, s, &ax, &t);
     }
     const int32_t st = ax == 0 ? s.stx : (ax == 1 ? s.sty : s.stz);
-    h.vx = s.vx; h.vy = s.vy; h.vz = s.vz;
+    h.vx = s.vx + ro.x; h.vy = s.vy + ro.y; h.vz = s.vz + ro.z;
     h.t = t;
     h.mat = m;
     h.face = (uint32_t)(2 * ax + (st > 0 ? 1 : 0));
@@ -342,16 +354,11 @@ struct Geo {
     uint32_t bx, bxy, tx, txy, cx, cxy, lx, lxy;
     uint32_t rox, roz;  // pos_mod(window corner x / z, dims): slot of window voxel 0
 };
-// FL's kFlPow2 bit: the slot is a mask and the window corner's fold is unused
 template <uint32_t FL>
 __device__ __forceinline__ Geo geo_of(const Dims &d, Ro ro) {
     Geo g;
-    if ((FL & kFlPow2) != 0u) {
-        g.rox = g.roz = 0u;
-    } else {
-        g.rox = (uint32_t)pos_mod(ro.x, d.vx);
-        g.roz = (uint32_t)pos_mod(ro.z, d.vz);
-    }
+    g.rox = (uint32_t)pos_mod(ro.x, d.vx);
+    g.roz = (uint32_t)pos_mod(ro.z, d.vz);
     g.bx = (uint32_t)d.bx;
     g.bxy = (uint32_t)(d.bx * d.by);
     g.tx = (uint32_t)d.tx;
@@ -440,22 +447,17 @@ __device__ __forceinline__ int walk_step(const DevWorld &w, const Geo &g, const 
     ++k.iters;
     if (k.t_cur > k.tmax) return WALK_END;
     // window test, then the toroidal slot (world_to_slot_voxel,
-    // raymarch.wgsl:17-23) from the window-relative voxel: lx < dims and
-    // rox < dims, so one conditional subtraction folds it
-    uint32_t sx, sz;
+    // raymarch.wgsl:17-23) from the window-relative voxel: rel < dims and
+    // rox < dims, so a mask (power-of-two dims) or one conditional
+    // subtraction folds it
+    const uint32_t lx = (uint32_t)s.vx, lz = (uint32_t)s.vz;
+    if (lx >= (uint32_t)d.vx || (uint32_t)s.vy >= (uint32_t)d.vy || lz >= (uint32_t)d.vz)
+        return WALK_END;
+    uint32_t sx = lx + g.rox, sz = lz + g.roz;
     if ((FL & kFlPow2) != 0u) {
-        if ((uint32_t)(s.vx - ro.x) >= (uint32_t)d.vx || (uint32_t)(s.vy - ro.y) >= (uint32_t)d.vy ||
-            (uint32_t)(s.vz - ro.z) >= (uint32_t)d.vz)
-            return WALK_END;
-        sx = (uint32_t)s.vx & (uint32_t)(d.vx - 1);
-        sz = (uint32_t)s.vz & (uint32_t)(d.vz - 1);
+        sx &= (uint32_t)(d.vx - 1);
+        sz &= (uint32_t)(d.vz - 1);
     } else {
-        const uint32_t lx = (uint32_t)(s.vx - ro.x), lz = (uint32_t)(s.vz - ro.z);
-        if (lx >= (uint32_t)d.vx || (uint32_t)(s.vy - ro.y) >= (uint32_t)d.vy ||
-            lz >= (uint32_t)d.vz)
-            return WALK_END;
-        sx = lx + g.rox;
-        sz = lz + g.roz;
         if (sx >= (uint32_t)d.vx) sx -= (uint32_t)d.vx;
         if (sz >= (uint32_t)d.vz) sz -= (uint32_t)d.vz;
     }
@@ -505,19 +507,21 @@ __device__ __forceinline__ int walk_step(const DevWorld &w, const Geo &g, const 
                 lm = brick_topmost<STATS>(w, rbi, ld_occ(w, rbi), bytes);
             }
             if (lm != 0u && is_uniform_optimisable(lm)) {
-                set_hit(d, s, k.la, lm, true, h);
+                set_hit(d, s, ro, k.la, lm, true, h);
                 return WALK_HIT;
             }
         }
+        // tile LUT (raymarch.wgsl:4692-4706)
         if (f_lut) {
             if (STATS) bytes += 1;
             if (tum != 0u && is_uniform_optimisable(tum)) {
-                set_hit(d, s, k.la, tum, true, h);
+                set_hit(d, s, ro, k.la, tum, true, h);
                 return WALK_HIT;
             }
         }
         if (STATS) bytes += 8;
-        if (!bit64(tw, child_of(sx, sy, sz, 2))) {
+        const int tb = child_of(sx, sy, sz, 2);
+        if (!bit64(tw, tb)) {
             cell = 4;
         } else {
             const uint32_t bi = brick_index(g, sx >> 2, sy >> 2, sz >> 2);
@@ -525,9 +529,10 @@ __device__ __forceinline__ int walk_step(const DevWorld &w, const Geo &g, const 
             const uint64_t occ = ld_occ(w, bi);
             const uint32_t bum = f_lut ? ld_brick_uniform(w, bi) : 0u;
             if (f_lut) {
+                // brick LUT (raymarch.wgsl:4716-4731)
                 if (STATS) bytes += 1;
                 if (bum != 0u && is_uniform_optimisable(bum)) {
-                    set_hit(d, s, k.la, bum, true, h);
+                    set_hit(d, s, ro, k.la, bum, true, h);
                     return WALK_HIT;
                 }
             }
@@ -540,7 +545,7 @@ __device__ __forceinline__ int walk_step(const DevWorld &w, const Geo &g, const 
                 } else {
                     const uint32_t m = brick_topmost<STATS>(w, bi, occ, bytes);
                     if (!is_foliage(m)) {
-                        set_hit(d, s, k.la, m, true, h);
+                        set_hit(d, s, ro, k.la, m, true, h);
                         return WALK_HIT;
                     }
                 }
@@ -549,13 +554,13 @@ __device__ __forceinline__ int walk_step(const DevWorld &w, const Geo &g, const 
                 const int vi = child_of(sx, sy, sz, 0);
                 if (STATS) bytes += 8;
                 if (bit64(occ, vi)) {
-                    // batch 3: the material byte of a solid voxel
+                    // the material byte of a solid voxel
                     const uint32_t m = ld_mat(w, bi, (uint32_t)vi);
                     if (STATS) bytes += 1;
                     const bool stop = kind == KIND_TRACE ? resolves_cube(m)
                                       : (kind == KIND_ANY ? shadow_occludes(m) : !is_transparent(m));
                     if (stop) {
-                        if (kind != KIND_ANY) set_hit(d, s, k.la, m, false, h);
+                        if (kind != KIND_ANY) set_hit(d, s, ro, k.la, m, false, h);
                         return WALK_HIT;
                     }
                 }
@@ -563,10 +568,10 @@ __device__ __forceinline__ int walk_step(const DevWorld &w, const Geo &g, const 
         }
     }
     if (cell != 0) {
-        skip_to_cell(d, ro, cell, s, k.la);
+        skip_to_cell(s, sx, sy, sz, cell, k.la);
         if (kind != KIND_NO_WATER) k.t_cur = crossed_t(s, k.la);
     } else {
-        dda_step(d, s, k.t_cur, k.la);
+        dda_step(s, k.t_cur, k.la);
     }
     return WALK_CONT;
 }
