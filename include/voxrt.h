@@ -344,6 +344,21 @@ int vx_render_primary_host_packed(VxWorld *w, const VxCamera *cam, const VxTrace
                                   VxPackedRecord *out_host);
 int vx_render_primary_host_packed_async(VxWorld *w, const VxCamera *cam,
                                         const VxTraceParams *p, VxPackedRecord *out_host);
+/* The chunk generator's binary32 transcendentals, equal to the host C
+ * library's (as the reference's f32::powf / cos / sin are) on the
+ * generator's domains: fn 0 powf(x, 1.15f) and fn 1 powf(x, 0.85f) for
+ * every x in [0, 1] (src/voxel.rs:1262, :1623), fn 2 cosf and fn 3 sinf for
+ * every branch angle paint_tree forms (:1633-1641, :1689-1697).  Elsewhere
+ * in [0, 1] / |x| <= 16 they are the library's own double-precision
+ * evaluations rounded to binary32.  Built from an exception table that
+ * voxelg_b200/build.py writes beside the library for the C library it runs
+ * on; VX_ERR_INVALID when the table is missing or was built for another.
+ * vx_gen_math: n device inputs to n device outputs on the world's device
+ * (asynchronous on `stream`; NULL = the world's stream, waited for).
+ * vx_gen_math_host: the same on the host. */
+int vx_gen_math(VxWorld *w, uint32_t fn, const float *in_dev, size_t n, float *out_dev,
+                void *stream);
+int vx_gen_math_host(uint32_t fn, const float *in, size_t n, float *out);
 /* Host: n packed records back to VxHitRecord / VxShadowRecord, byte for
  * byte what vx_render_primary_host writes.  world_origin is the frame
  * camera's world_origin, window_voxels the world's voxel counts

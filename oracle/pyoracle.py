@@ -81,6 +81,7 @@ def load():
     P = C.POINTER
     vp = C.c_void_p
     sig = {
+        "or_libm_batch": (None, [C.c_int, vp, C.c_size_t, vp, C.c_int]),
         "or_rebuild_all_masks": (None, [P(OrWorld)]),
         "or_rebuild_all_uniform": (None, [P(OrWorld)]),
         "or_set_voxel": (C.c_int64, [P(OrWorld), C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint8]),
@@ -416,3 +417,11 @@ def default_params(flags=OR_F_L4 | OR_F_LUT | OR_F_LOD | OR_F_BEAM | OR_F_SHADOW
     p.cone_tan = float(f(0.0087268678))
     p.frame = float(f(frame))
     return p
+
+
+def libm_batch(fn: int, x: np.ndarray, threads=None) -> np.ndarray:
+    """glibc powf(x, 1.15f) (fn 0), powf(x, 0.85f) (1), cosf (2), sinf (3)."""
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    out = np.empty_like(x)
+    load().or_libm_batch(fn, x.ctypes.data, len(x), out.ctypes.data, threads or os.cpu_count() or 1)
+    return out

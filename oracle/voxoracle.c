@@ -1912,3 +1912,45 @@ double or_raycast_batch(const OrWorld *w, const int32_t origin[3], const float *
     for (int i = 1; i < used; ++i) pthread_join(th[i], NULL);
     return now_s() - t0;
 }
+
+/* ------------------------------------------------------------------ */
+/* the C library's binary32 transcendentals, batched                   */
+/* ------------------------------------------------------------------ */
+/* glibc powf / cosf / sinf are what the reference's f32::powf / cos / sin
+ * call (src/voxel.rs:1262, :1623, :1639-1641, :1695-1697). */
+typedef struct {
+    int fn;
+    const float *x;
+    float *out;
+    size_t a, b;
+} LibmJob;
+
+static void *libm_thread(void *arg) {
+    LibmJob *j = (LibmJob *)arg;
+    for (size_t i = j->a; i < j->b; ++i) {
+        const float v = j->x[i];
+        float r;
+        if (j->fn == 0) r = powf(v, 1.15f);
+        else if (j->fn == 1) r = powf(v, 0.85f);
+        else if (j->fn == 2) r = cosf(v);
+        else r = sinf(v);
+        j->out[i] = r;
+    }
+    return NULL;
+}
+
+void or_libm_batch(int fn, const float *x, size_t n, float *out, int nthreads) {
+    if (nthreads < 1) nthreads = 1;
+    if (nthreads > 256) nthreads = 256;
+    pthread_t th[256];
+    LibmJob jobs[256];
+    for (int t = 0; t < nthreads; ++t) {
+        jobs[t].fn = fn;
+        jobs[t].x = x;
+        jobs[t].out = out;
+        jobs[t].a = n * (size_t)t / (size_t)nthreads;
+        jobs[t].b = n * (size_t)(t + 1) / (size_t)nthreads;
+        pthread_create(&th[t], NULL, libm_thread, &jobs[t]);
+    }
+    for (int t = 0; t < nthreads; ++t) pthread_join(th[t], NULL);
+}

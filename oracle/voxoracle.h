@@ -239,4 +239,8 @@ double or_raycast_batch(const OrWorld *w, const int32_t origin[3], const float *
 #ifdef __cplusplus
 }
 #endif
+/* glibc powf(x, 1.15f) (fn 0), powf(x, 0.85f) (1), cosf (2), sinf (3) on n
+ * inputs with nthreads threads: the C library calls of the reference's
+ * generator (src/voxel.rs:1262, :1623, :1639-1641, :1695-1697) */
+void or_libm_batch(int fn, const float *x, size_t n, float *out, int nthreads);
 #endif

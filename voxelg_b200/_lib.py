@@ -177,6 +177,8 @@ SIGNATURES = [
     ("vx_render_primary_host_packed", C.c_int, [_vp, _P(VxCamera), _P(VxTraceParams), _vp]),
     ("vx_render_primary_host_packed_async", C.c_int,
      [_vp, _P(VxCamera), _P(VxTraceParams), _vp]),
+    ("vx_gen_math", C.c_int, [_vp, C.c_uint32, _vp, C.c_size_t, _vp, _vp]),
+    ("vx_gen_math_host", C.c_int, [C.c_uint32, _vp, C.c_size_t, _vp]),
     ("vx_unpack_records", C.c_int,
      [_vp, C.c_size_t, _P(C.c_int32), _P(C.c_uint32), _vp, _vp]),
     ("vx_render_ao", C.c_int, [_vp, _P(VxCamera), _vp, _vp, _vp]),

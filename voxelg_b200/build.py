@@ -26,6 +26,9 @@ CSRC = PKG / "csrc"
 BUILD = PKG / "_build"
 LIB = PKG / "lib" / "libvoxrt.so"
 LIB_CHECKED = PKG / "lib" / "libvoxrt_checked.so"
+# the chunk generator's powf / cosf / sinf exception table (vx_gmath.h),
+# written beside the library for the C library this host runs
+LMX_TABLE = PKG / "lib" / "vx_libm_exceptions.bin"
 INCLUDE = ROOT / "include"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -99,13 +102,40 @@ def _build_lib(build_dir: Path, lib: Path, defines: list[str], force: bool,
     return lib
 
 
+def build_libm_table(force: bool = False, verbose: bool = False) -> Path:
+    """vx_libm_exceptions.bin: compiles vx_libmx_gen.cpp for the host and runs
+    it (an exhaustive scan of powf over [0, 1], about 20 s on 8 cores) when the
+    table is missing or older than its sources."""
+    src = CSRC / "vx_libmx_gen.cpp"
+    deps = [src, CSRC / "vx_gmath.h"]
+    if not force and LMX_TABLE.exists() and not _newer(src, LMX_TABLE, deps):
+        return LMX_TABLE
+    BUILD.mkdir(parents=True, exist_ok=True)
+    LMX_TABLE.parent.mkdir(exist_ok=True)
+    exe = BUILD / "vx_libmx_gen"
+    cxx = shutil.which("g++") or "g++"
+    cmd = [cxx, "-O2", "-ffp-contract=off", "-std=c++17", "-pthread", f"-I{CSRC}", str(src), "-o",
+           str(exe)]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+    tmp = LMX_TABLE.with_suffix(".bin.tmp")
+    out = subprocess.run([str(exe), str(tmp)], check=True, capture_output=True, text=True)
+    if verbose:
+        print(out.stdout.strip(), flush=True)
+    os.replace(tmp, LMX_TABLE)
+    return LMX_TABLE
+
+
 def build(force: bool = False, verbose: bool = False, checked: bool = True) -> Path:
-    """libvoxrt.so, and the checked library beside it unless checked=False."""
+    """libvoxrt.so, the checked library beside it unless checked=False, and
+    the generator's math exception table."""
     jobs = [(BUILD, LIB, [])]
     if checked:
         jobs.append((BUILD / "checked", LIB_CHECKED, ["-DVX_CHECKED=1"]))
     with ThreadPoolExecutor(max_workers=len(jobs)) as ex:
         list(ex.map(lambda j: _build_lib(*j, force, verbose), jobs))
+    build_libm_table(force, verbose)
     return LIB
 
 

@@ -11,12 +11,15 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <dlfcn.h>
+#include <gnu/libc-version.h>
 #include <thread>
 #include <new>
 #include <string>
 #include <unordered_map>
 #include <vector>
 
+#include "vx_gmath.h"
 #include "vx_internal.h"
 
 namespace vx {
@@ -82,6 +85,7 @@ struct VxWorld {
     size_t gen_cap = 0;              // bytes
     void *h_gen = nullptr;           // pinned staging of the generator's plan
     size_t h_gen_cap = 0;            // bytes
+    uint32_t *d_lmx = nullptr;       // device copy of the generator's math exception table
     // empty-space distance fields of the learned form, rebuilt on demand when
     // the masks changed (mask_gen) since they were built (df_gen)
     uint8_t *bdf = nullptr, *tdf = nullptr, *df_tmp = nullptr;
@@ -207,6 +211,7 @@ void free_world(VxWorld *w) {
     cudaFree(w->df_tmp);
     cudaFree(w->lrn_depth);
     if (w->h_gen) cudaFreeHost(w->h_gen);
+    cudaFree(w->d_lmx);
     if (w->copy_stream) cudaStreamSynchronize(w->copy_stream);
     for (int i = 0; i < 2; ++i) {
         cudaFree(w->hrec[i]);
@@ -596,6 +601,74 @@ inline void window_corner(const VxWorld *w, int32_t &ox, int32_t &oz) {
     oz = w->gen_window ? w->gen_origin[1] * 32 : 0;
 }
 
+// The exception table of vx_gmath.h (built by voxelg_b200/build.py beside
+// the library as vx_libm_exceptions.bin), loaded once per process.  It holds
+// this host C library's powf / cosf / sinf results where they differ from
+// vx_gmath.h's, so it must come from the C library the process runs on.
+const std::vector<uint32_t> *lmx_table(std::string *err) {
+    static std::mutex mu;
+    static std::vector<uint32_t> blob;
+    static std::string failure;
+    static bool tried = false;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!tried) {
+        tried = true;
+        Dl_info info{};
+        std::string path = "vx_libm_exceptions.bin";
+        if (dladdr(reinterpret_cast<void *>(&vx_gen_math_host), &info) && info.dli_fname) {
+            std::string lib = info.dli_fname;
+            const size_t slash = lib.rfind('/');
+            if (slash != std::string::npos) path = lib.substr(0, slash + 1) + path;
+        }
+        FILE *f = std::fopen(path.c_str(), "rb");
+        if (!f) {
+            failure = "generator math table " + path +
+                      " missing (python -m voxelg_b200.build writes it)";
+        } else {
+            std::fseek(f, 0, SEEK_END);
+            const long bytes = std::ftell(f);
+            std::fseek(f, 0, SEEK_SET);
+            if (bytes > 0 && bytes % 4 == 0) {
+                blob.resize((size_t)bytes / 4);
+                if (std::fread(blob.data(), 4, blob.size(), f) != blob.size()) blob.clear();
+            }
+            std::fclose(f);
+            char ver[33] = {0};
+            if (blob.size() > vx::gm::LMX_HEADER) std::memcpy(ver, &blob[2], 32);
+            if (blob.size() <= vx::gm::LMX_HEADER || blob[0] != vx::gm::LMX_MAGIC ||
+                blob[1] != vx::gm::LMX_VERSION || blob[10] != vx::gm::LMX_FUNCS) {
+                failure = "generator math table " + path + " is not a version-" +
+                          std::to_string(vx::gm::LMX_VERSION) + " table";
+                blob.clear();
+            } else if (std::strcmp(ver, gnu_get_libc_version()) != 0) {
+                failure = std::string("generator math table was built against C library ") +
+                          ver + ", this process runs " + gnu_get_libc_version() +
+                          " (rebuild: python -m voxelg_b200.build)";
+                blob.clear();
+            }
+        }
+    }
+    if (blob.empty()) {
+        if (err) *err = failure;
+        return nullptr;
+    }
+    return &blob;
+}
+
+// the world's device copy of the table; caller holds w->mu
+int world_lmx(VxWorld *w, const char *fn) {
+    if (w->d_lmx) return VX_OK;
+    std::string err;
+    const std::vector<uint32_t> *t = lmx_table(&err);
+    if (!t) {
+        vx::set_error(std::string(fn) + ": " + err);
+        return VX_ERR_INVALID;
+    }
+    VX_CK(cudaMalloc(&w->d_lmx, t->size() * 4));
+    VX_CK(cudaMemcpyAsync(w->d_lmx, t->data(), t->size() * 4, cudaMemcpyHostToDevice, w->stream));
+    return VX_OK;
+}
+
 // Lays out the generator's scratch -- the plan's ints (explicit plans),
 // column words, tree headers and primitives -- uploads the ints through the
 // pinned staging buffer, runs the kernels and waits.  Caller holds w->mu.
@@ -632,6 +705,9 @@ int run_gen_plan(VxWorld *w, uint64_t seed, vx::GenPlan &plan, const std::vector
     plan.colw = reinterpret_cast<uint32_t *>(base + off_colw);
     plan.hdr = reinterpret_cast<int32_t *>(base + off_hdr);
     plan.prims = base + off_prim;
+    int rc = world_lmx(w, "chunk generator");
+    if (rc != VX_OK) return rc;
+    plan.lmx = w->d_lmx;
     vx::world_masks_changed(w);
     VX_CK(vx::launch_gen_slots(w->dw, seed, plan, w->stream));
     VX_CK(cudaStreamSynchronize(w->stream));
@@ -1800,3 +1876,45 @@ int vx_queue_graph_destroy(VxQueueGraph *g) {
 }
 
 }  // extern "C"
+
+int vx_gen_math(VxWorld *w, uint32_t fn, const float *in_dev, size_t n, float *out_dev,
+                void *stream) {
+    if (!w || fn >= vx::gm::LMX_FUNCS || ((!in_dev || !out_dev) && n)) {
+        vx::set_error("vx_gen_math: null argument or unknown function");
+        return VX_ERR_INVALID;
+    }
+    int rc = use_device(w);
+    if (rc != VX_OK) return rc;
+    std::lock_guard<std::mutex> lk(w->mu);
+    rc = world_lmx(w, "vx_gen_math");
+    if (rc != VX_OK) return rc;
+    cudaStream_t s = stream ? static_cast<cudaStream_t>(stream) : w->stream;
+    if (!stream) VX_CK(cudaStreamSynchronize(w->stream));
+    VX_CK(vx::launch_gen_math(w->d_lmx, fn, in_dev, n, out_dev, s));
+    if (!stream) VX_CK(cudaStreamSynchronize(s));
+    return VX_OK;
+}
+
+int vx_gen_math_host(uint32_t fn, const float *in, size_t n, float *out) {
+    if (fn >= vx::gm::LMX_FUNCS || ((!in || !out) && n)) {
+        vx::set_error("vx_gen_math_host: null argument or unknown function");
+        return VX_ERR_INVALID;
+    }
+    std::string err;
+    const std::vector<uint32_t> *t = lmx_table(&err);
+    if (!t) {
+        vx::set_error("vx_gen_math_host: " + err);
+        return VX_ERR_INVALID;
+    }
+    const uint32_t *blob = t->data();
+    for (size_t i = 0; i < n; ++i) {
+        const float x = in[i];
+        float v;
+        if (fn == vx::gm::LMX_POW115) v = vx::gm::pow01(x, 1.15f);
+        else if (fn == vx::gm::LMX_POW085) v = vx::gm::pow01(x, 0.85f);
+        else if (fn == vx::gm::LMX_COS) v = vx::gm::cos_small(x);
+        else v = vx::gm::sin_small(x);
+        out[i] = vx::gm::lmx_fix(blob, fn, x, v);
+    }
+    return VX_OK;
+}

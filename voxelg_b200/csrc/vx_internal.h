@@ -152,8 +152,12 @@ struct GenPlan {
     uint32_t *colw;
     void *prims;
     int32_t *hdr;
+    const uint32_t *lmx;       // vx_gmath.h exception table on the device
 };
 size_t gen_prim_bytes_per_src();
+// the generator's powf / cosf / sinf (vx_gmath.h function fn) on n inputs
+cudaError_t launch_gen_math(const uint32_t *lmx, uint32_t fn, const float *in, size_t n, float *out,
+                            cudaStream_t s);
 cudaError_t launch_gen_slots(const DevWorld &w, uint64_t seed, const GenPlan &p, cudaStream_t s);
 cudaError_t launch_generate(const DevWorld &w, const VxTerrainParams &t, int16_t *heights,
                             cudaStream_t s);

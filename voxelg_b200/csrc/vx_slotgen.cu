@@ -25,9 +25,12 @@
 //                  512 bricks, their occupancy words (occupancy == material
 //                  != 0, the invariant Brick::set keeps, :315-325) and
 //                  uniform bytes go to the slot's bricks.
-// pow, cos and sin are evaluated in double precision and rounded to float.
+// powf, cosf and sinf give the host C library's binary32 results, as the
+// reference's f32::powf / cos / sin do: vx_gmath.h's functions, corrected
+// by the exception table (Seed::lmx) on the generator's domains.
 #include <cuda_runtime.h>
 
+#include "vx_gmath.h"
 #include "vx_internal.h"
 #include "vx_noise.cuh"
 
@@ -62,17 +65,29 @@ __device__ __forceinline__ int32_t f2i(float x) {
 }
 __device__ __forceinline__ float fmaxr(float a, float b) { return a < b ? b : a; }
 __device__ __forceinline__ float fminr(float a, float b) { return b < a ? b : a; }
-__device__ __forceinline__ float pow_f(float x, float y) { return (float)pow((double)x, (double)y); }
-__device__ __forceinline__ float cos_f(float x) { return (float)cos((double)x); }
-__device__ __forceinline__ float sin_f(float x) { return (float)sin((double)x); }
+// the C library's powf(x, 1.15f), powf(x, 0.85f), cosf, sinf (vx_gmath.h)
+__device__ __forceinline__ float pow115(const uint32_t *lmx, float x) {
+    return gm::lmx_fix(lmx, gm::LMX_POW115, x, gm::pow01(x, 1.15f));
+}
+__device__ __forceinline__ float pow085(const uint32_t *lmx, float x) {
+    return gm::lmx_fix(lmx, gm::LMX_POW085, x, gm::pow01(x, 0.85f));
+}
+__device__ __forceinline__ float cos_f(const uint32_t *lmx, float a) {
+    return gm::lmx_fix(lmx, gm::LMX_COS, a, gm::cos_small(a));
+}
+__device__ __forceinline__ float sin_f(const uint32_t *lmx, float a) {
+    return gm::lmx_fix(lmx, gm::LMX_SIN, a, gm::sin_small(a));
+}
 
 struct Seed {
     uint64_t seed;
     float offx, offz;      // seed_offset_xz, voxel.rs:1163-1167
+    const uint32_t *lmx;   // exception table of vx_gmath.h (device copy)
 };
 
 // sample_terrain, voxel.rs:1244-1316 (ravine cut 0, rivers off)
-__device__ int32_t sample_terrain(float wx, float wz, float offx, float offz, int32_t *water_top) {
+__device__ int32_t sample_terrain(float wx, float wz, float offx, float offz, const uint32_t *lmx,
+                                  int32_t *water_top) {
     const float px = wx + offx, pz = wz + offz;
     const float warp_x = fbm_2d(px * 0.005f, pz * 0.005f, 2) * 8.0f;
     const float warp_z = fbm_2d(px * 0.005f + 50.0f, pz * 0.005f + 50.0f, 2) * 8.0f;
@@ -81,7 +96,7 @@ __device__ int32_t sample_terrain(float wx, float wz, float offx, float offz, in
     const float mountain_mask = fmaxr(fbm_2d(wpx * 0.0028f, wpz * 0.0028f, 2) + 0.2f, 0.0f);
     const float mountain_amp = fminr(mountain_mask, 1.0f);
     const float mountain_h =
-        pow_f(fmaxr(fbm_2d(wpx * 0.009f, wpz * 0.009f, 5), 0.0f), 1.15f) * mountain_amp * 110.0f;
+        pow115(lmx, fmaxr(fbm_2d(wpx * 0.009f, wpz * 0.009f, 5), 0.0f)) * mountain_amp * 110.0f;
     const float base_h = 64.0f + 8.0f + base + mountain_h - 0.0f;
     const float h = base_h < 2.0f ? 2.0f : (base_h > 255.0f ? 255.0f : base_h);
     const int32_t hi = f2i(h);
@@ -173,7 +188,7 @@ __device__ bool tree_candidate(int32_t cx, int32_t cz, uint32_t i, const Seed &g
     const uint32_t h = ch * 2654435761u + i * 7919u;
     const int32_t wx = cx * kCV + (int32_t)(h & 31u), wz = cz * kCV + (int32_t)((h >> 5) & 31u);
     int32_t wt;
-    const int32_t th = sample_terrain((float)wx, (float)wz, g.offx, g.offz, &wt);
+    const int32_t th = sample_terrain((float)wx, (float)wz, g.offx, g.offz, g.lmx, &wt);
     if ((uint32_t)th <= (uint32_t)(kSea + 1)) return false;
     if (th + 22 >= kWorldY) return false;
     const float lt = fbm_2d(((float)wx + g.offx) * 0.0006f, ((float)wz + g.offz) * 0.0006f, 3);
@@ -255,7 +270,7 @@ __device__ __forceinline__ float branch_jitter(uint32_t hash, uint32_t b) {
 }
 
 // paint_tree, voxel.rs:1605-1710
-__device__ void tree_prims(const Tree &t, Emit &e) {
+__device__ void tree_prims(const Tree &t, const uint32_t *lmx, Emit &e) {
     const float tau = 6.28318548202514648f;  // std::f32::consts::TAU
     const uint32_t h = t.hash;
     if (t.ttype == 2) {
@@ -264,7 +279,7 @@ __device__ void tree_prims(const Tree &t, Emit &e) {
         for (int32_t i = 0; i < 6; ++i) {
             const float tf = (float)i / 6.0f;
             const int32_t y = t.y + f2i((float)trunk_h * (0.35f + tf * 0.78f));
-            const int32_t r = f2i(pow_f(1.0f - tf, 0.85f) * 3.5f + 1.0f);
+            const int32_t r = f2i(pow085(lmx, 1.0f - tf) * 3.5f + 1.0f);
             e.canopy(t.x, y, t.z, r, M_LEAVES_PINE);
         }
     } else if (t.ttype == 1) {
@@ -275,8 +290,8 @@ __device__ void tree_prims(const Tree &t, Emit &e) {
             const float angle = ((float)b / (float)n) * tau + branch_jitter(h, (uint32_t)b) * 0.5f;
             const int32_t len = 2 + (int32_t)((h * ((uint32_t)b + 1u)) % 3u);
             const int32_t sy = t.y + f2i((float)trunk_h * 0.7f);
-            const int32_t ex = t.x + f2i(cos_f(angle) * (float)len);
-            const int32_t ez = t.z + f2i(sin_f(angle) * (float)len);
+            const int32_t ex = t.x + f2i(cos_f(lmx, angle) * (float)len);
+            const int32_t ez = t.z + f2i(sin_f(lmx, angle) * (float)len);
             e.line(t.x, sy, t.z, ex, sy + 1, ez, M_WOOD_BIRCH);
             e.canopy(ex, sy + 1, ez, 2, M_LEAVES_BIRCH);
         }
@@ -306,9 +321,9 @@ __device__ void tree_prims(const Tree &t, Emit &e) {
             const float angle = ((float)b / (float)n) * tau + branch_jitter(h, (uint32_t)b) * 0.6f;
             const int32_t len = 3 + (int32_t)((h * ((uint32_t)b + 7u)) % 3u);
             const int32_t sy = t.y + f2i((float)trunk_h * 0.65f);
-            const int32_t ex = t.x + f2i(cos_f(angle) * (float)len);
+            const int32_t ex = t.x + f2i(cos_f(lmx, angle) * (float)len);
             const int32_t ey = sy + f2i((float)len * 0.5f);
-            const int32_t ez = t.z + f2i(sin_f(angle) * (float)len);
+            const int32_t ez = t.z + f2i(sin_f(lmx, angle) * (float)len);
             e.line(t.x, sy, t.z, ex, ey, ez, M_WOOD);
             e.canopy(ex, ey, ez, 3, leaf);
         }
@@ -403,7 +418,7 @@ __global__ void __launch_bounds__(256) k_gen_columns(GenPlan p, Dims d, Seed g) 
     const int32_t wzi = ccz * kCV + (int32_t)(col >> 5);
     const float wx = (float)wxi, wz = (float)wzi;
     int32_t water_top;
-    const int32_t h = sample_terrain(wx, wz, g.offx, g.offz, &water_top);
+    const int32_t h = sample_terrain(wx, wz, g.offx, g.offz, g.lmx, &water_top);
     const uint32_t hu = (uint32_t)h;
     const float temperature = fbm_2d((wx + g.offx) * 0.0006f, (wz + g.offz) * 0.0006f, 3);
     const float humidity =
@@ -455,7 +470,7 @@ __global__ void __launch_bounds__(128) k_gen_trees(GenPlan p, Dims d, Seed g) {
         Emit e;
         e.out = reinterpret_cast<Prim *>(p.prims) + (size_t)c * kPrims;
         e.n = 0;
-        tree_prims(t, e);
+        tree_prims(t, g.lmx, e);
         h = e.n | (t.y << 8);
     }
     p.hdr[c] = h;
@@ -615,6 +630,28 @@ __global__ void __launch_bounds__(kSlotThreads, 4) k_gen_slot(DevWorld w, GenPla
 
 }  // namespace
 
+namespace {
+__global__ void k_gen_math(const uint32_t *lmx, uint32_t fn, const float *__restrict__ in, size_t n,
+                           float *__restrict__ out) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float x = in[i];
+    float v;
+    if (fn == gm::LMX_POW115) v = pow115(lmx, x);
+    else if (fn == gm::LMX_POW085) v = pow085(lmx, x);
+    else if (fn == gm::LMX_COS) v = cos_f(lmx, x);
+    else v = sin_f(lmx, x);
+    out[i] = v;
+}
+}  // namespace
+
+cudaError_t launch_gen_math(const uint32_t *lmx, uint32_t fn, const float *in, size_t n, float *out,
+                            cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    k_gen_math<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(lmx, fn, in, n, out);
+    return cudaGetLastError();
+}
+
 size_t gen_prim_bytes_per_src() { return sizeof(Prim) * kCand * kPrims; }
 
 cudaError_t launch_gen_slots(const DevWorld &w, uint64_t seed, const GenPlan &p, cudaStream_t s) {
@@ -624,6 +661,8 @@ cudaError_t launch_gen_slots(const DevWorld &w, uint64_t seed, const GenPlan &p,
     // seed_offset_xz, voxel.rs:1163-1167
     g.offx = (float)(int32_t)(uint32_t)(seed >> 32) * 0.01734f;
     g.offz = (float)(int32_t)(uint32_t)(seed & 0xFFFFFFFFull) * 0.02153f;
+    g.lmx = p.lmx;
+    if (!g.lmx) return cudaErrorInvalidValue;
     const uint32_t n_col_threads = p.n_cols * (uint32_t)(kCV * kCV);
     k_gen_columns<<<(n_col_threads + 255) / 256, 256, 0, s>>>(p, w.d, g);
     const uint32_t n_tree_threads = p.n_srcs * (uint32_t)kCand;
