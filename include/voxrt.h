@@ -438,7 +438,8 @@ typedef struct {
     uint64_t mem_budget_bytes;  /* device bytes for all slots (56 B per ray) */
     int32_t slots;              /* batches in flight at once, 1..16         */
     int32_t max_batch_rays;     /* rays per batch; 0 = budget / slots / 56  */
-    int32_t reserved[4];
+    int32_t max_batch_requests; /* requests per batch; 0 = as many as fit   */
+    int32_t reserved[3];
 } VxServeConfig;
 
 typedef struct {

@@ -113,14 +113,18 @@ def test_device_math_equals_glibc_exhaustively():
     try:
         xin = torch.empty(chunk, dtype=torch.float32, device="cuda")
         xout = torch.empty(chunk, dtype=torch.float32, device="cuda")
+        # torch writes the inputs on its stream; the library's calls (stream
+        # NULL = the world's own stream, waited for) start after a device sync
+        stream = None
         for fn in (POW115, POW085):
             bad = 0
             for start in range(0, ONE_BITS + 1, chunk):
                 n = min(chunk, ONE_BITS + 1 - start)
                 bits = torch.arange(start, start + n, dtype=torch.int64, device="cuda")
                 xin[:n] = bits.to(torch.int32).view(torch.float32)
+                torch.cuda.synchronize()
                 L.check(lib.vx_gen_math(dw.handle, fn, C.c_void_p(xin.data_ptr()), n,
-                                        C.c_void_p(xout.data_ptr()), None))
+                                        C.c_void_p(xout.data_ptr()), stream))
                 got = xout[:n].cpu().numpy().view(np.uint32)
                 want = po.libm_batch(fn, xin[:n].cpu().numpy(), threads).view(np.uint32)
                 bad += int(np.count_nonzero(got != want))
@@ -128,9 +132,10 @@ def test_device_math_equals_glibc_exhaustively():
         a = branch_angles()
         t = torch.from_numpy(a).cuda()
         out = torch.empty_like(t)
+        torch.cuda.synchronize()
         for fn in (COS, SIN):
             L.check(lib.vx_gen_math(dw.handle, fn, C.c_void_p(t.data_ptr()), len(a),
-                                    C.c_void_p(out.data_ptr()), None))
+                                    C.c_void_p(out.data_ptr()), stream))
             got = out.cpu().numpy().view(np.uint32)
             want = po.libm_batch(fn, a, threads).view(np.uint32)
             assert np.array_equal(got, want), fn

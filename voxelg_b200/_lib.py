@@ -82,7 +82,8 @@ class VxQueueTuning(C.Structure):
 
 class VxServeConfig(C.Structure):
     _fields_ = [("mem_budget_bytes", C.c_uint64), ("slots", C.c_int32),
-                ("max_batch_rays", C.c_int32), ("reserved", C.c_int32 * 4)]
+                ("max_batch_rays", C.c_int32), ("max_batch_requests", C.c_int32),
+                ("reserved", C.c_int32 * 3)]
 
 
 class VxServeStats(C.Structure):

@@ -665,7 +665,8 @@ int world_lmx(VxWorld *w, const char *fn) {
         return VX_ERR_INVALID;
     }
     VX_CK(cudaMalloc(&w->d_lmx, t->size() * 4));
-    VX_CK(cudaMemcpyAsync(w->d_lmx, t->data(), t->size() * 4, cudaMemcpyHostToDevice, w->stream));
+    // once per world; synchronous, so that work on any stream may read it
+    VX_CK(cudaMemcpy(w->d_lmx, t->data(), t->size() * 4, cudaMemcpyHostToDevice));
     return VX_OK;
 }
 

@@ -90,6 +90,7 @@ struct VxServer {
     int device = 0;
     vx::TraceArgs ta{};
     size_t cap = 0;
+    size_t max_reqs = 0;               // requests per batch, 0 = no limit
     std::vector<Slot> slots;
 
     std::mutex mu;  // fifo + tickets
@@ -285,7 +286,8 @@ void worker_loop(VxServer *s) {
             } else if (free_slot) {
                 size_t n = 0;
                 while (!s->fifo.empty() && s->fifo.front().req &&
-                       n + s->fifo.front().req->n <= s->cap) {
+                       n + s->fifo.front().req->n <= s->cap &&
+                       (s->max_reqs == 0 || free_slot->reqs.size() < s->max_reqs)) {
                     Request *r = s->fifo.front().req;
                     s->fifo.pop_front();
                     free_slot->reqs.push_back(r);
@@ -362,7 +364,8 @@ extern "C" {
 int vx_server_create(VxWorld *w, const int32_t origin[3], const VxTraceParams *p,
                      const VxServeConfig *cfg, VxServer **out) {
     if (!w || !origin || !p || !cfg || !out || cfg->slots < 1 || cfg->slots > 16 ||
-        cfg->max_batch_rays < 0 || cfg->mem_budget_bytes < 56ull * (uint64_t)cfg->slots) {
+        cfg->max_batch_rays < 0 || cfg->max_batch_requests < 0 ||
+        cfg->mem_budget_bytes < 56ull * (uint64_t)cfg->slots) {
         vx::set_error("vx_server_create: need 1..16 slots and a budget of at least 56 B per slot");
         return VX_ERR_INVALID;
     }
@@ -388,6 +391,7 @@ int vx_server_create(VxWorld *w, const int32_t origin[3], const VxTraceParams *p
     s->ta.ro[1] = origin[1];
     s->ta.ro[2] = origin[2];
     s->cap = cap;
+    s->max_reqs = (size_t)cfg->max_batch_requests;
     cudaError_t e = cudaSetDevice(s->device);
     s->slots.resize((size_t)cfg->slots);
     for (Slot &sl : s->slots) {

@@ -18,10 +18,11 @@ class Server:
     """Ray-query server over a DeviceWorld (which must outlive it)."""
 
     def __init__(self, world: DeviceWorld, params: L.VxTraceParams, origin=(0, 0, 0),
-                 mem_budget_bytes: int = 256 << 20, slots: int = 4, max_batch_rays: int = 0):
+                 mem_budget_bytes: int = 256 << 20, slots: int = 4, max_batch_rays: int = 0,
+                 max_batch_requests: int = 0):
         self._lib = L.load()
         self.world = world
-        cfg = L.VxServeConfig(mem_budget_bytes, slots, max_batch_rays)
+        cfg = L.VxServeConfig(mem_budget_bytes, slots, max_batch_rays, max_batch_requests)
         h = C.c_void_p()
         L.check(self._lib.vx_server_create(world.handle, L.i3(origin), C.byref(params),
                                            C.byref(cfg), C.byref(h)))
