@@ -36,7 +36,9 @@ picking    benches/trace.rs raycast_pick rays on the reference's demo world:
 learned    the learned start-distance proposal: on-device training, then the
            plain DDA, the learned form and the verification without a network
            on one 1920x1080 frame, with acceptance and iterations saved.
-serving    the ray-query server under 64 open-loop Poisson clients: p50/p99.
+serving    the ray-query server under 64 open-loop Poisson clients: p50/p99, at the
+           north star's load, at a query-sized load where batches form, and past
+           capacity with and without continuous batching.
 ao         (on the benchmark frame) contact AO of the primary hits.
 """
 from __future__ import annotations
@@ -520,18 +522,37 @@ def run_extras(vg, device: int) -> dict:
     out["picking"] = run_picking(vg, demo)
     demo.close()
     out["learned"] = run_learned(vg, dw)
-    srv = sv.Server(dw, p, mem_budget_bytes=1 << 30, slots=8)
-    st = srv.bench(clients=64, rate_per_client=200.0, seconds=3.0, min_rays=1, max_rays=50000,
-                   min_len=8.0, max_len=512.0, edit_fraction_per_s=0.01, seed=3)
-    srv.close()
+    def serve(rate, max_rays, max_len, max_req=0):
+        srv = sv.Server(dw, p, mem_budget_bytes=1 << 30, slots=8, max_batch_requests=max_req)
+        st = srv.bench(clients=64, rate_per_client=rate, seconds=3.0, min_rays=1,
+                       max_rays=max_rays, min_len=8.0, max_len=max_len,
+                       edit_fraction_per_s=0.01, seed=3)
+        srv.close()
+        return {"requests": st["requests"], "batches": st["batches"],
+                "requests_per_batch": round(st["requests"] / max(1, st["batches"]), 2),
+                "p50_ms": round(st["p50_ms"], 4), "p99_ms": round(st["p99_ms"], 4),
+                "max_ms": round(st["max_ms"], 4), "mrays_s": round(st["mrays_per_s"], 2),
+                "edits": st["edits"], "seconds": round(st["seconds"], 2)}
+
+    # the north star's load: large requests, the offered load well below capacity
     out["serving"] = {
         "workload": "64 clients, Poisson 200 req/s each, 1-50k rays per request (log-uniform), "
                     "max length 8-512, 1% of bricks re-randomized per second",
-        "requests": st["requests"], "p50_ms": round(st["p50_ms"], 4),
-        "p99_ms": round(st["p99_ms"], 4), "max_ms": round(st["max_ms"], 4),
-        "mrays_s": round(st["mrays_per_s"], 2), "batches": st["batches"], "edits": st["edits"],
-        "seconds": round(st["seconds"], 2),
-    }
+        **serve(200.0, 50000, 512.0)}
+    # query-sized requests (picking, line of sight) at a rate where batches form
+    out["serving_batched"] = {
+        "workload": "64 clients, Poisson 2000 req/s each, 1-4000 rays per request "
+                    "(log-uniform), max length 8-256, 1% of bricks re-randomized per second",
+        **serve(2000.0, 4000, 256.0)}
+    # the same requests past saturation: continuous batching against one request
+    # per batch (max_batch_requests = 1), the server's capacity either way
+    sat = serve(4000.0, 4000, 256.0)
+    one = serve(4000.0, 4000, 256.0, max_req=1)
+    out["serving_saturated"] = {
+        "workload": "64 clients, Poisson 4000 req/s each (past capacity: each client keeps 4 "
+                    "requests in flight), 1-4000 rays per request, max length 8-256",
+        "batched": sat, "one_request_per_batch": one,
+        "batching_gain": round(sat["mrays_s"] / max(1e-9, one["mrays_s"]), 3)}
     dw.close()
     return out
 
