@@ -245,7 +245,10 @@ int vx_world_load(VxWorld *w, const char *path);
 /* Incremental update from dirty bricks (renderer.rs:1345-1394): writes the
  * given bricks and recomputes the touched tile/chunk/L4 masks and uniform
  * LUT entries on the device (voxel.rs:879-946 semantics).  brick_idx and
- * bricks are host arrays of n entries; duplicates allowed (last wins). */
+ * bricks are host arrays of n entries, copied before the call returns;
+ * duplicates allowed (the last entry wins, resolved on the device).  With a
+ * stream the update is asynchronous and ordered on that stream (and before
+ * the library's later calls on this world); stream NULL waits for it. */
 int vx_world_apply_dirty(VxWorld *w, const uint32_t *brick_idx, const VxBrick *bricks,
                          size_t n, void *stream);
 /* The checked library.  libvoxrt_checked.so is built from the same sources

@@ -420,6 +420,52 @@ def test_apply_dirty_duplicates_last_wins(vg):
     dw.close()
 
 
+def test_apply_dirty_on_a_stream_is_ordered(vg):
+    """vx_world_apply_dirty on a caller's stream returns at once: three
+    updates in a row (duplicates within and across them, staging buffers
+    reused) on a torch stream, then a frame on that stream and a download on
+    the world's own stream, equal the oracle's world after the same updates
+    applied in order (last entry wins)."""
+    import torch
+    rng = np.random.default_rng(77)
+    ow = po.World(64, 16, 64)
+    dw = vg.DeviceWorld(64, 16, 64)
+    dw.upload(ow.a)
+    stream = torch.cuda.Stream()
+    nb = 64 * 16 * 64
+    for r in range(3):
+        n = 4000
+        idx = rng.integers(0, nb // 4, n).astype(np.uint32)  # many repeats
+        b = np.zeros(n, po.BRICK)
+        occ = rng.integers(0, 2 ** 63, n, dtype=np.uint64) & rng.integers(0, 2 ** 63, n,
+                                                                           dtype=np.uint64)
+        b["occupancy"] = occ
+        bits = ((occ[:, None] >> np.arange(64, dtype=np.uint64)) & 1).astype(bool)
+        mats = rng.integers(1, 5, (n, 64)).astype(np.uint8)
+        b["materials"] = np.where(bits, mats, 0)
+        full = rng.random(n) < 0.1
+        b["occupancy"][full] = np.uint64(0xFFFFFFFFFFFFFFFF)
+        b["materials"][full] = 4
+        dw.apply_dirty(idx, b, stream=stream.cuda_stream)
+        for i in range(n):  # the oracle: in order, so the last entry wins
+            ow.a["bricks"][idx[i]] = b[i]
+    ow.rebuild()
+    cam = vg.camera_from_pose((128.5, 40.2, 128.5), 0.6, -0.35, 1.2, 160, 90)
+    p = vg.default_params()
+    with torch.cuda.stream(stream):
+        rec = torch.empty(160 * 90 * 24, dtype=torch.uint8, device="cuda")
+        sh = torch.empty(160 * 90 * 8, dtype=torch.uint8, device="cuda")
+        vg.render_primary(dw, cam, p, rec, sh, stream=stream.cuda_stream)
+    stream.synchronize()
+    got = dw.download()
+    for k in ("tile_mask", "chunk_mask", "l4_mask", "brick_uniform", "tile_uniform"):
+        assert np.array_equal(got[k], ow.a[k]), k
+    assert np.array_equal(got["bricks"].view(np.uint8), ow.a["bricks"].view(np.uint8))
+    want, _, _, _, _ = po.render_frame(ow, cam, p)
+    assert np.array_equal(rec.cpu().numpy(), want.view(np.uint8))
+    dw.close()
+
+
 def test_render_host_equals_device(vg, dev_c1):
     cam = vg.default_camera(dev_c1, 320, 180)
     p = vg.default_params()

@@ -86,6 +86,20 @@ struct VxWorld {
     void *h_gen = nullptr;           // pinned staging of the generator's plan
     size_t h_gen_cap = 0;            // bytes
     uint32_t *d_lmx = nullptr;       // device copy of the generator's math exception table
+    // vx_world_apply_dirty: a claim word per brick (zero between updates),
+    // and two staging buffers (pinned host + device), each free again once
+    // its update's event has passed; every update waits for the previous one
+    uint32_t *d_dirty_win = nullptr;
+    struct DirtyStage {
+        uint32_t *h_idx = nullptr;
+        VxBrick *h_bricks = nullptr;
+        uint32_t *d_idx = nullptr;
+        VxBrick *d_bricks = nullptr;
+        size_t cap = 0;
+        cudaEvent_t done = nullptr;
+    } dirty[2];
+    uint64_t dirty_calls = 0;
+    cudaEvent_t dirty_last = nullptr;
     // empty-space distance fields of the learned form, rebuilt on demand when
     // the masks changed (mask_gen) since they were built (df_gen)
     uint8_t *bdf = nullptr, *tdf = nullptr, *df_tmp = nullptr;
@@ -212,6 +226,15 @@ void free_world(VxWorld *w) {
     cudaFree(w->lrn_depth);
     if (w->h_gen) cudaFreeHost(w->h_gen);
     cudaFree(w->d_lmx);
+    cudaFree(w->d_dirty_win);
+    for (auto &b : w->dirty) {
+        if (b.h_idx) cudaFreeHost(b.h_idx);
+        if (b.h_bricks) cudaFreeHost(b.h_bricks);
+        cudaFree(b.d_idx);
+        cudaFree(b.d_bricks);
+        if (b.done) cudaEventDestroy(b.done);
+    }
+    if (w->dirty_last) cudaEventDestroy(w->dirty_last);
     if (w->copy_stream) cudaStreamSynchronize(w->copy_stream);
     for (int i = 0; i < 2; ++i) {
         cudaFree(w->hrec[i]);
@@ -1120,44 +1143,65 @@ int vx_world_apply_dirty(VxWorld *w, const uint32_t *brick_idx, const VxBrick *b
         return VX_ERR_INVALID;
     }
     if (n == 0) return VX_OK;
+    if (n >= 0xFFFFFFFFull) {
+        vx::set_error("vx_world_apply_dirty: more than 2^32 - 2 entries");
+        return VX_ERR_INVALID;
+    }
     const vx::Dims &d = w->dw.d;
-    // last occurrence of an index wins (the order the caller edited in)
-    std::vector<uint32_t> idx;
-    std::vector<VxBrick> pay;
-    idx.reserve(n);
-    pay.reserve(n);
-    {
-        std::unordered_map<uint32_t, size_t> last;
-        last.reserve(n * 2);
-        for (size_t i = 0; i < n; ++i) {
-            if ((int64_t)brick_idx[i] >= d.n_bricks) {
-                vx::set_error("vx_world_apply_dirty: brick index out of range");
-                return VX_ERR_INVALID;
-            }
-            last[brick_idx[i]] = i;
+    for (size_t i = 0; i < n; ++i) {
+        if ((int64_t)brick_idx[i] >= d.n_bricks) {
+            vx::set_error("vx_world_apply_dirty: brick index out of range");
+            return VX_ERR_INVALID;
         }
-        for (size_t i = 0; i < n; ++i)
-            if (last[brick_idx[i]] == i) {
-                idx.push_back(brick_idx[i]);
-                pay.push_back(bricks[i]);
-            }
     }
     int rc = use_device(w);
     if (rc != VX_OK) return rc;
     std::lock_guard<std::mutex> lk(w->mu);
     cudaStream_t s = stream ? as_stream(stream) : w->stream;
-    if (w->idx_cap < idx.size() || w->bricks_cap < idx.size()) VX_CK(cudaStreamSynchronize(s));
-    rc = ensure(&w->d_idx, &w->idx_cap, idx.size());
-    if (rc == VX_OK) rc = ensure(&w->d_bricks, &w->bricks_cap, idx.size());
-    if (rc != VX_OK) return rc;
-    VX_CK(cudaMemcpyAsync(w->d_idx, idx.data(), idx.size() * sizeof(uint32_t),
-                          cudaMemcpyHostToDevice, s));
-    VX_CK(cudaMemcpyAsync(w->d_bricks, pay.data(), pay.size() * sizeof(VxBrick),
-                          cudaMemcpyHostToDevice, s));
+    if (!w->d_dirty_win) {
+        VX_CK(cudaMalloc(&w->d_dirty_win, (size_t)d.n_bricks * sizeof(uint32_t)));
+        VX_CK(cudaMemset(w->d_dirty_win, 0, (size_t)d.n_bricks * sizeof(uint32_t)));
+        for (auto &b : w->dirty) VX_CK(cudaEventCreateWithFlags(&b.done, cudaEventDisableTiming));
+        VX_CK(cudaEventCreateWithFlags(&w->dirty_last, cudaEventDisableTiming));
+    }
+    VxWorld::DirtyStage &b = w->dirty[w->dirty_calls & 1u];
+    // the staging buffer's previous update has finished (usually long ago)
+    VX_CK(cudaEventSynchronize(b.done));
+    if (b.cap < n) {
+        if (b.h_idx) cudaFreeHost(b.h_idx);
+        if (b.h_bricks) cudaFreeHost(b.h_bricks);
+        cudaFree(b.d_idx);
+        cudaFree(b.d_bricks);
+        b.h_idx = nullptr;
+        b.h_bricks = nullptr;
+        b.d_idx = nullptr;
+        b.d_bricks = nullptr;
+        b.cap = 0;
+        VX_CK(cudaHostAlloc(reinterpret_cast<void **>(&b.h_idx), n * sizeof(uint32_t),
+                            cudaHostAllocDefault));
+        VX_CK(cudaHostAlloc(reinterpret_cast<void **>(&b.h_bricks), n * sizeof(VxBrick),
+                            cudaHostAllocDefault));
+        VX_CK(cudaMalloc(&b.d_idx, n * sizeof(uint32_t)));
+        VX_CK(cudaMalloc(&b.d_bricks, n * sizeof(VxBrick)));
+        b.cap = n;
+    }
+    std::memcpy(b.h_idx, brick_idx, n * sizeof(uint32_t));
+    std::memcpy(b.h_bricks, bricks, n * sizeof(VxBrick));
+    // updates apply in call order, whatever streams they come on
+    if (w->dirty_calls > 0) VX_CK(cudaStreamWaitEvent(s, w->dirty_last, 0));
+    VX_CK(cudaMemcpyAsync(b.d_idx, b.h_idx, n * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+    VX_CK(cudaMemcpyAsync(b.d_bricks, b.h_bricks, n * sizeof(VxBrick), cudaMemcpyHostToDevice, s));
     vx::world_masks_changed(w);
-    VX_CK(vx::launch_apply_dirty(w->dw, w->d_idx, w->d_bricks, idx.size(), s));
-    // the staging vectors die with this call: finish the copies first
-    VX_CK(cudaStreamSynchronize(s));
+    VX_CK(vx::launch_apply_dirty_last_wins(w->dw, w->d_dirty_win, b.d_idx, b.d_bricks, n, s));
+    VX_CK(cudaEventRecord(b.done, s));
+    VX_CK(cudaEventRecord(w->dirty_last, s));
+    ++w->dirty_calls;
+    if (!stream) {
+        VX_CK(cudaStreamSynchronize(s));
+    } else if (s != w->stream) {
+        // the library's own calls on the world's stream come after the update
+        VX_CK(cudaStreamWaitEvent(w->stream, w->dirty_last, 0));
+    }
     return VX_OK;
 }
 

@@ -176,6 +176,10 @@ cudaError_t launch_tile_meta(const DevWorld &w, cudaStream_t s);
 // idx the distinct bricks they touch (uniform bytes and masks refreshed).
 cudaError_t launch_edits(const DevWorld &w, const uint2 *ed, size_t n_edits, const uint32_t *idx,
                          size_t n_bricks, cudaStream_t s);
+// launch_apply_dirty for n entries that may repeat a brick (the last entry
+// wins); win is a zeroed word per brick, zeroed again when the update ends
+cudaError_t launch_apply_dirty_last_wins(const DevWorld &w, uint32_t *win, const uint32_t *idx,
+                                         const VxBrick *bricks, size_t n, cudaStream_t s);
 cudaError_t launch_apply_dirty(const DevWorld &w, const uint32_t *idx, const VxBrick *bricks,
                                size_t n, cudaStream_t s);
 

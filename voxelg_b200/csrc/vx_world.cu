@@ -221,12 +221,8 @@ __global__ void k_build_l4(DevWorld w) {
 }
 
 // ------------------------------------------------------------- dirty
-__global__ void k_dirty_scatter(DevWorld w, const uint32_t *__restrict__ idx,
-                                const VxBrick *__restrict__ bricks, size_t n) {
-    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const int64_t bi = idx[i];
-    const uint2 *src = reinterpret_cast<const uint2 *>(bricks + i);
+__device__ __forceinline__ void scatter_brick(const DevWorld &w, int64_t bi, const VxBrick *b) {
+    const uint2 *src = reinterpret_cast<const uint2 *>(b);
     const uint2 o = src[0];
     const uint64_t occ = (uint64_t)o.x | ((uint64_t)o.y << 32);
     w.occ[bi] = occ;
@@ -234,6 +230,38 @@ __global__ void k_dirty_scatter(DevWorld w, const uint32_t *__restrict__ idx,
 #pragma unroll
     for (int k = 0; k < 8; ++k) dst[k] = src[1 + k];
     w.brick_uniform[bi] = uniform_of(occ, reinterpret_cast<const uint8_t *>(src + 1));
+}
+
+__global__ void k_dirty_scatter(DevWorld w, const uint32_t *__restrict__ idx,
+                                const VxBrick *__restrict__ bricks, size_t n) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    scatter_brick(w, idx[i], bricks + i);
+}
+
+// Duplicate brick indices in one update, last entry wins: each entry claims
+// its brick with its position + 1 (the largest wins), only the winner writes,
+// and the claims are cleared again once the update's kernels are done.
+__global__ void k_dirty_claim(uint32_t *__restrict__ win, const uint32_t *__restrict__ idx,
+                              size_t n) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    atomicMax(win + idx[i], (uint32_t)(i + 1));
+}
+__global__ void k_dirty_scatter_last(DevWorld w, const uint32_t *__restrict__ win,
+                                     const uint32_t *__restrict__ idx,
+                                     const VxBrick *__restrict__ bricks, size_t n) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t bi = idx[i];
+    if (win[bi] != (uint32_t)(i + 1)) return;
+    scatter_brick(w, bi, bricks + i);
+}
+__global__ void k_dirty_release(uint32_t *__restrict__ win, const uint32_t *__restrict__ idx,
+                                size_t n) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    win[idx[i]] = 0u;
 }
 
 // Each dirty brick re-derives its parent word; threads that share a parent
@@ -342,6 +370,19 @@ cudaError_t launch_generate(const DevWorld &w, const VxTerrainParams &t, int16_t
     k_heights<<<blocks_for((int64_t)w.d.vx * w.d.vz, 256), 256, 0, s>>>(g);
     k_gen_bricks<<<blocks_for(w.d.n_bricks, 128), 128, 0, s>>>(g);
     return launch_rebuild_pyramid(w, s);
+}
+
+cudaError_t launch_apply_dirty_last_wins(const DevWorld &w, uint32_t *win, const uint32_t *idx,
+                                         const VxBrick *bricks, size_t n, cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    const unsigned b = blocks_for((int64_t)n, 128);
+    k_dirty_claim<<<b, 128, 0, s>>>(win, idx, n);
+    k_dirty_scatter_last<<<b, 128, 0, s>>>(w, win, idx, bricks, n);
+    k_dirty_release<<<b, 128, 0, s>>>(win, idx, n);
+    k_dirty_tiles<<<b, 128, 0, s>>>(w, idx, n);
+    k_dirty_chunks<<<b, 128, 0, s>>>(w, idx, n);
+    k_dirty_l4<<<b, 128, 0, s>>>(w, idx, n);
+    return launch_tile_meta(w, s);
 }
 
 cudaError_t launch_apply_dirty(const DevWorld &w, const uint32_t *idx, const VxBrick *bricks,
