@@ -324,7 +324,7 @@ class Scene:
 
 # ---------------------------------------------------------------- traversal
 
-F_L4, F_LUT, F_LOD = 1, 2, 4
+F_L4, F_LUT, F_LOD, F_BEAM = 1, 2, 4, 8
 STOCK = F_L4 | F_LUT | F_LOD
 
 
@@ -658,6 +658,72 @@ def pick(sc: Scene, cam, d_in):
     return None
 
 
+# ---------------------------------------------------------------- beam
+
+BEAM_NONE = lit("1e9")
+BEAM_MARGIN = Q(16)
+
+
+def trunc_div(a: int, b: int) -> int:
+    """WGSL i32 division (toward zero)."""
+    q = abs(a) // b
+    return q if a >= 0 else -q
+
+
+def beam_first_tile(sc: Scene, origin, d):
+    """trace_first_tile, beam.wgsl:51-113: a walk over 16-voxel tiles in
+    world coordinates from the camera to the first tile whose bit is set in
+    its chunk word; its entry t, or 1e9."""
+    lo = [Q(sc.ro[k]) for k in range(3)]
+    hi = [add(lo[k], Q(sc.V[k])) for k in range(3)]
+    inv = [safe_inv(v) for v in d]
+    t0 = [mul(sub(lo[k], origin[k]), inv[k]) for k in range(3)]
+    t1 = [mul(sub(hi[k], origin[k]), inv[k]) for k in range(3)]
+    tmn = [min(t0[k], t1[k]) for k in range(3)]
+    tmx = [max(t0[k], t1[k]) for k in range(3)]
+    t_enter = max(max(tmn[0], tmn[1]), max(tmn[2], Q(0)))
+    t_exit = min(min(tmx[0], tmx[1]), tmx[2])
+    if t_enter >= t_exit or t_exit < 0:
+        return BEAM_NONE
+    te = add(t_enter, lit("0.05"))
+    c01 = lit("0.01")
+    tile, step, tdel, tmax = [], [], [], []
+    for k in range(3):
+        p = add(origin[k], mul(d[k], te))
+        p = min(max(p, add(lo[k], c01)), sub(hi[k], c01))
+        tile.append(floor_i(div(p, 16)))
+        step.append(sgn(d[k]))
+        tdel.append(mul(abs(inv[k]), 16))
+        b = (tile[k] + 1) * 16 if step[k] > 0 else tile[k] * 16
+        tmax.append(mul(sub(Q(b), origin[k]), inv[k]))
+    otile = [trunc_div(sc.ro[k], 16) for k in range(3)]
+    T = [v // 16 for v in sc.V]
+    t_cur = t_enter
+    for _ in range(80):
+        if not all(0 <= tile[k] - otile[k] < T[k] for k in range(3)):
+            return BEAM_NONE
+        st = (pos_mod(tile[0], T[0]), tile[1], pos_mod(tile[2], T[2]))
+        if not sc.empty((16 * st[0], 16 * st[1], 16 * st[2]), 16):
+            return t_cur
+        if tmax[0] < tmax[1] and tmax[0] < tmax[2]:
+            ax = 0
+        elif tmax[1] < tmax[2]:
+            ax = 1
+        else:
+            ax = 2
+        tile[ax] += step[ax]
+        t_cur = tmax[ax]
+        tmax[ax] = add(tmax[ax], tdel[ax])
+    return BEAM_NONE
+
+
+def beam_pass(sc: Scene, cam):
+    """cs_beam, beam.wgsl:30-49: one first-tile t per 8x8 pixel block."""
+    bw, bh = (int(cam.res[0]) + 7) // 8, (int(cam.res[1]) + 7) // 8
+    return [[beam_first_tile(sc, cam.origin, cam.beam_dir(gx, gy)) for gx in range(bw)]
+            for gy in range(bh)]
+
+
 # ---------------------------------------------------------------- cameras
 
 
@@ -680,6 +746,16 @@ class Camera:
         half = Q(1, 2)
         u = div(add(add(Q(px), half), self.jitter[0]), self.res[0])
         v = div(add(add(Q(py), half), self.jitter[1]), self.res[1])
+        return self.dir_uv(u, v)
+
+    def beam_dir(self, gx, gy):
+        """cs_beam's ray through the centre of the 8x8 block (beam.wgsl:36-44):
+        uv = (8 g + 4) / resolution, no jitter."""
+        u = div(add(mul(Q(gx), 8), 4), self.res[0])
+        v = div(add(mul(Q(gy), 8), 4), self.res[1])
+        return self.dir_uv(u, v)
+
+    def dir_uv(self, u, v):
         ndc_x = sub(mul(u, 2), 1)
         ndc_y = sub(1, mul(v, 2))
         aspect = div(self.res[0], self.res[1])
@@ -1003,22 +1079,33 @@ def build():
     for name, cam in cams:
         sc = scenes[name]
         assert cam.world_origin == sc.ro
-        for flags in (STOCK, F_L4):
+        beam = beam_pass(sc, cam)
+        for flags in (STOCK, F_L4, STOCK | F_BEAM):
             P = Params(flags=flags)
             recs = []
             W, H = int(cam.res[0]), int(cam.res[1])
             for py in range(H):
                 for px in range(W):
                     d = cam.ray_dir(px, py)
+                    org, skip = cam.origin, Q(0)
+                    if flags & F_BEAM:
+                        # cs_main's beam skip (raymarch.wgsl:603-609, :629-631)
+                        skip = max(Q(0), sub(beam[py // 8][px // 8], BEAM_MARGIN))
+                        org = [add(cam.origin[k], mul(d[k], skip)) for k in range(3)]
                     try:
-                        r = trace(sc, cam.origin, d, P.max_dist, P)
+                        r = trace(sc, org, d, P.max_dist, P)
                     except Deviation:
                         recs.append(None)       # a sub-voxel pixel: not pinned
                         continue
-                    check_geometry(sc, cam.origin, d, r, P, False)
+                    if flags & F_BEAM:
+                        if r["flags"] & 1:
+                            r["t"] = add(r["t"], skip)
+                    else:
+                        check_geometry(sc, cam.origin, d, r, P, False)
                     recs.append(record_json(r))
             suite["frames"].append({"world": name, "camera": cam.to_json(),
-                                    "params": P.to_json(), "expect": recs})
+                                    "params": P.to_json(), "expect": recs,
+                                    "beam": [[float(b) for b in row] for row in beam]})
 
     # picking (src/raycast.rs): axis rays and unnormalised oblique ones
     sc = scenes["lanes"]

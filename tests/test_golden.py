@@ -14,7 +14,9 @@ skip_to_cell's landing; uniform tile and brick exits; brick LOD beyond 400
 (topmost material, recorded at the voxel where the walk stands) and tile
 LOD beyond 520 (representative material); the 700 distance budget; glass,
 far water, far leaves, decoration and turf; toroidal slots of a window whose
-origin is not cell aligned; camera rays through ray_dir_uv; picking.
+origin is not cell aligned; camera rays through ray_dir_uv; the beam
+pre-pass (beam.wgsl: the block-centre ray's tile walk in world coordinates,
+its skip of the pixel rays' origins, t re-based); picking.
 """
 import ctypes as C
 import importlib.util
@@ -226,9 +228,13 @@ def test_oracle_rays_match_golden():
 
 def test_oracle_frames_match_golden():
     for fr in GOLDEN["frames"]:
-        rec, _, _, _, _ = po.render_frame(oracle_world(fr["world"]), camera_of(fr["camera"]),
-                                          params_of(fr["params"]), threads=4)
+        rec, _, beam, _, _ = po.render_frame(oracle_world(fr["world"]), camera_of(fr["camera"]),
+                                             params_of(fr["params"]), threads=4)
         assert_records(rec, fr["expect"], f"oracle frame {fr['world']} {fr['params']['flags']}")
+        if fr["params"]["flags"] & 8:
+            # the beam pre-pass itself (beam.wgsl): one first-tile t per 8x8 block
+            want = np.array(fr["beam"], np.float32).reshape(-1)
+            assert np.array_equal(beam.view(np.uint32), want.view(np.uint32)), fr["world"]
 
 
 def test_oracle_picks_match_golden():
@@ -323,6 +329,8 @@ def test_learned_frames_match_golden_except_steps(device_worlds):
     import voxelg_b200 as vg
     from voxelg_b200 import learned as vl
     for fr in GOLDEN["frames"]:
+        if fr["params"]["flags"] & 8:
+            continue  # the learned form runs without the beam pre-pass
         dw = device_worlds[fr["world"]]
         cam, p = camera_of(fr["camera"], True), params_of(fr["params"], True)
         plain, _ = vg.render_primary(dw, cam, p)
