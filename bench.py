@@ -38,7 +38,8 @@ learned    the learned start-distance proposal: on-device training, then the
            on one 1920x1080 frame, with acceptance and iterations saved.
 serving    the ray-query server under 64 open-loop Poisson clients: p50/p99, at the
            north star's load, at a query-sized load where batches form, and past
-           capacity with and without continuous batching.
+           capacity with and without continuous batching; then the same three loads
+           on the device-resident request loop.
 ao         (on the benchmark frame) contact AO of the primary hits.
 """
 from __future__ import annotations
@@ -522,17 +523,25 @@ def run_extras(vg, device: int) -> dict:
     out["picking"] = run_picking(vg, demo)
     demo.close()
     out["learned"] = run_learned(vg, dw)
-    def serve(rate, max_rays, max_len, max_req=0):
-        srv = sv.Server(dw, p, mem_budget_bytes=1 << 30, slots=8, max_batch_requests=max_req)
+    def serve(rate, max_rays, max_len, max_req=0, resident=False):
+        srv = sv.Server(dw, p, mem_budget_bytes=1 << 30, slots=8, max_batch_requests=max_req,
+                        resident=resident)
         st = srv.bench(clients=64, rate_per_client=rate, seconds=3.0, min_rays=1,
                        max_rays=max_rays, min_len=8.0, max_len=max_len,
                        edit_fraction_per_s=0.01, seed=3)
         srv.close()
-        return {"requests": st["requests"], "batches": st["batches"],
-                "requests_per_batch": round(st["requests"] / max(1, st["batches"]), 2),
-                "p50_ms": round(st["p50_ms"], 4), "p99_ms": round(st["p99_ms"], 4),
-                "max_ms": round(st["max_ms"], 4), "mrays_s": round(st["mrays_per_s"], 2),
-                "edits": st["edits"], "seconds": round(st["seconds"], 2)}
+        r = {"requests": st["requests"], "p50_ms": round(st["p50_ms"], 4),
+             "p99_ms": round(st["p99_ms"], 4), "max_ms": round(st["max_ms"], 4),
+             "mrays_s": round(st["mrays_per_s"], 2), "edits": st["edits"],
+             "seconds": round(st["seconds"], 2)}
+        if resident:
+            # launches of the loop: one per edit (an edit ends the launch), per
+            # idle gap and per quarter second
+            r["loop_launches"] = st["batches"]
+        else:
+            r["batches"] = st["batches"]
+            r["requests_per_batch"] = round(st["requests"] / max(1, st["batches"]), 2)
+        return r
 
     # the north star's load: large requests, the offered load well below capacity
     out["serving"] = {
@@ -553,6 +562,15 @@ def run_extras(vg, device: int) -> dict:
                     "requests in flight), 1-4000 rays per request, max length 8-256",
         "batched": sat, "one_request_per_batch": one,
         "batching_gain": round(sat["mrays_s"] / max(1e-9, one["mrays_s"]), 3)}
+    # the device-resident request loop (VX_SERVE_RESIDENT) under the same three loads
+    out["serving_resident"] = {
+        "workload": "the loads of serving, serving_batched and serving_saturated, served by "
+                    "the device-resident request loop (one persistent launch takes requests "
+                    "from mapped host memory; page-locked client buffers read and written "
+                    "in place)",
+        "north_star_load": serve(200.0, 50000, 512.0, resident=True),
+        "query_load": serve(2000.0, 4000, 256.0, resident=True),
+        "past_capacity": serve(4000.0, 4000, 256.0, resident=True)}
     dw.close()
     return out
 

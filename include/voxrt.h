@@ -429,22 +429,43 @@ int vx_queue_graph_destroy(VxQueueGraph *g);
  * The reference's headless server (src/server.rs:6-102) relays edits and
  * poses and holds no world; picking runs client-side (src/app.rs:523-557).
  * This is the device-resident counterpart: clients submit batches of
- * VxRay queries (picking, line-of-sight, physics probes) against one world;
- * a server thread forms batches continuously from whatever has arrived,
- * admits them into a fixed set of device slots sized by the memory budget
- * (a request waits while no slot is free), and runs each batch on its own
- * stream, so batches that arrive while others are on the GPU overlap on the
- * device.  World edits enter the same FIFO and are ordered against every
- * batch before and after them.  Results are byte-identical to running each
- * request alone through vx_trace on the same world. */
+ * VxRay queries (picking, line-of-sight, physics probes) against one world.
+ * World edits enter the same FIFO and are ordered against every request
+ * before and after them.  Results are byte-identical to running each
+ * request alone through vx_trace on the same world.  Two modes:
+ *
+ * VX_SERVE_SLOTS: a server thread forms batches continuously from whatever
+ * has arrived, admits them into a fixed set of device slots sized by the
+ * memory budget (a request waits while no slot is free), and runs each
+ * batch on its own stream, so batches that arrive while others are on the
+ * GPU overlap on the device.
+ *
+ * VX_SERVE_RESIDENT: one persistent launch stays on the device and takes
+ * requests from a descriptor ring in page-locked host memory mapped into
+ * the device's address space; its warps split requests into 32-ray units
+ * as they arrive, read the rays and write the records straight from and to
+ * host memory (the caller's buffers when they are page-locked, else
+ * page-locked staging), and mark each request done in host memory.  The
+ * budget bounds the rays in flight (56 B per ray: ray plus record).  The
+ * launch ends after idle_us without a request, at an edit (which runs on
+ * the same stream after it), or after a fraction of a second (the server
+ * starts the next); every wait in it is bounded and a wait that runs out
+ * is reported (VX_ERR_DEVICE) instead of hanging. */
+#define VX_SERVE_SLOTS 0
+#define VX_SERVE_RESIDENT 1
 typedef struct {
-    uint64_t mem_budget_bytes;  /* device bytes for all slots (56 B per ray) */
-    int32_t slots;              /* batches in flight at once, 1..16         */
-    int32_t max_batch_rays;     /* rays per batch; 0 = budget / slots / 56  */
-    int32_t max_batch_requests; /* requests per batch; 0 = as many as fit   */
-    int32_t reserved[3];
+    uint64_t mem_budget_bytes;  /* bytes for all requests in flight (56 B per ray) */
+    int32_t slots;              /* SLOTS: batches in flight at once, 1..16     */
+    int32_t max_batch_rays;     /* rays per batch (per request when RESIDENT);
+                                   0 = budget / slots / 56 (budget / 56)       */
+    int32_t max_batch_requests; /* SLOTS: requests per batch; 0 = as many as fit */
+    int32_t mode;               /* VX_SERVE_SLOTS or VX_SERVE_RESIDENT         */
+    int32_t idle_us;            /* RESIDENT: idle time before the launch ends;
+                                   0 = 2000                                     */
+    int32_t reserved[1];
 } VxServeConfig;
 
+/* batches: SLOTS batches launched, or RESIDENT launches of the loop. */
 typedef struct {
     uint64_t requests, rays, batches, rejected, edits, edited_bricks;
     double p50_ms, p99_ms, mean_ms, max_ms; /* submit -> results in the caller's buffer */

@@ -161,3 +161,20 @@ def test_noalloc_refuses_misaligned_arrays_without_gpu():
         rc = lib.vx_render_primary_noalloc(C.byref(view), C.byref(cam), C.byref(p),
                                            C.c_void_p(rec), C.c_void_p(sh), None)
         assert rc == L.VX_ERR_INVALID and b"8-byte aligned" in lib.vx_last_error()
+
+
+def test_serve_config_layout_and_mode_check_without_gpu():
+    """VxServeConfig keeps its 32-byte layout with the mode fields; an unknown
+    mode is refused before the world handle is touched."""
+    from voxelg_b200 import _lib as L
+    assert C.sizeof(L.VxServeConfig) == 32
+    assert L.VxServeConfig.mode.offset == 20 and L.VxServeConfig.idle_us.offset == 24
+    lib = L.load()
+    p = L.VxTraceParams()
+    h = C.c_void_p()
+    for mode, idle in ((2, 0), (-1, 0), (L.VX_SERVE_RESIDENT, -5)):
+        cfg = L.VxServeConfig(64 << 20, 1, 0, 0, mode, idle)
+        # a non-null handle that must not be dereferenced: the check comes first
+        assert lib.vx_server_create(C.c_void_p(16), L.i3((0, 0, 0)), C.byref(p), C.byref(cfg),
+                                    C.byref(h)) == L.VX_ERR_INVALID
+        assert b"mode" in lib.vx_last_error()

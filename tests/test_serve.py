@@ -1,5 +1,7 @@
-"""The ray-query serving loop: continuous batching over device slots, edits
-ordered in the request stream, and the open-loop load generator."""
+"""The ray-query serving loop, in both modes (continuous batching over
+device slots; the device-resident request loop): results equal vx_trace
+alone and the oracle, edits ordered in the request stream, the resident
+loop's idle exit and restart, and the open-loop load generator."""
 import numpy as np
 import pytest
 
@@ -32,15 +34,19 @@ def query_rays(rng, n, vox=(512, 256, 512)):
     return r
 
 
-@pytest.mark.parametrize("slots,budget", [(4, 64 << 20), (1, 8 << 20), (8, 4 << 20)])
-def test_batched_results_equal_alone(env, slots, budget, c1_oracle_world):
+@pytest.mark.parametrize("resident,slots,budget", [
+    (False, 4, 64 << 20), (False, 1, 8 << 20), (False, 8, 4 << 20),
+    # the resident loop: ample budget, and one the 120 requests overrun (the
+    # staging ring wraps and admission waits for completions)
+    (True, 1, 64 << 20), (True, 1, 2 << 20)])
+def test_batched_results_equal_alone(env, resident, slots, budget, c1_oracle_world):
     """Each request's records in the mix equal the same rays traced alone
     (vx_trace) and the oracle."""
     import voxelg_b200.serve as sv
     vg, dw = env
     p = vg.default_params(vg._lib.VX_F_L4 | vg._lib.VX_F_LUT | vg._lib.VX_F_LOD)
-    srv = sv.Server(dw, p, mem_budget_bytes=budget, slots=slots)
-    rng = np.random.default_rng(slots)
+    srv = sv.Server(dw, p, mem_budget_bytes=budget, slots=slots, resident=resident)
+    rng = np.random.default_rng(slots + 10 * resident + budget % 7)
     cap = min(20000, budget // slots // 56)
     reqs = [query_rays(rng, int(n)) for n in
             np.minimum(np.exp(rng.uniform(0, np.log(cap), 120)).astype(int) + 1, cap)]
@@ -48,7 +54,11 @@ def test_batched_results_equal_alone(env, slots, budget, c1_oracle_world):
     outs = [srv.wait(t) for t in tickets]
     st = srv.stats()
     assert st["requests"] == len(reqs) and st["rays"] == sum(len(r) for r in reqs)
+    # slots: batches launched; resident: launches of the loop
     assert st["batches"] < len(reqs) or slots == 1, "requests were never batched together"
+    if resident:
+        assert 1 <= st["batches"] < len(reqs)
+        assert st["peak_inflight_rays"] <= budget // 56
     for r, o in zip(reqs, outs):
         alone = vg.records(vg.trace(dw, r, p))
         assert np.array_equal(o.view(np.uint8), alone.view(np.uint8))
@@ -58,7 +68,8 @@ def test_batched_results_equal_alone(env, slots, budget, c1_oracle_world):
     srv.close()
 
 
-def test_edits_are_ordered_between_requests(env):
+@pytest.mark.parametrize("resident", [False, True])
+def test_edits_are_ordered_between_requests(env, resident):
     """A request submitted before an edit sees the old world, one submitted
     after it the new world, while both are in the same stream of work."""
     import voxelg_b200.serve as sv
@@ -67,7 +78,7 @@ def test_edits_are_ordered_between_requests(env):
     # a private world so the module world stays untouched
     w2 = vg.DeviceWorld(128, 64, 128)
     w2.upload(dw.download())
-    srv = sv.Server(w2, p, slots=2)
+    srv = sv.Server(w2, p, slots=2, resident=resident)
     n = 4096
     rays = np.zeros(n, po.RAY)
     rays["org"] = np.array([256.0, 250.0, 256.0], np.float32)
@@ -95,22 +106,83 @@ def test_edits_are_ordered_between_requests(env):
     w2.close()
 
 
-def test_rejects_request_larger_than_slot(env):
+@pytest.mark.parametrize("resident", [False, True])
+def test_rejects_request_larger_than_slot(env, resident):
     import voxelg_b200.serve as sv
     vg, dw = env
-    srv = sv.Server(dw, vg.default_params(), mem_budget_bytes=56 * 1000, slots=1)
+    srv = sv.Server(dw, vg.default_params(), mem_budget_bytes=56 * 1000, slots=1,
+                    resident=resident)
     with pytest.raises(vg._lib.VxError) as e:
         srv.submit(query_rays(np.random.default_rng(0), 1001))
     assert e.value.code == vg._lib.VX_ERR_BUSY
+    # a request that fits still runs
+    r = query_rays(np.random.default_rng(1), 1000)
+    o = srv.wait(srv.submit(r))
+    assert np.array_equal(o.view(np.uint8), vg.records(vg.trace(dw, r, vg.default_params())).view(np.uint8))
     srv.close()
 
 
-def test_load_generator_short_run(env):
+def pinned(n, dtype):
+    """A numpy array of n elements in page-locked host memory."""
+    import torch
+    buf = torch.empty(n * dtype.itemsize, dtype=torch.uint8, pin_memory=True)
+    return buf, buf.numpy().view(dtype)
+
+
+def test_resident_reads_and_writes_page_locked_buffers_in_place(env, c1_oracle_world):
+    """Page-locked request buffers are read and written by the loop itself
+    (no staging): records equal vx_trace alone and the oracle."""
+    import voxelg_b200.serve as sv
+    vg, dw = env
+    p = vg.default_params(vg._lib.VX_F_L4 | vg._lib.VX_F_LUT | vg._lib.VX_F_LOD)
+    srv = sv.Server(dw, p, mem_budget_bytes=32 << 20, resident=True)
+    rng = np.random.default_rng(5)
+    keep, live = [], []
+    for n in (1, 31, 32, 33, 4096, 20000):
+        hold_r, rays = pinned(n, vg._lib.RAY_DTYPE)
+        rays[:] = query_rays(rng, n).view(vg._lib.RAY_DTYPE)
+        hold_o, out = pinned(n, vg._lib.RECORD_DTYPE)
+        out.view(np.uint8)[:] = 0xAB
+        keep += [hold_r, hold_o]
+        live.append((rays, out, srv.submit(rays, out)))
+    for rays, out, t in live:
+        got = srv.wait(t)
+        assert got is out
+        alone = vg.records(vg.trace(dw, rays, p))
+        assert np.array_equal(out.view(np.uint8), alone.view(np.uint8))
+    rays, out, _ = live[3]
+    want = po.trace_batch(c1_oracle_world, np.asarray(rays).view(po.RAY), p)[0]
+    assert np.array_equal(out.view(np.uint8), want.view(np.uint8))
+    srv.close()
+
+
+def test_resident_loop_ends_when_idle_and_restarts(env):
+    """The loop's idle wait runs out (idle_us = 100): the launch ends, and the
+    next request starts another one; results are unaffected."""
+    import time
+    import voxelg_b200.serve as sv
+    vg, dw = env
+    p = vg.default_params()
+    srv = sv.Server(dw, p, mem_budget_bytes=16 << 20, resident=True, idle_us=100)
+    rng = np.random.default_rng(9)
+    for k in range(4):
+        r = query_rays(rng, 500 + k)
+        o = srv.wait(srv.submit(r))
+        assert np.array_equal(o.view(np.uint8), vg.records(vg.trace(dw, r, p)).view(np.uint8))
+        time.sleep(0.02)  # 200x the idle time
+    st = srv.stats()
+    assert st["requests"] == 4 and st["batches"] == 4, st
+    srv.close()
+
+
+@pytest.mark.parametrize("resident", [False, True])
+def test_load_generator_short_run(env, resident):
     import voxelg_b200.serve as sv
     vg, dw = env
     w2 = vg.DeviceWorld(128, 64, 128)
     w2.upload(dw.download())
-    srv = sv.Server(w2, vg.default_params(), mem_budget_bytes=256 << 20, slots=4)
+    srv = sv.Server(w2, vg.default_params(), mem_budget_bytes=256 << 20, slots=4,
+                    resident=resident)
     st = srv.bench(clients=16, rate_per_client=100.0, seconds=1.0, max_rays=20000,
                    edit_fraction_per_s=0.01)
     assert st["requests"] > 500 and st["rays"] > 0 and st["edits"] > 10

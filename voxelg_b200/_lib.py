@@ -32,6 +32,8 @@ VX_F_BEAM = 1 << 3
 VX_F_SHADOW = 1 << 4
 VX_F_METHOD = VX_F_L4 | VX_F_LUT | VX_F_LOD | VX_F_BEAM
 VX_RAY_SPAWN_SHADOW = 1 << 8
+VX_SERVE_SLOTS = 0
+VX_SERVE_RESIDENT = 1
 
 
 class VxError(RuntimeError):
@@ -83,7 +85,7 @@ class VxQueueTuning(C.Structure):
 class VxServeConfig(C.Structure):
     _fields_ = [("mem_budget_bytes", C.c_uint64), ("slots", C.c_int32),
                 ("max_batch_rays", C.c_int32), ("max_batch_requests", C.c_int32),
-                ("reserved", C.c_int32 * 3)]
+                ("mode", C.c_int32), ("idle_us", C.c_int32), ("reserved", C.c_int32 * 1)]
 
 
 class VxServeStats(C.Structure):

@@ -44,6 +44,7 @@ SOURCES = [
     ("vx_slotgen.cu", EXACT),
     ("vx_noalloc.cu", EXACT),
     ("vx_queue.cu", EXACT),
+    ("vx_resident.cu", EXACT),
     ("vx_learned.cu", EXACT),
     ("vx_distfield.cu", []),
     ("vx_pack.cu", []),

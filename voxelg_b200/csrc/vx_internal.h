@@ -262,6 +262,83 @@ cudaError_t launch_learned(const TraceArgs &ta, const VxCamera &cam, const float
                            const float *proposal, float scale, VxHitRecord *rec,
                            unsigned long long *stats, cudaStream_t s);
 
+// ---- device-resident request loop (vx_resident.cu, driven by vx_serve.cpp) ----
+// The host publishes request descriptors into a ring in page-locked host
+// memory mapped into the device's address space; one persistent launch (an
+// "instance") takes them in order, splits each into 32-ray units and traces
+// the units on every warp it holds, writes the records straight into host
+// memory and, for each finished request, a completion word the host polls.
+// Every wait in the loop is bounded.
+constexpr uint32_t kResRing = 1024;  // descriptor and completion slots
+enum : uint32_t { RES_REQ = 0, RES_FENCE = 1 };
+// how an instance ended (ResReplyBox::status)
+enum : uint32_t {
+    RES_RUNNING = 0, RES_IDLE = 1, RES_ROTATE = 2, RES_FENCED = 3, RES_STOPPED = 4
+};
+// ResReplyBox::error: a wait of the loop ran out (the loop then ends)
+enum : uint32_t { RES_ERR_NONE = 0, RES_ERR_UNIT_WAIT = 1, RES_ERR_RING_WAIT = 2 };
+struct ResDesc {    // 32 bytes, written by the host
+    uint64_t rays;  // device address of the request's VxRay array (mapped host memory, < 2^48)
+    uint64_t out;   // device address of its VxHitRecord array (< 2^48)
+    uint32_t n;     // rays, >= 1
+    uint32_t kind;  // RES_REQ, or RES_FENCE: an edit follows, the instance ends here
+    uint64_t seq;   // RES_FENCE: the edit's number (from 1)
+};
+struct ResHostBox {  // mapped host memory, written by the host
+    uint64_t head;   // descriptors published (release order after the descriptor)
+    uint32_t stop;   // 1: the instance ends at its next poll
+    uint32_t pad[13];
+    ResDesc desc[kResRing];  // position p in desc[p % kResRing]
+};
+// completion word of the request at position p: res_done_word(p), in slot p % kResRing
+__host__ __device__ inline uint64_t res_done_word(uint64_t pos) {
+    return ((pos & 0xFFFFFFFFull) << 1) | 1ull;
+}
+struct ResReplyBox {              // mapped host memory, written by the device
+    uint64_t done[kResRing];      // res_done_word of the request finished in that slot
+    uint64_t consumed;            // descriptors taken by the loop
+    uint32_t unit_end;            // global unit number after the last one published
+    uint32_t status;              // how the last instance ended (RES_IDLE ...)
+    uint32_t error;               // RES_ERR_*, sticky
+    uint32_t pad;
+};
+// Device memory.  Workers read what the leader publishes with plain
+// device-coherent (relaxed) loads, never acquire loads (an acquire would
+// discard the SM's L1, which the tracing warps beside them live on): every
+// word carries a tag of the publication it belongs to, and a reader waits
+// until the tag matches.
+//   unit word  (global unit g) << 32 | (position p, low 32 bits)
+//   request    slot p % kResRing, four words:
+//                rays | (p & 0xFFFF) << 48,  out | (p & 0xFFFF) << 48,
+//                (p32) << 32 | n,           (p32) << 32 | first global unit
+struct ResCounters {              // zeroed before every instance
+    uint32_t pubw;                // bit 31: closing; bits 0-30: units published
+    uint32_t pad0[31];
+    uint32_t claim;               // next unit ticket (relative to the instance)
+    uint32_t pad1[31];
+    uint32_t done_units;          // units finished
+    uint32_t pad2[31];
+};
+struct ResArgs {
+    TraceArgs ta;
+    ResHostBox *host;             // device addresses of the two mailboxes
+    ResReplyBox *reply;
+    ResCounters *ctr;
+    unsigned long long *req;      // [kResRing][4] tagged request words
+    unsigned long long *unit;     // [unit_ring] tagged unit words
+    uint32_t *cnt;                // [kResRing] units finished of the slot's request (reset to 0 at its end)
+    uint32_t unit_ring;
+    uint32_t unit_base;           // global number of this instance's first unit
+    uint64_t consumed;            // descriptors taken before this instance
+    uint64_t edits_before;        // edits ordered before this instance (fences up to it are past)
+    uint64_t idle_ns;             // the instance ends after this long without a descriptor
+    uint64_t life_ns;             // ... and takes no descriptor after this long in all
+    uint64_t wait_ns;             // bound on every other wait of the loop
+};
+// CTAs of one instance for the method flags of ta (SMs x resident CTAs, at most 4 per SM)
+cudaError_t serve_loop_grid(const TraceArgs &ta, unsigned *grid);
+cudaError_t launch_serve_loop(const ResArgs &a, unsigned grid, cudaStream_t s);
+
 // accessors for library parts outside vx_api.cpp
 DevWorld world_dev(const VxWorld *w);
 int world_device(const VxWorld *w);

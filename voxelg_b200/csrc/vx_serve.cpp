@@ -1,7 +1,10 @@
 // vx_serve.cpp -- device-resident ray-query serving loop with continuous
 // batching (vx_server_* / vx_serve_bench in include/voxrt.h).
 //
-// Threads: callers submit requests into a FIFO; one worker thread
+// Threads: callers submit requests into a FIFO; one worker thread drives
+// the device in one of two modes.
+//
+// VX_SERVE_SLOTS, each round:
 //   1. retires finished slots (event query), scatters each request's records
 //      into its caller buffer and marks it done;
 //   2. at the FIFO head: an edit is launched on the edit stream after every
@@ -12,6 +15,17 @@
 // Several slots are in flight at once, so a batch formed while others run
 // overlaps them on the device.  The slots' device buffers are the admission
 // budget: a request that does not fit in the free slot waits for the next.
+//
+// VX_SERVE_RESIDENT (the loop itself is vx_resident.cu), each round:
+//   1. retires requests whose completion word the loop has written (copying
+//      staged records to the caller) and notes an instance that has ended;
+//   2. at the FIFO head: a request is admitted while the rays in flight fit
+//      the budget and its descriptor slot is free, staged if the caller's
+//      buffers are not page-locked, and published (descriptor, then head);
+//      an edit publishes a fence, waits until an instance has taken it and
+//      ended, then runs on the loop's stream, so it lands after every
+//      request before it and before every request after it;
+//   3. starts an instance when none runs and published descriptors wait.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -45,6 +59,10 @@ struct Request {
     bool external = false;  // registered for vx_server_poll / vx_server_wait
     bool pinned_in = false;  // caller buffers in page-locked memory: copied
     bool pinned_out = false; // straight to / from the slot's device buffers
+    // device addresses of the caller's buffers when page-locked, mapped and
+    // 16-byte aligned: the resident loop reads and writes them in place;
+    // 0 = staged
+    uint64_t rays_dev = 0, out_dev = 0;
 };
 
 struct Edit {
@@ -79,6 +97,87 @@ bool is_pinned(const void *p) {
     return a.type == cudaMemoryTypeHost;
 }
 
+// the device address of page-locked host memory p, if mapped and aligned
+uint64_t mapped_address(const void *p, uintptr_t align) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    if (a.type != cudaMemoryTypeHost || a.devicePointer == nullptr) return 0;
+    const uintptr_t d = reinterpret_cast<uintptr_t>(a.devicePointer);
+    // the loop packs addresses into 48 bits beside a tag
+    return d % align == 0 && ((uint64_t)d >> 48) == 0 ? (uint64_t)d : 0;
+}
+
+// A published request of the resident loop (position order).
+struct ResFlight {
+    Request *r = nullptr;
+    uint64_t pos = 0;
+    size_t n = 0;
+    size_t off = SIZE_MAX;   // staging range [off, off + n), SIZE_MAX = none
+    bool stage_out = false;  // records land in staging and are copied out
+    bool done = false;
+};
+
+// Page-locked staging for callers whose buffers are not page-locked (or not
+// 16-byte aligned): one ring of rays and one of records, ranges taken in
+// position order and given back in position order.
+struct StageRing {
+    size_t cap = 0, head = 0;
+    std::deque<std::pair<size_t, size_t>> live;  // (offset, length), oldest first
+    size_t take(size_t n) {
+        if (n > cap) return SIZE_MAX;
+        if (live.empty()) {
+            head = n;
+            live.emplace_back(0, n);
+            return 0;
+        }
+        const size_t tail = live.front().first;
+        size_t off = SIZE_MAX;
+        if (head > tail) {
+            if (head + n <= cap) off = head;
+            else if (n <= tail) off = 0;
+        } else if (head < tail && head + n <= tail) {
+            off = head;
+        }
+        if (off != SIZE_MAX) {
+            head = off + n;
+            live.emplace_back(off, n);
+        }
+        return off;
+    }
+    void give_back() {
+        live.pop_front();
+        if (live.empty()) head = 0;
+    }
+};
+
+struct ResState {
+    vx::ResHostBox *hbox = nullptr, *hbox_d = nullptr;    // host / device addresses
+    vx::ResReplyBox *rbox = nullptr, *rbox_d = nullptr;
+    vx::ResCounters *ctr = nullptr;
+    unsigned long long *req = nullptr, *unit = nullptr;  // tagged words (vx_internal.h)
+    uint32_t *cnt = nullptr;
+    uint32_t unit_ring = 0;
+    VxRay *st_rays = nullptr;
+    VxHitRecord *st_out = nullptr;
+    uint64_t st_rays_d = 0, st_out_d = 0;
+    StageRing stage;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t inst_done = nullptr;
+    unsigned grid = 0;
+    bool live = false;              // an instance may still run
+    uint64_t published = 0;         // descriptors written (requests and fences)
+    uint64_t edits_enqueued = 0;    // edits on the stream so far
+    bool fence_pending = false;
+    uint64_t fence_pos = 0;
+    std::deque<ResFlight> flight;
+    size_t flight_rays = 0;
+    std::deque<Cmd> local;          // commands taken from the FIFO, in order
+    uint64_t idle_ns = 0, life_ns = 0, wait_ns = 0;
+};
+
 double ms_since(Clock::time_point t) {
     return std::chrono::duration<double, std::milli>(Clock::now() - t).count();
 }
@@ -89,12 +188,18 @@ struct VxServer {
     VxWorld *world = nullptr;
     int device = 0;
     vx::TraceArgs ta{};
-    size_t cap = 0;
+    size_t cap = 0;                    // rays of one request at most
     size_t max_reqs = 0;               // requests per batch, 0 = no limit
     std::vector<Slot> slots;
+    bool resident = false;             // VX_SERVE_RESIDENT
+    size_t budget_rays = 0;            // RESIDENT: rays in flight at most
+    ResState res;
 
     std::mutex mu;  // fifo + tickets
     std::deque<Cmd> fifo;
+    // commands in fifo: the worker takes the lock only when there are some,
+    // so that a spinning worker does not keep submitting clients off it
+    std::atomic<size_t> queued{0};
     std::unordered_map<uint64_t, Request *> tickets;
     std::atomic<uint64_t> next_ticket{1};
 
@@ -171,8 +276,12 @@ bool retire(VxServer *s, bool *progress) {
     return true;
 }
 
+// Enqueues the edit's copies and brick update on the edit stream (SLOTS:
+// after every batch on the device) or on the loop's stream (RESIDENT: after
+// the instance that took the edit's fence).
 bool run_edit(VxServer *s, Edit *e) {
     const size_t n = e->idx.size();
+    cudaStream_t es = s->resident ? s->res.stream : s->edit_stream;
     VxServer::EditBuf &b = s->ebuf[s->ecur];
     s->ecur ^= 1;
     cudaError_t err = cudaSuccess;
@@ -197,19 +306,19 @@ bool run_edit(VxServer *s, Edit *e) {
         std::memcpy(b.h_bricks, e->bricks.data(), n * sizeof(VxBrick));
         // after every batch already on the device
         for (Slot &sl : s->slots)
-            if (sl.busy && err == cudaSuccess) err = cudaStreamWaitEvent(s->edit_stream, sl.done, 0);
+            if (sl.busy && err == cudaSuccess) err = cudaStreamWaitEvent(es, sl.done, 0);
         if (err == cudaSuccess)
             err = cudaMemcpyAsync(b.d_idx, b.h_idx, n * sizeof(uint32_t), cudaMemcpyHostToDevice,
-                                  s->edit_stream);
+                                  es);
         if (err == cudaSuccess)
             err = cudaMemcpyAsync(b.d_bricks, b.h_bricks, n * sizeof(VxBrick),
-                                  cudaMemcpyHostToDevice, s->edit_stream);
+                                  cudaMemcpyHostToDevice, es);
         if (err == cudaSuccess) {
             vx::world_masks_changed(s->world);
-            err = vx::launch_apply_dirty(s->ta.w, b.d_idx, b.d_bricks, n, s->edit_stream);
+            err = vx::launch_apply_dirty(s->ta.w, b.d_idx, b.d_bricks, n, es);
         }
-        if (err == cudaSuccess) err = cudaEventRecord(b.used, s->edit_stream);
-        if (err == cudaSuccess) err = cudaEventRecord(s->edit_done, s->edit_stream);
+        if (err == cudaSuccess) err = cudaEventRecord(b.used, es);
+        if (err == cudaSuccess) err = cudaEventRecord(s->edit_done, es);
         if (err == cudaSuccess) {
             s->edited = true;
             b.pending = true;
@@ -266,8 +375,215 @@ bool launch_batch(VxServer *s, Slot &sl) {
     return true;
 }
 
+// ---------------------------------------------------------------- RESIDENT
+uint64_t res_consumed(const ResState &R) {
+    return __atomic_load_n(&R.rbox->consumed, __ATOMIC_ACQUIRE);
+}
+
+// a descriptor may go to position pos: its slot was taken by the loop and the
+// request that last used the slot is done
+bool res_slot_free(const ResState &R, uint64_t pos) {
+    if (pos - res_consumed(R) >= vx::kResRing) return false;
+    return R.flight.empty() || pos - R.flight.front().pos < vx::kResRing;
+}
+
+void res_write(ResState &R, const vx::ResDesc &d) {
+    R.hbox->desc[R.published % vx::kResRing] = d;
+    __atomic_store_n(&R.hbox->head, R.published + 1, __ATOMIC_RELEASE);
+    R.published += 1;
+}
+
+// completion words -> caller buffers; returns false on a loop error
+bool res_retire(VxServer *s, bool *progress) {
+    ResState &R = s->res;
+    for (ResFlight &f : R.flight) {
+        if (f.done) continue;
+        const uint64_t w = __atomic_load_n(&R.rbox->done[f.pos % vx::kResRing], __ATOMIC_ACQUIRE);
+        if (w != vx::res_done_word(f.pos)) continue;
+        if (f.stage_out)
+            std::memcpy(f.r->out, R.st_out + f.off, f.n * sizeof(VxHitRecord));
+        f.done = true;
+        R.flight_rays -= f.n;
+        {
+            std::lock_guard<std::mutex> lk(s->stat_mu);
+            s->inflight -= f.n;
+        }
+        complete(s, f.r);  // the caller may free f.r from here on
+        f.r = nullptr;
+        *progress = true;
+    }
+    while (!R.flight.empty() && R.flight.front().done) {
+        if (R.flight.front().off != SIZE_MAX) R.stage.give_back();
+        R.flight.pop_front();
+    }
+    if (R.live) {
+        const cudaError_t q = cudaEventQuery(R.inst_done);
+        if (q == cudaErrorNotReady) return true;
+        if (q != cudaSuccess) {
+            s->worker_error = cudaGetErrorString(q);
+            return false;
+        }
+        R.live = false;
+        *progress = true;
+    }
+    const uint32_t err = __atomic_load_n(&R.rbox->error, __ATOMIC_ACQUIRE);
+    if (err != vx::RES_ERR_NONE) {
+        s->worker_error = err == vx::RES_ERR_UNIT_WAIT
+                              ? "resident loop: a worker's wait for its unit ran out"
+                              : "resident loop: the wait for room in the unit table ran out";
+        return false;
+    }
+    return true;
+}
+
+bool res_launch(VxServer *s) {
+    ResState &R = s->res;
+    vx::ResArgs a{};
+    a.ta = s->ta;
+    a.host = R.hbox_d;
+    a.reply = R.rbox_d;
+    a.ctr = R.ctr;
+    a.req = R.req;
+    a.unit = R.unit;
+    a.cnt = R.cnt;
+    a.unit_ring = R.unit_ring;
+    // the previous instance has ended: its last words are final
+    a.consumed = res_consumed(R);
+    a.unit_base = __atomic_load_n(&R.rbox->unit_end, __ATOMIC_ACQUIRE);
+    a.edits_before = R.edits_enqueued;
+    a.idle_ns = R.idle_ns;
+    a.life_ns = R.life_ns;
+    a.wait_ns = R.wait_ns;
+    cudaError_t err = cudaMemsetAsync(R.ctr, 0, sizeof(vx::ResCounters), R.stream);
+    if (err == cudaSuccess) err = vx::launch_serve_loop(a, R.grid, R.stream);
+    if (err == cudaSuccess) err = cudaEventRecord(R.inst_done, R.stream);
+    if (err != cudaSuccess) {
+        s->worker_error = cudaGetErrorString(err);
+        return false;
+    }
+    R.live = true;
+    std::lock_guard<std::mutex> lk(s->stat_mu);
+    s->batches += 1;
+    return true;
+}
+
+// publish one request; false when it must wait for admission
+bool res_publish(VxServer *s, Request *r) {
+    ResState &R = s->res;
+    if (R.flight_rays + r->n > s->budget_rays || !res_slot_free(R, R.published)) return false;
+    ResFlight f;
+    f.r = r;
+    f.pos = R.published;
+    f.n = r->n;
+    uint64_t rays = r->rays_dev, out = r->out_dev;
+    if (!rays || !out) {
+        // whole units, so that every unit's records start 16-byte aligned
+        f.off = R.stage.take((r->n + 31) / 32 * 32);
+        if (f.off == SIZE_MAX) return false;
+        if (!rays) {
+            std::memcpy(R.st_rays + f.off, r->rays, r->n * sizeof(VxRay));
+            rays = R.st_rays_d + f.off * sizeof(VxRay);
+        }
+        if (!out) {
+            out = R.st_out_d + f.off * sizeof(VxHitRecord);
+            f.stage_out = true;
+        }
+    }
+    vx::ResDesc d;
+    d.rays = rays;
+    d.out = out;
+    d.n = (uint32_t)r->n;
+    d.kind = vx::RES_REQ;
+    d.seq = R.published;
+    res_write(R, d);
+    R.flight.push_back(f);
+    R.flight_rays += r->n;
+    std::lock_guard<std::mutex> lk(s->stat_mu);
+    s->inflight += r->n;
+    s->peak_inflight = std::max(s->peak_inflight, s->inflight);
+    return true;
+}
+
+// the edit at the FIFO head; *taken once it is on the stream
+bool res_edit(VxServer *s, Edit *e, bool *taken) {
+    ResState &R = s->res;
+    if (!R.fence_pending) {
+        if (!R.live && res_consumed(R) == R.published) {
+            R.edits_enqueued += 1;
+            *taken = true;
+            return run_edit(s, e);
+        }
+        if (!res_slot_free(R, R.published)) return true;
+        vx::ResDesc d{};
+        d.kind = vx::RES_FENCE;
+        d.seq = R.edits_enqueued + 1;
+        R.fence_pos = R.published;
+        res_write(R, d);
+        R.fence_pending = true;
+        return true;
+    }
+    if (!R.live && res_consumed(R) > R.fence_pos) {
+        R.fence_pending = false;
+        R.edits_enqueued += 1;
+        *taken = true;
+        return run_edit(s, e);
+    }
+    return true;
+}
+
+void resident_loop(VxServer *s) {
+    ResState &R = s->res;
+    while (!s->stop.load(std::memory_order_acquire)) {
+        bool progress = false;
+        if (!res_retire(s, &progress)) break;
+        bool ok = true;
+        if (s->queued.load(std::memory_order_acquire) != 0) {
+            // everything queued, in order, under one hold of the lock
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->queued.fetch_sub(s->fifo.size(), std::memory_order_relaxed);
+            for (Cmd &c : s->fifo) R.local.push_back(c);
+            s->fifo.clear();
+        }
+        while (!R.local.empty()) {
+            const Cmd head = R.local.front();
+            if (head.edit) {
+                bool taken = false;
+                ok = res_edit(s, head.edit, &taken);
+                if (taken) {  // run_edit has consumed the Edit
+                    R.local.pop_front();
+                    progress = true;
+                }
+                if (!ok || !taken) break;
+                continue;
+            }
+            Request *r = head.req;
+            if (r->n == 0) {
+                R.local.pop_front();
+                complete(s, r);
+                progress = true;
+                continue;
+            }
+            if (!res_publish(s, r)) break;
+            R.local.pop_front();
+            progress = true;
+        }
+        if (!ok) break;
+        if (!R.live && res_consumed(R) < R.published) {
+            if (!res_launch(s)) break;
+            progress = true;
+        }
+        if (!progress) std::this_thread::yield();
+    }
+    // the instance ends at its next poll
+    __atomic_store_n(&R.hbox->stop, 1u, __ATOMIC_RELEASE);
+}
+
 void worker_loop(VxServer *s) {
     cudaSetDevice(s->device);
+    if (s->resident) {
+        resident_loop(s);
+        return;
+    }
     while (!s->stop.load(std::memory_order_acquire)) {
         bool progress = false;
         if (!retire(s, &progress)) break;
@@ -278,11 +594,12 @@ void worker_loop(VxServer *s) {
                 break;
             }
         Edit *edit = nullptr;
-        {
+        if (s->queued.load(std::memory_order_acquire) != 0) {
             std::lock_guard<std::mutex> lk(s->mu);
             if (!s->fifo.empty() && s->fifo.front().edit) {
                 edit = s->fifo.front().edit;
                 s->fifo.pop_front();
+                s->queued.fetch_sub(1, std::memory_order_relaxed);
             } else if (free_slot) {
                 size_t n = 0;
                 while (!s->fifo.empty() && s->fifo.front().req &&
@@ -290,6 +607,7 @@ void worker_loop(VxServer *s) {
                        (s->max_reqs == 0 || free_slot->reqs.size() < s->max_reqs)) {
                     Request *r = s->fifo.front().req;
                     s->fifo.pop_front();
+                    s->queued.fetch_sub(1, std::memory_order_relaxed);
                     free_slot->reqs.push_back(r);
                     n += r->n;
                 }
@@ -306,7 +624,81 @@ void worker_loop(VxServer *s) {
     }
 }
 
+void free_resident(ResState &R) {
+    if (R.hbox) __atomic_store_n(&R.hbox->stop, 1u, __ATOMIC_RELEASE);
+    if (R.stream) cudaStreamSynchronize(R.stream);
+    cudaFreeHost(R.hbox);
+    cudaFreeHost(R.rbox);
+    cudaFreeHost(R.st_rays);
+    cudaFreeHost(R.st_out);
+    cudaFree(R.ctr);
+    cudaFree(R.req);
+    cudaFree(R.unit);
+    cudaFree(R.cnt);
+    if (R.inst_done) cudaEventDestroy(R.inst_done);
+    if (R.stream) cudaStreamDestroy(R.stream);
+}
+
+cudaError_t host_mapped(size_t bytes, void **host, uint64_t *dev) {
+    cudaError_t e = cudaHostAlloc(host, bytes, cudaHostAllocMapped | cudaHostAllocPortable);
+    if (e != cudaSuccess) {
+        *host = nullptr;
+        return e;
+    }
+    std::memset(*host, 0, bytes);
+    void *d = nullptr;
+    e = cudaHostGetDevicePointer(&d, *host, 0);
+    *dev = reinterpret_cast<uint64_t>(d);
+    return e;
+}
+
+cudaError_t create_resident(VxServer *s, int32_t idle_us) {
+    ResState &R = s->res;
+    R.idle_ns = (uint64_t)(idle_us > 0 ? idle_us : 2000) * 1000ull;
+    R.life_ns = 250ull * 1000 * 1000;                  // a quarter second per instance
+    R.wait_ns = R.life_ns + R.idle_ns + 1000000000ull;  // every other wait
+    R.unit_ring = (uint32_t)(s->budget_rays / 32 + vx::kResRing + 64);
+    void *h = nullptr;
+    uint64_t d = 0;
+    cudaError_t e = host_mapped(sizeof(vx::ResHostBox), &h, &d);
+    R.hbox = static_cast<vx::ResHostBox *>(h);
+    R.hbox_d = reinterpret_cast<vx::ResHostBox *>(d);
+    if (e == cudaSuccess) {
+        e = host_mapped(sizeof(vx::ResReplyBox), &h, &d);
+        R.rbox = static_cast<vx::ResReplyBox *>(h);
+        R.rbox_d = reinterpret_cast<vx::ResReplyBox *>(d);
+    }
+    // staging in whole units: room for any admissible request, rounded up
+    const size_t stage_rays = (s->budget_rays + 31) / 32 * 32;
+    if (e == cudaSuccess) {
+        e = host_mapped(stage_rays * sizeof(VxRay), &h, &R.st_rays_d);
+        R.st_rays = static_cast<VxRay *>(h);
+    }
+    if (e == cudaSuccess) {
+        e = host_mapped(stage_rays * sizeof(VxHitRecord), &h, &R.st_out_d);
+        R.st_out = static_cast<VxHitRecord *>(h);
+    }
+    R.stage.cap = stage_rays;
+    // the loop packs addresses into 48 bits beside a tag
+    if (e == cudaSuccess && ((uint64_t)(R.st_rays_d | R.st_out_d) >> 48) != 0)
+        e = cudaErrorInvalidValue;
+    if (e == cudaSuccess) e = cudaMalloc(&R.ctr, sizeof(vx::ResCounters));
+    // the tagged words start all ones: a tag that no position or unit of the
+    // rings' first turn carries
+    if (e == cudaSuccess) e = cudaMalloc(&R.req, vx::kResRing * 4 * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemset(R.req, 0xFF, vx::kResRing * 4 * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMalloc(&R.unit, (size_t)R.unit_ring * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMemset(R.unit, 0xFF, (size_t)R.unit_ring * sizeof(unsigned long long));
+    if (e == cudaSuccess) e = cudaMalloc(&R.cnt, vx::kResRing * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMemset(R.cnt, 0, vx::kResRing * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&R.stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&R.inst_done, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = vx::serve_loop_grid(s->ta, &R.grid);
+    return e;
+}
+
 void free_server(VxServer *s) {
+    if (s->resident) free_resident(s->res);
     for (Slot &sl : s->slots) {
         if (sl.stream) cudaStreamSynchronize(sl.stream);
         cudaFreeHost(sl.h_rays);
@@ -327,10 +719,11 @@ void free_server(VxServer *s) {
     if (s->edit_done) cudaEventDestroy(s->edit_done);
     if (s->edit_stream) cudaStreamDestroy(s->edit_stream);
     for (auto &kv : s->tickets) delete kv.second;
-    for (Cmd &c : s->fifo) {
-        delete c.edit;
-        if (c.req && !c.req->external) delete c.req;
-    }
+    for (std::deque<Cmd> *q : {&s->fifo, &s->res.local})
+        for (Cmd &c : *q) {
+            delete c.edit;
+            if (c.req && !c.req->external) delete c.req;
+        }
 }
 
 Request *submit_internal(VxServer *s, const VxRay *rays, size_t n, VxHitRecord *out,
@@ -341,12 +734,18 @@ Request *submit_internal(VxServer *s, const VxRay *rays, size_t n, VxHitRecord *
     r->out = out;
     r->ticket = s->next_ticket.fetch_add(1);
     r->external = external;
-    r->pinned_in = n > 0 && is_pinned(rays);
-    r->pinned_out = n > 0 && is_pinned(out);
+    if (s->resident) {
+        r->rays_dev = n > 0 ? mapped_address(rays, 16) : 0;
+        r->out_dev = n > 0 ? mapped_address(out, 16) : 0;
+    } else {
+        r->pinned_in = n > 0 && is_pinned(rays);
+        r->pinned_out = n > 0 && is_pinned(out);
+    }
     r->t_submit = Clock::now();
     std::lock_guard<std::mutex> lk(s->mu);
     if (external) s->tickets[r->ticket] = r;
     s->fifo.push_back(Cmd{r, nullptr});
+    s->queued.fetch_add(1, std::memory_order_release);
     return r;
 }
 
@@ -363,10 +762,21 @@ extern "C" {
 
 int vx_server_create(VxWorld *w, const int32_t origin[3], const VxTraceParams *p,
                      const VxServeConfig *cfg, VxServer **out) {
-    if (!w || !origin || !p || !cfg || !out || cfg->slots < 1 || cfg->slots > 16 ||
-        cfg->max_batch_rays < 0 || cfg->max_batch_requests < 0 ||
-        cfg->mem_budget_bytes < 56ull * (uint64_t)cfg->slots) {
+    if (!w || !origin || !p || !cfg || !out ||
+        (cfg->mode != VX_SERVE_SLOTS && cfg->mode != VX_SERVE_RESIDENT) || cfg->idle_us < 0) {
+        vx::set_error("vx_server_create: null argument, unknown mode or negative idle time");
+        return VX_ERR_INVALID;
+    }
+    const bool resident = cfg->mode == VX_SERVE_RESIDENT;
+    if (!resident && (cfg->slots < 1 || cfg->slots > 16 || cfg->max_batch_rays < 0 ||
+                      cfg->max_batch_requests < 0 ||
+                      cfg->mem_budget_bytes < 56ull * (uint64_t)cfg->slots)) {
         vx::set_error("vx_server_create: need 1..16 slots and a budget of at least 56 B per slot");
+        return VX_ERR_INVALID;
+    }
+    if (resident && (cfg->max_batch_rays < 0 || cfg->mem_budget_bytes < 56ull * 32 ||
+                     cfg->mem_budget_bytes / 56ull > (1ull << 31))) {
+        vx::set_error("vx_server_create: the resident loop needs a budget of 32 to 2^31 rays");
         return VX_ERR_INVALID;
     }
     if (p->max_iters < 0 || p->any_max_iters < 0 || p->max_iters > (1 << 20) ||
@@ -375,7 +785,7 @@ int vx_server_create(VxWorld *w, const int32_t origin[3], const VxTraceParams *p
         return VX_ERR_INVALID;
     }
     if (!vx::origin_ok(origin, "vx_server_create")) return VX_ERR_INVALID;
-    size_t cap = (size_t)(cfg->mem_budget_bytes / (uint64_t)cfg->slots / 56ull);
+    size_t cap = (size_t)(cfg->mem_budget_bytes / (uint64_t)(resident ? 1 : cfg->slots) / 56ull);
     if (cfg->max_batch_rays > 0) cap = std::min(cap, (size_t)cfg->max_batch_rays);
     if (cap < 1) {
         vx::set_error("vx_server_create: budget too small for one ray per slot");
@@ -393,7 +803,10 @@ int vx_server_create(VxWorld *w, const int32_t origin[3], const VxTraceParams *p
     s->cap = cap;
     s->max_reqs = (size_t)cfg->max_batch_requests;
     cudaError_t e = cudaSetDevice(s->device);
-    s->slots.resize((size_t)cfg->slots);
+    s->resident = resident;
+    s->budget_rays = (size_t)(cfg->mem_budget_bytes / 56ull);
+    if (resident && e == cudaSuccess) e = create_resident(s, cfg->idle_us);
+    s->slots.resize(resident ? 0 : (size_t)cfg->slots);
     for (Slot &sl : s->slots) {
         if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking);
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming);
@@ -503,6 +916,7 @@ int vx_server_edit(VxServer *s, const uint32_t *brick_idx, const VxBrick *bricks
         }
     std::lock_guard<std::mutex> lk(s->mu);
     s->fifo.push_back(Cmd{nullptr, e});
+    s->queued.fetch_add(1, std::memory_order_release);
     return VX_OK;
 }
 

@@ -1,5 +1,5 @@
-"""Device-resident ray-query serving loop with continuous batching
-(vx_server_* in include/voxrt.h)."""
+"""Ray-query serving loop with continuous batching over device slots, or as
+a device-resident request loop (vx_server_* in include/voxrt.h)."""
 from __future__ import annotations
 
 import ctypes as C
@@ -19,21 +19,30 @@ class Server:
 
     def __init__(self, world: DeviceWorld, params: L.VxTraceParams, origin=(0, 0, 0),
                  mem_budget_bytes: int = 256 << 20, slots: int = 4, max_batch_rays: int = 0,
-                 max_batch_requests: int = 0):
+                 max_batch_requests: int = 0, resident: bool = False, idle_us: int = 0):
+        """resident=True runs the device-resident request loop
+        (VX_SERVE_RESIDENT); slots and max_batch_requests then do not apply."""
         self._lib = L.load()
         self.world = world
-        cfg = L.VxServeConfig(mem_budget_bytes, slots, max_batch_rays, max_batch_requests)
+        mode = L.VX_SERVE_RESIDENT if resident else L.VX_SERVE_SLOTS
+        cfg = L.VxServeConfig(mem_budget_bytes, slots, max_batch_rays, max_batch_requests, mode,
+                              idle_us)
         h = C.c_void_p()
         L.check(self._lib.vx_server_create(world.handle, L.i3(origin), C.byref(params),
                                            C.byref(cfg), C.byref(h)))
         self.handle = h
         self._live = {}
 
-    def submit(self, rays: np.ndarray) -> int:
-        """Queue rays (RAY_DTYPE); returns a ticket.  The result array is
-        held by the server object until collected with wait()."""
+    def submit(self, rays: np.ndarray, out: np.ndarray | None = None) -> int:
+        """Queue rays (RAY_DTYPE); returns a ticket.  The result array (a new
+        one, or `out` of RECORD_DTYPE and len(rays)) is held by the server
+        object until collected with wait().  Arrays in page-locked memory
+        are read and written in place by the resident loop."""
         rays = np.ascontiguousarray(rays).view(L.RAY_DTYPE)
-        out = np.zeros(len(rays), L.RECORD_DTYPE)
+        if out is None:
+            out = np.zeros(len(rays), L.RECORD_DTYPE)
+        elif out.dtype != L.RECORD_DTYPE or len(out) != len(rays) or not out.flags.c_contiguous:
+            raise ValueError("out must be a contiguous RECORD_DTYPE array of len(rays)")
         t = C.c_uint64()
         L.check(self._lib.vx_server_submit(self.handle, C.c_void_p(L.ptr(rays)), len(rays),
                                            C.c_void_p(L.ptr(out)), C.byref(t)))
