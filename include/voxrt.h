@@ -469,7 +469,9 @@ typedef struct {
 typedef struct {
     uint64_t requests, rays, batches, rejected, edits, edited_bricks;
     double p50_ms, p99_ms, mean_ms, max_ms; /* submit -> results in the caller's buffer */
-    double seconds;                         /* wall time covered (bench) */
+    double seconds;                         /* wall time covered (bench: from the
+                                               first arrival to the last request
+                                               reaped by its client) */
     double mrays_per_s;
     uint64_t peak_inflight_rays;
 } VxServeStats;

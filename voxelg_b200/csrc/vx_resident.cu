@@ -297,7 +297,15 @@ __device__ void worker(const ResArgs &a, uint4 *stage) {
         const uint32_t first = (g - u0) * 32u;
         const uint32_t cnt = min(32u, n - first);
         const char *src = reinterpret_cast<const char *>(rays) + (size_t)first * sizeof(VxRay);
-        for (uint32_t j = lane; j < 2u * cnt; j += 32u) stage[j] = ld_fresh_u4(src + 16u * j);
+        {
+            // both reads in flight before either lands in the stage
+            const bool h0 = lane < 2u * cnt, h1 = lane + 32u < 2u * cnt;
+            uint4 c0 = make_uint4(0u, 0u, 0u, 0u), c1 = c0;
+            if (h0) c0 = ld_fresh_u4(src + 16u * lane);
+            if (h1) c1 = ld_fresh_u4(src + 16u * (lane + 32u));
+            if (h0) stage[lane] = c0;
+            if (h1) stage[lane + 32u] = c1;
+        }
         __syncwarp();
         Hit h;
         if (lane < cnt) {

@@ -1096,12 +1096,14 @@ int vx_serve_bench(VxServer *s, const VxServeLoad *L, VxServeStats *st) {
     std::vector<std::thread> clients;
     for (int i = 0; i < L->clients; ++i) clients.emplace_back(client, i);
     for (auto &t : clients) t.join();
+    // every client has reaped its last request: the load is served
+    const double seconds = std::chrono::duration<double>(Clock::now() - t_start).count();
     editing = false;
     editor.join();
     for (auto p : pin_rays) cudaFreeHost(p);
     for (auto p : pin_out) cudaFreeHost(p);
     const int rc = vx_server_stats(s, st, 0);
-    st->seconds = std::chrono::duration<double>(Clock::now() - t_start).count();
+    st->seconds = seconds;
     st->mrays_per_s = (double)st->rays / st->seconds / 1e6;
     if (failed) {
         vx::set_error("vx_serve_bench: server stopped: " + s->worker_error);
