@@ -462,7 +462,11 @@ typedef struct {
     int32_t mode;               /* VX_SERVE_SLOTS or VX_SERVE_RESIDENT         */
     int32_t idle_us;            /* RESIDENT: idle time before the launch ends;
                                    0 = 2000                                     */
-    int32_t reserved[1];
+    int32_t wait_us;            /* RESIDENT: bound on a warp's wait for its work;
+                                   0 = the launch's lifetime plus one second.  A
+                                   wait that runs out stops the server with
+                                   VX_ERR_DEVICE (a watchdog: a shorter bound
+                                   than idle_us ends idle launches that way)   */
 } VxServeConfig;
 
 /* batches: SLOTS batches launched, or RESIDENT launches of the loop. */

@@ -169,11 +169,13 @@ def test_serve_config_layout_and_mode_check_without_gpu():
     from voxelg_b200 import _lib as L
     assert C.sizeof(L.VxServeConfig) == 32
     assert L.VxServeConfig.mode.offset == 20 and L.VxServeConfig.idle_us.offset == 24
+    assert L.VxServeConfig.wait_us.offset == 28
     lib = L.load()
     p = L.VxTraceParams()
     h = C.c_void_p()
-    for mode, idle in ((2, 0), (-1, 0), (L.VX_SERVE_RESIDENT, -5)):
-        cfg = L.VxServeConfig(64 << 20, 1, 0, 0, mode, idle)
+    for mode, idle, wait in ((2, 0, 0), (-1, 0, 0), (L.VX_SERVE_RESIDENT, -5, 0),
+                             (L.VX_SERVE_RESIDENT, 0, -1)):
+        cfg = L.VxServeConfig(64 << 20, 1, 0, 0, mode, idle, wait)
         # a non-null handle that must not be dereferenced: the check comes first
         assert lib.vx_server_create(C.c_void_p(16), L.i3((0, 0, 0)), C.byref(p), C.byref(cfg),
                                     C.byref(h)) == L.VX_ERR_INVALID

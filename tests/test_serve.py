@@ -175,6 +175,32 @@ def test_resident_loop_ends_when_idle_and_restarts(env):
     srv.close()
 
 
+def test_resident_wait_limit_stops_the_server_and_leaves_the_device_usable(env):
+    """A warp's wait for work is bounded.  With wait_us (1 ms) far below
+    idle_us (200 ms), the idle workers' waits run out while the launch is
+    still up: each records the loop's error word and returns, the server
+    stops with VX_ERR_DEVICE, and the device keeps working."""
+    import time
+    import voxelg_b200.serve as sv
+    vg, dw = env
+    p = vg.default_params()
+    srv = sv.Server(dw, p, mem_budget_bytes=16 << 20, resident=True, idle_us=200000,
+                    wait_us=1000)
+    r = query_rays(np.random.default_rng(11), 64)
+    o = srv.wait(srv.submit(r))  # served well inside the limit
+    alone = vg.records(vg.trace(dw, r, p))
+    assert np.array_equal(o.view(np.uint8), alone.view(np.uint8))
+    time.sleep(0.1)
+    with pytest.raises(vg._lib.VxError) as e:
+        srv.submit(r)
+    assert e.value.code == vg._lib.VX_ERR_DEVICE
+    assert "wait" in str(e.value)
+    srv.close()
+    # the context is intact
+    again = vg.records(vg.trace(dw, r, p))
+    assert np.array_equal(again.view(np.uint8), alone.view(np.uint8))
+
+
 @pytest.mark.parametrize("resident", [False, True])
 def test_load_generator_short_run(env, resident):
     import voxelg_b200.serve as sv

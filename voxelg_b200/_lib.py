@@ -85,7 +85,7 @@ class VxQueueTuning(C.Structure):
 class VxServeConfig(C.Structure):
     _fields_ = [("mem_budget_bytes", C.c_uint64), ("slots", C.c_int32),
                 ("max_batch_rays", C.c_int32), ("max_batch_requests", C.c_int32),
-                ("mode", C.c_int32), ("idle_us", C.c_int32), ("reserved", C.c_int32 * 1)]
+                ("mode", C.c_int32), ("idle_us", C.c_int32), ("wait_us", C.c_int32)]
 
 
 class VxServeStats(C.Structure):

@@ -208,7 +208,11 @@ struct VxServer {
 
     std::thread worker;
     std::atomic<bool> stop{false};
+    // Written by the worker thread only, before it sets `failed` and stops;
+    // other threads read it only after seeing `failed`.
     std::string worker_error;
+    std::atomic<bool> failed{false};
+    bool device_error = false;  // worker_error came from a kernel's error word
 
     cudaStream_t edit_stream = nullptr;
     cudaEvent_t edit_done = nullptr;  // last edit: later batches wait on it
@@ -428,6 +432,7 @@ bool res_retire(VxServer *s, bool *progress) {
     }
     const uint32_t err = __atomic_load_n(&R.rbox->error, __ATOMIC_ACQUIRE);
     if (err != vx::RES_ERR_NONE) {
+        s->device_error = true;
         s->worker_error = err == vx::RES_ERR_UNIT_WAIT
                               ? "resident loop: a worker's wait for its unit ran out"
                               : "resident loop: the wait for room in the unit table ran out";
@@ -578,12 +583,20 @@ void resident_loop(VxServer *s) {
     __atomic_store_n(&R.hbox->stop, 1u, __ATOMIC_RELEASE);
 }
 
+void worker_loop_body(VxServer *s);
+
 void worker_loop(VxServer *s) {
     cudaSetDevice(s->device);
-    if (s->resident) {
+    if (s->resident)
         resident_loop(s);
-        return;
-    }
+    else
+        worker_loop_body(s);
+    // every path out of the loops other than stop has set worker_error
+    if (!s->worker_error.empty()) s->failed.store(true, std::memory_order_release);
+    s->done_cv.notify_all();
+}
+
+void worker_loop_body(VxServer *s) {
     while (!s->stop.load(std::memory_order_acquire)) {
         bool progress = false;
         if (!retire(s, &progress)) break;
@@ -652,11 +665,12 @@ cudaError_t host_mapped(size_t bytes, void **host, uint64_t *dev) {
     return e;
 }
 
-cudaError_t create_resident(VxServer *s, int32_t idle_us) {
+cudaError_t create_resident(VxServer *s, int32_t idle_us, int32_t wait_us) {
     ResState &R = s->res;
     R.idle_ns = (uint64_t)(idle_us > 0 ? idle_us : 2000) * 1000ull;
-    R.life_ns = 250ull * 1000 * 1000;                  // a quarter second per instance
-    R.wait_ns = R.life_ns + R.idle_ns + 1000000000ull;  // every other wait
+    R.life_ns = 250ull * 1000 * 1000;  // a quarter second per instance
+    // every other wait: by default longer than any instance lives
+    R.wait_ns = wait_us > 0 ? (uint64_t)wait_us * 1000ull : R.life_ns + R.idle_ns + 1000000000ull;
     R.unit_ring = (uint32_t)(s->budget_rays / 32 + vx::kResRing + 64);
     void *h = nullptr;
     uint64_t d = 0;
@@ -763,8 +777,9 @@ extern "C" {
 int vx_server_create(VxWorld *w, const int32_t origin[3], const VxTraceParams *p,
                      const VxServeConfig *cfg, VxServer **out) {
     if (!w || !origin || !p || !cfg || !out ||
-        (cfg->mode != VX_SERVE_SLOTS && cfg->mode != VX_SERVE_RESIDENT) || cfg->idle_us < 0) {
-        vx::set_error("vx_server_create: null argument, unknown mode or negative idle time");
+        (cfg->mode != VX_SERVE_SLOTS && cfg->mode != VX_SERVE_RESIDENT) || cfg->idle_us < 0 ||
+        cfg->wait_us < 0) {
+        vx::set_error("vx_server_create: null argument, unknown mode or negative idle / wait time");
         return VX_ERR_INVALID;
     }
     const bool resident = cfg->mode == VX_SERVE_RESIDENT;
@@ -805,7 +820,7 @@ int vx_server_create(VxWorld *w, const int32_t origin[3], const VxTraceParams *p
     cudaError_t e = cudaSetDevice(s->device);
     s->resident = resident;
     s->budget_rays = (size_t)(cfg->mem_budget_bytes / 56ull);
-    if (resident && e == cudaSuccess) e = create_resident(s, cfg->idle_us);
+    if (resident && e == cudaSuccess) e = create_resident(s, cfg->idle_us, cfg->wait_us);
     s->slots.resize(resident ? 0 : (size_t)cfg->slots);
     for (Slot &sl : s->slots) {
         if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&sl.stream, cudaStreamNonBlocking);
@@ -840,9 +855,9 @@ int vx_server_submit(VxServer *s, const VxRay *rays, size_t n, VxHitRecord *out,
         vx::set_error("vx_server_submit: request larger than a batch slot");
         return VX_ERR_BUSY;
     }
-    if (!s->worker_error.empty()) {
+    if (s->failed.load(std::memory_order_acquire)) {
         vx::set_error("vx_server_submit: server stopped: " + s->worker_error);
-        return VX_ERR_CUDA;
+        return s->device_error ? VX_ERR_DEVICE : VX_ERR_CUDA;
     }
     *ticket = submit_internal(s, rays, n, out, true)->ticket;
     return VX_OK;
@@ -880,9 +895,9 @@ int vx_server_wait(VxServer *s, uint64_t ticket, double timeout_s) {
             Clock::now() + std::chrono::duration_cast<Clock::duration>(
                                std::chrono::duration<double>(timeout_s));
         while (!r->done.load(std::memory_order_acquire)) {
-            if (!s->worker_error.empty()) {
+            if (s->failed.load(std::memory_order_acquire)) {
                 vx::set_error("vx_server_wait: server stopped: " + s->worker_error);
-                return VX_ERR_CUDA;
+                return s->device_error ? VX_ERR_DEVICE : VX_ERR_CUDA;
             }
             if (Clock::now() >= deadline) break;
             const Clock::time_point tick = Clock::now() + std::chrono::milliseconds(50);
@@ -948,7 +963,8 @@ int vx_server_stats(VxServer *s, VxServeStats *st, int32_t reset) {
         s->peak_inflight = s->inflight;
         s->t0 = Clock::now();
     }
-    return s->worker_error.empty() ? VX_OK : VX_ERR_CUDA;
+    if (!s->failed.load(std::memory_order_acquire)) return VX_OK;
+    return s->device_error ? VX_ERR_DEVICE : VX_ERR_CUDA;
 }
 
 int vx_server_destroy(VxServer *s) {
@@ -1022,7 +1038,7 @@ int vx_serve_bench(VxServer *s, const VxServeLoad *L, VxServeStats *st) {
             for (int b = 0; b < kBufs; ++b) {
                 while (inflight[b] && !inflight[b]->done.load(std::memory_order_acquire)) {
                     if (!all) break;
-                    if (!s->worker_error.empty()) {
+                    if (s->failed.load(std::memory_order_acquire)) {
                         failed = true;
                         return;
                     }
@@ -1107,7 +1123,7 @@ int vx_serve_bench(VxServer *s, const VxServeLoad *L, VxServeStats *st) {
     st->mrays_per_s = (double)st->rays / st->seconds / 1e6;
     if (failed) {
         vx::set_error("vx_serve_bench: server stopped: " + s->worker_error);
-        return VX_ERR_CUDA;
+        return s->device_error ? VX_ERR_DEVICE : VX_ERR_CUDA;
     }
     return rc;
 }

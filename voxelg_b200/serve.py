@@ -19,14 +19,15 @@ class Server:
 
     def __init__(self, world: DeviceWorld, params: L.VxTraceParams, origin=(0, 0, 0),
                  mem_budget_bytes: int = 256 << 20, slots: int = 4, max_batch_rays: int = 0,
-                 max_batch_requests: int = 0, resident: bool = False, idle_us: int = 0):
+                 max_batch_requests: int = 0, resident: bool = False, idle_us: int = 0,
+                 wait_us: int = 0):
         """resident=True runs the device-resident request loop
         (VX_SERVE_RESIDENT); slots and max_batch_requests then do not apply."""
         self._lib = L.load()
         self.world = world
         mode = L.VX_SERVE_RESIDENT if resident else L.VX_SERVE_SLOTS
         cfg = L.VxServeConfig(mem_budget_bytes, slots, max_batch_rays, max_batch_requests, mode,
-                              idle_us)
+                              idle_us, wait_us)
         h = C.c_void_p()
         L.check(self._lib.vx_server_create(world.handle, L.i3(origin), C.byref(params),
                                            C.byref(cfg), C.byref(h)))
