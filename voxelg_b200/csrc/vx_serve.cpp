@@ -420,6 +420,15 @@ bool res_retire(VxServer *s, bool *progress) {
         if (R.flight.front().off != SIZE_MAX) R.stage.give_back();
         R.flight.pop_front();
     }
+    // a wait in the loop that ran out, whether or not the launch is still up
+    const uint32_t err = __atomic_load_n(&R.rbox->error, __ATOMIC_ACQUIRE);
+    if (err != vx::RES_ERR_NONE) {
+        s->device_error = true;
+        s->worker_error = err == vx::RES_ERR_UNIT_WAIT
+                              ? "resident loop: a worker's wait for its unit ran out"
+                              : "resident loop: the wait for room in the unit table ran out";
+        return false;
+    }
     if (R.live) {
         const cudaError_t q = cudaEventQuery(R.inst_done);
         if (q == cudaErrorNotReady) return true;
@@ -429,14 +438,6 @@ bool res_retire(VxServer *s, bool *progress) {
         }
         R.live = false;
         *progress = true;
-    }
-    const uint32_t err = __atomic_load_n(&R.rbox->error, __ATOMIC_ACQUIRE);
-    if (err != vx::RES_ERR_NONE) {
-        s->device_error = true;
-        s->worker_error = err == vx::RES_ERR_UNIT_WAIT
-                              ? "resident loop: a worker's wait for its unit ran out"
-                              : "resident loop: the wait for room in the unit table ran out";
-        return false;
     }
     return true;
 }
