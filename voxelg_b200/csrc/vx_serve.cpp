@@ -197,8 +197,7 @@ struct VxServer {
 
     std::mutex mu;  // fifo + tickets
     std::deque<Cmd> fifo;
-    // commands in fifo: the worker takes the lock only when there are some,
-    // so that a spinning worker does not keep submitting clients off it
+    // commands in fifo: the polling worker takes the lock only when there are some
     std::atomic<size_t> queued{0};
     std::unordered_map<uint64_t, Request *> tickets;
     std::atomic<uint64_t> next_ticket{1};
