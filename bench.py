@@ -636,9 +636,12 @@ def run_ours(args, cfg):
     # end to end through the host-buffer entry points: a frame pipeline, each
     # step's results copied into one of two pinned host buffers while the
     # next frame renders, every copy inside the timed region.  The headline
-    # delivers packed records (vx_render_primary_host_packed_async: 16 bytes
-    # per pixel holding the record and the shadow record without loss); the
-    # same pipeline with the full 24 + 8-byte records is timed beside it.
+    # delivers compact records (vx_render_primary_host_compact_async: 12
+    # bytes per pixel holding the record and the shadow record without loss);
+    # the same pipeline with 16-byte packed records and with the full 24 +
+    # 8-byte records is timed beside it.
+    cp_h = [torch.empty(n * 12, dtype=torch.uint8).pin_memory() for _ in range(2)]
+    cp_np = [r.numpy().view(L.COMPACT_DTYPE) for r in cp_h]
     pk_h = [torch.empty(n * 16, dtype=torch.uint8).pin_memory() for _ in range(2)]
     pk_np = [r.numpy().view(L.PACKED_DTYPE) for r in pk_h]
     rec_h = [torch.empty(n * 24, dtype=torch.uint8).pin_memory() for _ in range(2)]
@@ -661,9 +664,12 @@ def run_ours(args, cfg):
         barrier(world)
         return max_over_ranks(time.perf_counter() - t, world, device)
 
-    e2e_s = pipeline(lambda i: vg.render_primary_host_packed_async(dw, cam, params, pk_np[i & 1]),
-                     e2e_steps)
+    e2e_s = pipeline(lambda i: vg.render_primary_host_compact_async(dw, cam, params,
+                                                                    cp_np[i & 1]), e2e_steps)
     e2e_value = world * rays_per_step * e2e_steps / e2e_s / 1e6
+    pk_s = pipeline(lambda i: vg.render_primary_host_packed_async(dw, cam, params, pk_np[i & 1]),
+                    e2e_steps)
+    e2e_packed_value = world * rays_per_step * e2e_steps / pk_s / 1e6
     full_s = pipeline(lambda i: vg.render_primary_host_async(dw, cam, params, rec_np[i & 1],
                                                              sh_np[i & 1]), e2e_steps)
     e2e_full_value = world * rays_per_step * e2e_steps / full_s / 1e6
@@ -675,13 +681,17 @@ def run_ours(args, cfg):
         r2, s2 = vg.unpack_records(pk, tuple(cam.world_origin), window)
         assert r2.tobytes() == want.tobytes() and s2.tobytes() == want_sh.tobytes(), \
             "packed host records differ from the device records"
+    for cp in cp_np:
+        r2, s2 = vg.unpack_compact_records(cp, tuple(cam.world_origin), window)
+        assert r2.tobytes() == want.tobytes() and s2.tobytes() == want_sh.tobytes(), \
+            "compact host records differ from the device records"
     t_up = time.perf_counter()
-    vg.unpack_records(pk_np[0], tuple(cam.world_origin), window)
+    vg.unpack_compact_records(cp_np[0], tuple(cam.world_origin), window)
     unpack_ms = (time.perf_counter() - t_up) * 1e3
     # the synchronous calls, for reference
     t2 = time.perf_counter()
     for _ in range(10):
-        vg.render_primary_host_packed(dw, cam, params, pk_np[0])
+        vg.render_primary_host_compact(dw, cam, params, cp_np[0])
     e2e_sync_value = rays_per_step * 10 / (time.perf_counter() - t2) / 1e6
 
     peaks = measured_peaks()
@@ -769,16 +779,18 @@ def run_ours(args, cfg):
                         "bound by instruction issue (integer ALU pipe), not HBM"},
             "e2e": {"value": round(e2e_value, 3), "unit": UNIT,
                     "h2d_bytes_per_step": 80 + 76,
-                    "d2h_bytes_per_step": 16 * n,
-                    "api": "vx_render_primary_host_packed_async: frame pipeline, two pinned "
-                           "host buffers, every step's packed records (16 B per pixel: "
+                    "d2h_bytes_per_step": 12 * n,
+                    "api": "vx_render_primary_host_compact_async: frame pipeline, two pinned "
+                           "host buffers, every step's compact records (12 B per pixel: "
                            "record and shadow record, lossless) copied in the timed region",
                     "synchronous_call_value": round(e2e_sync_value, 3),
+                    "packed_records_value": round(e2e_packed_value, 3),
+                    "packed_records_api": "vx_render_primary_host_packed_async (16 B per pixel)",
                     "full_records_value": round(e2e_full_value, 3),
                     "full_records_d2h_bytes_per_step": record_bytes,
                     "full_records_api": "vx_render_primary_host_async (24 + 8 B per pixel)",
                     "host_unpack_ms": round(unpack_ms, 3),
-                    "packed_equals_full": True},
+                    "packed_equals_full": True, "compact_equals_full": True},
             "gpu_launches": 2 * args.steps,
             "clocks": clocks,
         }

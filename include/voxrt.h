@@ -136,6 +136,23 @@ typedef struct {
     uint32_t steps;
 } VxPackedRecord;
 
+/* The same pair losslessly in 12 bytes, for windows of at most 2^30 voxels
+ * (the 2048 x 256 x 2048 window has exactly 2^30) and max_iters <= 2047,
+ * any_max_iters <= 1023:
+ *   w[0]  bits 0-29 voxel (as VxPackedRecord), bit 30 flags bit 1 (a LUT or
+ *         LOD early-out), bit 31 shadow occluded
+ *   w[1]  bits 0-30 t (a frame's t is never negative: its sign bit is
+ *         dropped), bit 31 shadow traced
+ *   w[2]  bits 0-10 primary steps, 11-20 shadow steps, 21-23 face (7 for a
+ *         miss), 24-31 material
+ * A record's flags bit 0 (hit) is face != miss.  A frame holding a record
+ * this form cannot hold (which the limits above exclude) is reported as
+ * VX_ERR_DEVICE by the next synchronising call instead of being truncated.
+ * vx_unpack_compact_records restores both records. */
+typedef struct {
+    uint32_t w[3];
+} VxCompactRecord;
+
 /* src/raycast.rs:13-17 */
 typedef struct {
     int32_t voxel[3];
@@ -347,6 +364,13 @@ int vx_render_primary_host_packed(VxWorld *w, const VxCamera *cam, const VxTrace
                                   VxPackedRecord *out_host);
 int vx_render_primary_host_packed_async(VxWorld *w, const VxCamera *cam,
                                         const VxTraceParams *p, VxPackedRecord *out_host);
+/* The same with VxCompactRecord (12 bytes per pixel).  VX_ERR_INVALID when
+ * the window has more than 2^30 voxels, max_iters > 2047 or
+ * any_max_iters > 1023. */
+int vx_render_primary_host_compact(VxWorld *w, const VxCamera *cam, const VxTraceParams *p,
+                                   VxCompactRecord *out_host);
+int vx_render_primary_host_compact_async(VxWorld *w, const VxCamera *cam,
+                                         const VxTraceParams *p, VxCompactRecord *out_host);
 /* The chunk generator's binary32 transcendentals, equal to the host C
  * library's (as the reference's f32::powf / cos / sin are) on the
  * generator's domains: fn 0 powf(x, 1.15f) and fn 1 powf(x, 0.85f) for
@@ -368,6 +392,10 @@ int vx_gen_math_host(uint32_t fn, const float *in, size_t n, float *out);
  * (4 * bricks per axis).  Either output pointer may be NULL. */
 int vx_unpack_records(const VxPackedRecord *packed, size_t n, const int32_t world_origin[3],
                       const uint32_t window_voxels[3], VxHitRecord *rec, VxShadowRecord *shadow);
+/* The same for VxCompactRecord. */
+int vx_unpack_compact_records(const VxCompactRecord *compact, size_t n,
+                              const int32_t world_origin[3], const uint32_t window_voxels[3],
+                              VxHitRecord *rec, VxShadowRecord *shadow);
 /* The frame of vx_render_primary, run once more with algorithmic load
  * counters on: bytes the method reads (8 per mask word / occupancy, 1 per
  * LUT or material byte) and loop iterations, summed over all rays.

@@ -177,3 +177,105 @@ def test_packed_frame_limits(worlds):
     p = vg.default_params(cfg.flags)
     p.max_iters = 65535
     vg.render_primary_host_packed(dw, cam, p)
+
+
+# ---------------------------------------------------------------- compact
+def compact_np(rec, sh, origin, window):
+    """The 12-byte VxCompactRecord layout, restated with numpy."""
+    rec = np.ascontiguousarray(rec).view(L.RECORD_DTYPE)
+    sh = np.ascontiguousarray(sh).view(L.SHADOW_DTYPE)
+    hit = (rec["flags"] & 1) != 0
+    rel = rec["voxel"].astype(np.int64) - np.asarray(origin, np.int64)
+    idx = np.where(hit, rel[:, 0] + window[0] * (rel[:, 1] + window[1] * rel[:, 2]), 0)
+    out = np.zeros(len(rec), L.COMPACT_DTYPE)
+    early = (rec["flags"].astype(np.uint32) >> 1) & 1
+    tb = rec["t"].view(np.uint32)
+    face3 = np.where(hit, rec["face"].astype(np.uint32), 7)
+    out["w"][:, 0] = (idx.astype(np.uint32) & 0x3FFFFFFF) | (early << 30) | \
+        (sh["occluded"].astype(np.uint32) << 31)
+    out["w"][:, 1] = (tb & 0x7FFFFFFF) | (sh["traced"].astype(np.uint32) << 31)
+    out["w"][:, 2] = (rec["steps"].astype(np.uint32) & 0x7FF) | \
+        ((sh["steps"].astype(np.uint32) & 0x3FF) << 11) | (face3 << 21) | \
+        (rec["mat"].astype(np.uint32) << 24)
+    return out
+
+
+@pytest.mark.parametrize("origin,window", [((0, 0, 0), (512, 256, 512)),
+                                           ((-1237, 0, 98304), (2048, 256, 2048))])
+def test_compact_unpack_inverts_the_layout(origin, window):
+    """Host side, no GPU: the numpy compact layout and vx_unpack_compact_records
+    round-trip random records within the form's limits (11 / 10-bit steps, a
+    2^30-voxel window)."""
+    import voxelg_b200 as vg
+    rng = np.random.default_rng(7 + window[0])
+    rec, sh = _random_records(rng, 40000, origin, window)
+    rec["steps"] = rng.integers(0, 2048, len(rec))
+    sh["steps"] = np.where(sh["traced"] != 0, rng.integers(0, 1024, len(sh)), 0)
+    compact = compact_np(rec, sh, origin, window)
+    r2, s2 = vg.unpack_compact_records(compact, origin, window)
+    assert r2.tobytes() == rec.tobytes()
+    assert s2.tobytes() == sh.tobytes()
+    lib = L.load()
+    wv = (C.c_uint32 * 3)(*window)
+    assert lib.vx_unpack_compact_records(None, 4, L.i3(origin), wv, None, None) == L.VX_ERR_INVALID
+
+
+def _full_and_compact(vg, dw, cam, p, asynchronous):
+    n = int(cam.res_x) * int(cam.res_y)
+    rec = np.empty(n, L.RECORD_DTYPE)
+    sh = np.empty(n, L.SHADOW_DTYPE)
+    vg.render_primary_host(dw, cam, p, rec, sh)
+    if asynchronous:
+        compact = np.empty(n, L.COMPACT_DTYPE)
+        vg.render_primary_host_compact_async(dw, cam, p, compact)
+        vg.render_host_wait(dw)
+    else:
+        compact = vg.render_primary_host_compact(dw, cam, p)
+    return rec, sh, compact
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["c1", "c2"])
+@pytest.mark.parametrize("asynchronous", [False, True], ids=["sync", "async"])
+def test_compact_frame_unpacks_to_the_full_records(worlds, name, asynchronous):
+    """12 bytes per pixel, byte-equal to the full records after unpacking, on
+    the c1 and c2 frames (the c2 window holds exactly 2^30 voxels)."""
+    import voxelg_b200 as vg
+    dw, cfg = worlds[name]
+    window = tuple(4 * b for b in cfg.bricks)
+    for flags, pose in ((cfg.flags, None), (1 | 2 | 4 | L.VX_F_SHADOW, None),
+                        (cfg.flags, ((window[0] * 0.3, 170.0, window[2] * 0.7), 2.4, -0.35))):
+        if pose is None:
+            cam = vg.default_camera(dw, cfg.width, cfg.height)
+        else:
+            cam = vg.camera_from_pose(pose[0], pose[1], pose[2], math.radians(70), cfg.width,
+                                      cfg.height)
+        p = vg.default_params(flags)
+        rec, sh, compact = _full_and_compact(vg, dw, cam, p, asynchronous)
+        assert compact.nbytes * 8 == (rec.nbytes + sh.nbytes) * 3
+        assert np.array_equal(compact, compact_np(rec, sh, tuple(cam.world_origin), window))
+        r2, s2 = vg.unpack_compact_records(compact, tuple(cam.world_origin), window)
+        assert r2.tobytes() == rec.tobytes(), (name, flags)
+        assert s2.tobytes() == sh.tobytes(), (name, flags)
+        assert (rec["flags"] & 1).any()
+
+
+@pytest.mark.gpu
+def test_compact_frame_limits(worlds):
+    import voxelg_b200 as vg
+    dw, cfg = worlds["c1"]
+    cam = vg.default_camera(dw, 64, 36)
+    for field, bad in (("max_iters", 2048), ("any_max_iters", 1024)):
+        p = vg.default_params(cfg.flags)
+        setattr(p, field, bad)
+        with pytest.raises(L.VxError) as e:
+            vg.render_primary_host_compact(dw, cam, p)
+        assert e.value.code == L.VX_ERR_INVALID
+    p = vg.default_params(cfg.flags)
+    p.max_iters, p.any_max_iters = 2047, 1023
+    out = vg.render_primary_host_compact(dw, cam, p)
+    rec = np.empty(64 * 36, L.RECORD_DTYPE)
+    sh = np.empty(64 * 36, L.SHADOW_DTYPE)
+    vg.render_primary_host(dw, cam, p, rec, sh)
+    r2, s2 = vg.unpack_compact_records(out, tuple(cam.world_origin), tuple(4 * b for b in cfg.bricks))
+    assert r2.tobytes() == rec.tobytes() and s2.tobytes() == sh.tobytes()

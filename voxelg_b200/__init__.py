@@ -11,6 +11,8 @@ from .trace import (KIND_ANY, KIND_NO_WATER, KIND_TRACE, PickHit, camera_from_po
                     records, render_host_wait, render_primary, render_primary_gated,
                     render_primary_host, render_primary_host_async,
                     render_primary_host_packed, render_primary_host_packed_async,
+                    render_primary_host_compact, render_primary_host_compact_async,
+                    unpack_compact_records,
                     render_primary_rows, render_primary_timed, render_stats, shadows,
                     tile_mask_words, tile_refresh, trace, unpack_records)
 from .world import DeviceWorld, HostWorld, TerrainParams, dims_counts, empty_arrays
@@ -21,6 +23,8 @@ __all__ = [
     "default_params", "raycast", "raycast_batch", "records", "render_ao", "render_primary",
     "render_primary_host", "render_primary_host_async", "render_host_wait", "render_primary_rows",
     "render_primary_host_packed", "render_primary_host_packed_async", "unpack_records",
+    "render_primary_host_compact", "render_primary_host_compact_async",
+    "unpack_compact_records",
     "render_primary_timed", "render_stats", "shadows", "trace",
     "dims_counts", "empty_arrays", "project_dirty", "render_primary_gated", "tile_mask_words",
     "tile_refresh",

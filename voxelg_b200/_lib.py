@@ -141,6 +141,8 @@ PACKED_DTYPE = np.dtype([("voxel", "<u4"), ("face", "u1"), ("mat", "u1"), ("flag
 assert BRICK_DTYPE.itemsize == 72 and RECORD_DTYPE.itemsize == 24
 assert SHADOW_DTYPE.itemsize == 8 and RAY_DTYPE.itemsize == 32
 assert PACKED_DTYPE.itemsize == 16
+COMPACT_DTYPE = np.dtype([("w", "<u4", (3,))])
+assert COMPACT_DTYPE.itemsize == 12
 
 # every symbol include/voxrt.h declares: (name, restype, argtypes)
 _vp = C.c_void_p
@@ -180,9 +182,14 @@ SIGNATURES = [
     ("vx_render_primary_host_packed", C.c_int, [_vp, _P(VxCamera), _P(VxTraceParams), _vp]),
     ("vx_render_primary_host_packed_async", C.c_int,
      [_vp, _P(VxCamera), _P(VxTraceParams), _vp]),
+    ("vx_render_primary_host_compact", C.c_int, [_vp, _P(VxCamera), _P(VxTraceParams), _vp]),
+    ("vx_render_primary_host_compact_async", C.c_int,
+     [_vp, _P(VxCamera), _P(VxTraceParams), _vp]),
     ("vx_gen_math", C.c_int, [_vp, C.c_uint32, _vp, C.c_size_t, _vp, _vp]),
     ("vx_gen_math_host", C.c_int, [C.c_uint32, _vp, C.c_size_t, _vp]),
     ("vx_unpack_records", C.c_int,
+     [_vp, C.c_size_t, _P(C.c_int32), _P(C.c_uint32), _vp, _vp]),
+    ("vx_unpack_compact_records", C.c_int,
      [_vp, C.c_size_t, _P(C.c_int32), _P(C.c_uint32), _vp, _vp]),
     ("vx_render_ao", C.c_int, [_vp, _P(VxCamera), _vp, _vp, _vp]),
     ("vx_render_primary_stats", C.c_int, [_vp, _P(VxCamera), _P(VxTraceParams),

@@ -307,9 +307,15 @@ int take_fault(VxWorld *w, const char *fn) {
     const uint32_t v = *f;
     if (v == 0u) return VX_OK;
     *f = 0u;
-    vx::set_error(std::string(fn) + ": a beam pre-pass block exited before its bulk copy of the "
-                  "chunk masks completed (bounded wait ran out); records of the frame are "
-                  "valid, shared memory of a later block may have been overwritten");
+    std::string msg = std::string(fn) + ":";
+    if (v & vx::kFaultBeamCopyLost)
+        msg += " a beam pre-pass block exited before its bulk copy of the chunk masks "
+               "completed (bounded wait ran out); records of the frame are valid, shared "
+               "memory of a later block may have been overwritten;";
+    if (v & vx::kFaultCompactLossy)
+        msg += " a compact frame held a record VxCompactRecord cannot hold (its 12-byte "
+               "records are not the frame's);";
+    vx::set_error(msg);
     return VX_ERR_DEVICE;
 }
 
@@ -1539,7 +1545,8 @@ namespace {
 // packed form crosses to the host.
 int enqueue_host_frame(VxWorld *w, const VxCamera *cam, const VxTraceParams *p,
                        VxHitRecord *rec_host, VxShadowRecord *shadow_host,
-                       VxPackedRecord *packed_host, uint32_t bands) {
+                       VxPackedRecord *packed_host, uint32_t bands,
+                       VxCompactRecord *compact_host = nullptr) {
     static_assert(kSyncBands <= sizeof(w->band_ev) / sizeof(w->band_ev[0]), "one event per band");
     static_assert(kAsyncBands <= kSyncBands, "one event per band");
     vx::FrameArgs fa = make_frame(w, cam, p);
@@ -1552,7 +1559,9 @@ int enqueue_host_frame(VxWorld *w, const VxCamera *cam, const VxTraceParams *p,
     if (!w->copy_done[0]) {
         for (auto &e : w->copy_done) VX_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     }
-    const bool packed = packed_host != nullptr;
+    // the packed and compact forms share the device staging buffer (12 <= 16 bytes)
+    const bool compact = compact_host != nullptr;
+    const bool packed = packed_host != nullptr || compact;
     if (w->hrec_cap[buf] < n || w->hsh_cap[buf] < n || (packed && w->hpk_cap[buf] < n)) {
         VX_CK(cudaStreamSynchronize(w->copy_stream));   // no copy may read a freed buffer
         int rc = ensure(&w->hrec[buf], &w->hrec_cap[buf], n);
@@ -1581,11 +1590,23 @@ int enqueue_host_frame(VxWorld *w, const VxCamera *cam, const VxTraceParams *p,
         const size_t r0 = (size_t)fa.y0 * fa.W, rn = (size_t)(fa.y1 - fa.y0) * fa.W;
         if (packed) {
             const uint32_t wx = (uint32_t)w->dw.d.vx, wy = (uint32_t)w->dw.d.vy;
-            VX_CK(vx::launch_pack(fa.rec, fa.shadow, r0, rn, fa.ta.ro, wx, wy, w->hpk[buf],
-                                  w->stream));
+            if (compact)
+                VX_CK(vx::launch_pack_compact(fa.rec, fa.shadow, r0, rn, fa.ta.ro, wx, wy,
+                                              reinterpret_cast<VxCompactRecord *>(w->hpk[buf]),
+                                              fa.ta.w.fault, w->stream));
+            else
+                VX_CK(vx::launch_pack(fa.rec, fa.shadow, r0, rn, fa.ta.ro, wx, wy, w->hpk[buf],
+                                      w->stream));
         }
         VX_CK(cudaEventRecord(w->band_ev[b], w->stream));
         VX_CK(cudaStreamWaitEvent(w->copy_stream, w->band_ev[b], 0));
+        if (compact) {
+            VX_CK(cudaMemcpyAsync(compact_host + r0,
+                                  reinterpret_cast<VxCompactRecord *>(w->hpk[buf]) + r0,
+                                  rn * sizeof(VxCompactRecord), cudaMemcpyDeviceToHost,
+                                  w->copy_stream));
+            continue;
+        }
         if (packed) {
             VX_CK(cudaMemcpyAsync(packed_host + r0, w->hpk[buf] + r0, rn * sizeof(VxPackedRecord),
                                   cudaMemcpyDeviceToHost, w->copy_stream));
@@ -1693,6 +1714,53 @@ int vx_render_primary_host_packed_async(VxWorld *w, const VxCamera *cam,
 }
 
 namespace {
+// the compact form's limits: a 30-bit window voxel index, 11 / 10-bit step counts
+int compact_args(VxWorld *w, const VxTraceParams *p, const char *fn) {
+    const uint64_t nvox = (uint64_t)w->dw.d.vx * (uint64_t)w->dw.d.vy * (uint64_t)w->dw.d.vz;
+    if (nvox > (1ull << 30)) {
+        vx::set_error(std::string(fn) + ": the window has more than 2^30 voxels");
+        return VX_ERR_INVALID;
+    }
+    if (p->max_iters > 2047 || p->any_max_iters > 1023) {
+        vx::set_error(std::string(fn) + ": max_iters must be <= 2047 and any_max_iters <= 1023");
+        return VX_ERR_INVALID;
+    }
+    return VX_OK;
+}
+}  // namespace
+
+int vx_render_primary_host_compact(VxWorld *w, const VxCamera *cam, const VxTraceParams *p,
+                                   VxCompactRecord *out_host) {
+    vx::Range nvtx_range("vx_render_primary_host_compact");
+    VxHitRecord *probe = reinterpret_cast<VxHitRecord *>(out_host);
+    int rc = host_frame_args(w, cam, p, probe, "vx_render_primary_host_compact");
+    if (rc == VX_OK) rc = compact_args(w, p, "vx_render_primary_host_compact");
+    if (rc != VX_OK) return rc;
+    std::lock_guard<std::mutex> lk(w->mu);
+    rc = enqueue_host_frame(w, cam, p, nullptr, nullptr, nullptr, kSyncBands, out_host);
+    if (rc != VX_OK) return rc;
+    VX_CK(cudaStreamSynchronize(w->copy_stream));
+    VX_CK(cudaStreamSynchronize(w->stream));
+    return take_fault(w, "vx_render_primary_host_compact");
+}
+
+int vx_render_primary_host_compact_async(VxWorld *w, const VxCamera *cam,
+                                         const VxTraceParams *p, VxCompactRecord *out_host) {
+    vx::Range nvtx_range("vx_render_primary_host_compact_async");
+    VxHitRecord *probe = reinterpret_cast<VxHitRecord *>(out_host);
+    int rc = host_frame_args(w, cam, p, probe, "vx_render_primary_host_compact_async");
+    if (rc == VX_OK) rc = compact_args(w, p, "vx_render_primary_host_compact_async");
+    if (rc != VX_OK) return rc;
+    std::lock_guard<std::mutex> lk(w->mu);
+    return enqueue_host_frame(w, cam, p, nullptr, nullptr, nullptr, kAsyncBands, out_host);
+}
+
+namespace {
+// vx_unpack_compact_records over [i0, i1): the compact words back to the
+// 16-byte packed fields, then as vx_unpack_records
+void unpack_compact_range(const VxCompactRecord *cr, size_t i0, size_t i1, const int32_t ro[3],
+                          uint64_t wx, uint64_t wy, VxHitRecord *rec, VxShadowRecord *shadow);
+
 // vx_unpack_records over [i0, i1)
 void unpack_range(const VxPackedRecord *packed, size_t i0, size_t i1, const int32_t ro[3],
                   uint64_t wx, uint64_t wy, VxHitRecord *rec, VxShadowRecord *shadow) {
@@ -1744,6 +1812,64 @@ void unpack_range(const VxPackedRecord *packed, size_t i0, size_t i1, const int3
     }
 }
 }  // namespace
+
+namespace {
+void unpack_compact_range(const VxCompactRecord *cr, size_t i0, size_t i1, const int32_t ro[3],
+                          uint64_t wx, uint64_t wy, VxHitRecord *rec, VxShadowRecord *shadow) {
+    constexpr size_t kBlock = 1024;
+    VxPackedRecord tmp[kBlock];
+    for (size_t b0 = i0; b0 < i1; b0 += kBlock) {
+        const size_t nb = std::min(kBlock, i1 - b0);
+        for (size_t j = 0; j < nb; ++j) {
+            const uint32_t *w = cr[b0 + j].w;
+            const uint32_t face3 = (w[2] >> 21) & 7u;
+            const bool hit = face3 != 7u;
+            VxPackedRecord &q = tmp[j];
+            q.voxel = hit ? (w[0] & 0x3FFFFFFFu) : 0u;
+            q.face = (uint8_t)(hit ? face3 : 0xFFu);
+            q.mat = (uint8_t)(w[2] >> 24);
+            q.flags = (uint8_t)(hit ? (1u | (((w[0] >> 30) & 1u) << 1)) : 0u);
+            q.shadow = (uint8_t)((w[0] >> 31) | ((w[1] >> 31) << 1));
+            const uint32_t tb = w[1] & 0x7FFFFFFFu;
+            std::memcpy(&q.t, &tb, 4);
+            q.steps = (w[2] & 0x7FFu) | (((w[2] >> 11) & 0x3FFu) << 16);
+        }
+        unpack_range(tmp, 0, nb, ro, wx, wy, rec ? rec + b0 : nullptr,
+                     shadow ? shadow + b0 : nullptr);
+    }
+}
+}  // namespace
+
+int vx_unpack_compact_records(const VxCompactRecord *compact, size_t n,
+                              const int32_t world_origin[3], const uint32_t window_voxels[3],
+                              VxHitRecord *rec, VxShadowRecord *shadow) {
+    if ((!compact && n) || !world_origin || !window_voxels) {
+        vx::set_error("vx_unpack_compact_records: null argument");
+        return VX_ERR_INVALID;
+    }
+    const uint64_t wx = window_voxels[0], wy = window_voxels[1];
+    if (wx == 0 || wy == 0 || window_voxels[2] == 0) {
+        vx::set_error("vx_unpack_compact_records: empty window");
+        return VX_ERR_INVALID;
+    }
+    const size_t per = (size_t)1 << 18;
+    const size_t hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    const size_t nt = std::min(hw, (n + per - 1) / per);
+    if (nt <= 1) {
+        unpack_compact_range(compact, 0, n, world_origin, wx, wy, rec, shadow);
+        return VX_OK;
+    }
+    std::vector<std::thread> th;
+    th.reserve(nt - 1);
+    const size_t chunk = (n + nt - 1) / nt;
+    for (size_t t = 1; t < nt; ++t) {
+        const size_t i0 = std::min(n, t * chunk), i1 = std::min(n, (t + 1) * chunk);
+        th.emplace_back(unpack_compact_range, compact, i0, i1, world_origin, wx, wy, rec, shadow);
+    }
+    unpack_compact_range(compact, 0, std::min(n, chunk), world_origin, wx, wy, rec, shadow);
+    for (auto &t : th) t.join();
+    return VX_OK;
+}
 
 int vx_unpack_records(const VxPackedRecord *packed, size_t n, const int32_t world_origin[3],
                       const uint32_t window_voxels[3], VxHitRecord *rec, VxShadowRecord *shadow) {

@@ -81,6 +81,8 @@ struct DevWorld {
     const uint8_t *tdf;
 };
 constexpr uint32_t kFaultBeamCopyLost = 1u;
+// bit 1: a compact frame held a record VxCompactRecord cannot hold
+constexpr uint32_t kFaultCompactLossy = 2u;
 constexpr int32_t kBrickFieldCap = 16;  // bricks (64 voxels)
 constexpr int32_t kTileFieldCap = 12;   // tiles (192 voxels)
 
@@ -165,6 +167,11 @@ cudaError_t launch_rebuild_pyramid(const DevWorld &w, cudaStream_t s);
 // the brick and tile distance fields of w (tmp: n_bricks bytes of scratch)
 // a frame's records (and shadow records, or nullptr) [first, first + n) in
 // the 16-byte packed form (vx_pack.cu)
+// records [first, first + n) as VxCompactRecord; a record the form cannot
+// hold sets kFaultCompactLossy in *fault
+cudaError_t launch_pack_compact(const VxHitRecord *rec, const VxShadowRecord *sh, size_t first,
+                                size_t n, const int32_t ro[3], uint32_t wx, uint32_t wy,
+                                VxCompactRecord *out, uint32_t *fault, cudaStream_t s);
 cudaError_t launch_pack(const VxHitRecord *rec, const VxShadowRecord *sh, size_t first, size_t n,
                         const int32_t ro[3], uint32_t wx, uint32_t wy, VxPackedRecord *out,
                         cudaStream_t s);

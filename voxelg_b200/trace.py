@@ -197,6 +197,39 @@ def unpack_records(packed: np.ndarray, world_origin, window_voxels):
     return rec, sh
 
 
+def render_primary_host_compact(world: DeviceWorld, cam: L.VxCamera, params: L.VxTraceParams,
+                                out: Optional[np.ndarray] = None) -> np.ndarray:
+    """Frame through a host buffer of 12-byte compact records (records and
+    shadow records, losslessly); returns the COMPACT_DTYPE array."""
+    n = int(cam.res_x) * int(cam.res_y)
+    if out is None:
+        out = np.empty(n, L.COMPACT_DTYPE)
+    L.check(L.load().vx_render_primary_host_compact(world.handle, C.byref(cam), C.byref(params),
+                                                    C.c_void_p(L.ptr(out))))
+    return out
+
+
+def render_primary_host_compact_async(world: DeviceWorld, cam: L.VxCamera,
+                                      params: L.VxTraceParams, out: np.ndarray):
+    """Enqueue a compact frame into a (pinned) host buffer; it is there after
+    render_host_wait(world)."""
+    L.check(L.load().vx_render_primary_host_compact_async(world.handle, C.byref(cam),
+                                                          C.byref(params), C.c_void_p(L.ptr(out))))
+
+
+def unpack_compact_records(compact: np.ndarray, world_origin, window_voxels):
+    """Compact records back to (RECORD_DTYPE, SHADOW_DTYPE) arrays."""
+    compact = np.ascontiguousarray(compact).view(L.COMPACT_DTYPE)
+    n = len(compact)
+    rec = np.empty(n, L.RECORD_DTYPE)
+    sh = np.empty(n, L.SHADOW_DTYPE)
+    wv = (C.c_uint32 * 3)(*[int(v) for v in window_voxels])
+    L.check(L.load().vx_unpack_compact_records(C.c_void_p(L.ptr(compact)), n,
+                                               L.i3(world_origin), wv, C.c_void_p(L.ptr(rec)),
+                                               C.c_void_p(L.ptr(sh))))
+    return rec, sh
+
+
 def render_host_wait(world: DeviceWorld):
     """Wait until every enqueued host-buffer frame has landed."""
     L.check(L.load().vx_render_host_wait(world.handle))
