@@ -824,8 +824,11 @@ __global__ void k_tile_meta(DevWorld w) {
     if (lw == 0ull) code = 3u;
     else if (!bit64(lw, child_bit(cx & 3, cy & 3, cz & 3))) code = 2u;
     else if (tile_clear) code = 1u;
-    w.tile_meta[ti] =
-        (uint16_t)((uint32_t)w.tile_uniform[ti] | (code << 8) | (tile_clear ? kMetaChunkOnly : 0u));
+    // the LUT byte only where the tile LUT test ends a walk (a uniform,
+    // optimisable material), so the walk tests it against 0 alone
+    const uint32_t lut = w.tile_uniform[ti];
+    w.tile_meta[ti] = (uint16_t)((is_uniform_optimisable(lut) ? lut : 0u) | (code << 8) |
+                                 (tile_clear ? kMetaChunkOnly : 0u));
 }
 
 }  // namespace

@@ -395,7 +395,8 @@ __device__ __forceinline__ int child_of(uint32_t sx, uint32_t sy, uint32_t sz, i
 // DevWorld::tile_meta word.  Every voxel of a tile shares the tile's chunk
 // and L4 cell, so trace's L4 and chunk tests (raymarch.wgsl:4648-4668) have
 // one outcome per tile:
-//   bits 0-7   the tile LUT byte
+//   bits 0-7   the tile LUT byte where the tile LUT test ends a walk (the
+//              byte is a uniform_optimisable material), else 0
 //   bits 8-9   the cell the L4 and chunk tests skip: 0 none, 1 the 16-voxel
 //              tile, 2 the 64-voxel chunk, 3 the 256-voxel L4 cell
 //   bit 10     the chunk test alone skips the tile (walks without L4)
@@ -471,10 +472,12 @@ __device__ __forceinline__ int walk_step(const DevWorld &w, const Geo &g, const 
     // batch 1: every coarse word addressed by the slot coordinate
     const uint64_t tw = ld_tile(w, ti);
     uint32_t tum;
+    bool tum_exit = false;  // the tile LUT test ends the walk (with material tum)
     int32_t cell = 0;
     if (w.tile_meta != nullptr) {
         const uint32_t meta = ld_tile_meta(w, ti);
         tum = f_lut ? (meta & 0xFFu) : 0u;
+        tum_exit = tum != 0u;  // pre-filtered by k_tile_meta
         if (use_l4) {
             const uint32_t code = (meta >> 8) & 3u;
             if (STATS) bytes += code >= 2u ? 8 : 16;
@@ -488,6 +491,7 @@ __device__ __forceinline__ int walk_step(const DevWorld &w, const Geo &g, const 
         if (use_l4) lw = ld_l4(w, l4_index(g, sx, sy, sz));
         const uint64_t cw = ld_chunk(w, chunk_index(g, sx, sy, sz));
         tum = f_lut ? ld_tile_uniform(w, ti) : 0u;
+        tum_exit = tum != 0u && is_uniform_optimisable(tum);
         if (use_l4) {
             if (STATS) bytes += 8;
             if (lw == 0ull) cell = 256;
@@ -519,7 +523,7 @@ __device__ __forceinline__ int walk_step(const DevWorld &w, const Geo &g, const 
         // tile LUT (raymarch.wgsl:4692-4706)
         if (f_lut) {
             if (STATS) bytes += 1;
-            if (tum != 0u && is_uniform_optimisable(tum)) {
+            if (tum_exit) {
                 set_hit(d, s, ro, k.la, tum, true, h);
                 return WALK_HIT;
             }
