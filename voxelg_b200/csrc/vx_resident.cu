@@ -9,15 +9,16 @@
 // published that unit, reads the unit's rays from host memory, traces them
 // with the same walk as vx_trace (so records are identical), writes the
 // records into host memory and, when it finishes the request's last unit,
-// stores the request's position + 1 into the request's completion word.
+// stores res_done_word(position) into the request's completion word.
 //
 // Ordering.  The host writes a descriptor, then releases `head`; the leader
 // sees `head` move, takes one system-scope acquire fence and reads the
 // descriptors.  What the leader publishes to the workers (the request's
 // words, one word per unit, the published-unit count) carries tags and is
 // read by the workers with plain device-coherent loads that wait for the
-// right tag: no acquire load or fence in a worker's path, because those
-// discard the SM's L1, which the tracing warps beside it live on.  A warp
+// right tag: no acquire load or fence in a worker's path.  (Workers that
+// polled with acquire loads made the tracing warps on their SMs several
+// times slower under load, measured.)  A warp
 // counts its unit with a release atomic at system scope (its record stores
 // to host memory come first); the warp that counts the request's last unit
 // takes an acquire-release fence before it stores the completion word, so
@@ -28,9 +29,9 @@
 // idle_ns without a descriptor, or once it has run life_ns (the host starts
 // the next instance).  The leader then sets the closing bit beside the
 // final published count; workers finish every published unit and return.
-// Every wait is bounded (wait_ns, and an iteration cap): a wait that runs
-// out records RES_ERR_* in the reply box and the instance ends; the host
-// reports it.
+// Every wait is bounded (wait_ns, and an iteration cap): a warp whose wait
+// runs out records RES_ERR_* in the reply box and returns; the host reports
+// it and stops the loop.
 #include <cuda_runtime.h>
 
 #include "vx_internal.h"
