@@ -311,9 +311,8 @@ struct ResReplyBox {              // mapped host memory, written by the device
 };
 // Device memory.  Workers read what the leader publishes with plain
 // device-coherent (relaxed) loads, never acquire loads (polling with acquire
-// loads made the tracing warps beside them several times slower under
-// load): every word carries a tag of the publication it belongs to, and a
-// reader waits until the tag matches.
+// loads measured slower under load): every word carries a tag of the
+// publication it belongs to, and a reader waits until the tag matches.
 //   unit word  (global unit g) << 32 | (position p, low 32 bits)
 //   request    slot p % kResRing, four words:
 //                rays | (p & 0xFFFF) << 48,  out | (p & 0xFFFF) << 48,

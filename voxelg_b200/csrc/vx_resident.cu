@@ -16,9 +16,9 @@
 // descriptors.  What the leader publishes to the workers (the request's
 // words, one word per unit, the published-unit count) carries tags and is
 // read by the workers with plain device-coherent loads that wait for the
-// right tag: no acquire load or fence in a worker's path.  (Workers that
-// polled with acquire loads made the tracing warps on their SMs several
-// times slower under load, measured.)  A warp
+// right tag: no acquire load or fence in a worker's path.  (Polling with
+// acquire loads measured slower under load: a query-sized load's p99 2.6 ms
+// against 0.72.)  A warp
 // counts its unit with a release atomic at system scope (its record stores
 // to host memory come first); the warp that counts the request's last unit
 // takes an acquire-release fence before it stores the completion word, so
