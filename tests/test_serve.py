@@ -122,6 +122,49 @@ def test_rejects_request_larger_than_slot(env, resident):
     srv.close()
 
 
+@pytest.mark.parametrize("resident", [False, True])
+def test_many_edits_interleaved_with_requests(env, resident):
+    """Six rounds of mixed-size requests, each round followed by an edit of
+    random bricks: every request's records equal the rays traced on a second
+    world that received the same edits in the same order up to that request
+    (for the resident loop: a fence, a drained launch and a restart per
+    edit)."""
+    import voxelg_b200.serve as sv
+    vg, dw = env
+    p = vg.default_params(vg._lib.VX_F_L4 | vg._lib.VX_F_LUT | vg._lib.VX_F_LOD)
+    arrays = dw.download()
+    w_srv = vg.DeviceWorld(128, 64, 128)
+    w_ref = vg.DeviceWorld(128, 64, 128)
+    w_srv.upload(arrays)
+    w_ref.upload(arrays)
+    srv = sv.Server(w_srv, p, mem_budget_bytes=32 << 20, resident=resident)
+    rng = np.random.default_rng(21 + resident)
+    n_bricks = 128 * 64 * 128
+    live = []
+    try:
+        for rnd in range(6):
+            for n in (1, 37, 512, 3000, 64):
+                r = query_rays(rng, n)
+                live.append((srv.submit(r), vg.records(vg.trace(w_ref, r, p)).copy()))
+            k = 2000
+            idx = rng.choice(n_bricks, k, replace=False).astype(np.uint32)
+            bricks = np.zeros(k, po.BRICK)
+            occ = rng.integers(0, 2**63, k, dtype=np.uint64) | rng.integers(0, 2, k, dtype=np.uint64)
+            bricks["occupancy"] = occ
+            bits = ((occ[:, None] >> np.arange(64, dtype=np.uint64)) & np.uint64(1)).astype(bool)
+            bricks["materials"] = np.where(bits, rng.choice(np.array([2, 3, 4, 12], np.uint8), (k, 64)), 0)
+            srv.edit(idx, bricks)
+            w_ref.apply_dirty(idx, bricks)
+        for t, want in live:
+            got = srv.wait(t)
+            assert np.array_equal(got.view(np.uint8), want.view(np.uint8))
+        assert srv.stats()["edits"] == 6
+    finally:
+        srv.close()
+        w_srv.close()
+        w_ref.close()
+
+
 def pinned(n, dtype):
     """A numpy array of n elements in page-locked host memory."""
     import torch
