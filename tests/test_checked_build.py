@@ -131,6 +131,18 @@ def _workloads():
     b["steps"] = 0
     same(a, b, "learned")
     clean("learned")
+    # the device-resident request loop over the generic rays (degenerate ones included)
+    import voxelg_b200.serve as sv
+    p = vg.default_params(flags)
+    srv = sv.Server(dw, p, mem_budget_bytes=8 << 20, resident=True)
+    try:
+        for kind in (0, 1, 2):
+            rays["kind"] = kind
+            same(srv.wait(srv.submit(rays)), po.trace_batch(ow, rays, p)[0],
+                 f"resident kind {kind}")
+    finally:
+        srv.close()
+    clean("resident request loop")
     # a streamed window with edits (generator, edit replay, per-tile words)
     dw.fill_window(0xC0FFEE_F00D_BEEF, 0, 0)
     dw.apply_edit(300, 90, 200, 18)
@@ -158,7 +170,7 @@ def test_checked_library_runs_the_parity_workloads_clean():
     r = subprocess.run([sys.executable, str(Path(__file__).resolve())], env=env, cwd=ROOT,
                        capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stdout[-3000:] + r.stderr[-3000:]
-    assert "checked workloads clean: 18" in r.stdout, r.stdout[-2000:]
+    assert "checked workloads clean: 19" in r.stdout, r.stdout[-2000:]
 
 
 if __name__ == "__main__":
