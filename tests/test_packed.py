@@ -140,7 +140,8 @@ def test_packed_frame_unpacks_to_the_full_records(worlds, name, asynchronous):
 @pytest.mark.gpu
 def test_packed_frame_with_a_shifted_window():
     """A window whose corner is at negative x and large z (golden world
-    uniform_shifted): voxel indices are relative to that corner."""
+    uniform_shifted): voxel indices are relative to that corner, in the
+    packed and the compact form."""
     import voxelg_b200 as vg
     from test_golden import GOLDEN, WORLDS, camera_of, params_of, world_arrays
     fr = next(f for f in GOLDEN["frames"] if f["world"] == "uniform_shifted")
@@ -158,6 +159,11 @@ def test_packed_frame_with_a_shifted_window():
             assert r2.tobytes() == rec.tobytes()
             assert s2.tobytes() == sh.tobytes()
             assert (rec["voxel"][:, 0][(rec["flags"] & 1) != 0] < 0).any()
+            # the compact form of the same frame
+            rec, sh, compact = _full_and_compact(vg, dw, cam, p, asynchronous)
+            r2, s2 = vg.unpack_compact_records(compact, w["origin"], window)
+            assert r2.tobytes() == rec.tobytes()
+            assert s2.tobytes() == sh.tobytes()
     finally:
         dw.close()
 
