@@ -196,6 +196,17 @@ def test_resident_reads_and_writes_page_locked_buffers_in_place(env, c1_oracle_w
     rays, out, _ = live[3]
     want = po.trace_batch(c1_oracle_world, np.asarray(rays).view(po.RAY), p)[0]
     assert np.array_equal(out.view(np.uint8), want.view(np.uint8))
+    # page-locked but not 16-byte aligned: records 24 bytes into their buffer
+    # go through staging while the (aligned) rays are read in place
+    hold_r, rays = pinned(1000, vg._lib.RAY_DTYPE)
+    rays[:] = query_rays(rng, 1000).view(vg._lib.RAY_DTYPE)
+    hold_o, out_all = pinned(1001, vg._lib.RECORD_DTYPE)
+    out = out_all[1:]
+    assert out.ctypes.data % 16 == 8
+    got = srv.wait(srv.submit(rays, out))
+    assert got is out
+    alone = vg.records(vg.trace(dw, rays, p))
+    assert np.array_equal(out.view(np.uint8), alone.view(np.uint8))
     srv.close()
 
 
