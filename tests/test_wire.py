@@ -98,9 +98,11 @@ def test_malformed_frames_are_rejected():
 
 
 @pytest.mark.gpu
-def test_query_frame_served_end_to_end(c1_oracle_world):
-    """A RayQuery frame decoded, served by the ray-query server, and its
-    RayResult frame equal to the oracle's records for the same rays."""
+@pytest.mark.parametrize("resident", [False, True], ids=["slots", "resident"])
+def test_query_frame_served_end_to_end(c1_oracle_world, resident):
+    """A RayQuery frame decoded, served by the ray-query server (device slots,
+    or the device-resident request loop), and its RayResult frame equal to
+    the oracle's records for the same rays."""
     import torch
     if not torch.cuda.is_available():
         pytest.fail("CUDA GPU required for -m gpu tests")
@@ -111,7 +113,7 @@ def test_query_frame_served_end_to_end(c1_oracle_world):
     dw = vg.DeviceWorld(*cfg.bricks)
     dw.generate(cfg.terrain)
     p = vg.default_params(vg._lib.VX_F_L4 | vg._lib.VX_F_LUT | vg._lib.VX_F_LOD)
-    srv = sv.Server(dw, p, slots=2)
+    srv = sv.Server(dw, p, slots=2, resident=resident)
     rng = np.random.default_rng(5)
     rays = np.zeros(3000, po.RAY)
     rays["org"] = rng.uniform([0, 80, 0], [512, 200, 512], (3000, 3)).astype(np.float32)
